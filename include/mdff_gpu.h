@@ -1,0 +1,236 @@
+/*
+ * mdff_gpu.h -- C ABI of the B200 force engine for MDFF.
+ *
+ * The library replaces the body of the reference's per-step energy/force call
+ *   SUBROUTINE engforce            (src/engforce_driver.f90:102-190)
+ * which takes no arguments and communicates through module globals
+ * (config.f90:47-95, coulomb.f90:47-79, pim.f90:63-96, non_bonded.f90:58-116,
+ * control.f90:35-66, thermo.f90:27-120).  Here the same state crosses the
+ * boundary explicitly: static force-field parameters once (mdff_gpu_create),
+ * positions per call (mdff_gpu_engforce), results into caller-owned host
+ * arrays.  Plain C types only; no CUDA or torch types appear in signatures.
+ *
+ * Array conventions
+ *   - Per-type tables use 0-based C indexing [it][jt] (and [it][jt][kt]);
+ *     element [it][jt] is the reference's namelist entry (it+1, jt+1).
+ *     A Fortran caller transposes (see the iso_c_binding shim).
+ *   - Ions are grouped by type in POSFF order: natmi[0] ions of type 0 first,
+ *     then natmi[1] of type 1, ... (read_pos.f90:187-199).
+ *   - Cell matrix A[a][b] = simu_cell%A(a+1,b+1): column b is lattice vector b.
+ *   - Dipoles / fields: [natm][3] with xyz fastest, i.e. Fortran mu(3,natm).
+ *   - 3x3 tensors: [a][b] = Fortran tau(a+1,b+1).
+ *
+ * Every entry point returns an int status (MDFF_OK = 0); none exits or STOPs.
+ */
+#ifndef MDFF_GPU_H
+#define MDFF_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDFF_NTYPEMAX 16   /* config.f90:42 ntypemax */
+#define MDFF_ASPC_DEPTH 5  /* coulomb.f90:435 dipia_ind_t(5,3,natm) */
+#define MDFF_ABI_VERSION 1
+
+/* status codes */
+enum {
+  MDFF_OK = 0,
+  MDFF_ERR_BAD_ARGS = 1,       /* invalid argument or parameter combination   */
+  MDFF_ERR_CUDA = 2,           /* CUDA runtime error (message via last_error)  */
+  MDFF_ERR_CATASTROPHE = 3,    /* polarisation catastrophe, any mu_a > 10 eA
+                                  (moment_from_pola.f90:176-216)               */
+  MDFF_ERR_LIST_OVERFLOW = 4,  /* Verlet list capacity exceeded
+                                  (tools.f90:337-350); stats.list_needed holds
+                                  the required size                            */
+  MDFF_ERR_NOT_CONVERGED = 5,  /* dipole solve hit its iteration limit and
+                                  params.fail_on_nonconvergence is set         */
+  MDFF_ERR_TIMEOUT = 6,        /* a bounded device wait gave up                */
+  MDFF_ERR_NO_DEVICE = 7,      /* no CUDA device / sm_100 device unavailable   */
+  MDFF_ERR_UNSUPPORTED = 8,    /* feature of the reference not built here      */
+  MDFF_ERR_NOMEM = 9           /* device allocation failed                     */
+};
+
+/* control%calc (control.f90); selects the ASPC predictor use
+   (moment_from_pola.f90:374-378, 415) */
+enum { MDFF_CALC_MD = 0, MDFF_CALC_OPT = 1, MDFF_CALC_OTHER = 2 };
+
+/* non_bonded ctrunc (non_bonded.f90:253-255) */
+enum { MDFF_TRUNC_NONE = 0, MDFF_TRUNC_LINEAR = 1, MDFF_TRUNC_QUADRATIC = 2 };
+
+/* &gputag keywords (new; not in the reference) */
+enum { MDFF_PREC_FP64 = 0, MDFF_PREC_MIXED = 1 };
+enum { MDFF_SOLVER_SCF = 0, MDFF_SOLVER_CG = 1 };
+
+typedef struct mdff_params {
+  int natm;                               /* config%natm                        */
+  int ntype;                              /* config%ntype                       */
+  int natmi[MDFF_NTYPEMAX];               /* ions per type (POSFF order)        */
+
+  /* &controltag (control.f90:128-161) */
+  int lcoulomb, lbmhft, lbmhftd, lnmlj;   /* potentials switched on             */
+  int lsurf;                              /* Ewald surface term                 */
+  int lreduced;                           /* reduced units: coul_unit = press_unit = 1 */
+  int calc;                               /* MDFF_CALC_*                         */
+  double cutshortrange, cutlongrange;     /* Angstrom                           */
+  double skindiff;                        /* Verlet skin                        */
+
+  /* &fieldtag / coulomb (coulomb.f90:55-58) */
+  double qch[MDFF_NTYPEMAX];              /* charge per type                    */
+  double dip[MDFF_NTYPEMAX][3];           /* static dipole per type             */
+
+  /* &non_bondedtag (non_bonded.f90:135-150) */
+  int trunc;                              /* MDFF_TRUNC_* for n-m LJ             */
+  int symmetric_pot_nb;                   /* symmetrise tables (default 1)       */
+  double epslj[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double sigmalj[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double plj[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double qlj[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double Abmhftd[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double Bbmhftd[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double Cbmhftd[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double Dbmhftd[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double BDbmhftd[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+
+  /* &coulombtag (coulomb.f90:97-106) */
+  double alphaES;                         /* Ewald alpha (1/Angstrom)           */
+  int kES[3];                             /* kmax per reciprocal axis           */
+  int lautoES;                            /* DL_POLY rule from epsw             */
+  double epsw;
+
+  /* &pimtag (pim.f90:258-279) */
+  int ldip_polar[MDFF_NTYPEMAX];
+  double poldip[MDFF_NTYPEMAX][3][3];     /* polarisability tensor per type     */
+  int ldip_damping[MDFF_NTYPEMAX][MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double pol_damp_b[MDFF_NTYPEMAX][MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double pol_damp_c[MDFF_NTYPEMAX][MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  int pol_damp_k[MDFF_NTYPEMAX][MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+  double conv_tol_ind;
+  int min_scf_pol_iter, max_scf_pol_iter;
+  int extrapolate_order;                  /* ASPC order 0..4                    */
+  int symmetric_pot_pim;                  /* symmetrise damping tables          */
+
+  /* &gputag (new keywords; defaults reproduce the reference) */
+  int precision;                          /* MDFF_PREC_FP64 | MDFF_PREC_MIXED    */
+  int solver;                             /* MDFF_SOLVER_SCF | MDFF_SOLVER_CG    */
+  double cg_tol;                          /* CG stop: rms residual (e/A^2)       */
+  int cg_max_iter;
+  int fail_on_nonconvergence;
+  int device;                             /* CUDA device ordinal                 */
+  double wall24[MDFF_NTYPEMAX][MDFF_NTYPEMAX]; /* optional W/r^24 repulsive wall
+                                             added to BMH pairs (eV A^24);
+                                             0 = reference behaviour           */
+} mdff_params;
+
+/* Results of one engforce call; pointer members are caller-owned host arrays
+   (NULL = not wanted, except fx/fy/fz). */
+typedef struct mdff_result {
+  double *fx, *fy, *fz;                   /* [natm] forces (eV/A)                */
+  double *mu;                             /* [natm][3] total dipoles mu_t        */
+  double *ef;                             /* [natm][3] field ef_t (e/A^2)        */
+  double u_lj, vir_lj;                    /* thermodynamic module scalars        */
+  double u_bmhft, vir_bmhft;
+  double u_coul, u_pol, pvirial_coul;
+  double tau_nonb[3][3];                  /* GPa                                 */
+  double tau_coul[3][3];
+  double tau[3][3];                       /* tau_nonb + 2 tau_coul, as the
+                                             reference's double accumulation
+                                             (ewald.f90:245 + engforce_driver.f90:177) */
+} mdff_result;
+
+typedef struct mdff_stats {
+  int n_pol_iter;                         /* SCF or CG iterations last call      */
+  int converged;
+  double rmsd;                            /* final rmsd (e/A^2)                  */
+  int list_rebuilds;                      /* cumulative                          */
+  int list_capacity;                      /* full-list entries allocated         */
+  int list_needed;                        /* entries needed at last build        */
+  int nk;                                 /* half-space k vectors                */
+  double alphaES;                         /* after lautoES                       */
+  int kES[3];
+  double cutlongrange;                    /* after the half-cell clamp           */
+  int n_launches;                         /* kernels launched by last call       */
+  double ms_last;                         /* device time of last call (ms)       */
+} mdff_stats;
+
+typedef struct mdff_ctx* mdff_handle;
+
+int mdff_gpu_abi_version(void);
+/* sizeof the boundary structs as compiled into the library: which = 0
+   mdff_params, 1 mdff_result, 2 mdff_stats (bindings check their layout) */
+int mdff_gpu_struct_size(int which);
+const char* mdff_gpu_strerror(int status);
+/* last CUDA / validation message of this handle (or global if h == NULL) */
+const char* mdff_gpu_last_error(mdff_handle h);
+
+/* Replaces field_init / coulomb_init / pim_init / initialize_param_non_bonded
+   (non_bonded.f90:455-644, coulomb.f90:363-493, pim.f90:107-240,
+   read_pos.f90:160-237): expands per-type tables to ions, symmetrises,
+   clamps cutlongrange to half the cell (coulomb.f90:377-383), applies lautoES,
+   builds the k mesh (kspace.f90:143-207).  cell_A as in simu_cell%A. */
+int mdff_gpu_create(const mdff_params* p, const double cell_A[9], mdff_handle* out);
+
+/* New cell (lattice.f90:60): rebuilds B, omega, k mesh; forces a list rebuild. */
+int mdff_gpu_set_cell(mdff_handle h, const double cell_A[9]);
+
+/* engforce (engforce_driver.f90:102-190) on host arrays rx,ry,rz [natm].
+   itime drives the ASPC order ramp (moment_from_pola.f90:514-522).  The
+   Verlet list is checked (tools.f90:444-537) and rebuilt on device as needed. */
+int mdff_gpu_engforce(mdff_handle h, const double* rx, const double* ry,
+                      const double* rz, int itime, mdff_result* out);
+
+/* Same on device-resident arrays: d_pos = SoA [3][natm] doubles; outputs are
+   device arrays d_force [3][natm] (required), d_mu / d_ef [natm][3]
+   (optional); scalars/tensors go to *out (its pointer members are ignored).
+   The call is stream-ordered on the handle's stream and returns after the
+   scalars are on the host. */
+int mdff_gpu_engforce_device(mdff_handle h, const double* d_pos, int itime,
+                             double* d_force, double* d_mu, double* d_ef,
+                             mdff_result* out);
+
+/* ASPC history dipia_ind_t(5,3,natm) (coulomb.f90:435) for RESTART:
+   buf = [MDFF_ASPC_DEPTH][natm][3]. */
+int mdff_gpu_get_aspc_history(mdff_handle h, double* buf);
+int mdff_gpu_set_aspc_history(mdff_handle h, const double* buf);
+
+int mdff_gpu_get_stats(mdff_handle h, mdff_stats* s);
+
+/* Export the reference's half Verlet list (vnlist_pbc, tools.f90:273-368) for
+   positions rx,ry,rz: which = 0 -> verlet_vdw (cutshortrange + skindiff),
+   1 -> verlet_coul (cutlongrange + skindiff).  point[natm+1] and list[] are
+   1-based exactly as the reference (list order ascending ja within a row).
+   *n_out = number of entries; MDFF_ERR_LIST_OVERFLOW if capacity is short. */
+int mdff_gpu_verlet_half_list(mdff_handle h, int which, const double* rx,
+                              const double* ry, const double* rz, int* point,
+                              int* list, int capacity, int* n_out);
+
+/* Velocity-Verlet NVE steps on device (prop_velocity_verlet,
+   integration.f90:132-194): d_pos, d_vel SoA [3][natm], d_invmass [natm] in
+   internal units, dt in internal time units.  Each step calls the engine.
+   ekin_pot (optional host [nsteps][2]) receives kinetic and potential energy
+   per step (eV). */
+int mdff_gpu_md_nve(mdff_handle h, double* d_pos, double* d_vel,
+                    const double* d_invmass, double dt, int nsteps, int itime0,
+                    double* ekin_pot);
+
+/* Per-kernel-class device timing with CUDA events on the handle's stream
+   (for roofline figures).  Classes: 0 list build, 1 short range, 2 real-space
+   field, 3 real-space force, 4 structure factor, 5 reciprocal field/force,
+   6 everything else.  ms[c], launches[c] and work[c] (algorithmic units: (k, ion)
+   terms for 4/5, list entries for 1/2/3) accumulate while enabled; reset on
+   enable. */
+#define MDFF_NKCLASS 7
+int mdff_gpu_profile(mdff_handle h, int enable);
+int mdff_gpu_kernel_times(mdff_handle h, double* ms, long long* launches, double* work);
+
+/* Measured FMA throughput of a device (TFLOP/s, FMA = 2 flops) for fp64 = 1
+   (double) or 0 (float): a saturating register-resident FMA loop over every
+   SM, timed with CUDA events.  The denominator of the FP32/FP64 roofline. */
+int mdff_gpu_peak_flops(int device, int fp64, double* tflops);
+
+void mdff_gpu_destroy(mdff_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MDFF_GPU_H */

@@ -1,0 +1,426 @@
+// realspace.cuh -- real-space pair kernels over the full Verlet list.
+//
+//  * k_shortrange: engforce_bmhftd_pbc (non_bonded.f90:1076-1228) and
+//    engforce_nmlj_pbc (non_bonded.f90:660-827).
+//  * k_es_field:   the field-only Ewald real-space passes of the PIM solve
+//    (multipole_ES_dir with do_forces=.false., ewald_dir.f90:40-798): the
+//    damped charge field (static pass, moment_from_pola.f90:327-330) and the
+//    undamped dipole T2 field (induced pass, moment_from_pola.f90:401-404).
+//  * k_es_force:   the final multipole_ES_dir with qq + qd + dd tasks, damping,
+//    energy, field, forces and stress (engforce_driver.f90:164-166).
+//
+// Warp per atom i; lanes stride i's row.  Each pair is visited from both
+// sides; the reference's role of the pair (which ion is "ia") is recovered
+// from the parity mask, so asymmetric damping tables behave as in the
+// reference.  Per-atom sums are formed in registers with no atomics; pair
+// energies/stresses are halved and reduced per block in a fixed order.
+#pragma once
+#include "common.cuh"
+
+namespace mdff {
+
+struct NBPair {        // per ordered type pair (ti,tj), after symmetrisation
+  double A, B, C, D, BD, wall;
+  double rcutsq;
+  double epsp, plj, qlj, sigsq, fc, uc, uc1, uc2;
+};
+
+struct ESPair {        // per ordered role pair (ta = type of "ia", tb = type of "ja")
+  int ldamp;           // ldip_damping(ta,ta,tb) .or. ldip_damping(tb,ta,tb)
+  int ka, kb;          // TT orders for the field on a / on b
+  int pad;
+  double ba, ca, bb, cb;  // TT b, c for the field on a: (ta,ta,tb); on b: (tb,ta,tb)
+};
+
+// --------------------------------------------------------------------------
+// short range.  Partials per block: [u_bmh, vir_bmh, u_lj, vir_lj,
+// tau_bmh(6: xx yy zz xy xz yz), tau_lj(6)] -> 16 doubles.
+constexpr int kSRPart = 16;
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_shortrange(
+    const double4* __restrict__ s, const int* __restrict__ itype, const int* __restrict__ nbr,
+    const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
+    const NBPair* __restrict__ tab, int ntype, int do_bmh, int lbmhftd, int do_lj, int trunc,
+    double* __restrict__ force /* SoA [3][natm] */, double* __restrict__ part) {
+  __shared__ NBPair stab[MDFF_NT * MDFF_NT];
+  __shared__ double red[kSRPart * 8];
+  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
+  __syncthreads();
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  double acc[kSRPart];
+#pragma unroll
+  for (int k = 0; k < kSRPart; ++k) acc[k] = 0.0;
+  double fb[3] = {0, 0, 0}, fl[3] = {0, 0, 0};
+  if (i < natm) {
+    double4 si = s[i];
+    int ti = itype[i];
+    int n = nnb[i];
+    const int* row = nbr + (size_t)i * cap;
+    for (int k = lane; k < n; k += 32) {
+      int j = row[k];
+      double4 sj = s[j];
+      int tj = itype[j];
+      double rxd, ryd, rzd;
+      double r2d = min_image_exact(cell->A, xsub(si.x, sj.x), xsub(si.y, sj.y), xsub(si.z, sj.z),
+                                   rxd, ryd, rzd);
+      const NBPair& P = stab[ti * ntype + tj];
+      if (r2d >= P.rcutsq) continue;  // non_bonded.f90:1154 strict <
+      R rx = (R)rxd, ry = (R)ryd, rz = (R)rzd, rijsq = (R)r2d;
+      if (do_bmh && P.A != 0.0) {
+        R ir2 = R(1) / rijsq;
+        R d = rsqrt_<R>(rijsq);
+        R erh = (R)P.A * rexp<R>(-(R)P.B * d);
+        R ir6 = ir2 * ir2 * ir2;
+        R ir8 = ir6 * ir2;
+        R ir8r = ir8;
+        ir6 = ir6 * (R)P.C;
+        ir8 = ir8 * (R)P.D;
+        R f6 = R(1), f8 = R(1), fd6 = R(0), fd8 = R(0);
+        if (lbmhftd) {
+          tt_damp<R>((R)P.BD, R(1), d, 6, f6, fd6);
+          tt_damp<R>((R)P.BD, R(1), d, 8, f8, fd8);
+        }
+        R ir6d = ir6 * f6, ir8d = ir8 * f8;
+        R ir7 = R(6) * ir6d / d;
+        R ir9 = R(8) * ir8d / d;
+        R uw = R(0);
+        if (P.wall != 0.0) uw = (R)P.wall * (ir8r * ir8r * ir8r);
+        R u = erh - ir6d - ir8d + uw;
+        R wij = ((R)P.B * erh - ir7 - ir9 + ir6 * fd6 + ir8 * fd8 + R(24) * uw / d) / d;
+        R fx = wij * rx, fy = wij * ry, fz = wij * rz;
+        fb[0] += (double)fx;
+        fb[1] += (double)fy;
+        fb[2] += (double)fz;
+        acc[0] += 0.5 * (double)u;
+        acc[1] += 0.5 * (double)(rx * fx + ry * fy + rz * fz);
+        acc[4] += (double)(rx * fx);  // 0.5*(r_a f_b + r_b f_a) on the diagonal = r_a f_a
+        acc[5] += (double)(ry * fy);
+        acc[6] += (double)(rz * fz);
+        acc[7] += 0.5 * (double)(rx * fy + ry * fx);
+        acc[8] += 0.5 * (double)(rx * fz + rz * fx);
+        acc[9] += 0.5 * (double)(ry * fz + rz * fy);
+      }
+      if (do_lj) {
+        R sr2 = (R)P.sigsq / rijsq;
+        R srp, srq;
+        if (sizeof(R) == 8) {
+          srp = (R)pow((double)sr2, 0.5 * P.plj);
+          srq = (R)pow((double)sr2, 0.5 * P.qlj);
+        } else {
+          srp = powf((float)sr2, 0.5f * (float)P.plj);
+          srq = powf((float)sr2, 0.5f * (float)P.qlj);
+        }
+        R e = (R)P.epsp * ((R)P.plj * srq - (R)P.qlj * srp);
+        if (trunc == 1) e = e - (R)P.uc;
+        if (trunc == 2) e = e + (R)P.uc1 * rijsq - (R)P.uc2;
+        R wij = (R)P.fc * (srq - srp) * sr2;
+        R fx = wij * rx, fy = wij * ry, fz = wij * rz;
+        fl[0] += (double)fx;
+        fl[1] += (double)fy;
+        fl[2] += (double)fz;
+        acc[2] += 0.5 * (double)e;
+        acc[3] += 0.5 * (double)(wij * rijsq);
+        acc[10] += (double)(rx * fx);
+        acc[11] += (double)(ry * fy);
+        acc[12] += (double)(rz * fz);
+        acc[13] += 0.5 * (double)(rx * fy + ry * fx);
+        acc[14] += 0.5 * (double)(rx * fz + rz * fx);
+        acc[15] += 0.5 * (double)(ry * fz + rz * fy);
+      }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      fb[a] = warp_sum(fb[a]);
+      fl[a] = warp_sum(fl[a]);
+    }
+    if (lane == 0) {
+      // the reference zeroes fx in each short-range routine, so with both
+      // on only the BMH forces survive (non_bonded.f90:699-701, 1104-1106)
+      const double* f = do_bmh ? fb : fl;
+      force[i] = f[0];
+      force[natm + i] = f[1];
+      force[2 * natm + i] = f[2];
+    }
+  }
+  block_sum<kSRPart>(acc, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kSRPart; ++k) part[(size_t)blockIdx.x * kSRPart + k] = acc[k];
+}
+
+// --------------------------------------------------------------------------
+// Ewald real-space radial functions F0..F3 (ewald_dir.f90:230-236).
+template <typename R>
+struct Radial {
+  R d, dm1, dm3, dm5, dm7, F0, F1, F2, F3;
+};
+
+template <typename R, bool NEED_F3>
+__device__ __forceinline__ void radial(R d2, R alpha, Radial<R>& o) {
+  const R piroot = (R)1.7724538509055160273;
+  R d = rsqrt_<R>(d2);
+  o.d = d;
+  o.dm1 = R(1) / d;
+  o.dm3 = o.dm1 / d2;
+  o.dm5 = o.dm3 / d2;
+  o.dm7 = o.dm5 / d2;
+  R a2 = alpha * alpha, a3 = a2 * alpha;
+  R expon = rexp<R>(-a2 * d2) / piroot;
+  o.F0 = nr_erfc<R>(alpha * d);
+  o.F1 = o.F0 + R(2) * alpha * d * expon;
+  R d3 = d2 * d;
+  o.F2 = o.F1 + R(4) * a3 * d3 * expon / R(3);
+  if (NEED_F3) {
+    R a5 = a3 * a2, d5 = d3 * d2;
+    o.F3 = o.F2 + R(8) * a5 * d5 * expon / R(15);
+  } else {
+    o.F3 = R(0);
+  }
+}
+
+// --------------------------------------------------------------------------
+// field-only pass.  Adds into E (AoS double4 [natm]):
+//   QQ : E_i += q_j r_ij dm3 (F1 - F1d_i)       (qq block, ewald_dir.f90:533-541)
+//   DD : E_i += T2(r_ij) . mu_j                  (dd block, ewald_dir.f90:566-571)
+// dd_mask: 0 -> the reference's condition any(mu_i /= 0) .and. any(mu_j /= 0)
+//          1 -> both ions polarisable (the linear operator of the CG solve)
+template <typename R, bool QQ, bool DD>
+__global__ void __launch_bounds__(256) k_es_field(
+    const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
+    const int* __restrict__ ipolar, const double4* __restrict__ mu, const int* __restrict__ nbr,
+    const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
+    const ESPair* __restrict__ tab, int ntype, double alpha, double cutsq, int damp,
+    int dd_mask, double4* __restrict__ E) {
+  __shared__ ESPair stab[MDFF_NT * MDFF_NT];
+  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
+  __syncthreads();
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= natm) return;
+  double4 si = s[i];
+  int ti = itype[i];
+  double4 mui = DD ? mu[i] : make_double4(0, 0, 0, 0);
+  bool dip_i = DD && (dd_mask ? (ipolar[i] != 0) : (mui.x != 0.0 || mui.y != 0.0 || mui.z != 0.0));
+  int n = nnb[i];
+  const int* row = nbr + (size_t)i * cap;
+  double ex = 0.0, ey = 0.0, ez = 0.0;
+  if (QQ || dip_i) {
+    for (int k = lane; k < n; k += 32) {
+      int j = row[k];
+      double4 sj = s[j];
+      double rxd, ryd, rzd;
+      double r2d = min_image_exact(cell->A, xsub(si.x, sj.x), xsub(si.y, sj.y), xsub(si.z, sj.z),
+                                   rxd, ryd, rzd);
+      if (r2d > cutsq) continue;  // ewald_dir.f90:202 ( d2 .gt. cutsq ) cycle
+      double4 muj;
+      bool dd = false;
+      if (DD && dip_i) {
+        muj = mu[j];
+        dd = dd_mask ? (ipolar[j] != 0) : (muj.x != 0.0 || muj.y != 0.0 || muj.z != 0.0);
+      }
+      double qj = QQ ? q[j] : 0.0;
+      if (!dd && (!QQ || qj == 0.0)) continue;
+      R rx = (R)rxd, ry = (R)ryd, rz = (R)rzd;
+      Radial<R> g;
+      radial<R, false>((R)r2d, (R)alpha, g);
+      R e0 = R(0), e1 = R(0), e2 = R(0);
+      if (QQ && qj != 0.0) {
+        R F1d = R(0);
+        if (damp) {
+          int tj = itype[j];
+          bool i_is_a = half_mask(i, j);
+          int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
+          const ESPair& P = stab[ta * ntype + tb];
+          if (P.ldamp) {
+            R fdm, fdd;
+            if (i_is_a)
+              tt_damp<R>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
+            else
+              tt_damp<R>((R)P.bb, (R)P.cb, g.d, P.kb, fdm, fdd);
+            F1d = R(1) - fdm;
+          }
+        }
+        R c = (R)qj * g.dm3 * (g.F1 - F1d);
+        e0 += c * rx;
+        e1 += c * ry;
+        e2 += c * rz;
+      }
+      if (DD && dd) {
+        R B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5;
+        R mx = (R)muj.x, my = (R)muj.y, mz = (R)muj.z;
+        R rm = rx * mx + ry * my + rz * mz;
+        e0 += B2 * rx * rm - B1 * mx;
+        e1 += B2 * ry * rm - B1 * my;
+        e2 += B2 * rz * rm - B1 * mz;
+      }
+      ex += (double)e0;
+      ey += (double)e1;
+      ez += (double)e2;
+    }
+  }
+  ex = warp_sum(ex);
+  ey = warp_sum(ey);
+  ez = warp_sum(ez);
+  if (lane == 0) {
+    double4 o = E[i];
+    E[i] = make_double4(o.x + ex, o.y + ey, o.z + ez, 0.0);
+  }
+}
+
+// --------------------------------------------------------------------------
+// final real-space pass: qq + qd + dd with damping; energy, field, force,
+// stress.  Partials per block: [u, tau xx yy zz xy xz yz] -> 7 doubles
+// (tau is the reference's  - sum (r_j f_k + r_k f_j)  before *0.5/omega).
+constexpr int kESPart = 7;
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_es_force(
+    const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
+    const double4* __restrict__ mu, const int* __restrict__ nbr, const int* __restrict__ nnb,
+    int cap, int natm, const CellC* __restrict__ cell, const ESPair* __restrict__ tab, int ntype,
+    double alpha, double cutsq, int task_qq, int task_qd, int task_dd, int damp_ind,
+    double fscale, double4* __restrict__ E, double* __restrict__ force /* SoA [3][natm], += */,
+    double* __restrict__ part) {
+  __shared__ ESPair stab[MDFF_NT * MDFF_NT];
+  __shared__ double red[kESPart * 8];
+  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
+  __syncthreads();
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  double acc[kESPart];
+#pragma unroll
+  for (int k = 0; k < kESPart; ++k) acc[k] = 0.0;
+  if (i < natm) {
+    double4 si = s[i];
+    int ti = itype[i];
+    double qi = q[i];
+    double4 mui = mu[i];
+    int n = nnb[i];
+    const int* row = nbr + (size_t)i * cap;
+    double e[3] = {0, 0, 0}, f[3] = {0, 0, 0};
+    for (int k = lane; k < n; k += 32) {
+      int j = row[k];
+      double4 sj = s[j];
+      double rxd, ryd, rzd;
+      double r2d = min_image_exact(cell->A, xsub(si.x, sj.x), xsub(si.y, sj.y), xsub(si.z, sj.z),
+                                   rxd, ryd, rzd);
+      if (r2d > cutsq) continue;
+      int tj = itype[j];
+      double qj = q[j];
+      double4 muj = mu[j];
+      bool i_is_a = half_mask(i, j);
+      // canonical pair: a = "ia", b = "ja", r = r_a - r_b
+      R sg = i_is_a ? R(1) : R(-1);
+      R r[3] = {sg * (R)rxd, sg * (R)ryd, sg * (R)rzd};
+      int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
+      R qa = (R)(i_is_a ? qi : qj), qb = (R)(i_is_a ? qj : qi);
+      double4 ma4 = i_is_a ? mui : muj, mb4 = i_is_a ? muj : mui;
+      R ma[3] = {(R)ma4.x, (R)ma4.y, (R)ma4.z}, mb[3] = {(R)mb4.x, (R)mb4.y, (R)mb4.z};
+      bool dip_a = (ma4.x != 0.0 || ma4.y != 0.0 || ma4.z != 0.0);
+      bool dip_b = (mb4.x != 0.0 || mb4.y != 0.0 || mb4.z != 0.0);
+      Radial<R> g;
+      radial<R, true>((R)r2d, (R)alpha, g);
+      const ESPair& P = stab[ta * ntype + tb];
+      bool ldamp = damp_ind && P.ldamp;
+      R F1d = R(0), F2d = R(0), F1d2 = R(0), F2d2 = R(0);
+      if (ldamp) {
+        R fdm, fdd, fdm2, fdd2;
+        tt_damp<R>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
+        tt_damp<R>((R)P.bb, (R)P.cb, g.d, P.kb, fdm2, fdd2);
+        F1d = R(1) - fdm;
+        F2d = F1d + (g.d / R(3)) * fdd;
+        F1d2 = R(1) - fdm2;
+        F2d2 = F1d2 + (g.d / R(3)) * fdd2;
+      }
+      R B0 = g.dm1 * g.F0, B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5, B3 = R(15) * g.F3 * g.dm7;
+      R B1d = F1d * g.dm3, B2d = R(3) * F2d * g.dm5, B1d2 = F1d2 * g.dm3, B2d2 = R(3) * F2d2 * g.dm5;
+      R rma = r[0] * ma[0] + r[1] * ma[1] + r[2] * ma[2];
+      R rmb = r[0] * mb[0] + r[1] * mb[1] + r[2] * mb[2];
+      R mab = ma[0] * mb[0] + ma[1] * mb[1] + ma[2] * mb[2];
+      R u = R(0), fij[3] = {R(0), R(0), R(0)}, Ea[3] = {R(0), R(0), R(0)}, Eb[3] = {R(0), R(0), R(0)};
+      if (task_qq) {
+        u += qa * qb * B0;
+        R ca = qb * (B1 - (ldamp ? B1d : R(0)));
+        R cb = -qa * (B1 - (ldamp ? B1d2 : R(0)));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          Ea[c] += ca * r[c];
+          Eb[c] += cb * r[c];
+          fij[c] += -qa * qb * B1 * r[c];
+        }
+      }
+      if (task_dd && dip_a && dip_b) {
+        u += -(B2 * rma * rmb - B1 * mab);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          Ea[c] += B2 * r[c] * rmb - B1 * mb[c];
+          Eb[c] += B2 * r[c] * rma - B1 * ma[c];
+          fij[c] -= -B3 * rma * rmb * r[c] + B2 * (mab * r[c] + ma[c] * rmb + mb[c] * rma);
+        }
+      }
+      if (task_qd && (dip_a || dip_b)) {
+        u += qa * B1 * rmb - qb * B1 * rma;
+        if (ldamp) u += -qa * B1d2 * rmb + qb * B1d * rma;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          R T2mb = B2 * r[c] * rmb - B1 * mb[c];
+          R T2ma = B2 * r[c] * rma - B1 * ma[c];
+          fij[c] += -qa * T2mb + qb * T2ma;
+          if (ldamp) {
+            R T2dma = B2d * r[c] * rma - B1d * ma[c];
+            R T2d2mb = B2d2 * r[c] * rmb - B1d2 * mb[c];
+            fij[c] += -qb * T2dma + qa * T2d2mb;
+          }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        f[c] += (double)(i_is_a ? -fij[c] : fij[c]);
+        e[c] += (double)(i_is_a ? Ea[c] : Eb[c]);
+      }
+      acc[0] += 0.5 * (double)u;
+      acc[1] += -(double)(r[0] * fij[0]);
+      acc[2] += -(double)(r[1] * fij[1]);
+      acc[3] += -(double)(r[2] * fij[2]);
+      acc[4] += -0.5 * (double)(r[0] * fij[1] + r[1] * fij[0]);
+      acc[5] += -0.5 * (double)(r[0] * fij[2] + r[2] * fij[0]);
+      acc[6] += -0.5 * (double)(r[1] * fij[2] + r[2] * fij[1]);
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      e[c] = warp_sum(e[c]);
+      f[c] = warp_sum(f[c]);
+    }
+    if (lane == 0) {
+      double4 o = E[i];
+      E[i] = make_double4(o.x + e[0], o.y + e[1], o.z + e[2], 0.0);
+      force[i] += f[0] * fscale;
+      force[natm + i] += f[1] * fscale;
+      force[2 * natm + i] += f[2] * fscale;
+    }
+  }
+  block_sum<kESPart>(acc, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kESPart; ++k) part[(size_t)blockIdx.x * kESPart + k] = acc[k];
+}
+
+// fixed-order reduction of per-block partials: out[v] = sum_b part[b*nv+v]
+__global__ void k_reduce_partials(const double* __restrict__ part, int nblk, int nv,
+                                  double* __restrict__ out) {
+  __shared__ double sh[256];
+  for (int v = 0; v < nv; ++v) {
+    double acc = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc += part[(size_t)b * nv + v];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x >> 1; w > 0; w >>= 1) {
+      if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[v] = sh[0];
+    __syncthreads();
+  }
+}
+
+}  // namespace mdff

@@ -1,0 +1,327 @@
+// recip.cuh -- Ewald reciprocal-space sum (multipole_ES_rec, ewald_rec.f90:38-365).
+//
+// The reference evaluates COS/SIN(k.r) afresh for every (k, ion) pair of the
+// half-space mesh (kspace.f90:143-207).  Here k = 2 pi B n, so
+//   e^{i k.r} = X_nx(s_x) Y_ny(s_y) Z_nz(s_z),  X_n = e^{2 pi i n s_x}, ...
+// with s the direct coordinates.  Per-ion tables of X, Y, Z (one sincospi
+// each, FP64) are built once per pass; the mesh is walked as rows (nx, ny)
+// of consecutive nz, where the phase advances by one complex multiply.
+// Likewise k.mu = n . m with m = 2 pi B^T mu, and sum_k k f(k) = 2 pi B sum_k n f(k).
+//
+//   k_rec_rho   : rho(k) = sum_i (q_i + i k.mu_i) e^{i k.r_i}   (ewald_rec.f90:118-148)
+//                 block = (row, nz tile) x ion chunk; fixed-order partials.
+//   k_rec_sum   : rho over chunks; rho' = A_k rho; str = A_k |rho|^2 (:173)
+//   k_rec_energy: u_rec and the stress (:255-263, 300-358), one block, fixed order
+//   k_rec_field : per ion sum over k of recarg / recarg2 (:181-250), ion-major,
+//                 rho' of the block's k chunk staged in shared memory
+//   k_rec_field_sum : chunk sum, E = -2 pi B G, F = q E + 2 pi B H, scaled
+#pragma once
+#include "common.cuh"
+
+namespace mdff {
+
+template <typename R>
+struct cplx;
+template <>
+struct cplx<double> {
+  typedef double2 T;
+};
+template <>
+struct cplx<float> {
+  typedef float2 T;
+};
+
+struct RecMesh {
+  int kmax[3];
+  int nrows;
+  const int4* rows;      // (nx, ny, nz_lo, koff)
+  int nk;
+  const double* Ak;      // [nk] in row order
+  const double4* kvec;   // [nk] (kx, ky, kz, kcoe)
+};
+
+// per-ion phase tables: [n][natm], X: n = 0..kx, Y: 0..ky, Z: 0..kz (FP64).
+// s is wrapped to [-0.5, 0.5) first: e^{2 pi i n s} is periodic in s.
+template <typename R>
+__global__ void k_rec_tables(const double4* __restrict__ s, int natm, int kx, int ky, int kz,
+                             typename cplx<R>::T* __restrict__ tab) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natm) return;
+  double sv[3] = {s[i].x, s[i].y, s[i].z};
+  int km[3] = {kx, ky, kz};
+  int off = 0;
+  for (int a = 0; a < 3; ++a) {
+    double w = sv[a] - rint(sv[a]);
+    for (int n = 0; n <= km[a]; ++n) {
+      double sn, cs;
+      sincospi(2.0 * (double)n * w, &sn, &cs);
+      typename cplx<R>::T v;
+      v.x = (R)cs;
+      v.y = (R)sn;
+      tab[(size_t)(off + n) * natm + i] = v;
+    }
+    off += km[a] + 1;
+  }
+}
+
+// per-ion weights (q, m1, m2, m3), m = 2 pi B^T mu  (k.mu = n.m)
+__global__ void k_rec_weights(const double* __restrict__ q, const double4* __restrict__ mu,
+                              int natm, const CellC* __restrict__ cell, int has_q, int has_mu,
+                              double4* __restrict__ w) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natm) return;
+  const double* B = cell->B;
+  double qi = has_q ? q[i] : 0.0;
+  double m1 = 0.0, m2 = 0.0, m3 = 0.0;
+  if (has_mu) {
+    double4 u = mu[i];
+    m1 = kTwoPi * (B[0] * u.x + B[3] * u.y + B[6] * u.z);
+    m2 = kTwoPi * (B[1] * u.x + B[4] * u.y + B[7] * u.z);
+    m3 = kTwoPi * (B[2] * u.x + B[5] * u.y + B[8] * u.z);
+  }
+  w[i] = make_double4(qi, m1, m2, m3);
+}
+
+template <typename C>
+__device__ __forceinline__ C cmul(C a, C b) {
+  C r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename C>
+__device__ __forceinline__ C cconj(C a) {
+  a.y = -a.y;
+  return a;
+}
+
+// phase of (nx, ny, nz) for ion i from the tables
+template <typename R>
+__device__ __forceinline__ typename cplx<R>::T phase_xyz(const typename cplx<R>::T* __restrict__ tab,
+                                                         int natm, int i, int nx, int ny, int nz,
+                                                         int kx, int ky) {
+  typedef typename cplx<R>::T C;
+  C X = tab[(size_t)nx * natm + i];
+  int ay = ny < 0 ? -ny : ny;
+  C Y = tab[(size_t)(kx + 1 + ay) * natm + i];
+  if (ny < 0) Y = cconj(Y);
+  int az = nz < 0 ? -nz : nz;
+  C Z = tab[(size_t)(kx + 1 + ky + 1 + az) * natm + i];
+  if (nz < 0) Z = cconj(Z);
+  return cmul(cmul(X, Y), Z);
+}
+
+// rho partials.  grid.x = nrows * ntiles, grid.y = ion chunks; block 128.
+// part[chunk][k] (double2).
+template <typename R, bool HAS_Q, bool HAS_MU, int NZT>
+__global__ void __launch_bounds__(128) k_rec_rho(const typename cplx<R>::T* __restrict__ tab,
+                                                 const double4* __restrict__ w, int natm,
+                                                 int chunk, RecMesh M, int ntiles,
+                                                 double2* __restrict__ part) {
+  typedef typename cplx<R>::T C;
+  __shared__ double red[2 * NZT][4];
+  int row = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
+  int4 ri = M.rows[row];
+  int nx = ri.x, ny = ri.y, nz_lo = ri.z, koff = ri.w;
+  int kz = M.kmax[2];
+  int nz0 = nz_lo + tile * NZT;
+  if (nz0 > kz) return;
+  int nzn = kz - nz0 + 1;
+  if (nzn > NZT) nzn = NZT;
+  int a0 = blockIdx.y * chunk, a1 = a0 + chunk;
+  if (a1 > natm) a1 = natm;
+  R accR[NZT], accI[NZT];
+#pragma unroll
+  for (int t = 0; t < NZT; ++t) accR[t] = accI[t] = R(0);
+  const int kx = M.kmax[0], ky = M.kmax[1];
+  for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
+    C P = phase_xyz<R>(tab, natm, i, nx, ny, nz0, kx, ky);
+    C Z1 = tab[(size_t)(kx + 1 + ky + 1 + 1) * natm + i];
+    double4 wi = w[i];
+    R q = (R)wi.x;
+    R km = (R)(nx * wi.y + ny * wi.z + nz0 * wi.w);
+    R m3 = (R)wi.w;
+#pragma unroll
+    for (int t = 0; t < NZT; ++t) {
+      if (HAS_Q) {
+        accR[t] += q * P.x;
+        accI[t] += q * P.y;
+      }
+      if (HAS_MU) {
+        accR[t] -= km * P.y;
+        accI[t] += km * P.x;
+        km += m3;
+      }
+      P = cmul(P, Z1);
+    }
+  }
+  // block reduction in double, fixed order
+  int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < NZT; ++t) {
+    double vr = warp_sum((double)accR[t]);
+    double vi = warp_sum((double)accI[t]);
+    if (lane == 0) {
+      red[2 * t][wp] = vr;
+      red[2 * t + 1][wp] = vi;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < nzn) {
+    int t = threadIdx.x;
+    double vr = red[2 * t][0] + red[2 * t][1] + red[2 * t][2] + red[2 * t][3];
+    double vi = red[2 * t + 1][0] + red[2 * t + 1][1] + red[2 * t + 1][2] + red[2 * t + 1][3];
+    int k = koff + (nz0 - nz_lo) + t;
+    part[(size_t)blockIdx.y * M.nk + k] = make_double2(vr, vi);
+  }
+}
+
+// rho = sum over chunks; rhoA = A_k rho; str = A_k |rho|^2
+__global__ void k_rec_sum(const double2* __restrict__ part, int nchunk, RecMesh M,
+                          double2* __restrict__ rhoA, double* __restrict__ str) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= M.nk) return;
+  double r = 0.0, im = 0.0;
+  for (int c = 0; c < nchunk; ++c) {
+    double2 v = part[(size_t)c * M.nk + k];
+    r += v.x;
+    im += v.y;
+  }
+  double A = M.Ak[k];
+  rhoA[k] = make_double2(A * r, A * im);
+  str[k] = (r * r + im * im) * A;
+}
+
+// u_rec (x2 x tpi_V) and tau_rec (x2, symmetric, x tpi_V/omega): out[0..6] =
+// u, tau xx yy zz xy xz yz.  One block.
+__global__ void k_rec_energy(const double* __restrict__ str, RecMesh M, double tpi_V,
+                             double omega, int do_stress, double* __restrict__ out) {
+  __shared__ double red[7 * 32];
+  double v[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int k = threadIdx.x; k < M.nk; k += blockDim.x) {
+    double s = str[k];
+    double4 kv = M.kvec[k];
+    v[0] += s;
+    if (do_stress) {
+      v[1] += (1.0 - kv.w * kv.x * kv.x) * s;
+      v[2] += (1.0 - kv.w * kv.y * kv.y) * s;
+      v[3] += (1.0 - kv.w * kv.z * kv.z) * s;
+      v[4] -= kv.w * kv.x * kv.y * s;
+      v[5] -= kv.w * kv.x * kv.z * s;
+      v[6] -= kv.w * kv.y * kv.z * s;
+    }
+  }
+  block_sum<7>(v, red);
+  if (threadIdx.x == 0) {
+    out[0] = v[0] * 2.0 * tpi_V;
+    for (int a = 1; a < 7; ++a) out[a] = v[a] * 2.0 * tpi_V / omega;
+  }
+}
+
+// field / force partials.  grid.x = ion blocks (128), grid.y = k chunks
+// (row ranges rc[c]..rc[c+1]); dynamic smem = rho' of the chunk.
+// G accumulates sum_k n recarg, H accumulates sum_k n (k.mu) recarg2.
+template <typename R, bool HAS_MU_FORCE>
+__global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>::T* __restrict__ tab,
+                                                   const double4* __restrict__ w, int natm,
+                                                   RecMesh M, const int* __restrict__ rchunk,
+                                                   const double2* __restrict__ rhoA,
+                                                   double4* __restrict__ Gpart,
+                                                   double4* __restrict__ Hpart) {
+  typedef typename cplx<R>::T C;
+  extern __shared__ unsigned char shraw[];
+  C* sh = reinterpret_cast<C*>(shraw);
+  int r0 = rchunk[blockIdx.y], r1 = rchunk[blockIdx.y + 1];
+  int k0 = M.rows[r0].w;
+  int k1 = (r1 < M.nrows) ? M.rows[r1].w : M.nk;
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    double2 v = rhoA[k];
+    C c;
+    c.x = (R)v.x;
+    c.y = (R)v.y;
+    sh[k - k0] = c;
+  }
+  __syncthreads();
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natm) return;
+  const int kx = M.kmax[0], ky = M.kmax[1], kz = M.kmax[2];
+  double4 wi = w[i];
+  R m3 = (R)wi.w;
+  C Z1 = tab[(size_t)(kx + 1 + ky + 1 + 1) * natm + i];
+  double G[3] = {0, 0, 0}, H[3] = {0, 0, 0};
+  for (int r = r0; r < r1; ++r) {
+    int4 ri = M.rows[r];
+    int nx = ri.x, ny = ri.y, nz_lo = ri.z;
+    C P = phase_xyz<R>(tab, natm, i, nx, ny, nz_lo, kx, ky);
+    R S0 = R(0), Sz = R(0), T0 = R(0), Tz = R(0);
+    R nzd = (R)nz_lo;
+    R km = (R)(nx * wi.y + ny * wi.z + nz_lo * wi.w);
+    const C* rr = sh + (ri.w - k0);
+    int nn = kz - nz_lo + 1;
+    for (int t = 0; t < nn; ++t) {
+      C rho = rr[t];
+      R recarg = rho.y * P.x - rho.x * P.y;
+      S0 += recarg;
+      Sz += nzd * recarg;
+      if (HAS_MU_FORCE) {
+        R recarg2 = rho.x * P.x + rho.y * P.y;
+        R tt = km * recarg2;
+        T0 += tt;
+        Tz += nzd * tt;
+        km += m3;
+      }
+      nzd += R(1);
+      P = cmul(P, Z1);
+    }
+    G[0] += (double)nx * (double)S0;
+    G[1] += (double)ny * (double)S0;
+    G[2] += (double)Sz;
+    if (HAS_MU_FORCE) {
+      H[0] += (double)nx * (double)T0;
+      H[1] += (double)ny * (double)T0;
+      H[2] += (double)Tz;
+    }
+  }
+  Gpart[(size_t)blockIdx.y * natm + i] = make_double4(G[0], G[1], G[2], 0.0);
+  if (HAS_MU_FORCE) Hpart[(size_t)blockIdx.y * natm + i] = make_double4(H[0], H[1], H[2], 0.0);
+}
+
+// chunk sum and scaling.  E += -(2 pi B G) * 2 fpi_V (ewald_rec.f90:193-198,
+// 300-352); with do_forces, F += [q (-2 pi B G) + 2 pi B H] * 2 fpi_V * coul_unit.
+__global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const double4* __restrict__ Hpart,
+                                int nchunk, int natm, const CellC* __restrict__ cell,
+                                const double* __restrict__ q, double scale /* 2 fpi_V */,
+                                int has_mu_force, int do_forces, double coul_unit,
+                                double4* __restrict__ E, double* __restrict__ force) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natm) return;
+  double g[3] = {0, 0, 0}, h[3] = {0, 0, 0};
+  for (int c = 0; c < nchunk; ++c) {
+    double4 v = Gpart[(size_t)c * natm + i];
+    g[0] += v.x;
+    g[1] += v.y;
+    g[2] += v.z;
+    if (has_mu_force) {
+      double4 u = Hpart[(size_t)c * natm + i];
+      h[0] += u.x;
+      h[1] += u.y;
+      h[2] += u.z;
+    }
+  }
+  const double* B = cell->B;
+  double e[3], fm[3];
+  for (int a = 0; a < 3; ++a) {
+    e[a] = -kTwoPi * (B[3 * a + 0] * g[0] + B[3 * a + 1] * g[1] + B[3 * a + 2] * g[2]) * scale;
+    fm[a] = kTwoPi * (B[3 * a + 0] * h[0] + B[3 * a + 1] * h[1] + B[3 * a + 2] * h[2]) * scale;
+  }
+  double4 o = E[i];
+  E[i] = make_double4(o.x + e[0], o.y + e[1], o.z + e[2], 0.0);
+  if (do_forces) {
+    double qi = q[i];
+    force[i] += (qi * e[0] + (has_mu_force ? fm[0] : 0.0)) * coul_unit;
+    force[natm + i] += (qi * e[1] + (has_mu_force ? fm[1] : 0.0)) * coul_unit;
+    force[2 * natm + i] += (qi * e[2] + (has_mu_force ? fm[2] : 0.0)) * coul_unit;
+  }
+}
+
+}  // namespace mdff

@@ -1,0 +1,1380 @@
+/*
+ * mdff_oracle.c -- CPU FP64 restatement of the MDFF engforce path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker, never the product): see
+ * mdff_oracle.h.  Citations are file:line in the reference's src/ tree.
+ *
+ * Differences from the reference that are deliberate and documented:
+ *  - Positions are never modified in place: the reference converts rx,ry,rz
+ *    Cartesian->direct->Cartesian inside every pair routine (kardir/dirkar,
+ *    lattice.f90:183-270), perturbing them at the ulp level each call; here
+ *    each routine computes direct coordinates into a scratch copy with the
+ *    same arithmetic.
+ *  - Forces start from zero on every call (the reference keeps stale fx when
+ *    no short-range potential is switched on, engforce_driver.f90:116-135).
+ *  - The electric field returned is always the do_efield=.true. field.
+ *  - Quadrupole tasks (task_coul(4:6)) and Thole functions are not built
+ *    (theta is zeroed by engforce; thole_functions defaults to .false.).
+ *  - One optional extension: a W/r^24 wall added to BMH pairs (params.wall24,
+ *    zero = reference behaviour).
+ */
+#include "mdff_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define NT MDFF_NTYPEMAX
+#define TT_MAX 8
+
+/* constants.f90:65-94 */
+static const double PI = 3.14159265358979323846264338327950;
+#define TPI (2.0 * PI)
+#define COUL_UNIT_EV 14.3996441494161
+#define PRESS_UNIT_EV 0.00624150964712042
+
+struct or_ctx {
+  mdff_params p;      /* after symmetrisation / clamp / lautoES */
+  int natm;
+  int* itype;         /* [natm] 0-based */
+  int* ipolar;        /* [natm] */
+  double* qia;        /* [natm] */
+  double* dipia;      /* [natm][3] */
+  double* poldipia;   /* [natm][3][3]  [ia][a][b] = poldipia(a,b,ia) */
+  double* invpoldipia;
+  /* non_bonded derived (non_bonded.f90:455-644) */
+  double rcutsq[NT][NT], sigsq[NT][NT], epsp[NT][NT], fc[NT][NT];
+  double uc[NT][NT], uc1[NT][NT], uc2[NT][NT];
+  double E_TT[TT_MAX + 1];
+  /* cell (lattice.f90:60-180) */
+  double A[3][3], B[3][3], omega, WA, WB, WC, ANORM[3];
+  /* coulomb */
+  int task[6];
+  double coul_unit, press_unit;
+  int nk;
+  double *kx, *ky, *kz, *kk, *Ak, *kcoe;
+  /* ASPC history dipia_ind_t(5,3,natm) -> [5][natm][3] */
+  double* hist;
+  int lpolar_any;
+};
+
+static int g_threads = 0;
+
+void or_set_threads(int n) { g_threads = n; }
+int or_get_threads(void) {
+#ifdef _OPENMP
+  return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+/* ---------------------------------------------------------------------- */
+/* functions.f90:28-40 -- Numerical Recipes Chebyshev erfc (NOT libm erfc)  */
+double or_errfc(double x) {
+  double z = fabs(x);
+  double t = 1.0 / (1.0 + 0.5 * z);
+  double r = t * exp(-z * z - 1.26551223 +
+                     t * (1.00002368 +
+                          t * (.37409196 +
+                               t * (.09678418 +
+                                    t * (-.18628806 +
+                                         t * (.27886807 +
+                                              t * (-1.13520398 +
+                                                   t * (1.48851587 +
+                                                        t * (-.82215223 + t * .17087277)))))))));
+  if (x < 0.0) r = 2.0 - r;
+  return r;
+}
+
+/* tt_damp.f90:42-58 get_TT_damp, :68-97 TT_damping_functions */
+static double E_TT_tab[TT_MAX + 1];
+static void tt_table(double* e) {
+  e[0] = 1.0;
+  for (int k = 1; k <= TT_MAX; ++k) e[k] = e[k - 1] / (double)k;
+}
+
+static void tt_damp_tab(const double* E_TT, double b, double c, double r, int order, double* f,
+                        double* fd) {
+  double br = b * r;
+  double expbdr = exp(-br) * c;
+  double ff = E_TT[order];
+  for (int k = order - 1; k >= 1; --k) ff = ff * br + E_TT[k];
+  ff = ff * br + E_TT[0];
+  *f = 1.0 - ff * expbdr;
+  /* Fortran ( br ) ** ( order ) with an integer exponent */
+  double p = 1.0;
+  for (int k = 0; k < order; ++k) p *= br;
+  *fd = E_TT[order] * p * expbdr * b;
+}
+
+void or_tt_damp(double b, double c, double r, int order, double* f, double* fd) {
+  tt_table(E_TT_tab);
+  tt_damp_tab(E_TT_tab, b, c, r, order, f, fd);
+}
+
+/* Fortran NINT: round half away from zero */
+static inline double fnint(double x) { return round(x); }
+
+/* lattice.f90:60-180 (only the parts engforce needs) */
+static void or_lattice(or_ctx* c, const double* Ain) {
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) c->A[a][b] = Ain[a * 3 + b];
+  double(*A)[3] = c->A;
+  double(*B)[3] = c->B;
+  /* EXPRO (tools.f90:786-798): B(:,1) = A(:,2) x A(:,3) ... */
+  int cyc[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+  for (int col = 0; col < 3; ++col) {
+    int u = cyc[col][0], v = cyc[col][1];
+    B[0][col] = A[1][u] * A[2][v] - A[2][u] * A[1][v];
+    B[1][col] = A[2][u] * A[0][v] - A[0][u] * A[2][v];
+    B[2][col] = A[0][u] * A[1][v] - A[1][u] * A[0][v];
+  }
+  double omega = B[0][0] * A[0][0] + B[1][0] * A[1][0] + B[2][0] * A[2][0];
+  c->omega = omega;
+  c->WA = omega / sqrt(B[0][0] * B[0][0] + B[1][0] * B[1][0] + B[2][0] * B[2][0]);
+  c->WB = omega / sqrt(B[0][1] * B[0][1] + B[1][1] * B[1][1] + B[2][1] * B[2][1]);
+  c->WC = omega / sqrt(B[0][2] * B[0][2] + B[1][2] * B[1][2] + B[2][2] * B[2][2]);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) B[i][j] = B[i][j] / omega;
+  for (int i = 0; i < 3; ++i)
+    c->ANORM[i] = sqrt(A[0][i] * A[0][i] + A[1][i] * A[1][i] + A[2][i] * A[2][i]);
+}
+
+/* kardir (lattice.f90:183-225) into scratch arrays */
+static void or_kardir(const or_ctx* c, const double* rx, const double* ry, const double* rz,
+                      double* sx, double* sy, double* sz) {
+  const double(*B)[3] = c->B;
+  for (int n = 0; n < c->natm; ++n) {
+    double vx = rx[n], vy = ry[n], vz = rz[n];
+    sx[n] = vx * B[0][0] + vy * B[1][0] + vz * B[2][0];
+    sy[n] = vx * B[0][1] + vy * B[1][1] + vz * B[2][1];
+    sz[n] = vx * B[0][2] + vy * B[1][2] + vz * B[2][2];
+  }
+}
+
+/* minimum image through direct coordinates (e.g. non_bonded.f90:1136-1145) */
+static inline double min_image(const or_ctx* c, double dsx, double dsy, double dsz, double* rxij,
+                               double* ryij, double* rzij) {
+  double sxij = dsx - fnint(dsx);
+  double syij = dsy - fnint(dsy);
+  double szij = dsz - fnint(dsz);
+  const double(*A)[3] = c->A;
+  *rxij = sxij * A[0][0] + syij * A[0][1] + szij * A[0][2];
+  *ryij = sxij * A[1][0] + syij * A[1][1] + szij * A[1][2];
+  *rzij = sxij * A[2][0] + syij * A[2][1] + szij * A[2][2];
+  return *rxij * *rxij + *ryij * *ryij + *rzij * *rzij;
+}
+
+/* 3x3 inverse by LU with partial pivoting (DGETRF/DGETRI in
+   read_pos.f90:203-212); exact reciprocals for diagonal tensors. */
+static int inv3(const double* m, double* out) {
+  /* a diagonal tensor (the isotropic/axial polarisabilities of every deck)
+     is inverted entry by entry; a zero entry stays zero (pseudo-inverse), as
+     a site polarisable along x only (examples/ex04/control_twocharges_twopola.F
+     pol(3,1,1)) has no defined LAPACK inverse */
+  if (m[1] == 0.0 && m[2] == 0.0 && m[3] == 0.0 && m[5] == 0.0 && m[6] == 0.0 && m[7] == 0.0) {
+    for (int i = 0; i < 9; ++i) out[i] = 0.0;
+    for (int i = 0; i < 3; ++i) out[4 * i] = (m[4 * i] != 0.0) ? 1.0 / m[4 * i] : 0.0;
+    return 0;
+  }
+  double a[3][3];
+  int piv[3] = {0, 1, 2};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) a[i][j] = m[i * 3 + j];
+  for (int k = 0; k < 3; ++k) {
+    int p = k;
+    for (int i = k + 1; i < 3; ++i)
+      if (fabs(a[i][k]) > fabs(a[p][k])) p = i;
+    if (a[p][k] == 0.0) return -1;
+    if (p != k) {
+      for (int j = 0; j < 3; ++j) {
+        double t = a[k][j];
+        a[k][j] = a[p][j];
+        a[p][j] = t;
+      }
+      int t = piv[k];
+      piv[k] = piv[p];
+      piv[p] = t;
+    }
+    for (int i = k + 1; i < 3; ++i) {
+      a[i][k] /= a[k][k];
+      for (int j = k + 1; j < 3; ++j) a[i][j] -= a[i][k] * a[k][j];
+    }
+  }
+  /* solve for each unit vector */
+  for (int col = 0; col < 3; ++col) {
+    double y[3];
+    for (int i = 0; i < 3; ++i) {
+      double s = (piv[i] == col) ? 1.0 : 0.0;
+      for (int j = 0; j < i; ++j) s -= a[i][j] * y[j];
+      y[i] = s;
+    }
+    for (int i = 2; i >= 0; --i) {
+      double s = y[i];
+      for (int j = i + 1; j < 3; ++j) s -= a[i][j] * y[j];
+      y[i] = s / a[i][i];
+    }
+    for (int i = 0; i < 3; ++i) out[i * 3 + col] = y[i];
+  }
+  return 0;
+}
+
+/* symmetric_pot: X(:,it) = X(it,:) for it = 1..ntype (non_bonded.f90:287-301) */
+static void sym2(double X[NT][NT], int ntype) {
+  for (int it = 0; it < ntype; ++it) {
+    double row[NT];
+    for (int k = 0; k < NT; ++k) row[k] = X[it][k];
+    for (int k = 0; k < NT; ++k) X[k][it] = row[k];
+  }
+}
+/* pim.f90:186-199: X(it2,:,it) = X(it2,it,:) */
+#define SYM3(X, T)                                                  \
+  do {                                                              \
+    for (int it = 0; it < ntype; ++it)                              \
+      for (int it2 = 0; it2 < ntype; ++it2) {                       \
+        T row[NT];                                                  \
+        for (int k = 0; k < NT; ++k) row[k] = (X)[it2][it][k];      \
+        for (int k = 0; k < NT; ++k) (X)[it2][k][it] = row[k];      \
+      }                                                             \
+  } while (0)
+
+/* kpoint_sum_init (kspace.f90:143-207) + reorder_kpt (:286-342): stable sort
+   by k^2 (merge_sort, tools.f90:667-785, keeps equal keys in order). */
+static void or_kmesh(or_ctx* c) {
+  int kx = c->p.kES[0], ky = c->p.kES[1], kz = c->p.kES[2];
+  int nk = kz + ky * (2 * kz + 1) + kx * (2 * ky + 1) * (2 * kz + 1);
+  free(c->kx);
+  free(c->ky);
+  free(c->kz);
+  free(c->kk);
+  free(c->Ak);
+  free(c->kcoe);
+  double* tx = malloc(sizeof(double) * nk);
+  double* ty = malloc(sizeof(double) * nk);
+  double* tz = malloc(sizeof(double) * nk);
+  double* tk = malloc(sizeof(double) * nk);
+  double* ta = malloc(sizeof(double) * nk);
+  double* tc = malloc(sizeof(double) * nk);
+  double alpha = c->p.alphaES, alpha2 = alpha * alpha;
+  const double(*B)[3] = c->B;
+  int n = 0;
+  for (int nx = 0; nx <= kx; ++nx) {
+    int nymin = (nx == 0) ? 0 : -ky;
+    for (int ny = nymin; ny <= ky; ++ny) {
+      int nzmin = (nx == 0 && ny == 0) ? 1 : -kz;
+      for (int nz = nzmin; nz <= kz; ++nz) {
+        double X = (double)nx, Y = (double)ny, Z = (double)nz;
+        double kxx = TPI * (X * B[0][0] + Y * B[0][1] + Z * B[0][2]);
+        double kyy = TPI * (X * B[1][0] + Y * B[1][1] + Z * B[1][2]);
+        double kzz = TPI * (X * B[2][0] + Y * B[2][1] + Z * B[2][2]);
+        double kk = kxx * kxx + kyy * kyy + kzz * kzz;
+        tx[n] = kxx;
+        ty[n] = kyy;
+        tz[n] = kzz;
+        tk[n] = kk;
+        ta[n] = exp(-kk * 0.25 / alpha2) / kk;
+        tc[n] = 2.0 * (1.0 / kk + 1.0 / alpha2 / 4.0);
+        ++n;
+      }
+    }
+  }
+  /* stable ordering by kk: insertion-merge via index sort with tie on index */
+  int* idx = malloc(sizeof(int) * nk);
+  for (int i = 0; i < nk; ++i) idx[i] = i;
+  /* bottom-up stable merge sort on indices */
+  int* tmp = malloc(sizeof(int) * nk);
+  for (int w = 1; w < nk; w *= 2) {
+    for (int lo = 0; lo < nk; lo += 2 * w) {
+      int mid = lo + w < nk ? lo + w : nk, hi = lo + 2 * w < nk ? lo + 2 * w : nk;
+      int i = lo, j = mid, o = lo;
+      while (i < mid && j < hi) tmp[o++] = (tk[idx[i]] <= tk[idx[j]]) ? idx[i++] : idx[j++];
+      while (i < mid) tmp[o++] = idx[i++];
+      while (j < hi) tmp[o++] = idx[j++];
+    }
+    memcpy(idx, tmp, sizeof(int) * nk);
+  }
+  c->kx = malloc(sizeof(double) * nk);
+  c->ky = malloc(sizeof(double) * nk);
+  c->kz = malloc(sizeof(double) * nk);
+  c->kk = malloc(sizeof(double) * nk);
+  c->Ak = malloc(sizeof(double) * nk);
+  c->kcoe = malloc(sizeof(double) * nk);
+  for (int i = 0; i < nk; ++i) {
+    int l = idx[i];
+    c->kx[i] = tx[l];
+    c->ky[i] = ty[l];
+    c->kz[i] = tz[l];
+    c->kk[i] = tk[l];
+    c->Ak[i] = ta[l];
+    c->kcoe[i] = tc[l];
+  }
+  c->nk = nk;
+  free(idx);
+  free(tmp);
+  free(tx);
+  free(ty);
+  free(tz);
+  free(tk);
+  free(ta);
+  free(tc);
+}
+
+/* ewald_param (coulomb.f90:363-410) */
+static void or_ewald_param(or_ctx* c) {
+  double rcut = 0.5 * fmin(c->WA, fmin(c->WB, c->WC));
+  double cut = c->p.cutlongrange;
+  c->p.cutlongrange = fmin(cut, rcut);
+  cut = c->p.cutlongrange;
+  double eps = fmin(fabs(c->p.epsw), 0.5);
+  double tol = sqrt(fabs(log(eps * cut)));
+  double alpha = sqrt(fabs(log(eps * cut * tol))) / cut;
+  double tol1 = sqrt(-log(eps * cut * (2.0 * tol * alpha) * (2.0 * tol * alpha)));
+  if (c->p.lautoES) {
+    c->p.alphaES = alpha;
+    for (int i = 0; i < 3; ++i) c->p.kES[i] = (int)fnint(0.25 + c->ANORM[i] * alpha * tol1 / PI);
+  }
+}
+
+or_ctx* or_create(const mdff_params* pin, const double cell_A[9], int* status) {
+  *status = MDFF_OK;
+  if (!pin || pin->natm <= 0 || pin->ntype <= 0 || pin->ntype > NT) {
+    *status = MDFF_ERR_BAD_ARGS;
+    return NULL;
+  }
+  or_ctx* c = calloc(1, sizeof(or_ctx));
+  c->p = *pin;
+  int ntype = c->p.ntype, natm = c->p.natm;
+  int tot = 0;
+  for (int it = 0; it < ntype; ++it) tot += c->p.natmi[it];
+  if (tot != natm) {
+    *status = MDFF_ERR_BAD_ARGS;
+    free(c);
+    return NULL;
+  }
+  c->natm = natm;
+  tt_table(c->E_TT);
+  /* non_bonded_check_tag (non_bonded.f90:287-301) */
+  if (c->p.symmetric_pot_nb) {
+    sym2(c->p.epslj, ntype);
+    sym2(c->p.sigmalj, ntype);
+    sym2(c->p.plj, ntype);
+    sym2(c->p.qlj, ntype);
+    sym2(c->p.Abmhftd, ntype);
+    sym2(c->p.Bbmhftd, ntype);
+    sym2(c->p.Cbmhftd, ntype);
+    sym2(c->p.Dbmhftd, ntype);
+    sym2(c->p.BDbmhftd, ntype);
+    sym2(c->p.wall24, ntype);
+  }
+  /* pim_check_tag (pim.f90:186-204) */
+  if (c->p.symmetric_pot_pim) {
+    SYM3(c->p.ldip_damping, int);
+    SYM3(c->p.pol_damp_b, double);
+    SYM3(c->p.pol_damp_c, double);
+    SYM3(c->p.pol_damp_k, int);
+  }
+  for (int a = 0; a < NT; ++a)
+    for (int b = 0; b < NT; ++b)
+      for (int k = 0; k < NT; ++k)
+        if (c->p.pol_damp_k[a][b][k] > TT_MAX || c->p.pol_damp_k[a][b][k] < 0) {
+          *status = MDFF_ERR_BAD_ARGS;
+          or_destroy(c);
+          return NULL;
+        }
+  /* units (constants.f90:88-94, reduced_units :140-153) */
+  c->coul_unit = c->p.lreduced ? 1.0 : COUL_UNIT_EV;
+  c->press_unit = c->p.lreduced ? 1.0 : PRESS_UNIT_EV;
+  /* initialize_param_non_bonded (non_bonded.f90:455-644) */
+  double two16 = pow(2.0, 1.0 / 6.0);
+  for (int it = 0; it < ntype; ++it)
+    for (int jt = 0; jt < ntype; ++jt) {
+      double rcut = c->p.cutshortrange;
+      double pp = c->p.plj[it][jt], qq = c->p.qlj[it][jt];
+      c->rcutsq[it][jt] = rcut * rcut;
+      double ppqq = pp * qq;
+      c->epsp[it][jt] = c->p.epslj[it][jt] / (qq - pp);
+      c->sigsq[it][jt] = two16 * two16 * c->p.sigmalj[it][jt] * c->p.sigmalj[it][jt];
+      double sr2 = c->sigsq[it][jt] / c->rcutsq[it][jt];
+      double sr = sqrt(sr2);
+      double srp = pow(sr, pp), srq = pow(sr, qq);
+      c->uc[it][jt] = c->epsp[it][jt] * (pp * srq - qq * srp);
+      c->uc1[it][jt] = c->epsp[it][jt] * ppqq / (2.0 * c->rcutsq[it][jt]) * (srq - srp);
+      c->uc2[it][jt] = 0.5 * c->epsp[it][jt] *
+                       ((2.0 * pp + ppqq) * srq - (2.0 * qq + ppqq) * srp);
+      c->fc[it][jt] = ppqq * c->epsp[it][jt] / c->sigsq[it][jt];
+    }
+  /* typeinfo_init (read_pos.f90:160-237) */
+  c->itype = malloc(sizeof(int) * natm);
+  c->ipolar = malloc(sizeof(int) * natm);
+  c->qia = malloc(sizeof(double) * natm);
+  c->dipia = malloc(sizeof(double) * 3 * natm);
+  c->poldipia = calloc(9 * (size_t)natm, sizeof(double));
+  c->invpoldipia = calloc(9 * (size_t)natm, sizeof(double));
+  c->hist = calloc((size_t)MDFF_ASPC_DEPTH * 3 * natm, sizeof(double));
+  int ia = 0;
+  for (int it = 0; it < ntype; ++it) {
+    double inv[9];
+    int ok = 0;
+    if (c->p.ldip_polar[it]) {
+      ok = inv3(&c->p.poldip[it][0][0], inv);
+      if (ok != 0) {
+        *status = MDFF_ERR_BAD_ARGS;
+        or_destroy(c);
+        return NULL;
+      }
+    }
+    for (int n = 0; n < c->p.natmi[it]; ++n, ++ia) {
+      c->itype[ia] = it;
+      c->ipolar[ia] = c->p.ldip_polar[it] ? 1 : 0;
+      c->qia[ia] = c->p.qch[it];
+      for (int a = 0; a < 3; ++a) c->dipia[3 * ia + a] = c->p.dip[it][a];
+      for (int a = 0; a < 9; ++a) c->poldipia[9 * ia + a] = (&c->p.poldip[it][0][0])[a];
+      if (c->p.ldip_polar[it])
+        for (int a = 0; a < 9; ++a) c->invpoldipia[9 * ia + a] = inv[a];
+    }
+  }
+  /* coulomb_check_tag + pim_check_tag task selection (coulomb.f90:204-220,
+     pim.f90:160-184) */
+  int lqch = 0, ldip = 0, lpol = 0;
+  for (int it = 0; it < NT; ++it) {
+    if (c->p.qch[it] != 0.0) lqch = 1;
+    for (int a = 0; a < 3; ++a)
+      if (c->p.dip[it][a] != 0.0) ldip = 1;
+  }
+  for (int it = 0; it < ntype; ++it)
+    if (c->p.ldip_polar[it]) lpol = 1;
+  c->lpolar_any = lpol;
+  memset(c->task, 0, sizeof(c->task));
+  if (lqch) c->task[0] = 1;
+  if (ldip || lpol) {
+    if (lqch) c->task[1] = 1;
+    c->task[2] = 1;
+  }
+  or_lattice(c, cell_A);
+  if (c->p.lcoulomb) {
+    or_ewald_param(c);
+    or_kmesh(c);
+  }
+  return c;
+}
+
+void or_destroy(or_ctx* c) {
+  if (!c) return;
+  free(c->itype);
+  free(c->ipolar);
+  free(c->qia);
+  free(c->dipia);
+  free(c->poldipia);
+  free(c->invpoldipia);
+  free(c->hist);
+  free(c->kx);
+  free(c->ky);
+  free(c->kz);
+  free(c->kk);
+  free(c->Ak);
+  free(c->kcoe);
+  free(c);
+}
+
+int or_get_setup(or_ctx* c, or_setup_info* info) {
+  info->alphaES = c->p.alphaES;
+  for (int i = 0; i < 3; ++i) info->kES[i] = c->p.kES[i];
+  info->nk = c->nk;
+  info->cutlongrange = c->p.cutlongrange;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) info->B[i * 3 + j] = c->B[i][j];
+  info->omega = c->omega;
+  info->WA = c->WA;
+  info->WB = c->WB;
+  info->WC = c->WC;
+  for (int i = 0; i < 6; ++i) info->task[i] = c->task[i];
+  return MDFF_OK;
+}
+
+int or_get_kmesh(or_ctx* c, double* kx, double* ky, double* kz, double* kk, double* Ak,
+                 double* kcoe) {
+  size_t n = sizeof(double) * c->nk;
+  memcpy(kx, c->kx, n);
+  memcpy(ky, c->ky, n);
+  memcpy(kz, c->kz, n);
+  memcpy(kk, c->kk, n);
+  memcpy(Ak, c->Ak, n);
+  memcpy(kcoe, c->kcoe, n);
+  return MDFF_OK;
+}
+
+int or_get_aspc(or_ctx* c, double* buf) {
+  memcpy(buf, c->hist, sizeof(double) * MDFF_ASPC_DEPTH * 3 * c->natm);
+  return MDFF_OK;
+}
+int or_set_aspc(or_ctx* c, const double* buf) {
+  memcpy(c->hist, buf, sizeof(double) * MDFF_ASPC_DEPTH * 3 * c->natm);
+  return MDFF_OK;
+}
+
+/* ---------------------------------------------------------------------- */
+/* vnlist_pbc (tools.f90:273-368): O(N^2) half lists with the parity mask   */
+static int half_mask(int ia, int ja) {
+  /* 0-based indices have the same parity of ia+ja as 1-based ones */
+  return (ia > ja && ((ia + ja) % 2 == 0)) || (ia < ja && ((ia + ja) % 2 != 0));
+}
+
+int or_vnlist(or_ctx* c, const double* rx, const double* ry, const double* rz, int which,
+              int* point, int* list, int capacity, int* n_out) {
+  int natm = c->natm;
+  double cut = (which == 0) ? c->p.cutshortrange : c->p.cutlongrange;
+  double rskinsq = cut + c->p.skindiff;
+  rskinsq = rskinsq * rskinsq;
+  double* sx = malloc(sizeof(double) * natm);
+  double* sy = malloc(sizeof(double) * natm);
+  double* sz = malloc(sizeof(double) * natm);
+  or_kardir(c, rx, ry, rz, sx, sy, sz);
+  int icount = 1, status = MDFF_OK;
+  for (int ia = 0; ia < natm; ++ia) {
+    int k = 0;
+    for (int ja = 0; ja < natm; ++ja) {
+      if (!half_mask(ia, ja)) continue;
+      double rxij, ryij, rzij;
+      double rijsq = min_image(c, sx[ia] - sx[ja], sy[ia] - sy[ja], sz[ia] - sz[ja], &rxij,
+                               &ryij, &rzij);
+      if (rijsq <= rskinsq) {
+        icount++;
+        k++;
+        if (icount - 1 > capacity) {
+          status = MDFF_ERR_LIST_OVERFLOW;
+        } else {
+          list[icount - 2] = ja + 1;
+        }
+      }
+    }
+    point[ia] = icount - k;
+  }
+  point[natm] = icount;
+  *n_out = icount - 1;
+  free(sx);
+  free(sy);
+  free(sz);
+  return status;
+}
+
+/* CSR half list, 0-based, for internal use */
+typedef struct {
+  int* point;
+  int* list;
+  int n;
+} csr_t;
+
+static void build_half(or_ctx* c, const double* sx, const double* sy, const double* sz, double cut,
+                       csr_t* out) {
+  int natm = c->natm;
+  double rskinsq = cut + c->p.skindiff;
+  rskinsq = rskinsq * rskinsq;
+  int* cnt = calloc(natm + 1, sizeof(int));
+  int nth = or_get_threads();
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nth)
+  for (int ia = 0; ia < natm; ++ia) {
+    int k = 0;
+    for (int ja = 0; ja < natm; ++ja) {
+      if (!half_mask(ia, ja)) continue;
+      double x, y, z;
+      if (min_image(c, sx[ia] - sx[ja], sy[ia] - sy[ja], sz[ia] - sz[ja], &x, &y, &z) <= rskinsq)
+        k++;
+    }
+    cnt[ia] = k;
+  }
+  out->point = malloc(sizeof(int) * (natm + 1));
+  out->point[0] = 0;
+  for (int ia = 0; ia < natm; ++ia) out->point[ia + 1] = out->point[ia] + cnt[ia];
+  out->n = out->point[natm];
+  out->list = malloc(sizeof(int) * (out->n > 0 ? out->n : 1));
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nth)
+  for (int ia = 0; ia < natm; ++ia) {
+    int o = out->point[ia];
+    for (int ja = 0; ja < natm; ++ja) {
+      if (!half_mask(ia, ja)) continue;
+      double x, y, z;
+      if (min_image(c, sx[ia] - sx[ja], sy[ia] - sy[ja], sz[ia] - sz[ja], &x, &y, &z) <= rskinsq)
+        out->list[o++] = ja;
+    }
+  }
+  free(cnt);
+}
+static void free_csr(csr_t* l) {
+  free(l->point);
+  free(l->list);
+}
+
+/* ---------------------------------------------------------------------- */
+/* engforce_bmhftd_pbc (non_bonded.f90:1076-1228) + optional r^-24 wall      */
+static void or_bmhftd(or_ctx* c, const double* sx, const double* sy, const double* sz,
+                      const csr_t* L, double* fx, double* fy, double* fz, double* u_out,
+                      double* vir_out, double tau[3][3]) {
+  int natm = c->natm;
+  int lbmhftd = c->p.lbmhftd;
+  double u = 0.0, vir = 0.0;
+  double t[3][3] = {{0}};
+  memset(fx, 0, sizeof(double) * natm);
+  memset(fy, 0, sizeof(double) * natm);
+  memset(fz, 0, sizeof(double) * natm);
+  for (int ia = 0; ia < natm; ++ia) {
+    for (int j1 = L->point[ia]; j1 < L->point[ia + 1]; ++j1) {
+      int ja = L->list[j1];
+      if (ja == ia) continue;
+      double rxij, ryij, rzij;
+      double rijsq =
+          min_image(c, sx[ia] - sx[ja], sy[ia] - sy[ja], sz[ia] - sz[ja], &rxij, &ryij, &rzij);
+      int p1 = c->itype[ia], p2 = c->itype[ja];
+      if (c->p.Abmhftd[p1][p2] == 0.0) continue;
+      if (rijsq < c->rcutsq[p1][p2]) {
+        double ir2 = 1.0 / rijsq;
+        double d = sqrt(rijsq);
+        double erh = c->p.Abmhftd[p1][p2] * exp(-c->p.Bbmhftd[p1][p2] * d);
+        double ir6 = ir2 * ir2 * ir2;
+        double ir8 = ir6 * ir2;
+        ir6 = ir6 * c->p.Cbmhftd[p1][p2];
+        ir8 = ir8 * c->p.Dbmhftd[p1][p2];
+        double f6, f8, fdiff6, fdiff8, ir6d, ir8d;
+        if (lbmhftd) {
+          tt_damp_tab(c->E_TT, c->p.BDbmhftd[p1][p2], 1.0, d, 6, &f6, &fdiff6);
+          tt_damp_tab(c->E_TT, c->p.BDbmhftd[p1][p2], 1.0, d, 8, &f8, &fdiff8);
+          ir6d = ir6 * f6;
+          ir8d = ir8 * f8;
+        } else {
+          fdiff6 = 0.0;
+          fdiff8 = 0.0;
+          ir6d = ir6;
+          ir8d = ir8;
+        }
+        double ir7 = 6.0 * ir6d / d;
+        double ir9 = 8.0 * ir8d / d;
+        double uw = 0.0;
+        if (c->p.wall24[p1][p2] != 0.0) {
+          double ir8r = (ir2 * ir2) * (ir2 * ir2);
+          uw = c->p.wall24[p1][p2] * (ir8r * ir8r * ir8r);
+        }
+        u = u + erh - ir6d - ir8d + uw;
+        double wij = c->p.Bbmhftd[p1][p2] * erh - ir7 - ir9 + ir6 * fdiff6 + ir8 * fdiff8 +
+                     24.0 * uw / d;
+        wij = wij / d;
+        double fxij = wij * rxij, fyij = wij * ryij, fzij = wij * rzij;
+        vir = vir + (rxij * fxij + ryij * fyij + rzij * fzij);
+        fx[ia] += fxij;
+        fy[ia] += fyij;
+        fz[ia] += fzij;
+        fx[ja] -= fxij;
+        fy[ja] -= fyij;
+        fz[ja] -= fzij;
+        double r[3] = {rxij, ryij, rzij}, f[3] = {fxij, fyij, fzij};
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) t[a][b] += (r[a] * f[b] + r[b] * f[a]);
+      }
+    }
+  }
+  vir = vir / 3.0;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) tau[a][b] = t[a][b] / c->omega / c->press_unit * 0.5;
+  *u_out = u;
+  *vir_out = vir;
+}
+
+/* engforce_nmlj_pbc (non_bonded.f90:660-827) */
+static void or_nmlj(or_ctx* c, const double* sx, const double* sy, const double* sz,
+                    const csr_t* L, double* fx, double* fy, double* fz, double* u_out,
+                    double* vir_out, double tau[3][3]) {
+  int natm = c->natm, trunc = c->p.trunc;
+  double u = 0.0, vir = 0.0;
+  double t[3][3] = {{0}};
+  memset(fx, 0, sizeof(double) * natm);
+  memset(fy, 0, sizeof(double) * natm);
+  memset(fz, 0, sizeof(double) * natm);
+  for (int ia = 0; ia < natm; ++ia) {
+    for (int j1 = L->point[ia]; j1 < L->point[ia + 1]; ++j1) {
+      int ja = L->list[j1];
+      if (ja == ia) continue;
+      double rxij, ryij, rzij;
+      double rijsq =
+          min_image(c, sx[ia] - sx[ja], sy[ia] - sy[ja], sz[ia] - sz[ja], &rxij, &ryij, &rzij);
+      int p1 = c->itype[ia], p2 = c->itype[ja];
+      if (rijsq < c->rcutsq[p1][p2]) {
+        double sr2 = c->sigsq[p1][p2] / rijsq;
+        double srp = pow(sr2, c->p.plj[p1][p2] * 0.5);
+        double srq = pow(sr2, c->p.qlj[p1][p2] * 0.5);
+        double e = c->epsp[p1][p2] * (c->p.plj[p1][p2] * srq - c->p.qlj[p1][p2] * srp);
+        if (trunc == 0) u = u + e;
+        if (trunc == 1) u = u + e - c->uc[p1][p2];
+        if (trunc == 2) u = u + e + c->uc1[p1][p2] * rijsq - c->uc2[p1][p2];
+        double wij = c->fc[p1][p2] * (srq - srp) * sr2;
+        double fxij = wij * rxij, fyij = wij * ryij, fzij = wij * rzij;
+        vir = vir + wij * rijsq;
+        fx[ia] += fxij;
+        fy[ia] += fyij;
+        fz[ia] += fzij;
+        fx[ja] -= fxij;
+        fy[ja] -= fyij;
+        fz[ja] -= fzij;
+        double r[3] = {rxij, ryij, rzij}, f[3] = {fxij, fyij, fzij};
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) t[a][b] += (r[a] * f[b] + r[b] * f[a]) * 0.5;
+      }
+    }
+  }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) tau[a][b] = t[a][b] / c->omega / c->press_unit;
+  *u_out = u;
+  *vir_out = vir / 3.0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* multipole_ES_dir (ewald_dir.f90:40-798), tasks qq / qd / dd              */
+typedef struct {
+  double u;
+  double* ef;   /* [natm][3] */
+  double* efg;  /* [natm][9] */
+  double* f;    /* [natm][3] */
+  double tau[3][3];
+} es_acc;
+
+static void es_dir(or_ctx* c, const double* sx, const double* sy, const double* sz,
+                   const csr_t* L, const double* q, const double* mu, const int* task, int damp_ind,
+                   int do_efield, int do_efg, int do_forces, int do_stress, es_acc* out) {
+  int natm = c->natm;
+  const mdff_params* p = &c->p;
+  double alphaES = p->alphaES;
+  double cutsq = p->cutlongrange * p->cutlongrange;
+  double alpha2 = alphaES * alphaES, alpha3 = alpha2 * alphaES, alpha5 = alpha3 * alpha2;
+  double alpha7 = alpha5 * alpha2, alpha9 = alpha7 * alpha2;
+  double piroot = sqrt(PI);
+  int charge_charge = task[0], charge_dipole = task[1], dipole_dipole = task[2];
+  int nth = or_get_threads();
+  double u_tot = 0.0;
+  double tau_tot[9] = {0};
+  double* ef_t = calloc((size_t)nth * natm * 3, sizeof(double));
+  double* efg_t = do_efg ? calloc((size_t)nth * natm * 9, sizeof(double)) : NULL;
+  double* f_t = calloc((size_t)nth * natm * 3, sizeof(double));
+#pragma omp parallel num_threads(nth) reduction(+ : u_tot)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double* ef = ef_t + (size_t)tid * natm * 3;
+    double* efg = efg_t ? efg_t + (size_t)tid * natm * 9 : NULL;
+    double* fo = f_t + (size_t)tid * natm * 3;
+    double tl[3][3] = {{0}};
+    double u_dir = 0.0;
+#pragma omp for schedule(dynamic, 8)
+    for (int ia = 0; ia < natm; ++ia) {
+      int ita = c->itype[ia];
+      double qi = q[ia];
+      const double* mui = mu + 3 * ia;
+      int dip_i = (mui[0] != 0.0 || mui[1] != 0.0 || mui[2] != 0.0);
+      for (int j1 = L->point[ia]; j1 < L->point[ia + 1]; ++j1) {
+        int ja = L->list[j1];
+        if (ja == ia) continue;
+        double fij[3] = {0.0, 0.0, 0.0};
+        int jta = c->itype[ja];
+        double qj = q[ja];
+        const double* muj = mu + 3 * ja;
+        int dip_j = (muj[0] != 0.0 || muj[1] != 0.0 || muj[2] != 0.0);
+        double qij = qi * qj;
+        double r[3];
+        double d2 = min_image(c, sx[ia] - sx[ja], sy[ia] - sy[ja], sz[ia] - sz[ja], &r[0], &r[1],
+                              &r[2]);
+        if (d2 > cutsq) continue;
+        double d = sqrt(d2);
+        double d3 = d2 * d, d5 = d3 * d2, d7 = d5 * d2;
+        double dm1 = 1.0 / d;
+        double dm3 = dm1 / d2, dm5 = dm3 / d2, dm7 = dm5 / d2;
+        /* damping (ewald_dir.f90:216-228) */
+        int ldamp = p->ldip_damping[ita][ita][jta] || p->ldip_damping[jta][ita][jta];
+        if (!damp_ind) ldamp = 0;
+        double fdamp = 1.0, fdamp2 = 1.0, fdampdiff = 0.0, fdampdiff2 = 0.0;
+        if (ldamp) {
+          tt_damp_tab(c->E_TT, p->pol_damp_b[ita][ita][jta], p->pol_damp_c[ita][ita][jta], d,
+                      p->pol_damp_k[ita][ita][jta], &fdamp, &fdampdiff);
+          tt_damp_tab(c->E_TT, p->pol_damp_b[jta][ita][jta], p->pol_damp_c[jta][ita][jta], d,
+                      p->pol_damp_k[jta][ita][jta], &fdamp2, &fdampdiff2);
+        }
+        double expon = exp(-alpha2 * d2) / piroot;
+        double F0 = or_errfc(alphaES * d);
+        double F1 = F0 + 2.0 * alphaES * d * expon;
+        double F2 = F1 + 4.0 * alpha3 * d3 * expon / 3.0;
+        double F3 = F2 + 8.0 * alpha5 * d5 * expon / 15.0;
+        (void)alpha7;
+        (void)alpha9;
+        double F1d = -fdamp + 1.0;
+        double F2d = F1d + (d / 3.0) * fdampdiff;
+        double F1d2 = -fdamp2 + 1.0;
+        double F2d2 = F1d2 + (d / 3.0) * fdampdiff2;
+        double T0 = dm1 * F0;
+        double T1[3], T1d[3], T1d2[3];
+        for (int a = 0; a < 3; ++a) {
+          T1[a] = -r[a] * dm3;
+          if (ldamp) {
+            T1d[a] = T1[a] * F1d;
+            T1d2[a] = T1[a] * F1d2;
+          }
+          T1[a] = T1[a] * F1;
+        }
+        double F2_dm5 = 3.0 * F2 * dm5, F2d_dm5 = 3.0 * F2d * dm5, F2d2_dm5 = 3.0 * F2d2 * dm5;
+        double F1_dm3 = F1 * dm3, F1d_dm3 = F1d * dm3, F1d2_dm3 = F1d2 * dm3;
+        double T2[3][3], T2d[3][3], T2d2[3][3];
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) {
+            T2[a][b] = r[a] * r[b] * F2_dm5;
+            if (a == b) T2[a][a] = T2[a][a] - F1_dm3;
+            if (ldamp) {
+              T2d[a][b] = r[a] * r[b] * F2d_dm5;
+              T2d2[a][b] = r[a] * r[b] * F2d2_dm5;
+              if (a == b) {
+                T2d[a][a] = T2d[a][a] - F1d_dm3;
+                T2d2[a][a] = T2d2[a][a] - F1d2_dm3;
+              }
+            }
+          }
+        double F3_dm7 = F3 * dm7 * 15.0;
+        double T3[3][3][3];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) {
+              double v = -r[i] * r[j] * r[k] * F3_dm7;
+              if (i == j) v = v + r[k] * F2_dm5;
+              if (i == k) v = v + r[j] * F2_dm5;
+              if (j == k) v = v + r[i] * F2_dm5;
+              T3[i][j][k] = v;
+            }
+        /* qq (ewald_dir.f90:528-553) */
+        if (charge_charge) {
+          u_dir = u_dir + qij * T0;
+          if (do_efield) {
+            for (int a = 0; a < 3; ++a) {
+              ef[3 * ia + a] = ef[3 * ia + a] - qj * T1[a];
+              ef[3 * ja + a] = ef[3 * ja + a] + qi * T1[a];
+            }
+            if (ldamp)
+              for (int a = 0; a < 3; ++a) {
+                ef[3 * ia + a] = ef[3 * ia + a] + qj * T1d[a];
+                ef[3 * ja + a] = ef[3 * ja + a] - qi * T1d2[a];
+              }
+          }
+          if (do_efg)
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) {
+                efg[9 * ia + 3 * a + b] -= qj * T2[a][b];
+                efg[9 * ja + 3 * a + b] -= qi * T2[a][b];
+              }
+          if (do_forces)
+            for (int a = 0; a < 3; ++a) fij[a] = fij[a] + qij * T1[a];
+        }
+        /* dd (ewald_dir.f90:557-593); T2_thole = T2 (no Thole functions) */
+        if (dipole_dipole && (dip_i && dip_j)) {
+          for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) u_dir = u_dir - mui[j] * T2[j][k] * muj[k];
+          if (do_efield)
+            for (int k = 0; k < 3; ++k)
+              for (int a = 0; a < 3; ++a) {
+                ef[3 * ia + a] = ef[3 * ia + a] + T2[a][k] * muj[k];
+                ef[3 * ja + a] = ef[3 * ja + a] + T2[a][k] * mui[k];
+              }
+          if (do_efg)
+            for (int k = 0; k < 3; ++k)
+              for (int a = 0; a < 3; ++a)
+                for (int b = 0; b < 3; ++b) {
+                  efg[9 * ia + 3 * a + b] += T3[a][b][k] * muj[k];
+                  efg[9 * ja + 3 * a + b] -= T3[a][b][k] * mui[k];
+                }
+          if (do_forces)
+            for (int j = 0; j < 3; ++j)
+              for (int k = 0; k < 3; ++k)
+                for (int a = 0; a < 3; ++a) fij[a] = fij[a] - mui[j] * T3[j][a][k] * muj[k];
+        }
+        /* qd (ewald_dir.f90:599-644) */
+        if (charge_dipole && (dip_i || dip_j)) {
+          for (int k = 0; k < 3; ++k) {
+            u_dir = u_dir - qi * T1[k] * muj[k];
+            u_dir = u_dir + qj * T1[k] * mui[k];
+            if (ldamp) {
+              u_dir = u_dir + qi * T1d2[k] * muj[k];
+              u_dir = u_dir - qj * T1d[k] * mui[k];
+            }
+          }
+          if (do_forces) {
+            for (int j = 0; j < 3; ++j)
+              for (int k = 0; k < 3; ++k) {
+                fij[k] = fij[k] - qi * T2[k][j] * muj[j];
+                fij[k] = fij[k] + qj * T2[k][j] * mui[j];
+              }
+          }
+          if (ldamp && do_forces)
+            for (int j = 0; j < 3; ++j)
+              for (int k = 0; k < 3; ++k) {
+                fij[k] = fij[k] - qj * T2d[j][k] * mui[j];
+                fij[k] = fij[k] + qi * T2d2[j][k] * muj[j];
+              }
+        }
+        if (do_forces)
+          for (int a = 0; a < 3; ++a) {
+            fo[3 * ia + a] -= fij[a];
+            fo[3 * ja + a] += fij[a];
+          }
+        if (do_stress)
+          for (int j = 0; j < 3; ++j)
+            for (int k = 0; k < 3; ++k) tl[j][k] = tl[j][k] - (r[j] * fij[k] + r[k] * fij[j]);
+      }
+    }
+    u_tot += u_dir;
+#pragma omp critical
+    {
+      for (int j = 0; j < 3; ++j)
+        for (int k = 0; k < 3; ++k) tau_tot[3 * j + k] += tl[j][k];
+    }
+  }
+  /* thread reduction, fixed order */
+  for (int t = 0; t < nth; ++t) {
+    for (size_t i = 0; i < (size_t)natm * 3; ++i) {
+      out->ef[i] += ef_t[(size_t)t * natm * 3 + i];
+      out->f[i] += f_t[(size_t)t * natm * 3 + i];
+    }
+    if (do_efg)
+      for (size_t i = 0; i < (size_t)natm * 9; ++i) out->efg[i] += efg_t[(size_t)t * natm * 9 + i];
+  }
+  out->u = u_tot;
+  for (int j = 0; j < 3; ++j)
+    for (int k = 0; k < 3; ++k)
+      out->tau[j][k] = do_stress ? tau_tot[3 * j + k] / c->omega * 0.5 : 0.0;
+  free(ef_t);
+  free(efg_t);
+  free(f_t);
+}
+
+/* multipole_ES_rec (ewald_rec.f90:38-365) */
+static void es_rec(or_ctx* c, const double* rx, const double* ry, const double* rz,
+                   const double* q, const double* mu, const int* task, int do_efield, int do_efg,
+                   int do_forces, int do_stress, es_acc* out) {
+  int natm = c->natm;
+  double tpi_V = TPI / c->omega, fpi_V = tpi_V * 2.0;
+  int ldip = task[1] || task[2];
+  int nth = or_get_threads();
+  double u_rec = 0.0;
+  double tr[3][3] = {{0}};
+  double* ef_t = calloc((size_t)nth * natm * 3, sizeof(double));
+  double* efg_t = do_efg ? calloc((size_t)nth * natm * 9, sizeof(double)) : NULL;
+  double* f_t = calloc((size_t)nth * natm * 3, sizeof(double));
+  double* str_k = calloc(c->nk, sizeof(double));
+#pragma omp parallel num_threads(nth)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double* ef = ef_t + (size_t)tid * natm * 3;
+    double* efg = efg_t ? efg_t + (size_t)tid * natm * 9 : NULL;
+    double* fo = f_t + (size_t)tid * natm * 3;
+    double* ckr = malloc(sizeof(double) * natm);
+    double* skr = malloc(sizeof(double) * natm);
+#pragma omp for schedule(dynamic, 4)
+    for (int ik = 0; ik < c->nk; ++ik) {
+      if (c->kk[ik] == 0.0) continue;
+      double kx = c->kx[ik], ky = c->ky[ik], kz = c->kz[ik], Ak = c->Ak[ik];
+      double rhonk_R = 0.0, rhonk_I = 0.0;
+      for (int ia = 0; ia < natm; ++ia) {
+        double qi = q[ia];
+        double k_dot_r = (kx * rx[ia] + ky * ry[ia] + kz * rz[ia]);
+        ckr[ia] = cos(k_dot_r);
+        skr[ia] = sin(k_dot_r);
+        rhonk_R = rhonk_R + qi * ckr[ia];
+        rhonk_I = rhonk_I + qi * skr[ia];
+        if (!ldip) continue;
+        double k_dot_mu = (mu[3 * ia] * kx + mu[3 * ia + 1] * ky + mu[3 * ia + 2] * kz);
+        rhonk_R = rhonk_R - k_dot_mu * skr[ia];
+        rhonk_I = rhonk_I + k_dot_mu * ckr[ia];
+      }
+      double str = (rhonk_R * rhonk_R + rhonk_I * rhonk_I) * Ak;
+      str_k[ik] = str;
+      for (int ia = 0; ia < natm; ++ia) {
+        double ckria = ckr[ia], skria = skr[ia];
+        double recarg2 = Ak * (rhonk_R * ckria + rhonk_I * skria);
+        double recarg = Ak * (rhonk_I * ckria - rhonk_R * skria);
+        double fxij = kx * recarg, fyij = ky * recarg, fzij = kz * recarg;
+        if (do_efield) {
+          ef[3 * ia] -= fxij;
+          ef[3 * ia + 1] -= fyij;
+          ef[3 * ia + 2] -= fzij;
+        }
+        if (do_efg) {
+          /* only the upper triangle is accumulated (ewald_rec.f90:209-217) */
+          efg[9 * ia + 0] += kx * kx * recarg2;
+          efg[9 * ia + 4] += ky * ky * recarg2;
+          efg[9 * ia + 8] += kz * kz * recarg2;
+          efg[9 * ia + 1] += kx * ky * recarg2;
+          efg[9 * ia + 2] += kx * kz * recarg2;
+          efg[9 * ia + 5] += ky * kz * recarg2;
+        }
+        if (do_forces) {
+          double qi = q[ia];
+          fo[3 * ia] -= qi * fxij;
+          fo[3 * ia + 1] -= qi * fyij;
+          fo[3 * ia + 2] -= qi * fzij;
+          if (!ldip) continue;
+          double k_dot_mu =
+              (mu[3 * ia] * kx + mu[3 * ia + 1] * ky + mu[3 * ia + 2] * kz) * recarg2;
+          fo[3 * ia] += kx * k_dot_mu;
+          fo[3 * ia + 1] += ky * k_dot_mu;
+          fo[3 * ia + 2] += kz * k_dot_mu;
+        }
+      }
+    }
+    free(ckr);
+    free(skr);
+  }
+  /* energy and stress in k order (ewald_rec.f90:173, 252-263) */
+  for (int ik = 0; ik < c->nk; ++ik) {
+    if (c->kk[ik] == 0.0) continue;
+    double str = str_k[ik];
+    u_rec = u_rec + str;
+    if (do_stress) {
+      double kv[3] = {c->kx[ik], c->ky[ik], c->kz[ik]}, kcoe = c->kcoe[ik];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          if (a == b)
+            tr[a][a] = tr[a][a] + (1.0 - kcoe * kv[a] * kv[a]) * str;
+          else
+            tr[a][b] = tr[a][b] - kcoe * kv[a] * kv[b] * str;
+        }
+    }
+  }
+  for (int t = 0; t < nth; ++t) {
+    for (size_t i = 0; i < (size_t)natm * 3; ++i) {
+      out->ef[i] += ef_t[(size_t)t * natm * 3 + i] * 2.0 * fpi_V;
+      out->f[i] += f_t[(size_t)t * natm * 3 + i] * 2.0 * fpi_V;
+    }
+    if (do_efg)
+      for (size_t i = 0; i < (size_t)natm * 9; ++i)
+        out->efg[i] += efg_t[(size_t)t * natm * 9 + i] * 2.0 * fpi_V;
+  }
+  out->u = u_rec * 2.0 * tpi_V;
+  if (do_stress) {
+    double tmp[3][3];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) tmp[a][b] = tr[a][b] * 2.0;
+    double s[3][3];
+    for (int a = 0; a < 3; ++a) s[a][a] = tmp[a][a];
+    s[0][1] = s[1][0] = (tmp[0][1] + tmp[1][0]) * 0.5;
+    s[0][2] = s[2][0] = (tmp[0][2] + tmp[2][0]) * 0.5;
+    s[1][2] = s[2][1] = (tmp[1][2] + tmp[2][1]) * 0.5;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) out->tau[a][b] = s[a][b] * tpi_V / c->omega;
+  } else {
+    memset(out->tau, 0, sizeof(out->tau));
+  }
+  free(ef_t);
+  free(efg_t);
+  free(f_t);
+  free(str_k);
+}
+
+/* multipole_ES (ewald.f90:49-314).  Adds forces into f (already scaled by
+   coul_unit), returns u_coul (with u_pol), field ef (internal units), efg
+   (x coul_unit), tau_coul (x coul_unit / press_unit). */
+typedef struct {
+  double u_coul, u_dir, u_rec, u_self, u_surf;
+  double tau_coul[3][3];
+  double pvirial_coul;
+} es_out;
+
+static void multipole_ES(or_ctx* c, const double* rx, const double* ry, const double* rz,
+                         const double* sx, const double* sy, const double* sz, const csr_t* L,
+                         const double* q, const double* mu, const int* task, int damp_ind,
+                         int do_efield, int do_efg, int do_forces, int do_stress, double u_pol,
+                         double* ef, double* efg, double* f /* [natm][3], += */, es_out* o) {
+  int natm = c->natm;
+  double alphaES = c->p.alphaES;
+  double piroot = sqrt(PI);
+  double qtot[3] = {0, 0, 0}, mutot[3] = {0, 0, 0}, qsq = 0.0, musq = 0.0;
+  for (int ia = 0; ia < natm; ++ia) {
+    mutot[0] += mu[3 * ia];
+    mutot[1] += mu[3 * ia + 1];
+    mutot[2] += mu[3 * ia + 2];
+    musq = musq + (mu[3 * ia] * mu[3 * ia] + mu[3 * ia + 1] * mu[3 * ia + 1] +
+                   mu[3 * ia + 2] * mu[3 * ia + 2]);
+    qtot[0] += q[ia] * rx[ia];
+    qtot[1] += q[ia] * ry[ia];
+    qtot[2] += q[ia] * rz[ia];
+    qsq = qsq + q[ia] * q[ia];
+  }
+  double qmu_sum[3] = {qtot[0] + mutot[0], qtot[1] + mutot[1], qtot[2] + mutot[2]};
+  double tpi_V = TPI / c->omega;
+  double tpi_3V = tpi_V / 3.0;
+  double fpi_3V = tpi_3V * 2.0;
+  double alpha2 = alphaES * alphaES;
+  double selfa = alphaES / piroot;
+  double selfa2 = 2.0 * selfa * alpha2 / 3.0;
+
+  es_acc dir = {0}, rec = {0};
+  dir.ef = calloc((size_t)natm * 3, sizeof(double));
+  dir.f = calloc((size_t)natm * 3, sizeof(double));
+  dir.efg = calloc((size_t)natm * 9, sizeof(double));
+  rec.ef = calloc((size_t)natm * 3, sizeof(double));
+  rec.f = calloc((size_t)natm * 3, sizeof(double));
+  rec.efg = calloc((size_t)natm * 9, sizeof(double));
+  es_dir(c, sx, sy, sz, L, q, mu, task, damp_ind, do_efield, do_efg, do_forces, do_stress, &dir);
+  es_rec(c, rx, ry, rz, q, mu, task, do_efield, do_efg, do_forces, do_stress, &rec);
+
+  double u_surf = (qtot[0] * qtot[0] + qtot[1] * qtot[1] + qtot[2] * qtot[2]) +
+                  2.0 * (qtot[0] * mutot[0] + qtot[1] * mutot[1] + qtot[2] * mutot[2]) +
+                  (mutot[0] * mutot[0] + mutot[1] * mutot[1] + mutot[2] * mutot[2]);
+  u_surf = u_surf * tpi_3V;
+  double u_self = -selfa * qsq - selfa2 * musq;
+  int lsurf = c->p.lsurf;
+  double cu = c->coul_unit;
+  o->u_dir = dir.u;
+  o->u_rec = rec.u;
+  o->u_self = u_self;
+  o->u_surf = lsurf ? u_surf : 0.0;
+  o->u_coul = (dir.u + rec.u + (lsurf ? u_surf : 0.0) + u_self + u_pol) * cu;
+  for (int ia = 0; ia < natm; ++ia)
+    for (int a = 0; a < 3; ++a) {
+      double e = dir.ef[3 * ia + a] + rec.ef[3 * ia + a];
+      if (lsurf) e += -qmu_sum[a] * fpi_3V;
+      e += 2.0 * selfa2 * mu[3 * ia + a];
+      if (ef) ef[3 * ia + a] = e;
+      f[3 * ia + a] += (rec.f[3 * ia + a] + dir.f[3 * ia + a]) * cu;
+    }
+  if (efg)
+    for (int ia = 0; ia < natm; ++ia)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          double s = (a == b) ? -2.0 * selfa2 * q[ia] : 0.0;
+          efg[9 * ia + 3 * a + b] = (dir.efg[9 * ia + 3 * a + b] + rec.efg[9 * ia + 3 * a + b] + s) * cu;
+        }
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      o->tau_coul[a][b] = (dir.tau[a][b] + rec.tau[a][b]) * cu / c->press_unit;
+  o->pvirial_coul =
+      1.0 / 3.0 * (o->tau_coul[0][0] + o->tau_coul[1][1] + o->tau_coul[2][2]) * c->press_unit;
+  free(dir.ef);
+  free(dir.f);
+  free(dir.efg);
+  free(rec.ef);
+  free(rec.f);
+  free(rec.efg);
+}
+
+/* induced_moment (moment_from_pola.f90:955-993) */
+static void induced_moment(or_ctx* c, const double* E, double* mu_ind) {
+  for (int ia = 0; ia < c->natm; ++ia) {
+    for (int a = 0; a < 3; ++a) mu_ind[3 * ia + a] = 0.0;
+    if (!c->ipolar[ia]) continue;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        mu_ind[3 * ia + a] = mu_ind[3 * ia + a] + c->poldipia[9 * ia + 3 * a + b] * E[3 * ia + b];
+  }
+}
+
+/* get_rmsd_mu (moment_from_pola.f90:998-1027) */
+static double get_rmsd_mu(or_ctx* c, const double* g0, const double* mu) {
+  double rmsd = 0.0;
+  int npol = 0;
+  for (int ia = 0; ia < c->natm; ++ia) {
+    if (!c->ipolar[ia]) continue;
+    npol++;
+    for (int a = 0; a < 3; ++a) {
+      double al = c->poldipia[9 * ia + 4 * a];
+      if (al == 0.0) continue;
+      double d = mu[3 * ia + a] / al - g0[3 * ia + a];
+      rmsd = rmsd + d * d;
+    }
+  }
+  return sqrt(rmsd / (double)npol);
+}
+
+/* extrapolate_dipole_aspc (moment_from_pola.f90:493-598) */
+static void aspc(or_ctx* c, double* mu_ind, const double* Efield, int key, int itime) {
+  int natm = c->natm, eo = c->p.extrapolate_order, ext_ord;
+  if (itime >= eo + 1)
+    ext_ord = eo;
+  else if (itime == 1 || itime == 0)
+    ext_ord = 0;
+  else
+    ext_ord = itime - 1;
+  double B[6] = {0}, W = 0.0;
+  switch (ext_ord) {
+    case 0: B[0] = 1.0; W = 0.0; break;
+    case 1: B[0] = 2.0; B[1] = -1.0; W = 2.0 / 3.0; break;
+    case 2: B[0] = 2.5; B[1] = -2.0; B[2] = 0.5; W = 0.6; break;
+    case 3: B[0] = 2.8; B[1] = -2.8; B[2] = 1.2; B[3] = -0.2; W = 4.0 / 7.0; break;
+    case 4:
+      B[0] = 3.0; B[1] = -24.0 / 7.0; B[2] = 27.0 / 14.0; B[3] = -4.0 / 7.0; B[4] = 1.0 / 14.0;
+      W = 5.0 / 9.0;
+      break;
+    default: break;
+  }
+  size_t n3 = (size_t)natm * 3;
+  if (key == 1) {
+    for (size_t i = 0; i < n3; ++i) {
+      double s = 0.0;
+      for (int k = 0; k < ext_ord + 1; ++k) s = s + B[k] * c->hist[k * n3 + i];
+      mu_ind[i] = s;
+    }
+    for (int k = ext_ord; k >= 1; --k) memcpy(c->hist + k * n3, c->hist + (k - 1) * n3, sizeof(double) * n3);
+  } else {
+    double* save = malloc(sizeof(double) * n3);
+    memcpy(save, mu_ind, sizeof(double) * n3);
+    induced_moment(c, Efield, mu_ind);
+    for (size_t i = 0; i < n3; ++i) mu_ind[i] = W * mu_ind[i] + (1.0 - W) * save[i];
+    free(save);
+  }
+}
+
+int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz, int itime,
+                mdff_result* out, or_extra* ex) {
+  int natm = c->natm;
+  if (c->p.extrapolate_order < 0 || c->p.extrapolate_order > 4) return MDFF_ERR_BAD_ARGS;
+  double* sx = malloc(sizeof(double) * natm);
+  double* sy = malloc(sizeof(double) * natm);
+  double* sz = malloc(sizeof(double) * natm);
+  or_kardir(c, rx, ry, rz, sx, sy, sz);
+  double* f = calloc((size_t)natm * 3, sizeof(double));
+  double* fx = calloc(natm, sizeof(double));
+  double* fy = calloc(natm, sizeof(double));
+  double* fz = calloc(natm, sizeof(double));
+  int status = MDFF_OK;
+  memset(out->tau, 0, sizeof(out->tau));
+  memset(out->tau_nonb, 0, sizeof(out->tau_nonb));
+  memset(out->tau_coul, 0, sizeof(out->tau_coul));
+  out->u_lj = out->vir_lj = out->u_bmhft = out->vir_bmhft = 0.0;
+  out->u_coul = out->u_pol = out->pvirial_coul = 0.0;
+  if (ex) {
+    ex->n_scf = 0;
+    ex->rmsd = 0.0;
+  }
+  /* short range (engforce_driver.f90:116-135) on the vdw half list */
+  if (c->p.lnmlj || c->p.lbmhft || c->p.lbmhftd) {
+    csr_t Lv;
+    build_half(c, sx, sy, sz, c->p.cutshortrange, &Lv);
+    if (c->p.lnmlj) {
+      or_nmlj(c, sx, sy, sz, &Lv, fx, fy, fz, &out->u_lj, &out->vir_lj, out->tau_nonb);
+      for (int a = 0; a < 9; ++a) (&out->tau[0][0])[a] += (&out->tau_nonb[0][0])[a];
+    }
+    if (c->p.lbmhft || c->p.lbmhftd) {
+      or_bmhftd(c, sx, sy, sz, &Lv, fx, fy, fz, &out->u_bmhft, &out->vir_bmhft, out->tau_nonb);
+      for (int a = 0; a < 9; ++a) (&out->tau[0][0])[a] += (&out->tau_nonb[0][0])[a];
+    }
+    free_csr(&Lv);
+  }
+  for (int ia = 0; ia < natm; ++ia) {
+    f[3 * ia] = fx[ia];
+    f[3 * ia + 1] = fy[ia];
+    f[3 * ia + 2] = fz[ia];
+  }
+  if (c->p.lcoulomb) {
+    csr_t Lc;
+    build_half(c, sx, sy, sz, c->p.cutlongrange, &Lc);
+    size_t n3 = (size_t)natm * 3;
+    double* mu = calloc(n3, sizeof(double));
+    double* ef = calloc(n3, sizeof(double));
+    double* dipia_ind = calloc(n3, sizeof(double));
+    double u_pol = 0.0;
+    double* zero_f = calloc(n3, sizeof(double));
+    /* get_dipole_moments (moment_from_pola.f90:84-224) -> moment_from_pola_scf
+       (:240-485) */
+    if (c->lpolar_any) {
+      double* Estat = calloc(n3, sizeof(double));
+      double* Eind = calloc(n3, sizeof(double));
+      double* Efield = calloc(n3, sizeof(double));
+      double* qzero = calloc(natm, sizeof(double));
+      int ldip = 0;
+      for (int it = 0; it < MDFF_NTYPEMAX; ++it)
+        for (int a = 0; a < 3; ++a)
+          if (c->p.dip[it][a] != 0.0) ldip = 1;
+      int task_static[6] = {1, 0, 0, 0, 0, 0};
+      if (ldip)
+        for (int i = 0; i < 6; ++i) task_static[i] = 1;
+      es_out o;
+      multipole_ES(c, rx, ry, rz, sx, sy, sz, &Lc, c->qia, c->dipia, task_static, 1, 1, 0, 0, 0,
+                   0.0, Estat, NULL, zero_f, &o);
+      memcpy(Efield, Estat, sizeof(double) * n3);
+      int iscf = 0;
+      double rmsd = HUGE_VAL;
+      int task_ind[6] = {0, 0, 1, 0, 0, 0};
+      int ismd = (c->p.calc == MDFF_CALC_MD), isopt = (c->p.calc == MDFF_CALC_OPT);
+      while (((iscf < c->p.max_scf_pol_iter) && (rmsd > c->p.conv_tol_ind)) ||
+             (iscf < c->p.min_scf_pol_iter)) {
+        iscf++;
+        if (iscf != 1 || (!ismd && !isopt))
+          induced_moment(c, Efield, dipia_ind);
+        else
+          aspc(c, dipia_ind, Efield, 1, itime);
+        u_pol = 0.0;
+        for (int ia = 0; ia < natm; ++ia)
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b)
+              u_pol = u_pol + dipia_ind[3 * ia + a] * c->invpoldipia[9 * ia + 3 * a + b] *
+                                  dipia_ind[3 * ia + b];
+        u_pol = u_pol * 0.5;
+        memset(zero_f, 0, sizeof(double) * n3);
+        multipole_ES(c, rx, ry, rz, sx, sy, sz, &Lc, qzero, dipia_ind, task_ind, 0, 1, 0, 0, 0,
+                     u_pol, Eind, NULL, zero_f, &o);
+        for (size_t i = 0; i < n3; ++i) Efield[i] = Estat[i] + Eind[i];
+        if (iscf == 1 && ismd) aspc(c, dipia_ind, Efield, 2, itime);
+        rmsd = get_rmsd_mu(c, Efield, dipia_ind);
+      }
+      memcpy(c->hist, dipia_ind, sizeof(double) * n3);
+      if (ex) {
+        ex->n_scf = iscf;
+        ex->rmsd = rmsd;
+      }
+      free(Estat);
+      free(Eind);
+      free(Efield);
+      free(qzero);
+    }
+    for (size_t i = 0; i < n3; ++i) mu[i] = c->dipia[i] + dipia_ind[i];
+    /* polarisation catastrophe (moment_from_pola.f90:176-216) */
+    for (int ia = 0; ia < natm && status == MDFF_OK; ++ia)
+      for (int a = 0; a < 3; ++a)
+        if (mu[3 * ia + a] > 10.0) status = MDFF_ERR_CATASTROPHE;
+    if (status == MDFF_OK) {
+      es_out o;
+      int do_efg = ex ? ex->do_efg : 0;
+      multipole_ES(c, rx, ry, rz, sx, sy, sz, &Lc, c->qia, mu, c->task, 1, 1, do_efg, 1, 1, u_pol,
+                   ef, (ex && ex->efg) ? ex->efg : NULL, f, &o);
+      out->u_coul = o.u_coul;
+      out->u_pol = u_pol;
+      out->pvirial_coul = o.pvirial_coul;
+      memcpy(out->tau_coul, o.tau_coul, sizeof(o.tau_coul));
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) out->tau[a][b] += 2.0 * o.tau_coul[a][b];
+      if (ex) {
+        ex->u_dir = o.u_dir;
+        ex->u_rec = o.u_rec;
+        ex->u_self = o.u_self;
+        ex->u_surf = o.u_surf;
+      }
+      if (out->mu) memcpy(out->mu, mu, sizeof(double) * n3);
+      if (out->ef) memcpy(out->ef, ef, sizeof(double) * n3);
+    }
+    free(mu);
+    free(ef);
+    free(dipia_ind);
+    free(zero_f);
+    free_csr(&Lc);
+  }
+  for (int ia = 0; ia < natm; ++ia) {
+    out->fx[ia] = f[3 * ia];
+    out->fy[ia] = f[3 * ia + 1];
+    out->fz[ia] = f[3 * ia + 2];
+  }
+  free(sx);
+  free(sy);
+  free(sz);
+  free(f);
+  free(fx);
+  free(fy);
+  free(fz);
+  return status;
+}

@@ -1,0 +1,46 @@
+"""The C-ABI library loads and exports every symbol include/mdff_gpu.h
+declares, with the struct layouts the Python mirror assumes (no GPU needed:
+no compute entry point is called)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from mdff_b200 import _abi
+
+HDR = os.path.join(os.path.dirname(__file__), "..", "include", "mdff_gpu.h")
+
+
+def _declared():
+    txt = open(HDR).read()
+    return sorted(set(re.findall(r"\b(mdff_gpu_\w+)\s*\(", txt)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from mdff_b200 import build
+    build.build()
+    return _abi.load_library()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = _declared()
+    assert len(names) >= 14
+    for n in names:
+        assert hasattr(lib, n), n
+        assert n in _abi.SIGNATURES, n
+
+
+def test_struct_layouts_match(lib):
+    assert lib.mdff_gpu_abi_version() == _abi.ABI_VERSION
+    assert lib.mdff_gpu_struct_size(0) == ctypes.sizeof(_abi.MdffParams)
+    assert lib.mdff_gpu_struct_size(1) == ctypes.sizeof(_abi.MdffResult)
+    assert lib.mdff_gpu_struct_size(2) == ctypes.sizeof(_abi.MdffStats)
+
+
+def test_strerror_and_bad_args(lib):
+    assert lib.mdff_gpu_strerror(_abi.MDFF_ERR_CATASTROPHE).decode().startswith("polarization")
+    h = ctypes.c_void_p()
+    # a NULL parameter block is rejected before any device work
+    assert lib.mdff_gpu_create(None, None, ctypes.byref(h)) == _abi.MDFF_ERR_BAD_ARGS

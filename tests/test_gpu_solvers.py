@@ -1,0 +1,68 @@
+"""GPU: the CG dipole solve (FP64 and mixed) and the mixed-precision engine
+against the FP64 oracle run to a tight SCF tolerance."""
+import numpy as np
+import pytest
+
+from mdff_b200 import _abi, systems
+from mdff_b200.engine import ForceEngine
+from mdff_b200.params import params_copy
+
+from .gpu_util import compare, forces, rel, rms_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _pim_cases():
+    return [
+        systems.random_ionic((24, 24), L=13.0, seed=51, calc=_abi.CALC_OTHER, conv_tol_ind=1e-13,
+                             max_scf_pol_iter=500,
+                             ldip_damping={(1, 1, 0): 1}, pol_damp_b={(1, 1, 0): 3.0},
+                             pol_damp_c={(1, 1, 0): 1.0}, pol_damp_k={(1, 1, 0): 4}),
+        systems.mgo(ncell=2, calc=_abi.CALC_OTHER, conv_tol_ind=1e-13, max_scf_pol_iter=500),
+        systems.sio2(nsio2=150, seed=9, calc=_abi.CALC_OTHER, conv_tol_ind=1e-13,
+                     max_scf_pol_iter=500),
+    ]
+
+
+@pytest.mark.parametrize("case", range(3))
+def test_cg_fp64_matches_converged_scf(oracle, case):
+    s = _pim_cases()[case]
+    o = oracle.Oracle(s.params, s.cell).engforce(*s.soa())
+    p = params_copy(s.params)
+    p.solver = _abi.SOLVER_CG
+    p.cg_tol = 1e-12
+    with ForceEngine(p, s.cell) as eng:
+        g = eng.engforce(*s.soa())
+        st = eng.stats()
+    assert st["converged"] and st["n_pol_iter"] < o["n_scf"]
+    compare(g, o, 1e-9)
+
+
+@pytest.mark.parametrize("case", range(3))
+def test_mixed_precision_force_error(oracle, case):
+    """north_star bar: force error <= 1e-5 relative RMS vs the FP64 oracle."""
+    s = _pim_cases()[case]
+    o = oracle.Oracle(s.params, s.cell).engforce(*s.soa())
+    p = params_copy(s.params)
+    p.solver = _abi.SOLVER_CG
+    p.cg_tol = 1e-10
+    p.precision = _abi.PREC_MIXED
+    with ForceEngine(p, s.cell) as eng:
+        g = eng.engforce(*s.soa())
+    e_f = rms_rel(forces(g), forces(o))
+    e_mu = rms_rel(g["mu"], o["mu"])
+    e_u = abs(g["u_coul"] - o["u_coul"]) / abs(o["u_coul"])
+    assert e_f <= 1e-5, e_f
+    assert e_mu <= 1e-5, e_mu
+    assert e_u <= 1e-6, e_u
+
+
+def test_mixed_precision_nacl(oracle):
+    s = systems.nacl(ncell=2, kmax=6)
+    o = oracle.Oracle(s.params, s.cell).engforce(*s.soa())
+    p = params_copy(s.params)
+    p.precision = _abi.PREC_MIXED
+    with ForceEngine(p, s.cell) as eng:
+        g = eng.engforce(*s.soa())
+    assert rms_rel(forces(g), forces(o)) <= 1e-5
+    assert abs(g["u_coul"] - o["u_coul"]) / abs(o["u_coul"]) <= 1e-6

@@ -1,0 +1,504 @@
+"""Benchmark: PIM + Ewald MD steps/s on one B200 (and N replicas).
+
+Workload (default): the 12,000-ion SiO2-like glass (4000 Si +2.4, 8000 O -1.2;
+BKS Buckingham + r^-24 wall, O polarisability 1.3 A^3 with Tang-Toennies
+damping, Ewald alpha 0.3, rc 10 A, kmax 12), seeded synthetic positions and
+Maxwell velocities at 300 K.  One step = one velocity-Verlet MD step (the
+engforce call of the engine plus the two kicks), positions / velocities /
+forces resident in HBM.  The engine runs mixed precision (FP32 pair,
+T-tensor and phase arithmetic, FP64 sums) with the CG dipole solve to the
+config's 1e-8 rms tolerance.
+
+Reported beside the headline: the plain FP64 engine (the reference's SCF
+algorithm) and FP64 + CG, the RMS force error of the mixed engine vs the FP64
+engine on the same configuration, e2e through the C ABI with host buffers,
+roofline of the dominant kernel class, the CPU oracle baseline, clocks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DT_FS = 1.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sio2", choices=["sio2", "mgo", "nacl"])
+    ap.add_argument("--fp64-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--relax", type=int, default=300, help="FIRE iterations before MD")
+    ap.add_argument("--equil", type=int, default=50, help="rescaled MD steps before warm-up")
+    return ap.parse_args()
+
+
+def make_system(name):
+    from mdff_b200 import _abi, systems
+    if name == "sio2":
+        s = systems.sio2()
+        wl = dict(workload="sio2_pim_ewald_12000", natm=s.natm, box_A=round(s.info["L"], 4),
+                  rcut_A=10.0, alpha=0.3, kmax=12, pim="O 1.3 A^3 + TT damping",
+                  short_range="BKS Buckingham + r^-24 wall", dt_fs=DT_FS, ensemble="NVE")
+    elif name == "mgo":
+        s = systems.mgo()
+        wl = dict(workload="mgo_pim_ewald_8000", natm=s.natm, box_A=round(s.info["L"], 4),
+                  rcut_A=10.0, alpha=0.35, kmax=s.info["kmax"], dt_fs=DT_FS, ensemble="NVE")
+    else:
+        s = systems.nacl()
+        wl = dict(workload="nacl_bmh_ewald_1728", natm=s.natm, box_A=round(s.info["L"], 4),
+                  rcut_A=12.0, alpha=0.3, kmax=10, dt_fs=DT_FS, ensemble="NVE")
+    s.params.calc = _abi.CALC_MD
+    return s, wl
+
+
+def load_state(name, s):
+    """Prepared starting state (tests/golden/make_bench_states.py), or None."""
+    path = os.path.join(ROOT, "tests", "golden", f"{name}_state.npz")
+    if not os.path.exists(path):
+        return None
+    z = np.load(path)
+    if int(z["natm"]) != s.natm or not np.allclose(z["cell"], s.cell):
+        return None
+    return z["pos"], z["vel"], str(z["protocol"])
+
+
+def engine_params(s, precision, solver):
+    from mdff_b200 import _abi
+    from mdff_b200.params import params_copy
+    p = params_copy(s.params)
+    p.precision = _abi.PREC_MIXED if precision == "mixed" else _abi.PREC_FP64
+    p.solver = _abi.SOLVER_CG if solver == "cg" else _abi.SOLVER_SCF
+    p.cg_tol = p.conv_tol_ind
+    return p
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for nm, v in zip(names, r[5:9]):
+                    if "Active" in v and "Not" not in v:
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def fire_relax(eng, pos, mass, iters, fmax_stop=0.5):
+    """FIRE minimisation (Bitzek et al., PRL 97, 170201 (2006)) of the seeded
+    random-insertion structure on the device, displacements capped at
+    0.05 A per iteration: the insertion leaves ion pairs far from their
+    minima and NVE from there heats the glass by thousands of K."""
+    import torch
+    f = torch.zeros_like(pos)
+    v = torch.zeros_like(pos)
+    m = torch.as_tensor(mass, dtype=torch.float64, device=pos.device)[None, :]
+    dt, dtmax, a, npos = 0.02, 0.1, 0.1, 0
+    eng.engforce_device(pos.data_ptr(), f.data_ptr())
+    for it in range(iters):
+        P = float((f * v).sum())
+        if P > 0:
+            npos += 1
+            fn = float(f.norm())
+            vn = float(v.norm())
+            v = (1 - a) * v + a * vn * f / max(fn, 1e-30)
+            if npos > 5:
+                dt = min(dt * 1.1, dtmax)
+                a *= 0.99
+        else:
+            npos = 0
+            dt *= 0.5
+            v.zero_()
+            a = 0.1
+        v += dt * f / m
+        dx = dt * v
+        mx = float(dx.abs().max())
+        if mx > 0.05:
+            dx *= 0.05 / mx
+        pos += dx
+        eng.engforce_device(pos.data_ptr(), f.data_ptr())
+        if float(f.abs().max()) < fmax_stop:
+            break
+    return it + 1
+
+
+def equilibrate(eng, pos, vel, invm, mass, dt, steps, temp, itime):
+    """Velocity-Verlet with velocity rescaling to temp each step (the
+    reference's equilibration rescale, runmd.f90:321-331)."""
+    import torch
+    from mdff_b200 import systems
+    n = mass.size
+    m = torch.as_tensor(mass, dtype=torch.float64, device=pos.device)[None, :]
+    for _ in range(steps):
+        eng.md_nve(pos.data_ptr(), vel.data_ptr(), invm.data_ptr(), dt, 1, itime, energies=False)
+        itime += 1
+        ek = 0.5 * float((m * vel * vel).sum())
+        T = 2 * ek / (3 * n * systems.BOLTZ_UNIT)
+        vel *= (temp / T) ** 0.5
+    return itime
+
+
+def flush_l2(buf):
+    buf.add_(1.0)  # 256 MiB read + write, larger than the 126 MB L2
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from mdff_b200 import _abi, systems
+    from mdff_b200.engine import ForceEngine
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    s, wl = make_system(args.workload)
+    n = s.natm
+    dt = DT_FS * 1e-3 * systems.TIME_UNIT
+    p = engine_params(s, "mixed", "cg")
+    p.device = local_rank
+    eng = ForceEngine(p, s.cell)
+    pos = torch.tensor(np.ascontiguousarray(s.pos.T), dtype=torch.float64, device=dev).contiguous()
+    vel = torch.tensor(np.ascontiguousarray(s.vel.T), dtype=torch.float64, device=dev).contiguous()
+    invm = torch.tensor(1.0 / s.mass, dtype=torch.float64, device=dev)
+    l2buf = torch.zeros(256 * 2 ** 20 // 4, dtype=torch.float32, device=dev)
+    itime = 0
+    st0 = load_state(args.workload, s)
+    if st0 is not None:
+        pos.copy_(torch.tensor(np.ascontiguousarray(st0[0].T), device=dev))
+        vel.copy_(torch.tensor(np.ascontiguousarray(st0[1].T), device=dev))
+        wl["start"] = "tests/golden/%s_state.npz: %s" % (args.workload, st0[2])
+    else:
+        t_prep = time.perf_counter()
+        n_relax = fire_relax(eng, pos, s.mass, args.relax) if args.relax > 0 else 0
+        vel.copy_(torch.tensor(np.ascontiguousarray(
+            systems.maxwell(np.random.default_rng(7), s.mass, 300.0).T), dtype=torch.float64,
+            device=dev))
+        itime = equilibrate(eng, pos, vel, invm, s.mass, dt, args.equil, 300.0, itime)
+        wl["start"] = (f"prepared in place: FIRE {n_relax} iterations, Maxwell 300 K, {args.equil} "
+                       f"rescaled VV steps ({time.perf_counter() - t_prep:.1f} s)")
+    for _ in range(args.warmup):
+        eng.md_nve(pos.data_ptr(), vel.data_ptr(), invm.data_ptr(), dt, 1, itime, energies=False)
+        itime += 1
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    clk = Clocks(local_rank) if rank == 0 else None
+    eng_prof = eng._lib.mdff_gpu_profile(eng._h, 1)
+    assert eng_prof == 0
+    step_ms, launches, iters = [], 0, []
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    for _ in range(args.steps):
+        flush_l2(l2buf)
+        torch.cuda.synchronize()
+        eng.md_nve(pos.data_ptr(), vel.data_ptr(), invm.data_ptr(), dt, 1, itime, energies=False)
+        itime += 1
+        st = eng.stats()
+        step_ms.append(st["ms_last"])
+        launches += st["n_launches"]
+        iters.append(st["n_pol_iter"])
+    torch.cuda.synchronize()
+    dist_barrier(world)
+    clocks = clk.stop() if clk else None
+    kms = np.zeros(_abi.NKCLASS)
+    kl = np.zeros(_abi.NKCLASS, dtype=np.int64)
+    kw = np.zeros(_abi.NKCLASS)
+    eng._lib.mdff_gpu_kernel_times(eng._h, _abi.dptr(kms), kl.ctypes.data_as(
+        __import__("ctypes").POINTER(__import__("ctypes").c_longlong)), _abi.dptr(kw))
+    eng._lib.mdff_gpu_profile(eng._h, 0)
+    total_s = sum(step_ms) / 1e3
+    total_s = dist_max(world, total_s)
+    value = world * args.steps / total_s
+    res = dict(value=value, ms_per_step=1e3 * total_s / args.steps, launches=launches,
+               cg_iters_mean=float(np.mean(iters)), clocks=clocks, wl=wl,
+               kms=kms, kl=kl, kw=kw)
+    if rank != 0:
+        return res, None
+    # ---- extras on rank 0 ---------------------------------------------------
+    extra = {}
+    pos_h = pos.cpu().numpy()
+    soa = tuple(np.ascontiguousarray(pos_h[a]) for a in range(3))
+    hist = eng.aspc_history()
+    # FP64 engines on the same trajectory point (same ASPC history)
+    for tag, prec, solver in (("fp64_scf", "fp64", "scf"), ("fp64_cg", "fp64", "cg")):
+        pe = engine_params(s, prec, solver)
+        pe.device = local_rank
+        e2 = ForceEngine(pe, s.cell)
+        pos2 = pos.clone()
+        vel2 = vel.clone()
+        e2.set_aspc_history(hist)
+        ms, it2 = [], []
+        it = itime
+        for k in range(max(args.fp64_steps, 1) + 2):
+            flush_l2(l2buf)
+            torch.cuda.synchronize()
+            e2.md_nve(pos2.data_ptr(), vel2.data_ptr(), invm.data_ptr(), dt, 1, it, energies=False)
+            it += 1
+            if k >= 2:
+                st2 = e2.stats()
+                ms.append(st2["ms_last"])
+                it2.append(st2["n_pol_iter"])
+        extra[tag + "_steps_per_s"] = 1e3 / float(np.mean(ms))
+        extra[tag + "_iters_mean"] = float(np.mean(it2))
+        e2.close()
+    # force error of the mixed engine vs the FP64 engine (tight SCF) on one config
+    pt = engine_params(s, "fp64", "scf")
+    pt.conv_tol_ind = 1e-11
+    pt.max_scf_pol_iter = 400
+    pt.calc = _abi.CALC_OTHER
+    e3 = ForceEngine(pt, s.cell)
+    ref = e3.engforce(*soa)
+    e3.close()
+    pm = engine_params(s, "mixed", "cg")
+    pm.calc = _abi.CALC_OTHER
+    e4 = ForceEngine(pm, s.cell)
+    mix = e4.engforce(*soa)
+    e4.close()
+    fr = np.stack([ref["fx"], ref["fy"], ref["fz"]], 1)
+    fm = np.stack([mix["fx"], mix["fy"], mix["fz"]], 1)
+    extra["force_err_rms_rel_vs_fp64"] = float(np.sqrt(((fm - fr) ** 2).sum() / (fr ** 2).sum()))
+    extra["dipole_err_rms_rel_vs_fp64"] = float(np.sqrt(((mix["mu"] - ref["mu"]) ** 2).sum()
+                                                        / (ref["mu"] ** 2).sum()))
+    extra["energy_err_rel_vs_fp64"] = abs(mix["u_coul"] + mix["u_bmhft"] - ref["u_coul"]
+                                          - ref["u_bmhft"]) / abs(ref["u_coul"] + ref["u_bmhft"])
+    # e2e through the C ABI with pinned host buffers (what a Fortran caller does)
+    ne = args.e2e_steps or args.steps
+    rx = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    ry = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    rz = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    v_h = vel.cpu().numpy().copy()
+    rx[:], ry[:], rz[:] = soa
+    invm_h = 1.0 / s.mass
+    r0 = eng.engforce(rx, ry, rz, itime=itime, want_ef=False)
+    f = np.stack([r0["fx"], r0["fy"], r0["fz"]])
+    e_ms = []
+    for k in range(ne):
+        v_h += 0.5 * dt * f * invm_h
+        rx += dt * v_h[0]
+        ry += dt * v_h[1]
+        rz += dt * v_h[2]
+        flush_l2(l2buf)
+        torch.cuda.synchronize()
+        itime += 1
+        r = eng.engforce(rx, ry, rz, itime=itime, want_ef=False)
+        e_ms.append(eng.stats()["ms_last"])
+        f = np.stack([r["fx"], r["fy"], r["fz"]])
+        v_h += 0.5 * dt * f * invm_h
+    extra["e2e"] = {"value": 1e3 / float(np.mean(e_ms)), "unit": "steps/s",
+                    "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 3 * n * 8 * 2 + 8 * 7 + 8 * 27}
+    # roofline of the dominant kernel class
+    peak32 = __import__("ctypes").c_double(0)
+    peak64 = __import__("ctypes").c_double(0)
+    eng._lib.mdff_gpu_peak_flops(local_rank, 0, __import__("ctypes").byref(peak32))
+    eng._lib.mdff_gpu_peak_flops(local_rank, 1, __import__("ctypes").byref(peak64))
+    extra["peak_fp32_tflops"] = peak32.value
+    extra["peak_fp64_tflops"] = peak64.value
+    extra["stats"] = eng.stats()
+    extra["_cpu_point"] = (soa, hist, itime)
+    eng.close()
+    return res, extra
+
+
+def dist_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def dist_max(world, x):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline_sample(s, hist, itime, pos_soa):
+    """Oracle (C restatement of the reference engforce, OpenMP over all host
+    threads): one warm-start engforce (SCF, ASPC history from the GPU run) of
+    the same workload = one MD step of the reference algorithm."""
+    from oracle import oracle as O
+    from mdff_b200.params import params_copy
+    o = O.Oracle(params_copy(s.params), s.cell)
+    o.set_aspc(hist)
+    t = time.perf_counter()
+    r = o.engforce(*pos_soa, itime=itime)
+    dt_s = time.perf_counter() - t
+    return dt_s, r["n_scf"], O.lib().or_get_threads()
+
+
+KCLS = ("list_build", "short_range", "real_space_field", "real_space_force",
+        "structure_factor", "reciprocal_field", "other")
+
+
+def roofline_block(res, extra):
+    kms, kl, kw = res["kms"], res["kl"], res["kw"]
+    c = int(np.argmax(kms))
+    if kw[c] == 0:
+        # dominant class without an algorithmic op count: report the reciprocal one
+        c = 4 if kms[4] >= kms[5] else 5
+    avg_ms = kms[c] / max(kl[c], 1)
+    ops_per_launch = kw[c] / max(kl[c], 1)
+    achieved = ops_per_launch / (avg_ms * 1e-3) / 1e12
+    peak = extra["peak_fp32_tflops"]
+    share = {KCLS[i]: round(float(kms[i] / kms.sum()), 4) for i in range(len(KCLS)) if kms[i] > 0}
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        traffic = json.load(open(tf)).get(KCLS[c])
+    return {"kernel": KCLS[c], "bound": "fp32_fma", "achieved": round(achieved, 3),
+            "peak": round(peak, 3), "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+            "traffic": traffic, "launches": int(kl[c]), "avg_launch_ms": round(avg_ms, 5),
+            "peak_source": "measured live: register-resident FP32 FMA loop on all SMs (mdff_gpu_peak_flops); "
+                           "MEASURED_PEAKS.json has HBM and bf16 tensor peaks only",
+            "time_share": share}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from mdff_b200 import systems
+    from oracle import oracle as O
+    from mdff_b200.params import params_copy
+    s, wl = make_system(args.workload)
+    o = O.Oracle(params_copy(s.params), s.cell)
+    dt = DT_FS * 1e-3 * systems.TIME_UNIT
+    st0 = load_state(args.workload, s)
+    pos = (st0[0] if st0 is not None else s.pos).copy()
+    vel = (st0[1] if st0 is not None else s.vel).copy()
+    wl["start"] = ("tests/golden/%s_state.npz" % args.workload) if st0 is not None else \
+        "random-insertion state (no prepared state file)"
+    invm = (1.0 / s.mass)[:, None]
+    soa = lambda p: tuple(np.ascontiguousarray(p[:, a]) for a in range(3))
+    r = o.engforce(*soa(pos), itime=0)
+    f = np.stack([r["fx"], r["fy"], r["fz"]], 1)
+    times = []
+    itime = 0
+    for k in range(args.warmup + args.steps):
+        vel += 0.5 * dt * f * invm
+        pos += dt * vel
+        itime += 1
+        t = time.perf_counter()
+        r = o.engforce(*soa(pos), itime=itime)
+        el = time.perf_counter() - t
+        f = np.stack([r["fx"], r["fy"], r["fz"]], 1)
+        vel += 0.5 * dt * f * invm
+        if k >= args.warmup:
+            times.append(el)
+    tot = sum(times)
+    val = args.steps / tot
+    cores = O.lib().or_get_threads()
+    line = {"metric": "PIM+Ewald MD steps/s @12k ions", "impl": "reference", "value": val,
+            "unit": "steps/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": dict(wl, solver="scf (reference algorithm)", precision="fp64"),
+            "cpu_baseline": {"value": val, "unit": "steps/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} MD steps (velocity Verlet, warm ASPC) of the "
+                                       f"{wl['natm']}-ion workload, C restatement of engforce, "
+                                       f"OpenMP {cores} threads"},
+            "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from mdff_b200 import build
+    build.build()
+    res, extra = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        wl = res["wl"]
+        line = {
+            "metric": "PIM+Ewald MD steps/s @12k ions (mixed FP32/FP64 engine)",
+            "value": res["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
+            "config": dict(wl, precision="mixed", solver="cg", cg_tol=1e-8,
+                           parallelism=f"replicas x{world}",
+                           l2="flushed between steps (256 MiB write)"),
+            "ns_per_day": res["value"] / world * 86400 * DT_FS * 1e-6,
+            "atom_steps_per_s": res["value"] * wl["natm"],
+            "cg_iters_mean": res["cg_iters_mean"],
+            "gpu_launches": int(res["launches"]),
+            "clocks": res["clocks"],
+        }
+        line.update({k: v for k, v in extra.items() if k not in ("stats", "_cpu_point")})
+        line["speedup_vs_fp64_scf"] = res["value"] / world / extra["fp64_scf_steps_per_s"]
+        line["speedup_vs_fp64_cg"] = res["value"] / world / extra["fp64_cg_steps_per_s"]
+        line["roofline"] = roofline_block(res, extra)
+        if world == 1 and not args.no_cpu:
+            s, _ = make_system(args.workload)
+            soa, hist, itime = extra["_cpu_point"]
+            dt_s, nscf, cores = cpu_baseline_sample(s, hist, itime, soa)
+            line["cpu_baseline"] = {
+                "value": 1.0 / dt_s, "unit": "steps/s", "cores": cores, "kind": "port",
+                "sample": f"one warm-start engforce (= one MD step, SCF to 1e-8, {nscf} iterations) "
+                          f"of the {wl['natm']}-ion workload at the GPU run's last configuration; "
+                          f"C restatement of the reference engforce, OpenMP {cores} threads"}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

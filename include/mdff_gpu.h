@@ -216,9 +216,9 @@ int mdff_gpu_md_nve(mdff_handle h, double* d_pos, double* d_vel,
 /* Per-kernel-class device timing with CUDA events on the handle's stream
    (for roofline figures).  Classes: 0 list build, 1 short range, 2 real-space
    field, 3 real-space force, 4 structure factor, 5 reciprocal field/force,
-   6 everything else.  ms[c], launches[c] and work[c] (algorithmic units: (k, ion)
-   terms for 4/5, list entries for 1/2/3) accumulate while enabled; reset on
-   enable. */
+   6 everything else.  ms[c], launches[c] and work[c] accumulate while enabled
+   (reset on enable); work is the algorithmic op count of the reciprocal
+   classes 4 and 5 ((k, ion) terms x ops per term), 0 for the others. */
 #define MDFF_NKCLASS 7
 int mdff_gpu_profile(mdff_handle h, int enable);
 int mdff_gpu_kernel_times(mdff_handle h, double* ms, long long* launches, double* work);

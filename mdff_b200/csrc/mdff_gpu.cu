@@ -534,7 +534,12 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   int ntiles = cdiv(2 * M.kmax[2] + 1, kNZT);
   dim3 g((unsigned)(M.nrows * ntiles), (unsigned)h->n_rho_chunks);
   int chunk = kRhoChunk;
-  int pr = prof_begin(h, KC_RHO, (double)h->nk * n);
+  // algorithmic op counts per (k, ion) term (add = mul = 1, FMA = 2,
+  // sin/cos/exp/sqrt = 1): structure factor k.r 5 + sin,cos 2 + q part 4 +
+  // k.mu 5 + mu part 4; field/force pass: recarg/recarg2 8 + field 6 + F_q 6 + F_mu 12
+  double ops_rho = (has_q && has_mu) ? 20.0 : (has_mu ? 16.0 : 11.0);
+  double ops_fld = (forces && has_mu) ? 32.0 : (forces ? 17.0 : 20.0);
+  int pr = prof_begin(h, KC_RHO, (double)h->nk * n * ops_rho);
   if (has_q && has_mu)
     k_rec_rho<R, true, true, kNZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
   else if (has_q)
@@ -554,7 +559,7 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   dim3 gf((unsigned)cdiv(n, kFieldThreads), (unsigned)nch);
   size_t smem = (size_t)h->max_chunk_k * sizeof(typename cplx<R>::T);
   bool muf = forces && has_mu;
-  pr = prof_begin(h, KC_RECF, (double)h->nk * n);
+  pr = prof_begin(h, KC_RECF, (double)h->nk * n * ops_fld);
   if (muf)
     k_rec_field<R, true><<<gf, kFieldThreads, smem, h->st>>>(tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_G, h->d_H);
   else

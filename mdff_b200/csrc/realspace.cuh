@@ -68,27 +68,36 @@ __global__ void __launch_bounds__(256) k_shortrange(
       const NBPair& P = stab[ti * ntype + tj];
       if (r2d >= P.rcutsq) continue;  // non_bonded.f90:1154 strict <
       R rx = (R)rxd, ry = (R)ryd, rz = (R)rzd, rijsq = (R)r2d;
-      if (do_bmh && P.A != 0.0) {
+      // the reference skips pairs with A = 0 (non_bonded.f90:1153); the
+      // optional r^-24 wall extension acts on its own
+      if (do_bmh && (P.A != 0.0 || P.wall != 0.0)) {
         R ir2 = R(1) / rijsq;
         R d = rsqrt_<R>(rijsq);
-        R erh = (R)P.A * rexp<R>(-(R)P.B * d);
-        R ir6 = ir2 * ir2 * ir2;
-        R ir8 = ir6 * ir2;
-        R ir8r = ir8;
-        ir6 = ir6 * (R)P.C;
-        ir8 = ir8 * (R)P.D;
-        R f6 = R(1), f8 = R(1), fd6 = R(0), fd8 = R(0);
-        if (lbmhftd) {
-          tt_damp<R>((R)P.BD, R(1), d, 6, f6, fd6);
-          tt_damp<R>((R)P.BD, R(1), d, 8, f8, fd8);
+        R u = R(0), wnum = R(0);
+        if (P.A != 0.0) {
+          R erh = (R)P.A * rexp<R>(-(R)P.B * d);
+          R ir6 = ir2 * ir2 * ir2;
+          R ir8 = ir6 * ir2;
+          ir6 = ir6 * (R)P.C;
+          ir8 = ir8 * (R)P.D;
+          R f6 = R(1), f8 = R(1), fd6 = R(0), fd8 = R(0);
+          if (lbmhftd) {
+            tt_damp<R>((R)P.BD, R(1), d, 6, f6, fd6);
+            tt_damp<R>((R)P.BD, R(1), d, 8, f8, fd8);
+          }
+          R ir6d = ir6 * f6, ir8d = ir8 * f8;
+          R ir7 = R(6) * ir6d / d;
+          R ir9 = R(8) * ir8d / d;
+          u = erh - ir6d - ir8d;
+          wnum = (R)P.B * erh - ir7 - ir9 + ir6 * fd6 + ir8 * fd8;
         }
-        R ir6d = ir6 * f6, ir8d = ir8 * f8;
-        R ir7 = R(6) * ir6d / d;
-        R ir9 = R(8) * ir8d / d;
-        R uw = R(0);
-        if (P.wall != 0.0) uw = (R)P.wall * (ir8r * ir8r * ir8r);
-        R u = erh - ir6d - ir8d + uw;
-        R wij = ((R)P.B * erh - ir7 - ir9 + ir6 * fd6 + ir8 * fd8 + R(24) * uw / d) / d;
+        if (P.wall != 0.0) {
+          R ir8r = (ir2 * ir2) * (ir2 * ir2);
+          R uw = (R)P.wall * (ir8r * ir8r * ir8r);
+          u += uw;
+          wnum += R(24) * uw / d;
+        }
+        R wij = wnum / d;
         R fx = wij * rx, fy = wij * ry, fz = wij * rz;
         fb[0] += (double)fx;
         fb[1] += (double)fy;

@@ -175,7 +175,10 @@ def mgo(ncell=10, seed=4321, density=3.58, jitter=0.2, temp=2000.0, rcut=10.0,
         alpha=0.35, epsw=1e-7, skin=1.0, kmax=None, **extra):
     """Polarisable MgO: Lewis-Catlow Buckingham, O polarisability 1.6 A^3,
     Tang-Toennies damping (b = 3.0 1/A, c = 1.0, order 4) of the Mg charge ->
-    O dipole field; Ewald alpha 0.35 with kmax from the ewald_param rule at
+    O dipole field (ldip_damping(O, Mg, O): the reference symmetrises the
+    last two indices from the upper triangle, pim.f90:189-199, so the entry
+    is given with the lower type index second, like ldip_damping(1,1,2) in
+    examples/ex09/config/pot_mdff/PIMD.POT); Ewald alpha 0.35 with kmax from the ewald_param rule at
     epsw.  Types: 0 = Mg (+2), 1 = O (-2)."""
     rng = np.random.default_rng(seed)
     nf = 4 * ncell ** 3
@@ -190,8 +193,8 @@ def mgo(ncell=10, seed=4321, density=3.58, jitter=0.2, temp=2000.0, rcut=10.0,
               qch=[2.0, -2.0], Abmhftd=A, Bbmhftd=B, Cbmhftd=C,
               alphaES=alpha, kES=(kmax,) * 3, epsw=epsw,
               ldip_polar=[0, 1], poldip_iso={1: 1.6},
-              ldip_damping={(1, 1, 0): 1}, pol_damp_b={(1, 1, 0): 3.0},
-              pol_damp_c={(1, 1, 0): 1.0}, pol_damp_k={(1, 1, 0): 4},
+              ldip_damping={(1, 0, 1): 1}, pol_damp_b={(1, 0, 1): 3.0},
+              pol_damp_c={(1, 0, 1): 1.0}, pol_damp_k={(1, 0, 1): 4},
               conv_tol_ind=1e-8, extrapolate_order=2)
     kw.update(extra)
     p = make_params([nf, nf], **kw)
@@ -245,8 +248,10 @@ def rsi(rng, n_per_type, L, dmin):
 def sio2(nsio2=4000, seed=2024, density=2.2, temp=300.0, rcut=10.0, alpha=0.3, kmax=12,
          skin=1.0, dmin_sio=1.4, dmin_oo=2.2, dmin_sisi=2.5, **extra):
     """SiO2-like glass: 3*nsio2 ions (Si +2.4 then O -1.2) by seeded random
-    sequential insertion; BKS Buckingham plus a W/r^24 wall (W_SiO = 10 eV A^24,
-    W_OO = 1.5^24 eV A^24); O polarisability 1.3 A^3 with Tang-Toennies damping
+    sequential insertion; BKS Buckingham plus a (sigma/r)^24 eV wall on every
+    pair (sigma Si-O 1.2, O-O 1.9, Si-Si 2.4 A: BKS alone has an unphysical
+    Si-O well below 1.2 A and no Si-Si repulsion, and O-O pairs must stay out of
+    the dipole catastrophe radius); O polarisability 1.3 A^3 with Tang-Toennies damping
     of the fields on O (b, c, order from examples/ex09/config/pot_mdff/PIMD.POT:
     O-O 5.584/2.890/4, O-Si 3.664/1.446/4); Ewald alpha 0.3, kmax 12, rc 10.
     Minimum separations: Si-O 1.4 A; O-O and Si-Si larger (2.2 / 2.5 A) so no
@@ -260,13 +265,13 @@ def sio2(nsio2=4000, seed=2024, density=2.2, temp=300.0, rcut=10.0, alpha=0.3, k
     rc = min(rcut, 0.5 * L)
     kw = dict(lcoulomb=1, lbmhft=1, cutshortrange=rc, cutlongrange=rc, skindiff=skin,
               qch=[2.4, -1.2], Abmhftd=A, Bbmhftd=B, Cbmhftd=C,
-              wall24={(0, 1): 10.0, (1, 1): 1.5 ** 24},
+              wall24={(0, 1): 1.2 ** 24, (1, 1): 1.9 ** 24, (0, 0): 2.4 ** 24},
               alphaES=alpha, kES=(kmax,) * 3,
               ldip_polar=[0, 1], poldip_iso={1: 1.3},
-              ldip_damping={(1, 1, 1): 1, (1, 1, 0): 1},
-              pol_damp_b={(1, 1, 1): 5.58406251008641721012, (1, 1, 0): 3.66418041600447487325},
-              pol_damp_c={(1, 1, 1): 2.8904937083, (1, 1, 0): 1.4460000000},
-              pol_damp_k={(1, 1, 1): 4, (1, 1, 0): 4},
+              ldip_damping={(1, 1, 1): 1, (1, 0, 1): 1},
+              pol_damp_b={(1, 1, 1): 5.58406251008641721012, (1, 0, 1): 3.66418041600447487325},
+              pol_damp_c={(1, 1, 1): 2.8904937083, (1, 0, 1): 1.4460000000},
+              pol_damp_k={(1, 1, 1): 4, (1, 0, 1): 4},
               conv_tol_ind=1e-8, extrapolate_order=2)
     kw.update(extra)
     p = make_params([nsio2, 2 * nsio2], **kw)

@@ -628,38 +628,45 @@ static void or_bmhftd(or_ctx* c, const double* sx, const double* sy, const doubl
       double rijsq =
           min_image(c, sx[ia] - sx[ja], sy[ia] - sy[ja], sz[ia] - sz[ja], &rxij, &ryij, &rzij);
       int p1 = c->itype[ia], p2 = c->itype[ja];
-      if (c->p.Abmhftd[p1][p2] == 0.0) continue;
+      /* the reference skips pairs with A = 0 (non_bonded.f90:1153); the
+         optional wall extension acts on its own */
+      double Aij = c->p.Abmhftd[p1][p2], Wij = c->p.wall24[p1][p2];
+      if (Aij == 0.0 && Wij == 0.0) continue;
       if (rijsq < c->rcutsq[p1][p2]) {
         double ir2 = 1.0 / rijsq;
         double d = sqrt(rijsq);
-        double erh = c->p.Abmhftd[p1][p2] * exp(-c->p.Bbmhftd[p1][p2] * d);
-        double ir6 = ir2 * ir2 * ir2;
-        double ir8 = ir6 * ir2;
-        ir6 = ir6 * c->p.Cbmhftd[p1][p2];
-        ir8 = ir8 * c->p.Dbmhftd[p1][p2];
-        double f6, f8, fdiff6, fdiff8, ir6d, ir8d;
-        if (lbmhftd) {
-          tt_damp_tab(c->E_TT, c->p.BDbmhftd[p1][p2], 1.0, d, 6, &f6, &fdiff6);
-          tt_damp_tab(c->E_TT, c->p.BDbmhftd[p1][p2], 1.0, d, 8, &f8, &fdiff8);
-          ir6d = ir6 * f6;
-          ir8d = ir8 * f8;
-        } else {
-          fdiff6 = 0.0;
-          fdiff8 = 0.0;
-          ir6d = ir6;
-          ir8d = ir8;
+        double u_pair = 0.0, wnum = 0.0;
+        if (Aij != 0.0) {
+          double erh = Aij * exp(-c->p.Bbmhftd[p1][p2] * d);
+          double ir6 = ir2 * ir2 * ir2;
+          double ir8 = ir6 * ir2;
+          ir6 = ir6 * c->p.Cbmhftd[p1][p2];
+          ir8 = ir8 * c->p.Dbmhftd[p1][p2];
+          double f6, f8, fdiff6, fdiff8, ir6d, ir8d;
+          if (lbmhftd) {
+            tt_damp_tab(c->E_TT, c->p.BDbmhftd[p1][p2], 1.0, d, 6, &f6, &fdiff6);
+            tt_damp_tab(c->E_TT, c->p.BDbmhftd[p1][p2], 1.0, d, 8, &f8, &fdiff8);
+            ir6d = ir6 * f6;
+            ir8d = ir8 * f8;
+          } else {
+            fdiff6 = 0.0;
+            fdiff8 = 0.0;
+            ir6d = ir6;
+            ir8d = ir8;
+          }
+          double ir7 = 6.0 * ir6d / d;
+          double ir9 = 8.0 * ir8d / d;
+          u_pair = erh - ir6d - ir8d;
+          wnum = c->p.Bbmhftd[p1][p2] * erh - ir7 - ir9 + ir6 * fdiff6 + ir8 * fdiff8;
         }
-        double ir7 = 6.0 * ir6d / d;
-        double ir9 = 8.0 * ir8d / d;
-        double uw = 0.0;
-        if (c->p.wall24[p1][p2] != 0.0) {
+        if (Wij != 0.0) {
           double ir8r = (ir2 * ir2) * (ir2 * ir2);
-          uw = c->p.wall24[p1][p2] * (ir8r * ir8r * ir8r);
+          double uw = Wij * (ir8r * ir8r * ir8r);
+          u_pair = u_pair + uw;
+          wnum = wnum + 24.0 * uw / d;
         }
-        u = u + erh - ir6d - ir8d + uw;
-        double wij = c->p.Bbmhftd[p1][p2] * erh - ir7 - ir9 + ir6 * fdiff6 + ir8 * fdiff8 +
-                     24.0 * uw / d;
-        wij = wij / d;
+        u = u + u_pair;
+        double wij = wnum / d;
         double fxij = wij * rxij, fyij = wij * ryij, fzij = wij * rzij;
         vir = vir + (rxij * fxij + ryij * fyij + rzij * fzij);
         fx[ia] += fxij;

@@ -52,10 +52,10 @@ def small_systems():
     out = []
     for tag in ("twocharges", "twodipoles", "twocharges_twopola"):
         out.append(systems.ex04(tag))
-    dampkw = dict(ldip_damping={(1, 1, 0): 1, (1, 1, 1): 1},
-                  pol_damp_b={(1, 1, 0): 3.0, (1, 1, 1): 4.1},
-                  pol_damp_c={(1, 1, 0): 1.0, (1, 1, 1): 1.7},
-                  pol_damp_k={(1, 1, 0): 4, (1, 1, 1): 3})
+    dampkw = dict(ldip_damping={(1, 0, 1): 1, (1, 1, 1): 1},
+                  pol_damp_b={(1, 0, 1): 3.0, (1, 1, 1): 4.1},
+                  pol_damp_c={(1, 0, 1): 1.0, (1, 1, 1): 1.7},
+                  pol_damp_k={(1, 0, 1): 4, (1, 1, 1): 3})
     out.append(systems.random_ionic((24, 24), L=13.0, seed=21, calc=P._abi.CALC_OTHER, **dampkw))
     out.append(systems.random_ionic((20, 28), L=13.5, seed=22, triclinic=True,
                                     q=(1.2, -0.857142857142857), calc=P._abi.CALC_OTHER, **dampkw))

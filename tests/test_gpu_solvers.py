@@ -16,8 +16,8 @@ def _pim_cases():
     return [
         systems.random_ionic((24, 24), L=13.0, seed=51, calc=_abi.CALC_OTHER, conv_tol_ind=1e-13,
                              max_scf_pol_iter=500,
-                             ldip_damping={(1, 1, 0): 1}, pol_damp_b={(1, 1, 0): 3.0},
-                             pol_damp_c={(1, 1, 0): 1.0}, pol_damp_k={(1, 1, 0): 4}),
+                             ldip_damping={(1, 0, 1): 1}, pol_damp_b={(1, 0, 1): 3.0},
+                             pol_damp_c={(1, 0, 1): 1.0}, pol_damp_k={(1, 0, 1): 4}),
         systems.mgo(ncell=2, calc=_abi.CALC_OTHER, conv_tol_ind=1e-13, max_scf_pol_iter=500),
         systems.sio2(nsio2=150, seed=9, calc=_abi.CALC_OTHER, conv_tol_ind=1e-13,
                      max_scf_pol_iter=500),

@@ -204,6 +204,24 @@ int mdff_gpu_verlet_half_list(mdff_handle h, int which, const double* rx,
                               const double* ry, const double* rz, int* point,
                               int* list, int capacity, int* n_out);
 
+/* The same half list as mdff_gpu_verlet_half_list, computed without any
+   device allocation and without a handle: all scratch lives in one
+   file-scope static device array of about 18.4 MB that every GPU loading the
+   library holds until exit.  It has no counterpart in the reference.  It is
+   for callers that cannot call cudaMalloc, e.g. a host program whose device
+   memory is owned by another runtime's caching pool (where a cudaMalloc can
+   fail or fragment that pool), or a utility that needs only the list and
+   should not create an engine.  Host inputs / outputs as for
+   mdff_gpu_verlet_half_list; params supplies natm, the cutoffs, skindiff,
+   lcoulomb (half-cell clamp of cutlongrange) and device.  Limits:
+   natm <= 32768 and list entries <= 4194304 (else MDFF_ERR_BAD_ARGS /
+   MDFF_ERR_LIST_OVERFLOW with a message on stderr).  The first call on a
+   device looks up the array's address.  Calls share the array: two calls
+   overlapping on the same GPU race. */
+int mdff_gpu_verlet_half_list_noalloc(const mdff_params* p, const double cell_A[9], int which,
+                                      const double* rx, const double* ry, const double* rz,
+                                      int* point, int* list, int capacity, int* n_out);
+
 /* Velocity-Verlet NVE steps on device (prop_velocity_verlet,
    integration.f90:132-194): d_pos, d_vel SoA [3][natm], d_invmass [natm] in
    internal units, dt in internal time units.  Each step calls the engine.

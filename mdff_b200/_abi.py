@@ -99,6 +99,8 @@ SIGNATURES = {
     "mdff_gpu_set_aspc_history": (_i, [_P, _DP]),
     "mdff_gpu_get_stats": (_i, [_P, ctypes.POINTER(MdffStats)]),
     "mdff_gpu_verlet_half_list": (_i, [_P, _i, _DP, _DP, _DP, _IP, _IP, _i, _IP]),
+    "mdff_gpu_verlet_half_list_noalloc": (_i, [ctypes.POINTER(MdffParams), _DP, _i, _DP, _DP, _DP,
+                                                _IP, _IP, _i, _IP]),
     "mdff_gpu_md_nve": (_i, [_P, _P, _P, _P, _d, _i, _i, _DP]),
     "mdff_gpu_profile": (_i, [_P, _i]),
     "mdff_gpu_kernel_times": (_i, [_P, _DP, ctypes.POINTER(ctypes.c_longlong), _DP]),

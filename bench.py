@@ -51,7 +51,9 @@ def parse():
 def make_system(name):
     from mdff_b200 import _abi, systems
     if name == "sio2":
-        s = systems.sio2()
+        # the insertion is skipped when the prepared starting state exists
+        have = os.path.exists(os.path.join(ROOT, "tests", "golden", "sio2_state.npz"))
+        s = systems.sio2(place=not have)
         wl = dict(workload="sio2_pim_ewald_12000", natm=s.natm, box_A=round(s.info["L"], 4),
                   rcut_A=10.0, alpha=0.3, kmax=12, pim="O 1.3 A^3 + TT damping",
                   short_range="BKS Buckingham + r^-24 wall", dt_fs=DT_FS, ensemble="NVE")

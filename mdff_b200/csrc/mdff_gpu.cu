@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -28,9 +29,8 @@ namespace {
 constexpr double kCoulUnit = 14.3996441494161;     // constants.f90:91
 constexpr double kPressUnit = 0.00624150964712042; // constants.f90:88
 constexpr int NT = MDFF_NTYPEMAX;
-constexpr int kNZT = 16;           // nz tile of the structure-factor kernel
 constexpr int kRhoThreads = 128;
-constexpr int kRhoChunk = 2048;    // ions per structure-factor block
+constexpr int kRhoChunk = 4096;    // ions per structure-factor block
 constexpr int kFieldThreads = 128;
 
 // scalar slots (device doubles, copied to the host at the end of a call)
@@ -94,6 +94,7 @@ struct mdff_ctx {
   double2* d_tab64 = nullptr;
   float2* d_tab32 = nullptr;
   double4* d_w = nullptr;
+  float4* d_w32 = nullptr;
   double2* d_rho_part = nullptr;
   double2* d_rhoA = nullptr;
   double* d_str = nullptr;
@@ -104,6 +105,7 @@ struct mdff_ctx {
   double4 *d_Estat = nullptr, *d_Eind = nullptr, *d_Efield = nullptr, *d_mu_ind = nullptr;
   double4 *d_mu_tot = nullptr, *d_hist = nullptr, *d_E = nullptr;
   double4 *d_r = nullptr, *d_z = nullptr, *d_pv = nullptr, *d_qv = nullptr, *d_Tp = nullptr;
+  float4* d_mu32 = nullptr;      // FP32 copy of the dipoles of an FP32 pass
   // outputs / reductions
   double* d_force = nullptr;     // [3][natm]
   double* d_part = nullptr;
@@ -369,7 +371,7 @@ static int build_mesh(mdff_ctx* h) {
   // k chunks of the field pass: enough blocks to fill 148 SMs several times,
   // at most 2048 k (32 KB of rho') per chunk
   int nrows = (int)h->rows.size();
-  int atom_blocks = cdiv(h->natm, kFieldThreads);
+  int atom_blocks = cdiv(h->natm, 2 * kFieldThreads);
   int nch = std::max(1, std::min(nrows, cdiv(4 * 148 * 2, atom_blocks)));
   nch = std::max(nch, std::min(nrows, cdiv(nk, 2048)));
   h->rchunk.assign(1, 0);
@@ -513,6 +515,42 @@ static int moments(mdff_ctx* h, const double4* mu, int has_q, double* out) {
 
 static PolDev poldev(mdff_ctx* h) { return PolDev{h->d_pol, h->d_invpol, h->d_ipolar}; }
 
+// nz tile of the structure factor: the width (8, 11, 13 or 16) that wastes
+// the fewest accumulator slots on rows of nzmax consecutive nz
+static int pick_nzt(int nzmax) {
+  const int cand[4] = {16, 13, 11, 8};
+  int best = 16, waste = 1 << 30;
+  for (int c : cand) {
+    int w = cdiv(nzmax, c) * c - nzmax;
+    if (w < waste) {
+      waste = w;
+      best = c;
+    }
+  }
+  return best;
+}
+
+template <typename R, int NZT>
+static void launch_rho(mdff_ctx* h, dim3 g, const typename cplx<R>::T* tab, int n, int chunk,
+                       const RecMesh& M, int ntiles, int has_q, int has_mu) {
+  if constexpr (std::is_same<R, float>::value) {
+    // FP32: two ions per thread in packed FP32x2 lanes
+    if (has_q && has_mu)
+      k_rec_rho_x2<true, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w32, n, chunk, M, ntiles, h->d_rho_part);
+    else if (has_q)
+      k_rec_rho_x2<true, false, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w32, n, chunk, M, ntiles, h->d_rho_part);
+    else
+      k_rec_rho_x2<false, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w32, n, chunk, M, ntiles, h->d_rho_part);
+    return;
+  }
+  if (has_q && has_mu)
+    k_rec_rho<R, true, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
+  else if (has_q)
+    k_rec_rho<R, true, false, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
+  else
+    k_rec_rho<R, false, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
+}
+
 // reciprocal pass: E += rec field; force += rec force * coul_unit (if forces);
 // energy (7 doubles) into e_out (if non-null)
 template <typename R>
@@ -529,9 +567,12 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   M.nk = h->nk;
   M.Ak = h->d_Ak;
   M.kvec = h->d_kvec;
-  k_rec_weights<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_q, mu, n, h->d_cell, has_q, has_mu, h->d_w);
+  constexpr bool F32 = std::is_same<R, float>::value;
+  k_rec_weights<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_q, mu, n, h->d_cell, has_q, has_mu, h->d_w,
+                                                 F32 ? h->d_w32 : nullptr);
   LAUNCH_CHECK();
-  int ntiles = cdiv(2 * M.kmax[2] + 1, kNZT);
+  int nzt = pick_nzt(2 * M.kmax[2] + 1);
+  int ntiles = cdiv(2 * M.kmax[2] + 1, nzt);
   dim3 g((unsigned)(M.nrows * ntiles), (unsigned)h->n_rho_chunks);
   int chunk = kRhoChunk;
   // algorithmic op counts per (k, ion) term (add = mul = 1, FMA = 2,
@@ -540,12 +581,12 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   double ops_rho = (has_q && has_mu) ? 20.0 : (has_mu ? 16.0 : 11.0);
   double ops_fld = (forces && has_mu) ? 32.0 : (forces ? 17.0 : 20.0);
   int pr = prof_begin(h, KC_RHO, (double)h->nk * n * ops_rho);
-  if (has_q && has_mu)
-    k_rec_rho<R, true, true, kNZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
-  else if (has_q)
-    k_rec_rho<R, true, false, kNZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
-  else
-    k_rec_rho<R, false, true, kNZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
+  switch (nzt) {
+    case 8: launch_rho<R, 8>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+    case 11: launch_rho<R, 11>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+    case 13: launch_rho<R, 13>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+    default: launch_rho<R, 16>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+  }
   LAUNCH_CHECK();
   prof_end(h, pr);
   k_rec_sum<<<cdiv(h->nk, 256), 256, 0, h->st>>>(h->d_rho_part, h->n_rho_chunks, M, h->d_rhoA, h->d_str);
@@ -560,7 +601,13 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   size_t smem = (size_t)h->max_chunk_k * sizeof(typename cplx<R>::T);
   bool muf = forces && has_mu;
   pr = prof_begin(h, KC_RECF, (double)h->nk * n * ops_fld);
-  if (muf)
+  if constexpr (std::is_same<R, float>::value) {
+    dim3 gx((unsigned)cdiv(n, 2 * kFieldThreads), (unsigned)nch);
+    if (muf)
+      k_rec_field_x2<true><<<gx, kFieldThreads, smem, h->st>>>(tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_G, h->d_H);
+    else
+      k_rec_field_x2<false><<<gx, kFieldThreads, smem, h->st>>>(tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_G, h->d_H);
+  } else if (muf)
     k_rec_field<R, true><<<gf, kFieldThreads, smem, h->st>>>(tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_G, h->d_H);
   else
     k_rec_field<R, false><<<gf, kFieldThreads, smem, h->st>>>(tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_G, h->d_H);
@@ -583,7 +630,7 @@ static int rec_pass(mdff_ctx* h, bool fp32, const double4* mu, int has_q, int ha
 static int build_tables(mdff_ctx* h) {
   if (h->nk == 0) return MDFF_OK;
   int n = h->natm;
-  int kzt = std::max(h->p.kES[2], 1);
+  int kzt = std::max(h->p.kES[2], 4);
   k_rec_tables<double><<<cdiv(n, 128), 128, 0, h->st>>>(h->d_s, n, h->p.kES[0], h->p.kES[1], kzt, h->d_tab64);
   LAUNCH_CHECK();
   if (h->p.precision == MDFF_PREC_MIXED) {
@@ -600,9 +647,13 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   CK(cudaMemsetAsync(E, 0, sizeof(double4) * n, h->st));
   double cutsq = h->p.cutlongrange * h->p.cutlongrange;
   int nb = cdiv((long)n * 32, 256);
+  if (fp32) {
+    k_to_float4<<<cdiv(n, 256), 256, 0, h->st>>>(mu, n, h->d_mu32);
+    LAUNCH_CHECK();
+  }
   int pr = prof_begin(h, KC_ESFIELD, 0);
   if (fp32)
-    k_es_field<float, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
+    k_es_field<float, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu32, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
   else
     k_es_field<double, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
   LAUNCH_CHECK();
@@ -629,20 +680,24 @@ static int static_field(mdff_ctx* h, bool fp32) {
   double cutsq = h->p.cutlongrange * h->p.cutlongrange;
   int nb = cdiv((long)n * 32, 256);
   bool qq = h->task_qq != 0, dd = h->ldip_static != 0;
-#define ESF(R, Q, D)                                                                                         \
-  k_es_field<R, Q, D><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_dipia, h->L.nbr, \
-                                             h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype,        \
+#define ESF(R, Q, D, MU)                                                                              \
+  k_es_field<R, Q, D><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, MU, h->L.nbr, \
+                                             h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, \
                                              h->p.alphaES, cutsq, 1, 0, E)
+  if (fp32 && dd) {
+    k_to_float4<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_dipia, n, h->d_mu32);
+    LAUNCH_CHECK();
+  }
   if (qq || dd) {
     int pr = prof_begin(h, KC_ESFIELD, 0);
     if (fp32) {
-      if (qq && dd) ESF(float, true, true);
-      else if (qq) ESF(float, true, false);
-      else ESF(float, false, true);
+      if (qq && dd) ESF(float, true, true, h->d_mu32);
+      else if (qq) ESF(float, true, false, h->d_mu32);
+      else ESF(float, false, true, h->d_mu32);
     } else {
-      if (qq && dd) ESF(double, true, true);
-      else if (qq) ESF(double, true, false);
-      else ESF(double, false, true);
+      if (qq && dd) ESF(double, true, true, h->d_dipia);
+      else if (qq) ESF(double, true, false, h->d_dipia);
+      else ESF(double, false, true, h->d_dipia);
     }
     LAUNCH_CHECK();
     prof_end(h, pr);
@@ -821,7 +876,10 @@ static int run_engforce(mdff_ctx* h, int itime) {
   if (h->lsr) {
     int do_bmh = (h->p.lbmhft || h->p.lbmhftd) ? 1 : 0;
     int pr = prof_begin(h, KC_SR, 0);
-    if (fp32)
+    // short range stays FP64 in the mixed mode too: BKS-type pair forces of
+    // tens of eV/A cancel to net forces of a few eV/A, and FP32 rounding of the
+    // pair terms alone gives ~1e-5 relative force error
+    if (false)
       k_shortrange<float><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_itype, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_nbtab, h->ntype, do_bmh, h->p.lbmhftd, h->p.lnmlj, h->p.trunc, h->d_force, h->d_part);
     else
       k_shortrange<double><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_itype, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_nbtab, h->ntype, do_bmh, h->p.lbmhftd, h->p.lnmlj, h->p.trunc, h->d_force, h->d_part);
@@ -1215,10 +1273,11 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   // reciprocal mesh and tables
   if (p.lcoulomb) {
     if ((s = build_mesh(h))) return s;
-    int ntab = p.kES[0] + 1 + p.kES[1] + 1 + std::max(p.kES[2], 1) + 1;
+    int ntab = p.kES[0] + 1 + p.kES[1] + 1 + std::max(p.kES[2], 4) + 1;
     DALLOC(h->d_tab64, (size_t)ntab * n);
     if (p.precision == MDFF_PREC_MIXED) DALLOC(h->d_tab32, (size_t)ntab * n);
     DALLOC(h->d_w, n);
+    DALLOC(h->d_w32, n);
   }
   // pim and outputs
   DALLOC(h->d_Estat, n);
@@ -1233,6 +1292,7 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_pv, n);
   DALLOC(h->d_qv, n);
   DALLOC(h->d_Tp, n);
+  DALLOC(h->d_mu32, n);
   DALLOC(h->d_force, 3 * (size_t)n);
   DALLOC(h->d_pack, 3 * (size_t)n);
   h->part_cap = (size_t)std::max(cdiv((long)n * 32, 256), cdiv(n, 256)) * 16 + 64;
@@ -1530,9 +1590,9 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_dipia, h->d_pol, h->d_invpol, h->d_nbtab, h->d_estab, h->L.nbr, h->L.nnb,
                   h->L.flags, h->L.sref, h->L.cell_of, h->L.cell_count, h->L.cell_start,
                   h->L.cell_fill, h->L.cell_atoms, h->d_disp_part, h->d_rows, h->d_Ak, h->d_kvec,
-                  h->d_rchunk, h->d_tab64, h->d_tab32, h->d_w, h->d_rho_part, h->d_rhoA, h->d_str,
+                  h->d_rchunk, h->d_tab64, h->d_tab32, h->d_w, h->d_w32, h->d_rho_part, h->d_rhoA, h->d_str,
                   h->d_G, h->d_H, h->d_Estat, h->d_Eind, h->d_Efield, h->d_mu_ind, h->d_mu_tot,
-                  h->d_hist, h->d_E, h->d_r, h->d_z, h->d_pv, h->d_qv, h->d_Tp, h->d_force,
+                  h->d_hist, h->d_E, h->d_r, h->d_z, h->d_pv, h->d_qv, h->d_Tp, h->d_mu32, h->d_force,
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part};
   for (void* q : ptrs)
     if (q) cudaFree(q);

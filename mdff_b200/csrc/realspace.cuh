@@ -188,52 +188,139 @@ __device__ __forceinline__ void radial(R d2, R alpha, Radial<R>& o) {
   }
 }
 
+// FP32: no IEEE divisions (each is a multi-instruction sequence): 1/d from
+// rsqrtf, powers by multiplication, constants folded
+template <>
+__device__ __forceinline__ void radial<float, false>(float d2, float alpha, Radial<float>& o) {
+  float rinv = rsqrtf(d2);
+  float dm2 = rinv * rinv;
+  o.d = d2 * rinv;
+  o.dm1 = rinv;
+  o.dm3 = rinv * dm2;
+  o.dm5 = o.dm3 * dm2;
+  o.dm7 = o.dm5 * dm2;
+  float a2 = alpha * alpha;
+  float expon = expf(-a2 * d2) * 0.56418958354775628695f;  // 1/sqrt(pi)
+  float z = alpha * o.d;
+  float t = __frcp_rn(1.0f + 0.5f * z);
+  float p = -.82215223f + t * .17087277f;
+  p = 1.48851587f + t * p;
+  p = -1.13520398f + t * p;
+  p = .27886807f + t * p;
+  p = -.18628806f + t * p;
+  p = .09678418f + t * p;
+  p = .37409196f + t * p;
+  p = 1.00002368f + t * p;
+  o.F0 = t * expf(-z * z - 1.26551223f + t * p);
+  float ade = alpha * o.d * expon;
+  o.F1 = o.F0 + 2.0f * ade;
+  o.F2 = o.F1 + (4.0f / 3.0f) * a2 * d2 * ade;
+  o.F3 = 0.0f;
+}
+template <>
+__device__ __forceinline__ void radial<float, true>(float d2, float alpha, Radial<float>& o) {
+  radial<float, false>(d2, alpha, o);
+  float a2 = alpha * alpha;
+  float ade = alpha * o.d * expf(-a2 * d2) * 0.56418958354775628695f;
+  o.F3 = o.F2 + (8.0f / 15.0f) * a2 * a2 * d2 * d2 * ade;
+}
+
 // --------------------------------------------------------------------------
 // field-only pass.  Adds into E (AoS double4 [natm]):
 //   QQ : E_i += q_j r_ij dm3 (F1 - F1d_i)       (qq block, ewald_dir.f90:533-541)
 //   DD : E_i += T2(r_ij) . mu_j                  (dd block, ewald_dir.f90:566-571)
 // dd_mask: 0 -> the reference's condition any(mu_i /= 0) .and. any(mu_j /= 0)
 //          1 -> both ions polarisable (the linear operator of the CG solve)
+template <typename R>
+struct vec4t;
+template <>
+struct vec4t<double> {
+  typedef double4 T;
+};
+template <>
+struct vec4t<float> {
+  typedef float4 T;
+};
+
+// minimum-image vector of the pair (i, j) and its square.  FP64: the
+// reference's exact arithmetic.  FP32: the direct-coordinate difference in
+// FP64 (positions of a 50 A box need it), the image shift and A.s in FP32.
+template <typename R>
+__device__ __forceinline__ R pair_vec(const double* A, double4 si, double4 sj, R& rx, R& ry, R& rz);
+template <>
+__device__ __forceinline__ double pair_vec<double>(const double* A, double4 si, double4 sj,
+                                                   double& rx, double& ry, double& rz) {
+  return min_image_exact(A, xsub(si.x, sj.x), xsub(si.y, sj.y), xsub(si.z, sj.z), rx, ry, rz);
+}
+template <>
+__device__ __forceinline__ float pair_vec<float>(const double* A, double4 si, double4 sj,
+                                                 float& rx, float& ry, float& rz) {
+  float dx = (float)(si.x - sj.x), dy = (float)(si.y - sj.y), dz = (float)(si.z - sj.z);
+  dx -= rintf(dx);
+  dy -= rintf(dy);
+  dz -= rintf(dz);
+  rx = dx * (float)A[0] + dy * (float)A[1] + dz * (float)A[2];
+  ry = dx * (float)A[3] + dy * (float)A[4] + dz * (float)A[5];
+  rz = dx * (float)A[6] + dy * (float)A[7] + dz * (float)A[8];
+  return rx * rx + ry * ry + rz * rz;
+}
+
+// dipoles converted for the FP32 passes
+__global__ void k_to_float4(const double4* __restrict__ in, int n, float4* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 v = in[i];
+  out[i] = make_float4((float)v.x, (float)v.y, (float)v.z, 0.f);
+}
+
+// field-only pass.  Adds into E (AoS double4 [natm]):
+//   QQ : E_i += q_j r_ij dm3 (F1 - F1d_i)       (qq block, ewald_dir.f90:533-541)
+//   DD : E_i += T2(r_ij) . mu_j                  (dd block, ewald_dir.f90:566-571)
+// dd_mask: 0 -> the reference's condition any(mu_i /= 0) .and. any(mu_j /= 0)
+//          1 -> both ions polarisable (the linear operator of the CG solve)
+// mu is double4 for FP64 and float4 for FP32 (k_to_float4).
 template <typename R, bool QQ, bool DD>
 __global__ void __launch_bounds__(256) k_es_field(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
-    const int* __restrict__ ipolar, const double4* __restrict__ mu, const int* __restrict__ nbr,
-    const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
-    const ESPair* __restrict__ tab, int ntype, double alpha, double cutsq, int damp,
-    int dd_mask, double4* __restrict__ E) {
+    const int* __restrict__ ipolar, const typename vec4t<R>::T* __restrict__ mu,
+    const int* __restrict__ nbr, const int* __restrict__ nnb, int cap, int natm,
+    const CellC* __restrict__ cell, const ESPair* __restrict__ tab, int ntype, double alpha,
+    double cutsq, int damp, int dd_mask, double4* __restrict__ E) {
+  typedef typename vec4t<R>::T M4;
   __shared__ ESPair stab[MDFF_NT * MDFF_NT];
+  __shared__ double cA[9];
   for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
+  if (threadIdx.x < 9) cA[threadIdx.x] = cell->A[threadIdx.x];
   __syncthreads();
   int lane = threadIdx.x & 31;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= natm) return;
   double4 si = s[i];
   int ti = itype[i];
-  double4 mui = DD ? mu[i] : make_double4(0, 0, 0, 0);
-  bool dip_i = DD && (dd_mask ? (ipolar[i] != 0) : (mui.x != 0.0 || mui.y != 0.0 || mui.z != 0.0));
+  M4 mui;
+  if (DD) mui = mu[i];
+  bool dip_i = DD && (dd_mask ? (ipolar[i] != 0) : (mui.x != 0 || mui.y != 0 || mui.z != 0));
   int n = nnb[i];
   const int* row = nbr + (size_t)i * cap;
-  double ex = 0.0, ey = 0.0, ez = 0.0;
+  R ex = R(0), ey = R(0), ez = R(0);
+  const R rc2 = (R)cutsq;
   if (QQ || dip_i) {
     for (int k = lane; k < n; k += 32) {
       int j = row[k];
       double4 sj = s[j];
-      double rxd, ryd, rzd;
-      double r2d = min_image_exact(cell->A, xsub(si.x, sj.x), xsub(si.y, sj.y), xsub(si.z, sj.z),
-                                   rxd, ryd, rzd);
-      if (r2d > cutsq) continue;  // ewald_dir.f90:202 ( d2 .gt. cutsq ) cycle
-      double4 muj;
+      R rx, ry, rz;
+      R r2 = pair_vec<R>(cA, si, sj, rx, ry, rz);
+      if (r2 > rc2) continue;  // ewald_dir.f90:202 ( d2 .gt. cutsq ) cycle
+      M4 muj;
       bool dd = false;
       if (DD && dip_i) {
         muj = mu[j];
-        dd = dd_mask ? (ipolar[j] != 0) : (muj.x != 0.0 || muj.y != 0.0 || muj.z != 0.0);
+        dd = dd_mask ? (ipolar[j] != 0) : (muj.x != 0 || muj.y != 0 || muj.z != 0);
       }
       double qj = QQ ? q[j] : 0.0;
       if (!dd && (!QQ || qj == 0.0)) continue;
-      R rx = (R)rxd, ry = (R)ryd, rz = (R)rzd;
       Radial<R> g;
-      radial<R, false>((R)r2d, (R)alpha, g);
-      R e0 = R(0), e1 = R(0), e2 = R(0);
+      radial<R, false>(r2, (R)alpha, g);
       if (QQ && qj != 0.0) {
         R F1d = R(0);
         if (damp) {
@@ -251,29 +338,24 @@ __global__ void __launch_bounds__(256) k_es_field(
           }
         }
         R c = (R)qj * g.dm3 * (g.F1 - F1d);
-        e0 += c * rx;
-        e1 += c * ry;
-        e2 += c * rz;
+        ex += c * rx;
+        ey += c * ry;
+        ez += c * rz;
       }
       if (DD && dd) {
         R B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5;
         R mx = (R)muj.x, my = (R)muj.y, mz = (R)muj.z;
         R rm = rx * mx + ry * my + rz * mz;
-        e0 += B2 * rx * rm - B1 * mx;
-        e1 += B2 * ry * rm - B1 * my;
-        e2 += B2 * rz * rm - B1 * mz;
+        ex += B2 * rx * rm - B1 * mx;
+        ey += B2 * ry * rm - B1 * my;
+        ez += B2 * rz * rm - B1 * mz;
       }
-      ex += (double)e0;
-      ey += (double)e1;
-      ez += (double)e2;
     }
   }
-  ex = warp_sum(ex);
-  ey = warp_sum(ey);
-  ez = warp_sum(ez);
+  double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
   if (lane == 0) {
     double4 o = E[i];
-    E[i] = make_double4(o.x + ex, o.y + ey, o.z + ez, 0.0);
+    E[i] = make_double4(o.x + dx, o.y + dy, o.z + dz, 0.0);
   }
 }
 

@@ -40,7 +40,7 @@ struct RecMesh {
   const double4* kvec;   // [nk] (kx, ky, kz, kcoe)
 };
 
-// per-ion phase tables: [n][natm], X: n = 0..kx, Y: 0..ky, Z: 0..kz (FP64).
+// per-ion phase tables: [n][natm], X: n = 0..kx, Y: 0..ky, Z: 0..max(kz, 4).
 // s is wrapped to [-0.5, 0.5) first: e^{2 pi i n s} is periodic in s.
 template <typename R>
 __global__ void k_rec_tables(const double4* __restrict__ s, int natm, int kx, int ky, int kz,
@@ -67,7 +67,7 @@ __global__ void k_rec_tables(const double4* __restrict__ s, int natm, int kx, in
 // per-ion weights (q, m1, m2, m3), m = 2 pi B^T mu  (k.mu = n.m)
 __global__ void k_rec_weights(const double* __restrict__ q, const double4* __restrict__ mu,
                               int natm, const CellC* __restrict__ cell, int has_q, int has_mu,
-                              double4* __restrict__ w) {
+                              double4* __restrict__ w, float4* __restrict__ w32) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   const double* B = cell->B;
@@ -80,6 +80,7 @@ __global__ void k_rec_weights(const double* __restrict__ q, const double4* __res
     m3 = kTwoPi * (B[2] * u.x + B[5] * u.y + B[8] * u.z);
   }
   w[i] = make_double4(qi, m1, m2, m3);
+  if (w32) w32[i] = make_float4((float)qi, (float)m1, (float)m2, (float)m3);
 }
 
 template <typename C>
@@ -111,8 +112,23 @@ __device__ __forceinline__ typename cplx<R>::T phase_xyz(const typename cplx<R>:
   return cmul(cmul(X, Y), Z);
 }
 
+// XY * Z_nz for ion i (Z_{-n} = conj Z_n); |nz| must not exceed the table's kz
+template <typename R>
+__device__ __forceinline__ typename cplx<R>::T phase_z(const typename cplx<R>::T* __restrict__ tab,
+                                                       int natm, int i, typename cplx<R>::T XY,
+                                                       int nz, int kx, int ky) {
+  typedef typename cplx<R>::T C;
+  int az = nz < 0 ? -nz : nz;
+  C Z = tab[(size_t)(kx + 1 + ky + 1 + az) * natm + i];
+  if (nz < 0) Z = cconj(Z);
+  return cmul(XY, Z);
+}
+
 // rho partials.  grid.x = nrows * ntiles, grid.y = ion chunks; block 128.
-// part[chunk][k] (double2).
+// part[chunk][k] (double2).  Each thread keeps NZT accumulators (one per nz
+// of the tile) over its ions; the phase advances by one complex multiply per
+// nz and is re-anchored on the exact table every 4 nz (FP32 drift bound).
+// Warp partial sums in R, block and chunk sums in FP64, fixed order.
 template <typename R, bool HAS_Q, bool HAS_MU, int NZT>
 __global__ void __launch_bounds__(128) k_rec_rho(const typename cplx<R>::T* __restrict__ tab,
                                                  const double4* __restrict__ w, int natm,
@@ -134,15 +150,24 @@ __global__ void __launch_bounds__(128) k_rec_rho(const typename cplx<R>::T* __re
 #pragma unroll
   for (int t = 0; t < NZT; ++t) accR[t] = accI[t] = R(0);
   const int kx = M.kmax[0], ky = M.kmax[1];
+  const size_t zoff = (size_t)(kx + 1 + ky + 1);
   for (int i = a0 + threadIdx.x; i < a1; i += blockDim.x) {
-    C P = phase_xyz<R>(tab, natm, i, nx, ny, nz0, kx, ky);
-    C Z1 = tab[(size_t)(kx + 1 + ky + 1 + 1) * natm + i];
+    C XY = phase_xyz<R>(tab, natm, i, nx, ny, 0, kx, ky);
+    C Z1 = tab[(zoff + 1) * natm + i];
     double4 wi = w[i];
     R q = (R)wi.x;
-    R km = (R)(nx * wi.y + ny * wi.z + nz0 * wi.w);
     R m3 = (R)wi.w;
+    R km = (R)(nx * wi.y + ny * wi.z + nz0 * wi.w);
+    C P;
 #pragma unroll
     for (int t = 0; t < NZT; ++t) {
+      if ((t & 3) == 0 && (t == 0 || sizeof(R) == 4)) {
+        // anchor on the table; slots beyond the row's end only compute
+        // values that are never stored, so clamp their index into the table
+        int nz = nz0 + t;
+        nz = nz > kz ? kz : nz;
+        P = phase_z<R>(tab, natm, i, XY, nz, kx, ky);
+      }
       if (HAS_Q) {
         accR[t] += q * P.x;
         accI[t] += q * P.y;
@@ -152,18 +177,18 @@ __global__ void __launch_bounds__(128) k_rec_rho(const typename cplx<R>::T* __re
         accI[t] += km * P.x;
         km += m3;
       }
-      P = cmul(P, Z1);
+      if (t + 1 < NZT && ((t + 1) & 3) != 0) P = cmul(P, Z1);
+      else if (t + 1 < NZT && sizeof(R) == 8) P = cmul(P, Z1);
     }
   }
-  // block reduction in double, fixed order
   int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
 #pragma unroll
   for (int t = 0; t < NZT; ++t) {
-    double vr = warp_sum((double)accR[t]);
-    double vi = warp_sum((double)accI[t]);
+    R vr = warp_sum(accR[t]);
+    R vi = warp_sum(accI[t]);
     if (lane == 0) {
-      red[2 * t][wp] = vr;
-      red[2 * t + 1][wp] = vi;
+      red[2 * t][wp] = (double)vr;
+      red[2 * t + 1][wp] = (double)vi;
     }
   }
   __syncthreads();
@@ -252,34 +277,63 @@ __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>::T* __
   for (int r = r0; r < r1; ++r) {
     int4 ri = M.rows[r];
     int nx = ri.x, ny = ri.y, nz_lo = ri.z;
-    C P = phase_xyz<R>(tab, natm, i, nx, ny, nz_lo, kx, ky);
+    C XY = phase_xyz<R>(tab, natm, i, nx, ny, 0, kx, ky);
+    // sums over the row, nz measured from the row start: Sz = sum t recarg
     R S0 = R(0), Sz = R(0), T0 = R(0), Tz = R(0);
-    R nzd = (R)nz_lo;
     R km = (R)(nx * wi.y + ny * wi.z + nz_lo * wi.w);
     const C* rr = sh + (ri.w - k0);
     int nn = kz - nz_lo + 1;
-    for (int t = 0; t < nn; ++t) {
-      C rho = rr[t];
-      R recarg = rho.y * P.x - rho.x * P.y;
-      S0 += recarg;
-      Sz += nzd * recarg;
-      if (HAS_MU_FORCE) {
-        R recarg2 = rho.x * P.x + rho.y * P.y;
-        R tt = km * recarg2;
-        T0 += tt;
-        Tz += nzd * tt;
-        km += m3;
+    C P = phase_z<R>(tab, natm, i, XY, nz_lo, kx, ky);
+    int t0 = 0;
+    R tf = R(0);  // t0 as R, advanced by 4 (no int->float conversion per term)
+    for (; t0 + 4 <= nn; t0 += 4, tf += R(4)) {
+      if (sizeof(R) == 4 && t0 > 0) P = phase_z<R>(tab, natm, i, XY, nz_lo + t0, kx, ky);
+      R a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        C rho = rr[t0 + u];
+        a[u] = rho.y * P.x - rho.x * P.y;
+        if (HAS_MU_FORCE) b[u] = (km + R(u) * m3) * (rho.x * P.x + rho.y * P.y);
+        if (u < 3 || sizeof(R) == 8) P = cmul(P, Z1);
       }
-      nzd += R(1);
-      P = cmul(P, Z1);
+      // sum_u a_u and sum_u u a_u of the group (u = 0..3)
+      R sa = (a[0] + a[1]) + (a[2] + a[3]);
+      R sb = a[1] + R(2) * a[2] + R(3) * a[3];
+      S0 += sa;
+      Sz += tf * sa + sb;
+      if (HAS_MU_FORCE) {
+        R ta = (b[0] + b[1]) + (b[2] + b[3]);
+        R tb = b[1] + R(2) * b[2] + R(3) * b[3];
+        T0 += ta;
+        Tz += tf * ta + tb;
+        km += R(4) * m3;
+      }
+    }
+    if (t0 < nn) {
+      if (sizeof(R) == 4 && t0 > 0) P = phase_z<R>(tab, natm, i, XY, nz_lo + t0, kx, ky);
+      for (int t = t0; t < nn; ++t) {
+        C rho = rr[t];
+        R recarg = rho.y * P.x - rho.x * P.y;
+        R tt_ = (R)t;
+        S0 += recarg;
+        Sz += tt_ * recarg;
+        if (HAS_MU_FORCE) {
+          R recarg2 = rho.x * P.x + rho.y * P.y;
+          R tt = km * recarg2;
+          T0 += tt;
+          Tz += tt_ * tt;
+          km += m3;
+        }
+        P = cmul(P, Z1);
+      }
     }
     G[0] += (double)nx * (double)S0;
     G[1] += (double)ny * (double)S0;
-    G[2] += (double)Sz;
+    G[2] += (double)nz_lo * (double)S0 + (double)Sz;
     if (HAS_MU_FORCE) {
       H[0] += (double)nx * (double)T0;
       H[1] += (double)ny * (double)T0;
-      H[2] += (double)Tz;
+      H[2] += (double)nz_lo * (double)T0 + (double)Tz;
     }
   }
   Gpart[(size_t)blockIdx.y * natm + i] = make_double4(G[0], G[1], G[2], 0.0);
@@ -321,6 +375,237 @@ __global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const double4
     force[i] += (qi * e[0] + (has_mu_force ? fm[0] : 0.0)) * coul_unit;
     force[natm + i] += (qi * e[1] + (has_mu_force ? fm[1] : 0.0)) * coul_unit;
     force[2 * natm + i] += (qi * e[2] + (has_mu_force ? fm[2] : 0.0)) * coul_unit;
+  }
+}
+
+}  // namespace mdff
+
+namespace mdff {
+
+// ===========================================================================
+// FP32 reciprocal kernels with Blackwell packed FP32x2 arithmetic.  Each
+// thread carries two ions in the two lanes of float2 values (lane x = ion a,
+// lane y = ion b), so one packed FFMA2 advances both ions' phases, one shared
+// rho' load serves both, and the per-term instruction count halves.  Same
+// operations and roundings per ion as the scalar FP32 kernels above.
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2s(float a) { return make_float2(a, a); }
+
+// packed complex multiply of (re, im) lane pairs by (zr, zi) lane pairs
+__device__ __forceinline__ void cmul2(float2& re, float2& im, float2 zr, float2 zi) {
+  float2 nre = __ffma2_rn(re, zr, __fmul2_rn(im, f2(-zi.x, -zi.y)));
+  float2 nim = __ffma2_rn(re, zi, __fmul2_rn(im, zr));
+  re = nre;
+  im = nim;
+}
+
+// table phase X_nx Y_ny Z_nz of one ion (float)
+__device__ __forceinline__ float2 phase1(const float2* __restrict__ tab, int natm, int i, int nx,
+                                         int ny, int nz, int kx, int ky) {
+  return phase_xyz<float>(tab, natm, i, nx, ny, nz, kx, ky);
+}
+
+// structure factor, FP32x2.  Thread t of the block handles ions a = i, b = i + 128
+// of each 256-ion step of its chunk (b absent -> weight 0).
+template <bool HAS_Q, bool HAS_MU, int NZT>
+__global__ void __launch_bounds__(128) k_rec_rho_x2(const float2* __restrict__ tab,
+                                                    const float4* __restrict__ w, int natm,
+                                                    int chunk, RecMesh M, int ntiles,
+                                                    double2* __restrict__ part) {
+  __shared__ double red[2 * NZT][4];
+  int row = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
+  int4 ri = M.rows[row];
+  int nx = ri.x, ny = ri.y, nz_lo = ri.z, koff = ri.w;
+  int kz = M.kmax[2];
+  int nz0 = nz_lo + tile * NZT;
+  if (nz0 > kz) return;
+  int nzn = kz - nz0 + 1;
+  if (nzn > NZT) nzn = NZT;
+  int a0 = blockIdx.y * chunk, a1 = a0 + chunk;
+  if (a1 > natm) a1 = natm;
+  float2 accR[NZT], accI[NZT];
+#pragma unroll
+  for (int t = 0; t < NZT; ++t) accR[t] = accI[t] = f2s(0.f);
+  const int kx = M.kmax[0], ky = M.kmax[1];
+  const size_t zoff = (size_t)(kx + 1 + ky + 1);
+  const float fnx = (float)nx, fny = (float)ny, fnz0 = (float)nz0;
+  for (int base = a0; base < a1; base += 256) {
+    int ia = base + threadIdx.x, ib = ia + 128;
+    if (ia >= a1) break;
+    bool vb = ib < a1;
+    int ibb = vb ? ib : ia;
+    float2 XYa = phase1(tab, natm, ia, nx, ny, 0, kx, ky);
+    float2 XYb = phase1(tab, natm, ibb, nx, ny, 0, kx, ky);
+    float2 Pa = phase_z<float>(tab, natm, ia, XYa, nz0, kx, ky);
+    float2 Pb = phase_z<float>(tab, natm, ibb, XYb, nz0, kx, ky);
+    float2 Z1a = tab[(zoff + 1) * natm + ia], Z1b = tab[(zoff + 1) * natm + ibb];
+    float2 Z4a = tab[(zoff + 4) * natm + ia], Z4b = tab[(zoff + 4) * natm + ibb];
+    float2 zr = f2(Z1a.x, Z1b.x), zi = f2(Z1a.y, Z1b.y);
+    float2 z4r = f2(Z4a.x, Z4b.x), z4i = f2(Z4a.y, Z4b.y);
+    float4 wa = w[ia], wb = w[ibb];
+    float2 q = f2(wa.x, vb ? wb.x : 0.f);
+    float2 m3 = f2(wa.w, vb ? wb.w : 0.f);
+    float2 km = f2(fnx * wa.y + fny * wa.z + fnz0 * wa.w,
+                   vb ? fnx * wb.y + fny * wb.z + fnz0 * wb.w : 0.f);
+    // phase at t = 4g + u: (P0 Z4^g) Z1^u
+    float2 gre = f2(Pa.x, Pb.x), gim = f2(Pa.y, Pb.y);
+    float2 pre = gre, pim = gim;
+#pragma unroll
+    for (int t = 0; t < NZT; ++t) {
+      if (t > 0) {
+        if ((t & 3) == 0) {
+          cmul2(gre, gim, z4r, z4i);
+          pre = gre;
+          pim = gim;
+        } else {
+          cmul2(pre, pim, zr, zi);
+        }
+      }
+      if (HAS_Q) {
+        accR[t] = __ffma2_rn(q, pre, accR[t]);
+        accI[t] = __ffma2_rn(q, pim, accI[t]);
+      }
+      if (HAS_MU) {
+        accR[t] = __ffma2_rn(f2(-km.x, -km.y), pim, accR[t]);
+        accI[t] = __ffma2_rn(km, pre, accI[t]);
+        km = __fadd2_rn(km, m3);
+      }
+    }
+  }
+  int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < NZT; ++t) {
+    float vr = warp_sum(accR[t].x + accR[t].y);
+    float vi = warp_sum(accI[t].x + accI[t].y);
+    if (lane == 0) {
+      red[2 * t][wp] = (double)vr;
+      red[2 * t + 1][wp] = (double)vi;
+    }
+  }
+  __syncthreads();
+  if ((int)threadIdx.x < nzn) {
+    int t = threadIdx.x;
+    double vr = red[2 * t][0] + red[2 * t][1] + red[2 * t][2] + red[2 * t][3];
+    double vi = red[2 * t + 1][0] + red[2 * t + 1][1] + red[2 * t + 1][2] + red[2 * t + 1][3];
+    int k = koff + (nz0 - nz_lo) + t;
+    part[(size_t)blockIdx.y * M.nk + k] = make_double2(vr, vi);
+  }
+}
+
+// field / force partials, FP32x2: ions a = blockIdx.x*256 + tid, b = a + 128.
+template <bool HAS_MU_FORCE>
+__global__ void __launch_bounds__(128) k_rec_field_x2(const float2* __restrict__ tab,
+                                                      const float4* __restrict__ w, int natm,
+                                                      RecMesh M, const int* __restrict__ rchunk,
+                                                      const double2* __restrict__ rhoA,
+                                                      double4* __restrict__ Gpart,
+                                                      double4* __restrict__ Hpart) {
+  extern __shared__ unsigned char shraw[];
+  float2* sh = reinterpret_cast<float2*>(shraw);
+  int r0 = rchunk[blockIdx.y], r1 = rchunk[blockIdx.y + 1];
+  int k0 = M.rows[r0].w;
+  int k1 = (r1 < M.nrows) ? M.rows[r1].w : M.nk;
+  for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
+    double2 v = rhoA[k];
+    sh[k - k0] = make_float2((float)v.x, (float)v.y);
+  }
+  __syncthreads();
+  int ia = blockIdx.x * 256 + threadIdx.x, ib = ia + 128;
+  if (ia >= natm) return;
+  bool vb = ib < natm;
+  int ibb = vb ? ib : ia;
+  const int kx = M.kmax[0], ky = M.kmax[1], kz = M.kmax[2];
+  const size_t zoff = (size_t)(kx + 1 + ky + 1);
+  float4 wa = w[ia], wb = w[ibb];
+  float2 m3 = f2(wa.w, wb.w);
+  float2 Z1a = tab[(zoff + 1) * natm + ia], Z1b = tab[(zoff + 1) * natm + ibb];
+  float2 Z4a = tab[(zoff + 4) * natm + ia], Z4b = tab[(zoff + 4) * natm + ibb];
+  float2 zr = f2(Z1a.x, Z1b.x), zi = f2(Z1a.y, Z1b.y);
+  float2 z4r = f2(Z4a.x, Z4b.x), z4i = f2(Z4a.y, Z4b.y);
+  double Ga[3] = {0, 0, 0}, Gb[3] = {0, 0, 0}, Ha[3] = {0, 0, 0}, Hb[3] = {0, 0, 0};
+  for (int r = r0; r < r1; ++r) {
+    int4 ri = M.rows[r];
+    int nx = ri.x, ny = ri.y, nz_lo = ri.z;
+    float2 XYa = phase1(tab, natm, ia, nx, ny, 0, kx, ky);
+    float2 XYb = phase1(tab, natm, ibb, nx, ny, 0, kx, ky);
+    float2 Pa = phase_z<float>(tab, natm, ia, XYa, nz_lo, kx, ky);
+    float2 Pb = phase_z<float>(tab, natm, ibb, XYb, nz_lo, kx, ky);
+    float2 gre = f2(Pa.x, Pb.x), gim = f2(Pa.y, Pb.y);
+    float2 S0 = f2s(0.f), Sz = f2s(0.f), T0 = f2s(0.f), Tz = f2s(0.f);
+    float fnx = (float)nx, fny = (float)ny, fnz = (float)nz_lo;
+    float2 km = f2(fnx * wa.y + fny * wa.z + fnz * wa.w, fnx * wb.y + fny * wb.z + fnz * wb.w);
+    const float2* rr = sh + (ri.w - k0);
+    int nn = kz - nz_lo + 1;
+    int t0 = 0;
+    float tf = 0.f;
+    for (; t0 + 4 <= nn; t0 += 4, tf += 4.f) {
+      if (t0 > 0) cmul2(gre, gim, z4r, z4i);
+      float2 pre = gre, pim = gim;
+      float2 a[4], b[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        float2 rho = rr[t0 + u];
+        // recarg = rho_I cos - rho_R sin ; recarg2 = rho_R cos + rho_I sin
+        a[u] = __ffma2_rn(f2s(rho.y), pre, __fmul2_rn(f2s(-rho.x), pim));
+        if (HAS_MU_FORCE) {
+          float2 r2 = __ffma2_rn(f2s(rho.x), pre, __fmul2_rn(f2s(rho.y), pim));
+          float2 kmu = __ffma2_rn(f2s((float)u), m3, km);
+          b[u] = __fmul2_rn(kmu, r2);
+        }
+        if (u < 3) cmul2(pre, pim, zr, zi);
+      }
+      float2 sa = __fadd2_rn(__fadd2_rn(a[0], a[1]), __fadd2_rn(a[2], a[3]));
+      float2 sb = __ffma2_rn(f2s(3.f), a[3], __ffma2_rn(f2s(2.f), a[2], a[1]));
+      S0 = __fadd2_rn(S0, sa);
+      Sz = __fadd2_rn(Sz, __ffma2_rn(f2s(tf), sa, sb));
+      if (HAS_MU_FORCE) {
+        float2 ta = __fadd2_rn(__fadd2_rn(b[0], b[1]), __fadd2_rn(b[2], b[3]));
+        float2 tb = __ffma2_rn(f2s(3.f), b[3], __ffma2_rn(f2s(2.f), b[2], b[1]));
+        T0 = __fadd2_rn(T0, ta);
+        Tz = __fadd2_rn(Tz, __ffma2_rn(f2s(tf), ta, tb));
+        km = __ffma2_rn(f2s(4.f), m3, km);
+      }
+    }
+    if (t0 < nn) {
+      if (t0 > 0) cmul2(gre, gim, z4r, z4i);
+      float2 pre = gre, pim = gim;
+      for (int t = t0; t < nn; ++t) {
+        float2 rho = rr[t];
+        float2 a = __ffma2_rn(f2s(rho.y), pre, __fmul2_rn(f2s(-rho.x), pim));
+        float2 tt_ = f2s((float)t);
+        S0 = __fadd2_rn(S0, a);
+        Sz = __ffma2_rn(tt_, a, Sz);
+        if (HAS_MU_FORCE) {
+          float2 r2 = __ffma2_rn(f2s(rho.x), pre, __fmul2_rn(f2s(rho.y), pim));
+          float2 b = __fmul2_rn(km, r2);
+          T0 = __fadd2_rn(T0, b);
+          Tz = __ffma2_rn(tt_, b, Tz);
+          km = __fadd2_rn(km, m3);
+        }
+        cmul2(pre, pim, zr, zi);
+      }
+    }
+    Ga[0] += (double)nx * (double)S0.x;
+    Ga[1] += (double)ny * (double)S0.x;
+    Ga[2] += (double)nz_lo * (double)S0.x + (double)Sz.x;
+    Gb[0] += (double)nx * (double)S0.y;
+    Gb[1] += (double)ny * (double)S0.y;
+    Gb[2] += (double)nz_lo * (double)S0.y + (double)Sz.y;
+    if (HAS_MU_FORCE) {
+      Ha[0] += (double)nx * (double)T0.x;
+      Ha[1] += (double)ny * (double)T0.x;
+      Ha[2] += (double)nz_lo * (double)T0.x + (double)Tz.x;
+      Hb[0] += (double)nx * (double)T0.y;
+      Hb[1] += (double)ny * (double)T0.y;
+      Hb[2] += (double)nz_lo * (double)T0.y + (double)Tz.y;
+    }
+  }
+  Gpart[(size_t)blockIdx.y * natm + ia] = make_double4(Ga[0], Ga[1], Ga[2], 0.0);
+  if (HAS_MU_FORCE) Hpart[(size_t)blockIdx.y * natm + ia] = make_double4(Ha[0], Ha[1], Ha[2], 0.0);
+  if (vb) {
+    Gpart[(size_t)blockIdx.y * natm + ib] = make_double4(Gb[0], Gb[1], Gb[2], 0.0);
+    if (HAS_MU_FORCE) Hpart[(size_t)blockIdx.y * natm + ib] = make_double4(Hb[0], Hb[1], Hb[2], 0.0);
   }
 }
 

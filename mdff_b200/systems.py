@@ -246,7 +246,7 @@ def rsi(rng, n_per_type, L, dmin):
 
 
 def sio2(nsio2=4000, seed=2024, density=2.2, temp=300.0, rcut=10.0, alpha=0.3, kmax=12,
-         skin=1.0, dmin_sio=1.4, dmin_oo=2.2, dmin_sisi=2.5, **extra):
+         skin=1.0, dmin_sio=1.4, dmin_oo=2.2, dmin_sisi=2.5, place=True, **extra):
     """SiO2-like glass: 3*nsio2 ions (Si +2.4 then O -1.2) by seeded random
     sequential insertion; BKS Buckingham plus a (sigma/r)^24 eV wall on every
     pair (sigma Si-O 1.2, O-O 1.9, Si-Si 2.4 A: BKS alone has an unphysical
@@ -260,7 +260,8 @@ def sio2(nsio2=4000, seed=2024, density=2.2, temp=300.0, rcut=10.0, alpha=0.3, k
     rng = np.random.default_rng(seed)
     L = box_length(nsio2, 28.0855 + 2 * 15.9994, density)
     dmin = [[dmin_sisi, dmin_sio], [dmin_sio, dmin_oo]]
-    pos = rsi(rng, [nsio2, 2 * nsio2], L, dmin)
+    # place=False skips the insertion (positions then come from a prepared state)
+    pos = rsi(rng, [nsio2, 2 * nsio2], L, dmin) if place else np.zeros((3 * nsio2, 3))
     A, B, C = bks_sio2()
     rc = min(rcut, 0.5 * L)
     kw = dict(lcoulomb=1, lbmhft=1, cutshortrange=rc, cutlongrange=rc, skindiff=skin,

@@ -41,9 +41,10 @@ enum {
   S_MOM = 30,    // 8: moments of the final pass
   S_UPOL = 38,   // u_pol
   S_RMS = 39,    // SCF rmsd^2 sum
-  S_CG = 40,     // 40 rz, 41 rmsd^2 (init), 42 pq, 43 rzn, 44 rmsd^2 (update)
-  S_MOM2 = 48,   // 8: moments of field passes
-  S_DISP = 56,
+  S_CG = 40,     // 40 rz, 41 rmsd^2 (init), 42 pq, 43 rzn, 44 rmsd^2 (update),
+                 // 45 inner tolerance, 46 iterations, 47 iteration cap, 48 rmsd
+  S_MOM2 = 52,   // 8: moments of field passes
+  S_DISP = 60,
   S_NSCAL = 64
 };
 
@@ -121,6 +122,13 @@ struct mdff_ctx {
   int launches = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int launches_call = 0;         // kernels launched by the current API call
+  // CUDA graph of one inner CG iteration inside a device-side while loop
+  cudaGraph_t cg_graph = nullptr;
+  cudaGraphExec_t cg_exec = nullptr;
+  int cg_gen = -1;              // buffer generation the graph was built for
+  int cg_fp32 = -1;
+  int cg_body_launches = 0;
+  int gen = 0;                  // bumped whenever device buffers are reallocated
   // MD driver state: forces in d_force belong to the positions of md_pos
   bool md_valid = false;
   const double* md_pos = nullptr;
@@ -339,6 +347,7 @@ static void lattice(mdff_ctx* h, const double* Ain) {
 // k mesh as rows (nx, ny) of consecutive nz (kspace.f90:143-207, same
 // half-space; the reference's |k|^2 order only changes summation order)
 static int build_mesh(mdff_ctx* h) {
+  h->gen++;
   int kx = h->p.kES[0], ky = h->p.kES[1], kz = h->p.kES[2];
   h->rows.clear();
   int koff = 0;
@@ -443,6 +452,7 @@ static int setup_list_cells(mdff_ctx* h) {
 
 static int alloc_list(mdff_ctx* h, int cap) {
   cap = ((cap + 31) / 32) * 32;
+  h->gen++;
   cudaFree(h->L.nbr);
   h->L.nbr = nullptr;
   DALLOC(h->L.nbr, (size_t)h->natm * cap);
@@ -555,7 +565,7 @@ static void launch_rho(mdff_ctx* h, dim3 g, const typename cplx<R>::T* tab, int 
 // energy (7 doubles) into e_out (if non-null)
 template <typename R>
 static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4* mu, int has_q,
-                      int has_mu, int forces, double4* E, double* e_out) {
+                      int has_mu, int forces, double4* E, double* e_out, float4* mu32) {
   int n = h->natm;
   if (h->nk == 0) return MDFF_OK;
   RecMesh M;
@@ -569,7 +579,7 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   M.kvec = h->d_kvec;
   constexpr bool F32 = std::is_same<R, float>::value;
   k_rec_weights<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_q, mu, n, h->d_cell, has_q, has_mu, h->d_w,
-                                                 F32 ? h->d_w32 : nullptr);
+                                                 F32 ? h->d_w32 : nullptr, mu32);
   LAUNCH_CHECK();
   int nzt = pick_nzt(2 * M.kmax[2] + 1);
   int ntiles = cdiv(2 * M.kmax[2] + 1, nzt);
@@ -614,7 +624,7 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   LAUNCH_CHECK();
   prof_end(h, pr);
   double fpi_V = 2.0 * tpi_V;
-  k_rec_field_sum<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_G, h->d_H, nch, n, h->d_cell, h->d_q,
+  k_rec_field_sum<<<cdiv((long)n * 4, 256), 256, 0, h->st>>>(h->d_G, h->d_H, nch, n, h->d_cell, h->d_q,
                                                    2.0 * fpi_V, muf ? 1 : 0, forces, h->coul_unit, E,
                                                    h->d_force);
   LAUNCH_CHECK();
@@ -622,9 +632,9 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
 }
 
 static int rec_pass(mdff_ctx* h, bool fp32, const double4* mu, int has_q, int has_mu, int forces,
-                    double4* E, double* e_out) {
-  if (fp32) return rec_pass_t<float>(h, h->d_tab32, mu, has_q, has_mu, forces, E, e_out);
-  return rec_pass_t<double>(h, h->d_tab64, mu, has_q, has_mu, forces, E, e_out);
+                    double4* E, double* e_out, float4* mu32 = nullptr) {
+  if (fp32) return rec_pass_t<float>(h, h->d_tab32, mu, has_q, has_mu, forces, E, e_out, mu32);
+  return rec_pass_t<double>(h, h->d_tab64, mu, has_q, has_mu, forces, E, e_out, mu32);
 }
 
 static int build_tables(mdff_ctx* h) {
@@ -647,10 +657,9 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   CK(cudaMemsetAsync(E, 0, sizeof(double4) * n, h->st));
   double cutsq = h->p.cutlongrange * h->p.cutlongrange;
   int nb = cdiv((long)n * 32, 256);
-  if (fp32) {
-    k_to_float4<<<cdiv(n, 256), 256, 0, h->st>>>(mu, n, h->d_mu32);
-    LAUNCH_CHECK();
-  }
+  // reciprocal first: its weights kernel also writes the FP32 dipoles
+  int s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, fp32 ? h->d_mu32 : nullptr);
+  if (s) return s;
   int pr = prof_begin(h, KC_ESFIELD, 0);
   if (fp32)
     k_es_field<float, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu32, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
@@ -658,8 +667,6 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
     k_es_field<double, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
   LAUNCH_CHECK();
   prof_end(h, pr);
-  int s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr);
-  if (s) return s;
   double a = h->p.alphaES;
   double selfa2 = 2.0 * (a / std::sqrt(kPi)) * a * a / 3.0;
   double fpi_3V = 2.0 * (kTwoPi / h->omega / 3.0);
@@ -799,8 +806,89 @@ static int solve_scf(mdff_ctx* h, int itime, bool fp32) {
   return MDFF_OK;
 }
 
+// the step scalars after an inner CG iteration: rz <- rz_new, count, rmsd of
+// the recurrence residual, and (inside the graph) the while-loop condition
+__global__ void k_cg_inner_check(double* __restrict__ sc, int npol, int in_graph,
+                                 cudaGraphConditionalHandle hc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  sc[0] = sc[3];
+  double it = sc[6] + 1.0;
+  sc[6] = it;
+  double rm = sqrt(sc[4] / (double)npol);
+  sc[8] = rm;
+  if (in_graph) cudaGraphSetConditional(hc, (rm > sc[5] && it < sc[7]) ? 1u : 0u);
+}
+
+__global__ void k_setd2(double* __restrict__ a, double va, double* __restrict__ b, double vb) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    *a = va;
+    *b = vb;
+  }
+}
+
+// one inner CG iteration: p -> T p -> q = A p; x, r, z updated; p <- z + beta p
+static int cg_iteration(mdff_ctx* h, bool fp32, int in_graph, cudaGraphConditionalHandle hc) {
+  int n = h->natm, nb = cdiv(n, 256), s;
+  PolDev P = poldev(h);
+  double* sc = h->d_scal + S_CG;
+  if ((s = field_of_mu(h, h->d_pv, 1, fp32, h->d_Tp))) return s;
+  k_cg_Ap<<<nb, 256, 0, h->st>>>(h->d_pv, h->d_Tp, P, n, h->d_qv, h->d_part);
+  LAUNCH_CHECK();
+  if ((s = reduce_into(h, nb, 1, sc + 2))) return s;
+  k_cg_update<<<nb, 256, 0, h->st>>>(sc + 0, sc + 2, P, n, h->d_pv, h->d_qv, h->d_mu_ind, h->d_r, h->d_z, h->d_part);
+  LAUNCH_CHECK();
+  if ((s = reduce_into(h, nb, 2, sc + 3))) return s;
+  k_cg_dir<<<nb, 256, 0, h->st>>>(sc + 0, sc + 3, n, h->d_z, h->d_pv);
+  LAUNCH_CHECK();
+  k_cg_inner_check<<<1, 32, 0, h->st>>>(sc, h->npol, in_graph, hc);
+  LAUNCH_CHECK();
+  return MDFF_OK;
+}
+
+// graph: while (cond) { cg_iteration }  -- built once per buffer generation
+static int build_cg_graph(mdff_ctx* h, bool fp32) {
+  if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);
+  if (h->cg_graph) cudaGraphDestroy(h->cg_graph);
+  h->cg_exec = nullptr;
+  h->cg_graph = nullptr;
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  h->cg_graph = g;
+  cudaGraphConditionalHandle hc;
+  CK(cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = hc;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  bool prof = h->prof;
+  h->prof = false;
+  int launches0 = h->launches;
+  CK(cudaStreamBeginCaptureToGraph(h->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  int s = cg_iteration(h, fp32, 1, hc);
+  cudaGraph_t captured;
+  cudaError_t e = cudaStreamEndCapture(h->st, &captured);
+  h->prof = prof;
+  h->cg_body_launches = h->launches - launches0;
+  h->launches = launches0;
+  if (s) return s;
+  if (e != cudaSuccess) {
+    h->err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+    return MDFF_ERR_CUDA;
+  }
+  CK(cudaGraphInstantiate(&h->cg_exec, g, 0));
+  h->cg_gen = h->gen;
+  h->cg_fp32 = fp32 ? 1 : 0;
+  return MDFF_OK;
+}
+
 // preconditioned CG on (alpha^-1 - T) mu = E_stat.  fp32: matvecs in FP32,
-// residual refreshed with an FP64 matvec (iterative refinement).
+// residual refreshed with an FP64 matvec (iterative refinement).  The inner
+// iterations run as one CUDA-graph launch (device-side while loop); the
+// host reads one rmsd per outer (FP64 residual) iteration.
 static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
@@ -813,44 +901,42 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
   }
   double tol = h->p.cg_tol > 0 ? h->p.cg_tol : h->p.conv_tol_ind;
   int maxit = h->p.cg_max_iter > 0 ? h->p.cg_max_iter : 200;
-  int it = 0;
+  double* sc = h->d_scal + S_CG;
+  bool use_graph = !h->prof;
+  if (use_graph && (h->cg_exec == nullptr || h->cg_gen != h->gen || h->cg_fp32 != (fp32 ? 1 : 0)))
+    if ((s = build_cg_graph(h, fp32))) return s;
+  k_setd2<<<1, 32, 0, h->st>>>(sc + 6, 0.0, sc + 7, (double)maxit);
+  LAUNCH_CHECK();
   double rmsd = HUGE_VAL;
-  int outer = 0;
+  int outer = 0, it = 0;
   while (true) {
     // true residual (FP64 matvec)
     if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp))) return s;
     k_cg_init<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part);
     LAUNCH_CHECK();
-    if ((s = reduce_into(h, nb, 2, h->d_scal + S_CG))) return s;
-    double r2;
-    if ((s = read_scal(h, S_CG + 1, &r2))) return s;
-    rmsd = std::sqrt(r2 / (double)h->npol);
+    if ((s = reduce_into(h, nb, 2, sc))) return s;
+    CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * 9, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    rmsd = std::sqrt(h->h_scal[S_CG + 1] / (double)h->npol);
+    it = (int)h->h_scal[S_CG + 6];
     if (rmsd <= tol || it >= maxit || outer >= 8) break;
     outer++;
     // inner CG: FP64 runs to tol; FP32 reduces the residual by 1e-4 (or to tol)
     double tol_in = fp32 ? std::max(tol, 1e-4 * rmsd) : tol;
-    while (it < maxit) {
-      ++it;
-      if ((s = field_of_mu(h, h->d_pv, 1, fp32, h->d_Tp))) return s;
-      k_cg_Ap<<<nb, 256, 0, h->st>>>(h->d_pv, h->d_Tp, P, n, h->d_qv, h->d_part);
-      LAUNCH_CHECK();
-      if ((s = reduce_into(h, nb, 1, h->d_scal + S_CG + 2))) return s;
-      k_cg_update<<<nb, 256, 0, h->st>>>(h->d_scal + S_CG, h->d_scal + S_CG + 2, P, n, h->d_pv, h->d_qv, h->d_mu_ind, h->d_r, h->d_z, h->d_part);
-      LAUNCH_CHECK();
-      if ((s = reduce_into(h, nb, 2, h->d_scal + S_CG + 3))) return s;
-      k_cg_dir<<<nb, 256, 0, h->st>>>(h->d_scal + S_CG, h->d_scal + S_CG + 3, n, h->d_z, h->d_pv);
-      LAUNCH_CHECK();
-      k_copy1<<<1, 32, 0, h->st>>>(h->d_scal + S_CG, h->d_scal + S_CG + 3);
-      LAUNCH_CHECK();
-      if ((s = read_scal(h, S_CG + 4, &r2))) return s;
-      double rr = std::sqrt(r2 / (double)h->npol);
-      if (rr <= tol_in) break;
-    }
-    if (!fp32 && it > 0) {
-      // FP64: the recurrence residual is trusted; confirm once with the true one
-      continue;
+    k_setd2<<<1, 32, 0, h->st>>>(sc + 5, tol_in, sc + 7, (double)maxit);
+    LAUNCH_CHECK();
+    if (use_graph) {
+      CK(cudaGraphLaunch(h->cg_exec, h->st));
+    } else {
+      while (true) {
+        if ((s = cg_iteration(h, fp32, 0, 0))) return s;
+        CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * 9, cudaMemcpyDeviceToHost, h->st));
+        CK(cudaStreamSynchronize(h->st));
+        if (!(h->h_scal[S_CG + 8] > tol_in && h->h_scal[S_CG + 6] < maxit)) break;
+      }
     }
   }
+  if (use_graph) h->launches += h->cg_body_launches * it;
   h->stats.n_pol_iter = it;
   h->stats.rmsd = rmsd;
   h->stats.converged = rmsd <= tol;
@@ -1596,6 +1682,8 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);
+  if (h->cg_graph) cudaGraphDestroy(h->cg_graph);
   if (h->h_scal) cudaFreeHost(h->h_scal);
   if (h->h_flags) cudaFreeHost(h->h_flags);
   if (h->h_cata) cudaFreeHost(h->h_cata);

@@ -67,7 +67,8 @@ __global__ void k_rec_tables(const double4* __restrict__ s, int natm, int kx, in
 // per-ion weights (q, m1, m2, m3), m = 2 pi B^T mu  (k.mu = n.m)
 __global__ void k_rec_weights(const double* __restrict__ q, const double4* __restrict__ mu,
                               int natm, const CellC* __restrict__ cell, int has_q, int has_mu,
-                              double4* __restrict__ w, float4* __restrict__ w32) {
+                              double4* __restrict__ w, float4* __restrict__ w32,
+                              float4* __restrict__ mu32) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   const double* B = cell->B;
@@ -81,6 +82,10 @@ __global__ void k_rec_weights(const double* __restrict__ q, const double4* __res
   }
   w[i] = make_double4(qi, m1, m2, m3);
   if (w32) w32[i] = make_float4((float)qi, (float)m1, (float)m2, (float)m3);
+  if (mu32) {
+    double4 u = mu[i];
+    mu32[i] = make_float4((float)u.x, (float)u.y, (float)u.z, 0.f);
+  }
 }
 
 template <typename C>
@@ -342,26 +347,37 @@ __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>::T* __
 
 // chunk sum and scaling.  E += -(2 pi B G) * 2 fpi_V (ewald_rec.f90:193-198,
 // 300-352); with do_forces, F += [q (-2 pi B G) + 2 pi B H] * 2 fpi_V * coul_unit.
+// Four threads per ion split the chunk partials (fixed order, shuffle sum).
 __global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const double4* __restrict__ Hpart,
                                 int nchunk, int natm, const CellC* __restrict__ cell,
                                 const double* __restrict__ q, double scale /* 2 fpi_V */,
                                 int has_mu_force, int do_forces, double coul_unit,
                                 double4* __restrict__ E, double* __restrict__ force) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= natm) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int i = t >> 2, sub = t & 3;
   double g[3] = {0, 0, 0}, h[3] = {0, 0, 0};
-  for (int c = 0; c < nchunk; ++c) {
-    double4 v = Gpart[(size_t)c * natm + i];
-    g[0] += v.x;
-    g[1] += v.y;
-    g[2] += v.z;
-    if (has_mu_force) {
-      double4 u = Hpart[(size_t)c * natm + i];
-      h[0] += u.x;
-      h[1] += u.y;
-      h[2] += u.z;
+  if (i < natm) {
+    for (int c = sub; c < nchunk; c += 4) {
+      double4 v = Gpart[(size_t)c * natm + i];
+      g[0] += v.x;
+      g[1] += v.y;
+      g[2] += v.z;
+      if (has_mu_force) {
+        double4 u = Hpart[(size_t)c * natm + i];
+        h[0] += u.x;
+        h[1] += u.y;
+        h[2] += u.z;
+      }
     }
   }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    g[a] += __shfl_xor_sync(FULL_MASK, g[a], 1);
+    g[a] += __shfl_xor_sync(FULL_MASK, g[a], 2);
+    h[a] += __shfl_xor_sync(FULL_MASK, h[a], 1);
+    h[a] += __shfl_xor_sync(FULL_MASK, h[a], 2);
+  }
+  if (i >= natm || sub != 0) return;
   const double* B = cell->B;
   double e[3], fm[3];
   for (int a = 0; a < 3; ++a) {

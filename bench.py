@@ -30,6 +30,8 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from mdff_b200 import replicas  # noqa: E402
+
 DT_FS = 1.0
 
 
@@ -45,6 +47,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--relax", type=int, default=300, help="FIRE iterations before MD")
     ap.add_argument("--equil", type=int, default=50, help="rescaled MD steps before warm-up")
+    ap.add_argument("--drift-steps", type=int, default=5000, help="NVE steps for the energy drift")
     return ap.parse_args()
 
 
@@ -258,9 +261,7 @@ def run_ours(args, rank, world, local_rank):
     eng._lib.mdff_gpu_kernel_times(eng._h, _abi.dptr(kms), kl.ctypes.data_as(
         __import__("ctypes").POINTER(__import__("ctypes").c_longlong)), _abi.dptr(kw))
     eng._lib.mdff_gpu_profile(eng._h, 0)
-    total_s = sum(step_ms) / 1e3
-    total_s = dist_max(world, total_s)
-    value = world * args.steps / total_s
+    value, total_s = replicas.throughput(world, args.steps, sum(step_ms) / 1e3)
     res = dict(value=value, ms_per_step=1e3 * total_s / args.steps, launches=launches,
                cg_iters_mean=float(np.mean(iters)), clocks=clocks, wl=wl,
                kms=kms, kl=kl, kw=kw)
@@ -345,6 +346,38 @@ def run_ours(args, rank, world, local_rank):
     eng._lib.mdff_gpu_peak_flops(local_rank, 1, __import__("ctypes").byref(peak64))
     extra["peak_fp32_tflops"] = peak32.value
     extra["peak_fp64_tflops"] = peak64.value
+    # NVE energy drift (SiO2, 5000 steps in the configuration): the mixed engine
+    # and the FP64 CG engine continue from the same trajectory point
+    if args.drift_steps > 0:
+        extra["nve_drift"] = {"steps": args.drift_steps, "dt_fs": DT_FS}
+        for tag, prec in (("mixed", "mixed"), ("fp64_cg", "fp64")):
+            if tag == "mixed":
+                e_d = eng
+                p_d, v_d, it_d = pos.clone(), vel.clone(), itime
+            else:
+                pe = engine_params(s, prec, "cg")
+                pe.device = local_rank
+                e_d = ForceEngine(pe, s.cell)
+                e_d.set_aspc_history(hist)
+                p_d, v_d, it_d = pos.clone(), vel.clone(), itime
+            en = []
+            done = 0
+            while done < args.drift_steps:
+                nst = min(500, args.drift_steps - done)
+                en.append(e_d.md_nve(p_d.data_ptr(), v_d.data_ptr(), invm.data_ptr(), dt, nst, it_d))
+                it_d += nst
+                done += nst
+            en = np.concatenate(en)
+            etot = en[:, 0] + en[:, 1]
+            t_ps = np.arange(etot.size) * DT_FS * 1e-3
+            slope = np.polyfit(t_ps, etot, 1)[0]
+            extra["nve_drift"][tag] = {
+                "slope_meV_per_atom_per_ps": 1e3 * slope / n,
+                "max_dev_meV_per_atom": 1e3 * float(np.abs(etot - etot[0]).max()) / n,
+                "temperature_K_mean": float(2 * en[:, 0].mean() / (3 * n * systems.BOLTZ_UNIT)),
+            }
+            if tag != "mixed":
+                e_d.close()
     extra["stats"] = eng.stats()
     extra["_cpu_point"] = (soa, hist, itime)
     eng.close()
@@ -352,19 +385,7 @@ def run_ours(args, rank, world, local_rank):
 
 
 def dist_barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
-def dist_max(world, x):
-    if world <= 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    replicas.barrier(world)
 
 
 def cpu_baseline_sample(s, hist, itime, pos_soa):
@@ -457,9 +478,7 @@ def run_reference(args, rank, world):
 
 def main():
     args = parse()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local_rank = replicas.world()
     if args.impl == "reference":
         run_reference(args, rank, world)
         return

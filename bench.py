@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=10)
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-check", action="store_true", help="skip the mixed-vs-FP64 force check")
     ap.add_argument("--relax", type=int, default=300, help="FIRE iterations before MD")
     ap.add_argument("--equil", type=int, default=50, help="rescaled MD steps before warm-up")
     ap.add_argument("--drift-steps", type=int, default=5000, help="NVE steps for the energy drift")
@@ -273,7 +274,8 @@ def run_ours(args, rank, world, local_rank):
     soa = tuple(np.ascontiguousarray(pos_h[a]) for a in range(3))
     hist = eng.aspc_history()
     # FP64 engines on the same trajectory point (same ASPC history)
-    for tag, prec, solver in (("fp64_scf", "fp64", "scf"), ("fp64_cg", "fp64", "cg")):
+    for tag, prec, solver in ((("fp64_scf", "fp64", "scf"), ("fp64_cg", "fp64", "cg"))
+                              if args.fp64_steps > 0 else ()):
         pe = engine_params(s, prec, solver)
         pe.device = local_rank
         e2 = ForceEngine(pe, s.cell)
@@ -282,7 +284,7 @@ def run_ours(args, rank, world, local_rank):
         e2.set_aspc_history(hist)
         ms, it2 = [], []
         it = itime
-        for k in range(max(args.fp64_steps, 1) + 2):
+        for k in range(args.fp64_steps + 2):
             flush_l2(l2buf)
             torch.cuda.synchronize()
             e2.md_nve(pos2.data_ptr(), vel2.data_ptr(), invm.data_ptr(), dt, 1, it, energies=False)
@@ -295,51 +297,12 @@ def run_ours(args, rank, world, local_rank):
         extra[tag + "_iters_mean"] = float(np.mean(it2))
         e2.close()
     # force error of the mixed engine vs the FP64 engine (tight SCF) on one config
-    pt = engine_params(s, "fp64", "scf")
-    pt.conv_tol_ind = 1e-11
-    pt.max_scf_pol_iter = 400
-    pt.calc = _abi.CALC_OTHER
-    e3 = ForceEngine(pt, s.cell)
-    ref = e3.engforce(*soa)
-    e3.close()
-    pm = engine_params(s, "mixed", "cg")
-    pm.calc = _abi.CALC_OTHER
-    e4 = ForceEngine(pm, s.cell)
-    mix = e4.engforce(*soa)
-    e4.close()
-    fr = np.stack([ref["fx"], ref["fy"], ref["fz"]], 1)
-    fm = np.stack([mix["fx"], mix["fy"], mix["fz"]], 1)
-    extra["force_err_rms_rel_vs_fp64"] = float(np.sqrt(((fm - fr) ** 2).sum() / (fr ** 2).sum()))
-    extra["dipole_err_rms_rel_vs_fp64"] = float(np.sqrt(((mix["mu"] - ref["mu"]) ** 2).sum()
-                                                        / (ref["mu"] ** 2).sum()))
-    extra["energy_err_rel_vs_fp64"] = abs(mix["u_coul"] + mix["u_bmhft"] - ref["u_coul"]
-                                          - ref["u_bmhft"]) / abs(ref["u_coul"] + ref["u_bmhft"])
-    # e2e through the C ABI with pinned host buffers (what a Fortran caller does)
+    if not args.no_check:
+        check_force_error(extra, s, soa)
+    run_e2e = args.e2e_steps is None or args.e2e_steps > 0
     ne = args.e2e_steps or args.steps
-    rx = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-    ry = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-    rz = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-    v_h = vel.cpu().numpy().copy()
-    rx[:], ry[:], rz[:] = soa
-    invm_h = 1.0 / s.mass
-    r0 = eng.engforce(rx, ry, rz, itime=itime, want_ef=False)
-    f = np.stack([r0["fx"], r0["fy"], r0["fz"]])
-    e_ms = []
-    for k in range(ne):
-        v_h += 0.5 * dt * f * invm_h
-        rx += dt * v_h[0]
-        ry += dt * v_h[1]
-        rz += dt * v_h[2]
-        flush_l2(l2buf)
-        torch.cuda.synchronize()
-        itime += 1
-        r = eng.engforce(rx, ry, rz, itime=itime, want_ef=False)
-        e_ms.append(eng.stats()["ms_last"])
-        f = np.stack([r["fx"], r["fy"], r["fz"]])
-        v_h += 0.5 * dt * f * invm_h
-    extra["e2e"] = {"value": 1e3 / float(np.mean(e_ms)), "unit": "steps/s",
-                    "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 3 * n * 8 * 2 + 8 * 7 + 8 * 27}
-    # roofline of the dominant kernel class
+    if run_e2e:
+        run_e2e_loop(extra, eng, s, soa, vel, itime, ne, l2buf, dt)
     peak32 = __import__("ctypes").c_double(0)
     peak64 = __import__("ctypes").c_double(0)
     eng._lib.mdff_gpu_peak_flops(local_rank, 0, __import__("ctypes").byref(peak32))
@@ -382,6 +345,60 @@ def run_ours(args, rank, world, local_rank):
     extra["_cpu_point"] = (soa, hist, itime)
     eng.close()
     return res, extra
+
+
+def check_force_error(extra, s, soa):
+    from mdff_b200 import _abi
+    from mdff_b200.engine import ForceEngine
+    pt = engine_params(s, "fp64", "scf")
+    pt.conv_tol_ind = 1e-11
+    pt.max_scf_pol_iter = 400
+    pt.calc = _abi.CALC_OTHER
+    e3 = ForceEngine(pt, s.cell)
+    ref = e3.engforce(*soa)
+    e3.close()
+    pm = engine_params(s, "mixed", "cg")
+    pm.calc = _abi.CALC_OTHER
+    e4 = ForceEngine(pm, s.cell)
+    mix = e4.engforce(*soa)
+    e4.close()
+    fr = np.stack([ref["fx"], ref["fy"], ref["fz"]], 1)
+    fm = np.stack([mix["fx"], mix["fy"], mix["fz"]], 1)
+    extra["force_err_rms_rel_vs_fp64"] = float(np.sqrt(((fm - fr) ** 2).sum() / (fr ** 2).sum()))
+    extra["dipole_err_rms_rel_vs_fp64"] = float(np.sqrt(((mix["mu"] - ref["mu"]) ** 2).sum()
+                                                        / (ref["mu"] ** 2).sum()))
+    extra["energy_err_rel_vs_fp64"] = abs(mix["u_coul"] + mix["u_bmhft"] - ref["u_coul"]
+                                          - ref["u_bmhft"]) / abs(ref["u_coul"] + ref["u_bmhft"])
+
+
+def run_e2e_loop(extra, eng, s, soa, vel, itime, ne, l2buf, dt):
+    import torch
+    n = s.natm
+    # e2e through the C ABI with pinned host buffers (what a Fortran caller does)
+    rx = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    ry = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    rz = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    v_h = vel.cpu().numpy().copy()
+    rx[:], ry[:], rz[:] = soa
+    invm_h = 1.0 / s.mass
+    r0 = eng.engforce(rx, ry, rz, itime=itime, want_ef=False)
+    f = np.stack([r0["fx"], r0["fy"], r0["fz"]])
+    e_ms = []
+    for k in range(ne):
+        v_h += 0.5 * dt * f * invm_h
+        rx += dt * v_h[0]
+        ry += dt * v_h[1]
+        rz += dt * v_h[2]
+        flush_l2(l2buf)
+        torch.cuda.synchronize()
+        itime += 1
+        r = eng.engforce(rx, ry, rz, itime=itime, want_ef=False)
+        e_ms.append(eng.stats()["ms_last"])
+        f = np.stack([r["fx"], r["fy"], r["fz"]])
+        v_h += 0.5 * dt * f * invm_h
+    extra["e2e"] = {"value": 1e3 / float(np.mean(e_ms)), "unit": "steps/s",
+                    "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 3 * n * 8 * 2 + 8 * 7 + 8 * 27}
+
 
 
 def dist_barrier(world):
@@ -508,8 +525,9 @@ def main():
             "clocks": res["clocks"],
         }
         line.update({k: v for k, v in extra.items() if k not in ("stats", "_cpu_point")})
-        line["speedup_vs_fp64_scf"] = res["value"] / world / extra["fp64_scf_steps_per_s"]
-        line["speedup_vs_fp64_cg"] = res["value"] / world / extra["fp64_cg_steps_per_s"]
+        if "fp64_scf_steps_per_s" in extra:
+            line["speedup_vs_fp64_scf"] = res["value"] / world / extra["fp64_scf_steps_per_s"]
+            line["speedup_vs_fp64_cg"] = res["value"] / world / extra["fp64_cg_steps_per_s"]
         line["roofline"] = roofline_block(res, extra)
         if world == 1 and not args.no_cpu:
             s, _ = make_system(args.workload)

@@ -528,6 +528,10 @@ static PolDev poldev(mdff_ctx* h) { return PolDev{h->d_pol, h->d_invpol, h->d_ip
 // nz tile of the structure factor: the width (8, 11, 13 or 16) that wastes
 // the fewest accumulator slots on rows of nzmax consecutive nz
 static int pick_nzt(int nzmax) {
+  // a whole row in one tile when it fits in 25 accumulators (per-ion set-up
+  // of the phases is then shared by all nz of the row)
+  if (nzmax == 25) return 25;
+  if (nzmax == 21) return 21;
   const int cand[4] = {16, 13, 11, 8};
   int best = 16, waste = 1 << 30;
   for (int c : cand) {
@@ -595,6 +599,8 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
     case 8: launch_rho<R, 8>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
     case 11: launch_rho<R, 11>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
     case 13: launch_rho<R, 13>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+    case 21: launch_rho<R, 21>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+    case 25: launch_rho<R, 25>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
     default: launch_rho<R, 16>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
   }
   LAUNCH_CHECK();

@@ -21,13 +21,12 @@
 #include "pim.cuh"
 #include "realspace.cuh"
 #include "recip.cuh"
+#include "setup.h"
 
 using namespace mdff;
 
 namespace {
 
-constexpr double kCoulUnit = 14.3996441494161;     // constants.f90:91
-constexpr double kPressUnit = 0.00624150964712042; // constants.f90:88
 constexpr int NT = MDFF_NTYPEMAX;
 constexpr int kRhoThreads = 128;
 constexpr int kRhoChunk = 4096;    // ions per structure-factor block
@@ -274,109 +273,28 @@ __global__ void k_vv_kick(double* __restrict__ vel, const double* __restrict__ f
 // ---------------------------------------------------------------------------
 // set-up (host): the reference's *_init routines
 
-// symmetric_pot: X(:,it) = X(it,:) for it = 1..ntype (non_bonded.f90:287-301)
-static void sym2(double X[NT][NT], int ntype) {
-  for (int it = 0; it < ntype; ++it) {
-    double row[NT];
-    for (int k = 0; k < NT; ++k) row[k] = X[it][k];
-    for (int k = 0; k < NT; ++k) X[k][it] = row[k];
-  }
-}
-// pim.f90:189-199: X(it2,:,it) = X(it2,it,:)
-template <typename T>
-static void sym3(T X[NT][NT][NT], int ntype) {
-  for (int it = 0; it < ntype; ++it)
-    for (int it2 = 0; it2 < ntype; ++it2) {
-      T row[NT];
-      for (int k = 0; k < NT; ++k) row[k] = X[it2][it][k];
-      for (int k = 0; k < NT; ++k) X[it2][k][it] = row[k];
-    }
-}
-
-// 3x3 inverse; diagonal tensors are inverted entry by entry with zero
-// entries left zero (a site polarisable along one axis only).
-static bool inv3(const double* m, double* out) {
-  bool diag = m[1] == 0 && m[2] == 0 && m[3] == 0 && m[5] == 0 && m[6] == 0 && m[7] == 0;
-  if (diag) {
-    for (int i = 0; i < 9; ++i) out[i] = 0.0;
-    for (int i = 0; i < 3; ++i) out[4 * i] = m[4 * i] != 0.0 ? 1.0 / m[4 * i] : 0.0;
-    return true;
-  }
-  double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
-               m[2] * (m[3] * m[7] - m[4] * m[6]);
-  if (det == 0.0) return false;
-  out[0] = (m[4] * m[8] - m[5] * m[7]) / det;
-  out[1] = (m[2] * m[7] - m[1] * m[8]) / det;
-  out[2] = (m[1] * m[5] - m[2] * m[4]) / det;
-  out[3] = (m[5] * m[6] - m[3] * m[8]) / det;
-  out[4] = (m[0] * m[8] - m[2] * m[6]) / det;
-  out[5] = (m[2] * m[3] - m[0] * m[5]) / det;
-  out[6] = (m[3] * m[7] - m[4] * m[6]) / det;
-  out[7] = (m[1] * m[6] - m[0] * m[7]) / det;
-  out[8] = (m[0] * m[4] - m[1] * m[3]) / det;
-  return true;
-}
-
 // lattice (lattice.f90:60-130): B = reciprocal / omega, face widths, norms
 static void lattice(mdff_ctx* h, const double* Ain) {
-  double A[3][3], B[3][3];
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) A[a][b] = Ain[3 * a + b];
-  const int cyc[3][2] = {{1, 2}, {2, 0}, {0, 1}};
-  for (int col = 0; col < 3; ++col) {
-    int u = cyc[col][0], v = cyc[col][1];
-    B[0][col] = A[1][u] * A[2][v] - A[2][u] * A[1][v];
-    B[1][col] = A[2][u] * A[0][v] - A[0][u] * A[2][v];
-    B[2][col] = A[0][u] * A[1][v] - A[1][u] * A[0][v];
-  }
-  double omega = B[0][0] * A[0][0] + B[1][0] * A[1][0] + B[2][0] * A[2][0];
-  for (int c = 0; c < 3; ++c)
-    h->W[c] = omega / std::sqrt(B[0][c] * B[0][c] + B[1][c] * B[1][c] + B[2][c] * B[2][c]);
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) B[i][j] = B[i][j] / omega;
-  for (int i = 0; i < 3; ++i)
-    h->ANORM[i] = std::sqrt(A[0][i] * A[0][i] + A[1][i] * A[1][i] + A[2][i] * A[2][i]);
-  h->omega = omega;
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b) {
-      h->A[3 * a + b] = A[a][b];
-      h->B[3 * a + b] = B[a][b];
-    }
+  Lattice L;
+  lattice_of(Ain, L);
+  memcpy(h->A, L.A, sizeof(L.A));
+  memcpy(h->B, L.B, sizeof(L.B));
+  memcpy(h->W, L.W, sizeof(L.W));
+  memcpy(h->ANORM, L.ANORM, sizeof(L.ANORM));
+  h->omega = L.omega;
 }
 
 // k mesh as rows (nx, ny) of consecutive nz (kspace.f90:143-207, same
 // half-space; the reference's |k|^2 order only changes summation order)
 static int build_mesh(mdff_ctx* h) {
   h->gen++;
-  int kx = h->p.kES[0], ky = h->p.kES[1], kz = h->p.kES[2];
-  h->rows.clear();
-  int koff = 0;
-  for (int nx = 0; nx <= kx; ++nx) {
-    int nymin = (nx == 0) ? 0 : -ky;
-    for (int ny = nymin; ny <= ky; ++ny) {
-      int nzlo = (nx == 0 && ny == 0) ? 1 : -kz;
-      if (nzlo > kz) continue;
-      h->rows.push_back(make_int4(nx, ny, nzlo, koff));
-      koff += kz - nzlo + 1;
-    }
-  }
-  h->nk = koff;
+  KMesh KM;
+  kmesh_of(h->p.kES, h->B, h->p.alphaES, KM);
+  h->rows = KM.rows;
+  h->nk = KM.nk;
   int nk = h->nk;
-  std::vector<double> Ak(std::max(nk, 1));
-  std::vector<double4> kv(std::max(nk, 1));
-  double alpha2 = h->p.alphaES * h->p.alphaES;
-  const double* B = h->B;
-  for (auto& r : h->rows)
-    for (int nz = r.z; nz <= kz; ++nz) {
-      int k = r.w + nz - r.z;
-      double X = r.x, Y = r.y, Z = nz;
-      double kxx = kTwoPi * (X * B[0] + Y * B[1] + Z * B[2]);
-      double kyy = kTwoPi * (X * B[3] + Y * B[4] + Z * B[5]);
-      double kzz = kTwoPi * (X * B[6] + Y * B[7] + Z * B[8]);
-      double kk = kxx * kxx + kyy * kyy + kzz * kzz;
-      Ak[k] = std::exp(-kk * 0.25 / alpha2) / kk;
-      kv[k] = make_double4(kxx, kyy, kzz, 2.0 * (1.0 / kk + 1.0 / alpha2 / 4.0));
-    }
+  const std::vector<double>& Ak = KM.Ak;
+  const std::vector<double4>& kv = KM.kv;
   // k chunks of the field pass: enough blocks to fill 148 SMs several times,
   // at most 2048 k (32 KB of rho') per chunk
   int nrows = (int)h->rows.size();
@@ -1171,83 +1089,27 @@ const char* mdff_gpu_strerror(int s) {
 const char* mdff_gpu_last_error(mdff_handle h) { return h ? h->err.c_str() : g_err.c_str(); }
 
 static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA) {
-  h->p = *pin;
+  Setup S;
+  const char* serr = nullptr;
+  int s0 = setup_system(pin, cellA, S, &serr);
+  if (s0) {
+    h->err = serr;
+    return s0;
+  }
+  h->p = S.p;
   mdff_params& p = h->p;
-  if (p.natm <= 0 || p.ntype <= 0 || p.ntype > NT) {
-    h->err = "natm/ntype out of range";
-    return MDFF_ERR_BAD_ARGS;
-  }
-  long tot = 0;
-  for (int it = 0; it < p.ntype; ++it) tot += p.natmi[it];
-  if (tot != p.natm) {
-    h->err = "sum(natmi) != natm";
-    return MDFF_ERR_BAD_ARGS;
-  }
-  if (p.extrapolate_order < 0 || p.extrapolate_order > 4) {
-    h->err = "extrapolate_order must be 0..4 (moment_from_pola.f90:524-527)";
-    return MDFF_ERR_BAD_ARGS;
-  }
   h->natm = p.natm;
   h->ntype = p.ntype;
   int ntype = p.ntype, n = p.natm;
-  // symmetrisation (non_bonded_check_tag, pim_check_tag)
-  if (p.symmetric_pot_nb) {
-    sym2(p.epslj, ntype); sym2(p.sigmalj, ntype); sym2(p.plj, ntype); sym2(p.qlj, ntype);
-    sym2(p.Abmhftd, ntype); sym2(p.Bbmhftd, ntype); sym2(p.Cbmhftd, ntype);
-    sym2(p.Dbmhftd, ntype); sym2(p.BDbmhftd, ntype); sym2(p.wall24, ntype);
-  }
-  if (p.symmetric_pot_pim) {
-    sym3(p.ldip_damping, ntype); sym3(p.pol_damp_b, ntype);
-    sym3(p.pol_damp_c, ntype); sym3(p.pol_damp_k, ntype);
-  }
-  for (int a = 0; a < NT; ++a)
-    for (int b = 0; b < NT; ++b)
-      for (int c = 0; c < NT; ++c)
-        if (p.pol_damp_k[a][b][c] < 0 || p.pol_damp_k[a][b][c] > MDFF_TT_MAX) {
-          h->err = "pol_damp_k beyond the Tang-Toennies table (pim.f90:201-204)";
-          return MDFF_ERR_BAD_ARGS;
-        }
-  h->coul_unit = p.lreduced ? 1.0 : kCoulUnit;
-  h->press_unit = p.lreduced ? 1.0 : kPressUnit;
-  h->lsr = (p.lbmhft || p.lbmhftd || p.lnmlj) ? 1 : 0;
-  // tasks (coulomb.f90:204-220, pim.f90:160-184)
-  int lqch = 0, ldip = 0, lpol = 0;
-  for (int it = 0; it < NT; ++it) {
-    if (p.qch[it] != 0.0) lqch = 1;
-    for (int a = 0; a < 3; ++a)
-      if (p.dip[it][a] != 0.0) ldip = 1;
-  }
-  for (int it = 0; it < ntype; ++it)
-    if (p.ldip_polar[it]) lpol = 1;
-  h->task_qq = lqch;
-  h->task_qd = lqch && (ldip || lpol);
-  h->task_dd = (ldip || lpol);
-  h->lpolar = lpol && p.lcoulomb;
-  h->ldip_static = ldip;
+  h->coul_unit = S.coul_unit;
+  h->press_unit = S.press_unit;
+  h->lsr = S.lsr;
+  h->task_qq = S.task_qq;
+  h->task_qd = S.task_qd;
+  h->task_dd = S.task_dd;
+  h->lpolar = S.lpolar;
+  h->ldip_static = S.ldip_static;
   lattice(h, cellA);
-  // ewald_param (coulomb.f90:363-410): clamp the real-space cutoff, lautoES
-  if (p.lcoulomb) {
-    double rcut = 0.5 * std::min(h->W[0], std::min(h->W[1], h->W[2]));
-    p.cutlongrange = std::min(p.cutlongrange, rcut);
-    double cut = p.cutlongrange;
-    double eps = std::min(std::fabs(p.epsw), 0.5);
-    double tol = std::sqrt(std::fabs(std::log(eps * cut)));
-    double alpha = std::sqrt(std::fabs(std::log(eps * cut * tol))) / cut;
-    double tol1 = std::sqrt(-std::log(eps * cut * (2.0 * tol * alpha) * (2.0 * tol * alpha)));
-    if (p.lautoES) {
-      p.alphaES = alpha;
-      for (int i = 0; i < 3; ++i) p.kES[i] = (int)std::round(0.25 + h->ANORM[i] * alpha * tol1 / kPi);
-    }
-    if (p.cutlongrange <= 0.0 || p.alphaES <= 0.0) {
-      h->err = "cutlongrange and alphaES must be positive";
-      return MDFF_ERR_BAD_ARGS;
-    }
-    for (int i = 0; i < 3; ++i)
-      if (p.kES[i] < 0) {
-        h->err = "kES must be >= 0";
-        return MDFF_ERR_BAD_ARGS;
-      }
-  }
   h->stats.alphaES = p.alphaES;
   for (int i = 0; i < 3; ++i) h->stats.kES[i] = p.kES[i];
   h->stats.cutlongrange = p.cutlongrange;
@@ -1262,29 +1124,7 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
   CK(cudaEventCreate(&h->ev0));
   CK(cudaEventCreate(&h->ev1));
-  // per-ion tables (typeinfo_init, read_pos.f90:160-237)
-  std::vector<int> itype(n), ipol(n);
-  std::vector<double> q(n), pol(9 * (size_t)n, 0.0), inv(9 * (size_t)n, 0.0);
-  std::vector<double4> dip(n);
-  int ia = 0;
-  h->npol = 0;
-  for (int it = 0; it < ntype; ++it) {
-    double iv[9] = {0};
-    if (p.ldip_polar[it] && !inv3(&p.poldip[it][0][0], iv)) {
-      h->err = "singular polarisability tensor";
-      return MDFF_ERR_BAD_ARGS;
-    }
-    for (int k = 0; k < p.natmi[it]; ++k, ++ia) {
-      itype[ia] = it;
-      ipol[ia] = p.ldip_polar[it] ? 1 : 0;
-      h->npol += ipol[ia];
-      q[ia] = p.qch[it];
-      dip[ia] = make_double4(p.dip[it][0], p.dip[it][1], p.dip[it][2], 0.0);
-      for (int a = 0; a < 9; ++a) pol[9 * (size_t)ia + a] = (&p.poldip[it][0][0])[a];
-      if (p.ldip_polar[it])
-        for (int a = 0; a < 9; ++a) inv[9 * (size_t)ia + a] = iv[a];
-    }
-  }
+  h->npol = S.npol;
   DALLOC(h->d_cell, 1);
   DALLOC(h->d_pos, 3 * (size_t)n);
   DALLOC(h->d_s, n);
@@ -1295,47 +1135,14 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_dipia, n);
   DALLOC(h->d_pol, 9 * (size_t)n);
   DALLOC(h->d_invpol, 9 * (size_t)n);
-  CK(cudaMemcpyAsync(h->d_itype, itype.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(h->d_ipolar, ipol.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(h->d_q, q.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(h->d_dipia, dip.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(h->d_pol, pol.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, h->st));
-  CK(cudaMemcpyAsync(h->d_invpol, inv.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, h->st));
-  // pair tables (initialize_param_non_bonded, non_bonded.f90:455-644)
-  std::vector<NBPair> nb(ntype * ntype);
-  std::vector<ESPair> es(ntype * ntype);
-  double two16 = std::pow(2.0, 1.0 / 6.0);
-  for (int it = 0; it < ntype; ++it)
-    for (int jt = 0; jt < ntype; ++jt) {
-      NBPair& P = nb[it * ntype + jt];
-      P.A = p.Abmhftd[it][jt];
-      P.B = p.Bbmhftd[it][jt];
-      P.C = p.Cbmhftd[it][jt];
-      P.D = p.Dbmhftd[it][jt];
-      P.BD = p.BDbmhftd[it][jt];
-      P.wall = p.wall24[it][jt];
-      P.rcutsq = p.cutshortrange * p.cutshortrange;
-      double pp = p.plj[it][jt], qq = p.qlj[it][jt];
-      P.plj = pp;
-      P.qlj = qq;
-      P.epsp = p.epslj[it][jt] / (qq - pp);
-      P.sigsq = two16 * two16 * p.sigmalj[it][jt] * p.sigmalj[it][jt];
-      double sr = std::sqrt(P.sigsq / P.rcutsq);
-      double srp = std::pow(sr, pp), srq = std::pow(sr, qq);
-      P.uc = P.epsp * (pp * srq - qq * srp);
-      P.uc1 = P.epsp * pp * qq / (2.0 * P.rcutsq) * (srq - srp);
-      P.uc2 = 0.5 * P.epsp * ((2.0 * pp + pp * qq) * srq - (2.0 * qq + pp * qq) * srp);
-      P.fc = pp * qq * P.epsp / P.sigsq;
-      ESPair& E = es[it * ntype + jt];  // it = ta ("ia"), jt = tb ("ja")
-      E.ldamp = (p.ldip_damping[it][it][jt] || p.ldip_damping[jt][it][jt]) ? 1 : 0;
-      E.ka = p.pol_damp_k[it][it][jt];
-      E.ba = p.pol_damp_b[it][it][jt];
-      E.ca = p.pol_damp_c[it][it][jt];
-      E.kb = p.pol_damp_k[jt][it][jt];
-      E.bb = p.pol_damp_b[jt][it][jt];
-      E.cb = p.pol_damp_c[jt][it][jt];
-      E.pad = 0;
-    }
+  CK(cudaMemcpyAsync(h->d_itype, S.itype.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->d_ipolar, S.ipol.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->d_q, S.q.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->d_dipia, S.dip.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->d_pol, S.pol.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, h->st));
+  CK(cudaMemcpyAsync(h->d_invpol, S.inv.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, h->st));
+  const std::vector<NBPair>& nb = S.nb;
+  const std::vector<ESPair>& es = S.es;
   DALLOC(h->d_nbtab, nb.size());
   DALLOC(h->d_estab, es.size());
   CK(cudaMemcpyAsync(h->d_nbtab, nb.data(), sizeof(NBPair) * nb.size(), cudaMemcpyHostToDevice, h->st));

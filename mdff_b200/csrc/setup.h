@@ -1,0 +1,297 @@
+// setup.h -- host-side set-up shared by the single-configuration engine and
+// the batched engine: the reference's *_init routines that turn the control
+// keywords and the cell into the per-ion and per-pair tables the kernels read.
+//
+//  * symmetrisation of the pair / triple tables (non_bonded.f90:287-301,
+//    pim.f90:189-199)
+//  * lattice (lattice.f90:60-130): B = reciprocal / omega, face widths, norms
+//  * tasks (coulomb.f90:204-220, pim.f90:160-184)
+//  * ewald_param (coulomb.f90:363-410): real-space cutoff clamp, lautoES
+//  * typeinfo_init (read_pos.f90:160-237): per-ion charge, dipole, alpha, 1/alpha
+//  * initialize_param_non_bonded (non_bonded.f90:455-644): pair tables
+//  * kpoint_sum_init (kspace.f90:143-207): the half-space k mesh as rows
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "../../include/mdff_gpu.h"
+#include "common.cuh"
+#include "realspace.cuh"
+
+namespace mdff {
+
+constexpr double kCoulUnit = 14.3996441494161;      // constants.f90:91
+constexpr double kPressUnit = 0.00624150964712042;  // constants.f90:88
+constexpr int kNT = MDFF_NTYPEMAX;
+
+// symmetric_pot: X(:,it) = X(it,:) for it = 1..ntype (non_bonded.f90:287-301)
+inline void sym2(double X[kNT][kNT], int ntype) {
+  for (int it = 0; it < ntype; ++it) {
+    double row[kNT];
+    for (int k = 0; k < kNT; ++k) row[k] = X[it][k];
+    for (int k = 0; k < kNT; ++k) X[k][it] = row[k];
+  }
+}
+// pim.f90:189-199: X(it2,:,it) = X(it2,it,:)
+template <typename T>
+inline void sym3(T X[kNT][kNT][kNT], int ntype) {
+  for (int it = 0; it < ntype; ++it)
+    for (int it2 = 0; it2 < ntype; ++it2) {
+      T row[kNT];
+      for (int k = 0; k < kNT; ++k) row[k] = X[it2][it][k];
+      for (int k = 0; k < kNT; ++k) X[it2][k][it] = row[k];
+    }
+}
+
+// 3x3 inverse; diagonal tensors are inverted entry by entry with zero
+// entries left zero (a site polarisable along one axis only).
+inline bool inv3(const double* m, double* out) {
+  bool diag = m[1] == 0 && m[2] == 0 && m[3] == 0 && m[5] == 0 && m[6] == 0 && m[7] == 0;
+  if (diag) {
+    for (int i = 0; i < 9; ++i) out[i] = 0.0;
+    for (int i = 0; i < 3; ++i) out[4 * i] = m[4 * i] != 0.0 ? 1.0 / m[4 * i] : 0.0;
+    return true;
+  }
+  double det = m[0] * (m[4] * m[8] - m[5] * m[7]) - m[1] * (m[3] * m[8] - m[5] * m[6]) +
+               m[2] * (m[3] * m[7] - m[4] * m[6]);
+  if (det == 0.0) return false;
+  out[0] = (m[4] * m[8] - m[5] * m[7]) / det;
+  out[1] = (m[2] * m[7] - m[1] * m[8]) / det;
+  out[2] = (m[1] * m[5] - m[2] * m[4]) / det;
+  out[3] = (m[5] * m[6] - m[3] * m[8]) / det;
+  out[4] = (m[0] * m[8] - m[2] * m[6]) / det;
+  out[5] = (m[2] * m[3] - m[0] * m[5]) / det;
+  out[6] = (m[3] * m[7] - m[4] * m[6]) / det;
+  out[7] = (m[1] * m[6] - m[0] * m[7]) / det;
+  out[8] = (m[0] * m[4] - m[1] * m[3]) / det;
+  return true;
+}
+
+struct Lattice {
+  double A[9], B[9];  // row-major [a][b]; B = reciprocal vectors / omega
+  double omega, W[3], ANORM[3];
+};
+
+// lattice (lattice.f90:60-130)
+inline void lattice_of(const double* Ain, Lattice& L) {
+  double A[3][3], B[3][3];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) A[a][b] = Ain[3 * a + b];
+  const int cyc[3][2] = {{1, 2}, {2, 0}, {0, 1}};
+  for (int col = 0; col < 3; ++col) {
+    int u = cyc[col][0], v = cyc[col][1];
+    B[0][col] = A[1][u] * A[2][v] - A[2][u] * A[1][v];
+    B[1][col] = A[2][u] * A[0][v] - A[0][u] * A[2][v];
+    B[2][col] = A[0][u] * A[1][v] - A[1][u] * A[0][v];
+  }
+  double omega = B[0][0] * A[0][0] + B[1][0] * A[1][0] + B[2][0] * A[2][0];
+  for (int c = 0; c < 3; ++c)
+    L.W[c] = omega / std::sqrt(B[0][c] * B[0][c] + B[1][c] * B[1][c] + B[2][c] * B[2][c]);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) B[i][j] = B[i][j] / omega;
+  for (int i = 0; i < 3; ++i)
+    L.ANORM[i] = std::sqrt(A[0][i] * A[0][i] + A[1][i] * A[1][i] + A[2][i] * A[2][i]);
+  L.omega = omega;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      L.A[3 * a + b] = A[a][b];
+      L.B[3 * a + b] = B[a][b];
+    }
+}
+
+struct Setup {
+  mdff_params p;  // after symmetrisation, cutoff clamp and lautoES
+  Lattice L;
+  double coul_unit = 0, press_unit = 0;
+  int lsr = 0, task_qq = 0, task_qd = 0, task_dd = 0, lpolar = 0, ldip_static = 0, npol = 0;
+  std::vector<int> itype, ipol;
+  std::vector<double> q, pol, inv;  // pol / inv: [natm][9]
+  std::vector<double4> dip;
+  std::vector<NBPair> nb;  // [ntype][ntype]
+  std::vector<ESPair> es;  // [ta][tb]
+};
+
+// Everything of the reference's set-up that needs no device.  Returns
+// MDFF_OK, or MDFF_ERR_BAD_ARGS with *err set.
+inline int setup_system(const mdff_params* pin, const double* cellA, Setup& S, const char** err) {
+  S.p = *pin;
+  mdff_params& p = S.p;
+  if (p.natm <= 0 || p.ntype <= 0 || p.ntype > kNT) {
+    *err = "natm/ntype out of range";
+    return MDFF_ERR_BAD_ARGS;
+  }
+  long tot = 0;
+  for (int it = 0; it < p.ntype; ++it) tot += p.natmi[it];
+  if (tot != p.natm) {
+    *err = "sum(natmi) != natm";
+    return MDFF_ERR_BAD_ARGS;
+  }
+  if (p.extrapolate_order < 0 || p.extrapolate_order > 4) {
+    *err = "extrapolate_order must be 0..4 (moment_from_pola.f90:524-527)";
+    return MDFF_ERR_BAD_ARGS;
+  }
+  int ntype = p.ntype, n = p.natm;
+  if (p.symmetric_pot_nb) {
+    sym2(p.epslj, ntype); sym2(p.sigmalj, ntype); sym2(p.plj, ntype); sym2(p.qlj, ntype);
+    sym2(p.Abmhftd, ntype); sym2(p.Bbmhftd, ntype); sym2(p.Cbmhftd, ntype);
+    sym2(p.Dbmhftd, ntype); sym2(p.BDbmhftd, ntype); sym2(p.wall24, ntype);
+  }
+  if (p.symmetric_pot_pim) {
+    sym3(p.ldip_damping, ntype); sym3(p.pol_damp_b, ntype);
+    sym3(p.pol_damp_c, ntype); sym3(p.pol_damp_k, ntype);
+  }
+  for (int a = 0; a < kNT; ++a)
+    for (int b = 0; b < kNT; ++b)
+      for (int c = 0; c < kNT; ++c)
+        if (p.pol_damp_k[a][b][c] < 0 || p.pol_damp_k[a][b][c] > MDFF_TT_MAX) {
+          *err = "pol_damp_k beyond the Tang-Toennies table (pim.f90:201-204)";
+          return MDFF_ERR_BAD_ARGS;
+        }
+  S.coul_unit = p.lreduced ? 1.0 : kCoulUnit;
+  S.press_unit = p.lreduced ? 1.0 : kPressUnit;
+  S.lsr = (p.lbmhft || p.lbmhftd || p.lnmlj) ? 1 : 0;
+  int lqch = 0, ldip = 0, lpol = 0;
+  for (int it = 0; it < kNT; ++it) {
+    if (p.qch[it] != 0.0) lqch = 1;
+    for (int a = 0; a < 3; ++a)
+      if (p.dip[it][a] != 0.0) ldip = 1;
+  }
+  for (int it = 0; it < ntype; ++it)
+    if (p.ldip_polar[it]) lpol = 1;
+  S.task_qq = lqch;
+  S.task_qd = lqch && (ldip || lpol);
+  S.task_dd = (ldip || lpol);
+  S.lpolar = lpol && p.lcoulomb;
+  S.ldip_static = ldip;
+  lattice_of(cellA, S.L);
+  if (p.lcoulomb) {
+    double rcut = 0.5 * std::min(S.L.W[0], std::min(S.L.W[1], S.L.W[2]));
+    p.cutlongrange = std::min(p.cutlongrange, rcut);
+    double cut = p.cutlongrange;
+    double eps = std::min(std::fabs(p.epsw), 0.5);
+    double tol = std::sqrt(std::fabs(std::log(eps * cut)));
+    double alpha = std::sqrt(std::fabs(std::log(eps * cut * tol))) / cut;
+    double tol1 = std::sqrt(-std::log(eps * cut * (2.0 * tol * alpha) * (2.0 * tol * alpha)));
+    if (p.lautoES) {
+      p.alphaES = alpha;
+      for (int i = 0; i < 3; ++i)
+        p.kES[i] = (int)std::round(0.25 + S.L.ANORM[i] * alpha * tol1 / kPi);
+    }
+    if (p.cutlongrange <= 0.0 || p.alphaES <= 0.0) {
+      *err = "cutlongrange and alphaES must be positive";
+      return MDFF_ERR_BAD_ARGS;
+    }
+    for (int i = 0; i < 3; ++i)
+      if (p.kES[i] < 0) {
+        *err = "kES must be >= 0";
+        return MDFF_ERR_BAD_ARGS;
+      }
+  }
+  // per-ion tables
+  S.itype.assign(n, 0);
+  S.ipol.assign(n, 0);
+  S.q.assign(n, 0.0);
+  S.pol.assign(9 * (size_t)n, 0.0);
+  S.inv.assign(9 * (size_t)n, 0.0);
+  S.dip.assign(n, make_double4(0, 0, 0, 0));
+  int ia = 0;
+  S.npol = 0;
+  for (int it = 0; it < ntype; ++it) {
+    double iv[9] = {0};
+    if (p.ldip_polar[it] && !inv3(&p.poldip[it][0][0], iv)) {
+      *err = "singular polarisability tensor";
+      return MDFF_ERR_BAD_ARGS;
+    }
+    for (int k = 0; k < p.natmi[it]; ++k, ++ia) {
+      S.itype[ia] = it;
+      S.ipol[ia] = p.ldip_polar[it] ? 1 : 0;
+      S.npol += S.ipol[ia];
+      S.q[ia] = p.qch[it];
+      S.dip[ia] = make_double4(p.dip[it][0], p.dip[it][1], p.dip[it][2], 0.0);
+      for (int a = 0; a < 9; ++a) S.pol[9 * (size_t)ia + a] = (&p.poldip[it][0][0])[a];
+      if (p.ldip_polar[it])
+        for (int a = 0; a < 9; ++a) S.inv[9 * (size_t)ia + a] = iv[a];
+    }
+  }
+  // pair tables
+  S.nb.assign(ntype * ntype, NBPair{});
+  S.es.assign(ntype * ntype, ESPair{});
+  double two16 = std::pow(2.0, 1.0 / 6.0);
+  for (int it = 0; it < ntype; ++it)
+    for (int jt = 0; jt < ntype; ++jt) {
+      NBPair& P = S.nb[it * ntype + jt];
+      P.A = p.Abmhftd[it][jt];
+      P.B = p.Bbmhftd[it][jt];
+      P.C = p.Cbmhftd[it][jt];
+      P.D = p.Dbmhftd[it][jt];
+      P.BD = p.BDbmhftd[it][jt];
+      P.wall = p.wall24[it][jt];
+      P.rcutsq = p.cutshortrange * p.cutshortrange;
+      double pp = p.plj[it][jt], qq = p.qlj[it][jt];
+      P.plj = pp;
+      P.qlj = qq;
+      P.epsp = p.epslj[it][jt] / (qq - pp);
+      P.sigsq = two16 * two16 * p.sigmalj[it][jt] * p.sigmalj[it][jt];
+      double sr = std::sqrt(P.sigsq / P.rcutsq);
+      double srp = std::pow(sr, pp), srq = std::pow(sr, qq);
+      P.uc = P.epsp * (pp * srq - qq * srp);
+      P.uc1 = P.epsp * pp * qq / (2.0 * P.rcutsq) * (srq - srp);
+      P.uc2 = 0.5 * P.epsp * ((2.0 * pp + pp * qq) * srq - (2.0 * qq + pp * qq) * srp);
+      P.fc = pp * qq * P.epsp / P.sigsq;
+      ESPair& E = S.es[it * ntype + jt];  // it = ta ("ia"), jt = tb ("ja")
+      E.ldamp = (p.ldip_damping[it][it][jt] || p.ldip_damping[jt][it][jt]) ? 1 : 0;
+      E.ka = p.pol_damp_k[it][it][jt];
+      E.ba = p.pol_damp_b[it][it][jt];
+      E.ca = p.pol_damp_c[it][it][jt];
+      E.kb = p.pol_damp_k[jt][it][jt];
+      E.bb = p.pol_damp_b[jt][it][jt];
+      E.cb = p.pol_damp_c[jt][it][jt];
+      E.pad = 0;
+    }
+  return MDFF_OK;
+}
+
+// The half-space k mesh (kspace.f90:143-207) as rows (nx, ny, nz_lo, koff)
+// of consecutive nz; A_k = e^{-k^2/4 alpha^2}/k^2 and (k, kcoe) per k.  The
+// reference's |k|^2 order only changes the summation order.
+struct KMesh {
+  std::vector<int4> rows;
+  std::vector<double> Ak;
+  std::vector<double4> kv;
+  int nk = 0;
+};
+
+inline void kmesh_of(const int kES[3], const double* B, double alphaES, KMesh& M) {
+  int kx = kES[0], ky = kES[1], kz = kES[2];
+  M.rows.clear();
+  int koff = 0;
+  for (int nx = 0; nx <= kx; ++nx) {
+    int nymin = (nx == 0) ? 0 : -ky;
+    for (int ny = nymin; ny <= ky; ++ny) {
+      int nzlo = (nx == 0 && ny == 0) ? 1 : -kz;
+      if (nzlo > kz) continue;
+      M.rows.push_back(make_int4(nx, ny, nzlo, koff));
+      koff += kz - nzlo + 1;
+    }
+  }
+  M.nk = koff;
+  M.Ak.assign(std::max(koff, 1), 0.0);
+  M.kv.assign(std::max(koff, 1), make_double4(0, 0, 0, 0));
+  double alpha2 = alphaES * alphaES;
+  for (auto& r : M.rows)
+    for (int nz = r.z; nz <= kz; ++nz) {
+      int k = r.w + nz - r.z;
+      double X = r.x, Y = r.y, Z = nz;
+      double kxx = kTwoPi * (X * B[0] + Y * B[1] + Z * B[2]);
+      double kyy = kTwoPi * (X * B[3] + Y * B[4] + Z * B[5]);
+      double kzz = kTwoPi * (X * B[6] + Y * B[7] + Z * B[8]);
+      double kk = kxx * kxx + kyy * kyy + kzz * kzz;
+      M.Ak[k] = std::exp(-kk * 0.25 / alpha2) / kk;
+      M.kv[k] = make_double4(kxx, kyy, kzz, 2.0 * (1.0 / kk + 1.0 / alpha2 / 4.0));
+    }
+}
+
+}  // namespace mdff

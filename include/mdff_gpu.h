@@ -248,6 +248,67 @@ int mdff_gpu_peak_flops(int device, int fp64, double* tflops);
 
 void mdff_gpu_destroy(mdff_handle h);
 
+/* ---- batched evaluation ------------------------------------------------------
+   No counterpart in the reference, which evaluates one configuration per
+   engforce call.  Many independent configurations (each its own cell, ion
+   count and composition; up to MDFF_BATCH_MAXTYPES types and
+   MDFF_BATCH_MAXATM ions) are evaluated by one persistent kernel launched
+   through a CUDA graph: one thread-block cluster per configuration, taken from
+   a device queue in descending cost order.  Each configuration is one
+   engforce (engforce_driver.f90:102-190) with calc = 'other' (no ASPC
+   history): forces, energies, stress, dipoles and fields, the dipoles from PCG
+   (cg_tol, else conv_tol_ind; cg_max_iter).  precision of parameter set 0
+   selects FP64 or mixed for the whole batch.  The real-space pairs are all
+   minimum-image pairs within the cutoffs (the Verlet list's pair set). */
+#define MDFF_BATCH_MAXTYPES 4
+#define MDFF_BATCH_MAXATM 2048
+
+typedef struct mdff_batch* mdff_batch_handle;
+
+typedef struct mdff_batch_desc {
+  int nconf;
+  const int* pset;            /* [nconf] parameter set of each configuration       */
+  const int* natmi;           /* [nconf][MDFF_NTYPEMAX] ions per type (grouped)     */
+  const double* cell_A;       /* [nconf][9] simu_cell%A, row-major as in create     */
+} mdff_batch_desc;
+
+/* per-configuration outputs (the mdff_result scalars plus solver and set-up
+   figures) */
+typedef struct mdff_batch_conf {
+  double u_lj, vir_lj, u_bmhft, vir_bmhft, u_coul, u_pol, pvirial_coul;
+  double tau_nonb[3][3], tau_coul[3][3], tau[3][3];
+  double rmsd;                /* final dipole residual (e/A^2)                      */
+  int n_pol_iter, converged, catastrophe, nk;
+  double alphaES, cutlongrange;
+  int kES[3], pad;
+} mdff_batch_conf;
+
+/* psets[npsets]: parameter sets (natm / natmi of a set are ignored: each
+   configuration takes them from desc).  Positions of configuration c occupy
+   entries off_c .. off_c + natm_c - 1 of the concatenated arrays, off_c =
+   sum of the earlier configurations' ion counts. */
+int mdff_gpu_batch_create(const mdff_params* psets, int npsets, const mdff_batch_desc* desc,
+                          mdff_batch_handle* out);
+/* host arrays rx, ry, rz [ntot]; fx, fy, fz [ntot] (required); mu, ef
+   [ntot][3] (optional); conf [nconf] (optional) */
+int mdff_gpu_batch_engforce(mdff_batch_handle h, const double* rx, const double* ry,
+                            const double* rz, double* fx, double* fy, double* fz, double* mu,
+                            double* ef, mdff_batch_conf* conf);
+/* device arrays: d_pos, d_force SoA [3][ntot]; d_mu, d_ef [ntot][3] (optional);
+   conf (host, optional) */
+int mdff_gpu_batch_engforce_device(mdff_batch_handle h, const double* d_pos, double* d_force,
+                                   double* d_mu, double* d_ef, mdff_batch_conf* conf);
+/* Autotuner: times every launch shape (cluster size x threads per CTA) on the
+   positions of the last call and keeps the fastest; returns it and its time. */
+int mdff_gpu_batch_tune(mdff_batch_handle h, int* cluster, int* threads, double* ms);
+/* force a launch shape (cluster 1, 2, 4 or 8; threads 256 or 512) */
+int mdff_gpu_batch_set_shape(mdff_batch_handle h, int cluster, int threads);
+/* ntot, nconf, the launch shape and the device time of the last call */
+int mdff_gpu_batch_info(mdff_batch_handle h, int* ntot, int* nconf, int* cluster, int* threads,
+                        double* ms_last);
+const char* mdff_gpu_batch_last_error(mdff_batch_handle h);
+void mdff_gpu_batch_destroy(mdff_batch_handle h);
+
 #ifdef __cplusplus
 }
 #endif

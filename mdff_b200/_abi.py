@@ -82,6 +82,25 @@ class MdffStats(ctypes.Structure):
     ]
 
 
+BATCH_MAXTYPES = 4
+BATCH_MAXATM = 2048
+
+
+class MdffBatchDesc(ctypes.Structure):
+    _fields_ = [("nconf", _i), ("pset", ctypes.POINTER(_i)), ("natmi", ctypes.POINTER(_i)),
+                ("cell_A", ctypes.POINTER(_d))]
+
+
+class MdffBatchConf(ctypes.Structure):
+    _fields_ = [
+        ("u_lj", _d), ("vir_lj", _d), ("u_bmhft", _d), ("vir_bmhft", _d),
+        ("u_coul", _d), ("u_pol", _d), ("pvirial_coul", _d),
+        ("tau_nonb", (_d * 3) * 3), ("tau_coul", (_d * 3) * 3), ("tau", (_d * 3) * 3),
+        ("rmsd", _d), ("n_pol_iter", _i), ("converged", _i), ("catastrophe", _i), ("nk", _i),
+        ("alphaES", _d), ("cutlongrange", _d), ("kES", _i * 3), ("pad", _i),
+    ]
+
+
 # every symbol include/mdff_gpu.h declares, with its ctypes signature
 _P = ctypes.c_void_p
 _DP = ctypes.POINTER(_d)
@@ -106,6 +125,16 @@ SIGNATURES = {
     "mdff_gpu_kernel_times": (_i, [_P, _DP, ctypes.POINTER(ctypes.c_longlong), _DP]),
     "mdff_gpu_peak_flops": (_i, [_i, _i, _DP]),
     "mdff_gpu_destroy": (None, [_P]),
+    "mdff_gpu_batch_create": (_i, [ctypes.POINTER(MdffParams), _i, ctypes.POINTER(MdffBatchDesc),
+                                   ctypes.POINTER(_P)]),
+    "mdff_gpu_batch_engforce": (_i, [_P, _DP, _DP, _DP, _DP, _DP, _DP, _DP, _DP,
+                                     ctypes.POINTER(MdffBatchConf)]),
+    "mdff_gpu_batch_engforce_device": (_i, [_P, _P, _P, _P, _P, ctypes.POINTER(MdffBatchConf)]),
+    "mdff_gpu_batch_tune": (_i, [_P, _IP, _IP, _DP]),
+    "mdff_gpu_batch_set_shape": (_i, [_P, _i, _i]),
+    "mdff_gpu_batch_info": (_i, [_P, _IP, _IP, _IP, _IP, _DP]),
+    "mdff_gpu_batch_last_error": (ctypes.c_char_p, [_P]),
+    "mdff_gpu_batch_destroy": (None, [_P]),
 }
 
 _HERE = os.path.dirname(os.path.abspath(__file__))

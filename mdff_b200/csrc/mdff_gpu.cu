@@ -980,64 +980,7 @@ static void call_end(mdff_ctx* h) {
 // host scalars of the last call into *out (ewald.f90:228-246,
 // engforce_driver.f90:116-177, non_bonded.f90:1201-1205)
 static void fill_scalars(mdff_ctx* h, mdff_result* out) {
-  const double* sc = h->h_scal;
-  double inv_om = 1.0 / h->omega;
-  out->u_lj = out->vir_lj = out->u_bmhft = out->vir_bmhft = 0.0;
-  out->u_coul = out->u_pol = out->pvirial_coul = 0.0;
-  double tn[3][3] = {{0}}, tc[3][3] = {{0}}, t[3][3] = {{0}};
-  auto put6 = [](double m[3][3], const double* v, double f) {
-    m[0][0] = v[0] * f;
-    m[1][1] = v[1] * f;
-    m[2][2] = v[2] * f;
-    m[0][1] = m[1][0] = v[3] * f;
-    m[0][2] = m[2][0] = v[4] * f;
-    m[1][2] = m[2][1] = v[5] * f;
-  };
-  if (h->lsr) {
-    double f = inv_om / h->press_unit * 0.5;
-    if (h->p.lnmlj) {
-      out->u_lj = sc[S_SR + 2];
-      out->vir_lj = sc[S_SR + 3] / 3.0;
-      put6(tn, sc + S_SR + 10, f);
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) t[a][b] += tn[a][b];
-    }
-    if (h->p.lbmhft || h->p.lbmhftd) {
-      out->u_bmhft = sc[S_SR + 0];
-      out->vir_bmhft = sc[S_SR + 1] / 3.0;
-      put6(tn, sc + S_SR + 4, f);
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) t[a][b] += tn[a][b];
-    }
-  }
-  if (h->p.lcoulomb) {
-    double cu = h->coul_unit;
-    double a = h->p.alphaES;
-    double selfa = a / std::sqrt(kPi);
-    double selfa2 = 2.0 * selfa * a * a / 3.0;
-    const double* m = sc + S_MOM;
-    double u_self = -selfa * m[6] - selfa2 * m[7];
-    double tpi_3V = kTwoPi / h->omega / 3.0;
-    double u_surf = (m[0] * m[0] + m[1] * m[1] + m[2] * m[2]) +
-                    2.0 * (m[0] * m[3] + m[1] * m[4] + m[2] * m[5]) +
-                    (m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
-    u_surf *= tpi_3V;
-    double u_pol = h->lpolar ? sc[S_UPOL] * 0.5 : 0.0;
-    double u_dir = sc[S_DIR], u_rec = sc[S_REC];
-    out->u_pol = u_pol;
-    out->u_coul = (u_dir + u_rec + (h->p.lsurf ? u_surf : 0.0) + u_self + u_pol) * cu;
-    double td[3][3], tr[3][3];
-    put6(td, sc + S_DIR + 1, inv_om * 0.5);
-    put6(tr, sc + S_REC + 1, 1.0);
-    for (int x = 0; x < 3; ++x)
-      for (int y = 0; y < 3; ++y) tc[x][y] = (td[x][y] + tr[x][y]) * cu / h->press_unit;
-    out->pvirial_coul = 1.0 / 3.0 * (tc[0][0] + tc[1][1] + tc[2][2]) * h->press_unit;
-    for (int x = 0; x < 3; ++x)
-      for (int y = 0; y < 3; ++y) t[x][y] += 2.0 * tc[x][y];
-  }
-  memcpy(out->tau_nonb, tn, sizeof(tn));
-  memcpy(out->tau_coul, tc, sizeof(tc));
-  memcpy(out->tau, t, sizeof(t));
+  scalars_to_result(h->h_scal, h->p, h->lsr, h->lpolar, h->omega, h->coul_unit, h->press_unit, out);
 }
 
 // ---------------------------------------------------------------------------
@@ -1066,6 +1009,8 @@ int mdff_gpu_struct_size(int which) {
     case 0: return (int)sizeof(mdff_params);
     case 1: return (int)sizeof(mdff_result);
     case 2: return (int)sizeof(mdff_stats);
+    case 3: return (int)sizeof(mdff_batch_desc);
+    case 4: return (int)sizeof(mdff_batch_conf);
     default: return -1;
   }
 }
@@ -1100,7 +1045,7 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   mdff_params& p = h->p;
   h->natm = p.natm;
   h->ntype = p.ntype;
-  int ntype = p.ntype, n = p.natm;
+  int n = p.natm;
   h->coul_unit = S.coul_unit;
   h->press_unit = S.press_unit;
   h->lsr = S.lsr;

@@ -37,8 +37,62 @@ struct ESPair {        // per ordered role pair (ta = type of "ia", tb = type of
 // tau_bmh(6: xx yy zz xy xz yz), tau_lj(6)] -> 16 doubles.
 constexpr int kSRPart = 16;
 
+// one BMH / BMHFTD (+ r^-24 wall) pair at r^2 = rijsq: energy u and the force
+// scalar wij (F_i = wij r_ij) of engforce_bmhftd_pbc (non_bonded.f90:1153-1200).
+// The reference skips pairs with A = 0 (:1153); the optional wall acts on its own.
 template <typename R>
-__global__ void __launch_bounds__(256) k_shortrange(
+__device__ __forceinline__ void sr_pair_bmh(const NBPair& P, int lbmhftd, R rijsq, R& u, R& wij) {
+  R ir2 = R(1) / rijsq;
+  R d = rsqrt_<R>(rijsq);
+  R wnum = R(0);
+  u = R(0);
+  if (P.A != 0.0) {
+    R erh = (R)P.A * rexp<R>(-(R)P.B * d);
+    R ir6 = ir2 * ir2 * ir2;
+    R ir8 = ir6 * ir2;
+    ir6 = ir6 * (R)P.C;
+    ir8 = ir8 * (R)P.D;
+    R f6 = R(1), f8 = R(1), fd6 = R(0), fd8 = R(0);
+    if (lbmhftd) {
+      tt_damp<R>((R)P.BD, R(1), d, 6, f6, fd6);
+      tt_damp<R>((R)P.BD, R(1), d, 8, f8, fd8);
+    }
+    R ir6d = ir6 * f6, ir8d = ir8 * f8;
+    R ir7 = R(6) * ir6d / d;
+    R ir9 = R(8) * ir8d / d;
+    u = erh - ir6d - ir8d;
+    wnum = (R)P.B * erh - ir7 - ir9 + ir6 * fd6 + ir8 * fd8;
+  }
+  if (P.wall != 0.0) {
+    R ir8r = (ir2 * ir2) * (ir2 * ir2);
+    R uw = (R)P.wall * (ir8r * ir8r * ir8r);
+    u += uw;
+    wnum += R(24) * uw / d;
+  }
+  wij = wnum / d;
+}
+
+// one n-m LJ pair (engforce_nmlj_pbc, non_bonded.f90:740-790): energy with the
+// trunc shift, force scalar wij (F_i = wij r_ij)
+template <typename R>
+__device__ __forceinline__ void sr_pair_lj(const NBPair& P, int trunc, R rijsq, R& e, R& wij) {
+  R sr2 = (R)P.sigsq / rijsq;
+  R srp, srq;
+  if (sizeof(R) == 8) {
+    srp = (R)pow((double)sr2, 0.5 * P.plj);
+    srq = (R)pow((double)sr2, 0.5 * P.qlj);
+  } else {
+    srp = powf((float)sr2, 0.5f * (float)P.plj);
+    srq = powf((float)sr2, 0.5f * (float)P.qlj);
+  }
+  e = (R)P.epsp * ((R)P.plj * srq - (R)P.qlj * srp);
+  if (trunc == 1) e = e - (R)P.uc;
+  if (trunc == 2) e = e + (R)P.uc1 * rijsq - (R)P.uc2;
+  wij = (R)P.fc * (srq - srp) * sr2;
+}
+
+template <typename R>
+static __global__ void __launch_bounds__(256) k_shortrange(
     const double4* __restrict__ s, const int* __restrict__ itype, const int* __restrict__ nbr,
     const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
     const NBPair* __restrict__ tab, int ntype, int do_bmh, int lbmhftd, int do_lj, int trunc,
@@ -71,33 +125,8 @@ __global__ void __launch_bounds__(256) k_shortrange(
       // the reference skips pairs with A = 0 (non_bonded.f90:1153); the
       // optional r^-24 wall extension acts on its own
       if (do_bmh && (P.A != 0.0 || P.wall != 0.0)) {
-        R ir2 = R(1) / rijsq;
-        R d = rsqrt_<R>(rijsq);
-        R u = R(0), wnum = R(0);
-        if (P.A != 0.0) {
-          R erh = (R)P.A * rexp<R>(-(R)P.B * d);
-          R ir6 = ir2 * ir2 * ir2;
-          R ir8 = ir6 * ir2;
-          ir6 = ir6 * (R)P.C;
-          ir8 = ir8 * (R)P.D;
-          R f6 = R(1), f8 = R(1), fd6 = R(0), fd8 = R(0);
-          if (lbmhftd) {
-            tt_damp<R>((R)P.BD, R(1), d, 6, f6, fd6);
-            tt_damp<R>((R)P.BD, R(1), d, 8, f8, fd8);
-          }
-          R ir6d = ir6 * f6, ir8d = ir8 * f8;
-          R ir7 = R(6) * ir6d / d;
-          R ir9 = R(8) * ir8d / d;
-          u = erh - ir6d - ir8d;
-          wnum = (R)P.B * erh - ir7 - ir9 + ir6 * fd6 + ir8 * fd8;
-        }
-        if (P.wall != 0.0) {
-          R ir8r = (ir2 * ir2) * (ir2 * ir2);
-          R uw = (R)P.wall * (ir8r * ir8r * ir8r);
-          u += uw;
-          wnum += R(24) * uw / d;
-        }
-        R wij = wnum / d;
+        R u, wij;
+        sr_pair_bmh<R>(P, lbmhftd, rijsq, u, wij);
         R fx = wij * rx, fy = wij * ry, fz = wij * rz;
         fb[0] += (double)fx;
         fb[1] += (double)fy;
@@ -112,19 +141,8 @@ __global__ void __launch_bounds__(256) k_shortrange(
         acc[9] += 0.5 * (double)(ry * fz + rz * fy);
       }
       if (do_lj) {
-        R sr2 = (R)P.sigsq / rijsq;
-        R srp, srq;
-        if (sizeof(R) == 8) {
-          srp = (R)pow((double)sr2, 0.5 * P.plj);
-          srq = (R)pow((double)sr2, 0.5 * P.qlj);
-        } else {
-          srp = powf((float)sr2, 0.5f * (float)P.plj);
-          srq = powf((float)sr2, 0.5f * (float)P.qlj);
-        }
-        R e = (R)P.epsp * ((R)P.plj * srq - (R)P.qlj * srp);
-        if (trunc == 1) e = e - (R)P.uc;
-        if (trunc == 2) e = e + (R)P.uc1 * rijsq - (R)P.uc2;
-        R wij = (R)P.fc * (srq - srp) * sr2;
+        R e, wij;
+        sr_pair_lj<R>(P, trunc, rijsq, e, wij);
         R fx = wij * rx, fy = wij * ry, fz = wij * rz;
         fl[0] += (double)fx;
         fl[1] += (double)fy;
@@ -265,8 +283,47 @@ __device__ __forceinline__ float pair_vec<float>(const double* A, double4 si, do
   return rx * rx + ry * ry + rz * rz;
 }
 
+// field at i from j of the field-only passes (k_es_field): the charge field
+// q_j r dm3 (F1 - F1d) with the pair's damping roles, and the dipole field
+// T2 . mu_j (ewald_dir.f90:533-541, 566-571); added into (ex, ey, ez).
+template <typename R, bool QQ, bool DD>
+__device__ __forceinline__ void es_field_pair(const ESPair* stab, int ntype, int i, int j, int ti,
+                                              int tj, R rx, R ry, R rz, R r2, R alpha, int damp,
+                                              double qj, bool dd, R mx, R my, R mz, R& ex, R& ey,
+                                              R& ez) {
+  Radial<R> g;
+  radial<R, false>(r2, alpha, g);
+  if (QQ && qj != 0.0) {
+    R F1d = R(0);
+    if (damp) {
+      bool i_is_a = half_mask(i, j);
+      int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
+      const ESPair& P = stab[ta * ntype + tb];
+      if (P.ldamp) {
+        R fdm, fdd;
+        if (i_is_a)
+          tt_damp<R>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
+        else
+          tt_damp<R>((R)P.bb, (R)P.cb, g.d, P.kb, fdm, fdd);
+        F1d = R(1) - fdm;
+      }
+    }
+    R c = (R)qj * g.dm3 * (g.F1 - F1d);
+    ex += c * rx;
+    ey += c * ry;
+    ez += c * rz;
+  }
+  if (DD && dd) {
+    R B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5;
+    R rm = rx * mx + ry * my + rz * mz;
+    ex += B2 * rx * rm - B1 * mx;
+    ey += B2 * ry * rm - B1 * my;
+    ez += B2 * rz * rm - B1 * mz;
+  }
+}
+
 // dipoles converted for the FP32 passes
-__global__ void k_to_float4(const double4* __restrict__ in, int n, float4* __restrict__ out) {
+static __global__ void k_to_float4(const double4* __restrict__ in, int n, float4* __restrict__ out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double4 v = in[i];
@@ -280,7 +337,7 @@ __global__ void k_to_float4(const double4* __restrict__ in, int n, float4* __res
 //          1 -> both ions polarisable (the linear operator of the CG solve)
 // mu is double4 for FP64 and float4 for FP32 (k_to_float4).
 template <typename R, bool QQ, bool DD>
-__global__ void __launch_bounds__(256) k_es_field(
+static __global__ void __launch_bounds__(256) k_es_field(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
     const int* __restrict__ ipolar, const typename vec4t<R>::T* __restrict__ mu,
     const int* __restrict__ nbr, const int* __restrict__ nnb, int cap, int natm,
@@ -311,7 +368,7 @@ __global__ void __launch_bounds__(256) k_es_field(
       R rx, ry, rz;
       R r2 = pair_vec<R>(cA, si, sj, rx, ry, rz);
       if (r2 > rc2) continue;  // ewald_dir.f90:202 ( d2 .gt. cutsq ) cycle
-      M4 muj;
+      M4 muj{};
       bool dd = false;
       if (DD && dip_i) {
         muj = mu[j];
@@ -319,37 +376,10 @@ __global__ void __launch_bounds__(256) k_es_field(
       }
       double qj = QQ ? q[j] : 0.0;
       if (!dd && (!QQ || qj == 0.0)) continue;
-      Radial<R> g;
-      radial<R, false>(r2, (R)alpha, g);
-      if (QQ && qj != 0.0) {
-        R F1d = R(0);
-        if (damp) {
-          int tj = itype[j];
-          bool i_is_a = half_mask(i, j);
-          int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
-          const ESPair& P = stab[ta * ntype + tb];
-          if (P.ldamp) {
-            R fdm, fdd;
-            if (i_is_a)
-              tt_damp<R>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
-            else
-              tt_damp<R>((R)P.bb, (R)P.cb, g.d, P.kb, fdm, fdd);
-            F1d = R(1) - fdm;
-          }
-        }
-        R c = (R)qj * g.dm3 * (g.F1 - F1d);
-        ex += c * rx;
-        ey += c * ry;
-        ez += c * rz;
-      }
-      if (DD && dd) {
-        R B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5;
-        R mx = (R)muj.x, my = (R)muj.y, mz = (R)muj.z;
-        R rm = rx * mx + ry * my + rz * mz;
-        ex += B2 * rx * rm - B1 * mx;
-        ey += B2 * ry * rm - B1 * my;
-        ez += B2 * rz * rm - B1 * mz;
-      }
+      int tj = (QQ && damp) ? itype[j] : 0;
+      es_field_pair<R, QQ, DD>(stab, ntype, i, j, ti, tj, rx, ry, rz, r2, (R)alpha, damp, qj, dd,
+                               DD ? (R)muj.x : R(0), DD ? (R)muj.y : R(0), DD ? (R)muj.z : R(0),
+                               ex, ey, ez);
     }
   }
   double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
@@ -365,8 +395,76 @@ __global__ void __launch_bounds__(256) k_es_field(
 // (tau is the reference's  - sum (r_j f_k + r_k f_j)  before *0.5/omega).
 constexpr int kESPart = 7;
 
+// one canonical pair of the final real-space pass (multipole_ES_dir tasks qq,
+// qd, dd with damping, ewald_dir.f90:528-644): a = "ia", b = "ja", r = r_a - r_b.
+// Out: pair energy u, f_ij (the reference's f_i -= f_ij, f_j += f_ij,
+// ewald_dir.f90:714-721), fields Ea on a and Eb on b.
 template <typename R>
-__global__ void __launch_bounds__(256) k_es_force(
+__device__ __forceinline__ void es_force_pair(const ESPair& P, int damp_ind, R d2, R alpha,
+                                              const R (&r)[3], R qa, R qb, const R (&ma)[3],
+                                              const R (&mb)[3], bool dip_a, bool dip_b,
+                                              int task_qq, int task_qd, int task_dd, R& u,
+                                              R (&fij)[3], R (&Ea)[3], R (&Eb)[3]) {
+  Radial<R> g;
+  radial<R, true>(d2, alpha, g);
+  bool ldamp = damp_ind && P.ldamp;
+  R F1d = R(0), F2d = R(0), F1d2 = R(0), F2d2 = R(0);
+  if (ldamp) {
+    R fdm, fdd, fdm2, fdd2;
+    tt_damp<R>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
+    tt_damp<R>((R)P.bb, (R)P.cb, g.d, P.kb, fdm2, fdd2);
+    F1d = R(1) - fdm;
+    F2d = F1d + (g.d / R(3)) * fdd;
+    F1d2 = R(1) - fdm2;
+    F2d2 = F1d2 + (g.d / R(3)) * fdd2;
+  }
+  R B0 = g.dm1 * g.F0, B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5, B3 = R(15) * g.F3 * g.dm7;
+  R B1d = F1d * g.dm3, B2d = R(3) * F2d * g.dm5, B1d2 = F1d2 * g.dm3, B2d2 = R(3) * F2d2 * g.dm5;
+  R rma = r[0] * ma[0] + r[1] * ma[1] + r[2] * ma[2];
+  R rmb = r[0] * mb[0] + r[1] * mb[1] + r[2] * mb[2];
+  R mab = ma[0] * mb[0] + ma[1] * mb[1] + ma[2] * mb[2];
+  u = R(0);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) fij[c] = Ea[c] = Eb[c] = R(0);
+  if (task_qq) {
+    u += qa * qb * B0;
+    R ca = qb * (B1 - (ldamp ? B1d : R(0)));
+    R cb = -qa * (B1 - (ldamp ? B1d2 : R(0)));
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Ea[c] += ca * r[c];
+      Eb[c] += cb * r[c];
+      fij[c] += -qa * qb * B1 * r[c];
+    }
+  }
+  if (task_dd && dip_a && dip_b) {
+    u += -(B2 * rma * rmb - B1 * mab);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Ea[c] += B2 * r[c] * rmb - B1 * mb[c];
+      Eb[c] += B2 * r[c] * rma - B1 * ma[c];
+      fij[c] -= -B3 * rma * rmb * r[c] + B2 * (mab * r[c] + ma[c] * rmb + mb[c] * rma);
+    }
+  }
+  if (task_qd && (dip_a || dip_b)) {
+    u += qa * B1 * rmb - qb * B1 * rma;
+    if (ldamp) u += -qa * B1d2 * rmb + qb * B1d * rma;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      R T2mb = B2 * r[c] * rmb - B1 * mb[c];
+      R T2ma = B2 * r[c] * rma - B1 * ma[c];
+      fij[c] += -qa * T2mb + qb * T2ma;
+      if (ldamp) {
+        R T2dma = B2d * r[c] * rma - B1d * ma[c];
+        R T2d2mb = B2d2 * r[c] * rmb - B1d2 * mb[c];
+        fij[c] += -qb * T2dma + qa * T2d2mb;
+      }
+    }
+  }
+}
+
+template <typename R>
+static __global__ void __launch_bounds__(256) k_es_force(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
     const double4* __restrict__ mu, const int* __restrict__ nbr, const int* __restrict__ nnb,
     int cap, int natm, const CellC* __restrict__ cell, const ESPair* __restrict__ tab, int ntype,
@@ -410,61 +508,9 @@ __global__ void __launch_bounds__(256) k_es_force(
       R ma[3] = {(R)ma4.x, (R)ma4.y, (R)ma4.z}, mb[3] = {(R)mb4.x, (R)mb4.y, (R)mb4.z};
       bool dip_a = (ma4.x != 0.0 || ma4.y != 0.0 || ma4.z != 0.0);
       bool dip_b = (mb4.x != 0.0 || mb4.y != 0.0 || mb4.z != 0.0);
-      Radial<R> g;
-      radial<R, true>((R)r2d, (R)alpha, g);
-      const ESPair& P = stab[ta * ntype + tb];
-      bool ldamp = damp_ind && P.ldamp;
-      R F1d = R(0), F2d = R(0), F1d2 = R(0), F2d2 = R(0);
-      if (ldamp) {
-        R fdm, fdd, fdm2, fdd2;
-        tt_damp<R>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
-        tt_damp<R>((R)P.bb, (R)P.cb, g.d, P.kb, fdm2, fdd2);
-        F1d = R(1) - fdm;
-        F2d = F1d + (g.d / R(3)) * fdd;
-        F1d2 = R(1) - fdm2;
-        F2d2 = F1d2 + (g.d / R(3)) * fdd2;
-      }
-      R B0 = g.dm1 * g.F0, B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5, B3 = R(15) * g.F3 * g.dm7;
-      R B1d = F1d * g.dm3, B2d = R(3) * F2d * g.dm5, B1d2 = F1d2 * g.dm3, B2d2 = R(3) * F2d2 * g.dm5;
-      R rma = r[0] * ma[0] + r[1] * ma[1] + r[2] * ma[2];
-      R rmb = r[0] * mb[0] + r[1] * mb[1] + r[2] * mb[2];
-      R mab = ma[0] * mb[0] + ma[1] * mb[1] + ma[2] * mb[2];
-      R u = R(0), fij[3] = {R(0), R(0), R(0)}, Ea[3] = {R(0), R(0), R(0)}, Eb[3] = {R(0), R(0), R(0)};
-      if (task_qq) {
-        u += qa * qb * B0;
-        R ca = qb * (B1 - (ldamp ? B1d : R(0)));
-        R cb = -qa * (B1 - (ldamp ? B1d2 : R(0)));
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          Ea[c] += ca * r[c];
-          Eb[c] += cb * r[c];
-          fij[c] += -qa * qb * B1 * r[c];
-        }
-      }
-      if (task_dd && dip_a && dip_b) {
-        u += -(B2 * rma * rmb - B1 * mab);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          Ea[c] += B2 * r[c] * rmb - B1 * mb[c];
-          Eb[c] += B2 * r[c] * rma - B1 * ma[c];
-          fij[c] -= -B3 * rma * rmb * r[c] + B2 * (mab * r[c] + ma[c] * rmb + mb[c] * rma);
-        }
-      }
-      if (task_qd && (dip_a || dip_b)) {
-        u += qa * B1 * rmb - qb * B1 * rma;
-        if (ldamp) u += -qa * B1d2 * rmb + qb * B1d * rma;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          R T2mb = B2 * r[c] * rmb - B1 * mb[c];
-          R T2ma = B2 * r[c] * rma - B1 * ma[c];
-          fij[c] += -qa * T2mb + qb * T2ma;
-          if (ldamp) {
-            R T2dma = B2d * r[c] * rma - B1d * ma[c];
-            R T2d2mb = B2d2 * r[c] * rmb - B1d2 * mb[c];
-            fij[c] += -qb * T2dma + qa * T2d2mb;
-          }
-        }
-      }
+      R u, fij[3], Ea[3], Eb[3];
+      es_force_pair<R>(stab[ta * ntype + tb], damp_ind, (R)r2d, (R)alpha, r, qa, qb, ma, mb, dip_a,
+                       dip_b, task_qq, task_qd, task_dd, u, fij, Ea, Eb);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
         f[c] += (double)(i_is_a ? -fij[c] : fij[c]);
@@ -497,7 +543,7 @@ __global__ void __launch_bounds__(256) k_es_force(
 }
 
 // fixed-order reduction of per-block partials: out[v] = sum_b part[b*nv+v]
-__global__ void k_reduce_partials(const double* __restrict__ part, int nblk, int nv,
+static __global__ void k_reduce_partials(const double* __restrict__ part, int nblk, int nv,
                                   double* __restrict__ out) {
   __shared__ double sh[256];
   for (int v = 0; v < nv; ++v) {

@@ -43,7 +43,7 @@ struct RecMesh {
 // per-ion phase tables: [n][natm], X: n = 0..kx, Y: 0..ky, Z: 0..max(kz, 4).
 // s is wrapped to [-0.5, 0.5) first: e^{2 pi i n s} is periodic in s.
 template <typename R>
-__global__ void k_rec_tables(const double4* __restrict__ s, int natm, int kx, int ky, int kz,
+static __global__ void k_rec_tables(const double4* __restrict__ s, int natm, int kx, int ky, int kz,
                              typename cplx<R>::T* __restrict__ tab) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
@@ -65,7 +65,7 @@ __global__ void k_rec_tables(const double4* __restrict__ s, int natm, int kx, in
 }
 
 // per-ion weights (q, m1, m2, m3), m = 2 pi B^T mu  (k.mu = n.m)
-__global__ void k_rec_weights(const double* __restrict__ q, const double4* __restrict__ mu,
+static __global__ void k_rec_weights(const double* __restrict__ q, const double4* __restrict__ mu,
                               int natm, const CellC* __restrict__ cell, int has_q, int has_mu,
                               double4* __restrict__ w, float4* __restrict__ w32,
                               float4* __restrict__ mu32) {
@@ -135,7 +135,7 @@ __device__ __forceinline__ typename cplx<R>::T phase_z(const typename cplx<R>::T
 // nz and is re-anchored on the exact table every 4 nz (FP32 drift bound).
 // Warp partial sums in R, block and chunk sums in FP64, fixed order.
 template <typename R, bool HAS_Q, bool HAS_MU, int NZT>
-__global__ void __launch_bounds__(128) k_rec_rho(const typename cplx<R>::T* __restrict__ tab,
+static __global__ void __launch_bounds__(128) k_rec_rho(const typename cplx<R>::T* __restrict__ tab,
                                                  const double4* __restrict__ w, int natm,
                                                  int chunk, RecMesh M, int ntiles,
                                                  double2* __restrict__ part) {
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(128) k_rec_rho(const typename cplx<R>::T* __re
 }
 
 // rho = sum over chunks; rhoA = A_k rho; str = A_k |rho|^2
-__global__ void k_rec_sum(const double2* __restrict__ part, int nchunk, RecMesh M,
+static __global__ void k_rec_sum(const double2* __restrict__ part, int nchunk, RecMesh M,
                           double2* __restrict__ rhoA, double* __restrict__ str) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= M.nk) return;
@@ -224,7 +224,7 @@ __global__ void k_rec_sum(const double2* __restrict__ part, int nchunk, RecMesh 
 
 // u_rec (x2 x tpi_V) and tau_rec (x2, symmetric, x tpi_V/omega): out[0..6] =
 // u, tau xx yy zz xy xz yz.  One block.
-__global__ void k_rec_energy(const double* __restrict__ str, RecMesh M, double tpi_V,
+static __global__ void k_rec_energy(const double* __restrict__ str, RecMesh M, double tpi_V,
                              double omega, int do_stress, double* __restrict__ out) {
   __shared__ double red[7 * 32];
   double v[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -252,7 +252,7 @@ __global__ void k_rec_energy(const double* __restrict__ str, RecMesh M, double t
 // (row ranges rc[c]..rc[c+1]); dynamic smem = rho' of the chunk.
 // G accumulates sum_k n recarg, H accumulates sum_k n (k.mu) recarg2.
 template <typename R, bool HAS_MU_FORCE>
-__global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>::T* __restrict__ tab,
+static __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>::T* __restrict__ tab,
                                                    const double4* __restrict__ w, int natm,
                                                    RecMesh M, const int* __restrict__ rchunk,
                                                    const double2* __restrict__ rhoA,
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>::T* __
 // chunk sum and scaling.  E += -(2 pi B G) * 2 fpi_V (ewald_rec.f90:193-198,
 // 300-352); with do_forces, F += [q (-2 pi B G) + 2 pi B H] * 2 fpi_V * coul_unit.
 // Four threads per ion split the chunk partials (fixed order, shuffle sum).
-__global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const double4* __restrict__ Hpart,
+static __global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const double4* __restrict__ Hpart,
                                 int nchunk, int natm, const CellC* __restrict__ cell,
                                 const double* __restrict__ q, double scale /* 2 fpi_V */,
                                 int has_mu_force, int do_forces, double coul_unit,
@@ -425,7 +425,7 @@ __device__ __forceinline__ float2 phase1(const float2* __restrict__ tab, int nat
 // structure factor, FP32x2.  Thread t of the block handles ions a = i, b = i + 128
 // of each 256-ion step of its chunk (b absent -> weight 0).
 template <bool HAS_Q, bool HAS_MU, int NZT>
-__global__ void __launch_bounds__(128) k_rec_rho_x2(const float2* __restrict__ tab,
+static __global__ void __launch_bounds__(128) k_rec_rho_x2(const float2* __restrict__ tab,
                                                     const float4* __restrict__ w, int natm,
                                                     int chunk, RecMesh M, int ntiles,
                                                     double2* __restrict__ part) {
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(128) k_rec_rho_x2(const float2* __restrict__ t
 
 // field / force partials, FP32x2: ions a = blockIdx.x*256 + tid, b = a + 128.
 template <bool HAS_MU_FORCE>
-__global__ void __launch_bounds__(128) k_rec_field_x2(const float2* __restrict__ tab,
+static __global__ void __launch_bounds__(128) k_rec_field_x2(const float2* __restrict__ tab,
                                                       const float4* __restrict__ w, int natm,
                                                       RecMesh M, const int* __restrict__ rchunk,
                                                       const double2* __restrict__ rhoA,

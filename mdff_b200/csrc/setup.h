@@ -294,4 +294,71 @@ inline void kmesh_of(const int kES[3], const double* B, double alphaES, KMesh& M
     }
 }
 
+// Scalar slots of one evaluation -> the reference's thermodynamic outputs:
+// slots 0-15 short range (k_shortrange), 16-22 real-space energy and stress,
+// 23-29 reciprocal, 30-37 moments [sum q r, sum mu, sum q^2, sum mu^2],
+// 38 sum mu alpha^-1 mu.  Units and factors of ewald.f90:206-245,
+// non_bonded.f90:1205 and engforce_driver.f90:164-177 (tau = tau_nonb + 2 tau_coul).
+inline void scalars_to_result(const double* sc, const mdff_params& p, int lsr, int lpolar,
+                              double omega, double coul_unit, double press_unit, mdff_result* out) {
+  const int S_SR = 0, S_DIR = 16, S_REC = 23, S_MOM = 30, S_UPOL = 38;
+  double inv_om = 1.0 / omega;
+  out->u_lj = out->vir_lj = out->u_bmhft = out->vir_bmhft = 0.0;
+  out->u_coul = out->u_pol = out->pvirial_coul = 0.0;
+  double tn[3][3] = {{0}}, tc[3][3] = {{0}}, t[3][3] = {{0}};
+  auto put6 = [](double m[3][3], const double* v, double f) {
+    m[0][0] = v[0] * f;
+    m[1][1] = v[1] * f;
+    m[2][2] = v[2] * f;
+    m[0][1] = m[1][0] = v[3] * f;
+    m[0][2] = m[2][0] = v[4] * f;
+    m[1][2] = m[2][1] = v[5] * f;
+  };
+  if (lsr) {
+    double f = inv_om / press_unit * 0.5;
+    if (p.lnmlj) {
+      out->u_lj = sc[S_SR + 2];
+      out->vir_lj = sc[S_SR + 3] / 3.0;
+      put6(tn, sc + S_SR + 10, f);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) t[a][b] += tn[a][b];
+    }
+    if (p.lbmhft || p.lbmhftd) {
+      out->u_bmhft = sc[S_SR + 0];
+      out->vir_bmhft = sc[S_SR + 1] / 3.0;
+      put6(tn, sc + S_SR + 4, f);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) t[a][b] += tn[a][b];
+    }
+  }
+  if (p.lcoulomb) {
+    double cu = coul_unit;
+    double a = p.alphaES;
+    double selfa = a / std::sqrt(kPi);
+    double selfa2 = 2.0 * selfa * a * a / 3.0;
+    const double* m = sc + S_MOM;
+    double u_self = -selfa * m[6] - selfa2 * m[7];
+    double tpi_3V = kTwoPi / omega / 3.0;
+    double u_surf = (m[0] * m[0] + m[1] * m[1] + m[2] * m[2]) +
+                    2.0 * (m[0] * m[3] + m[1] * m[4] + m[2] * m[5]) +
+                    (m[3] * m[3] + m[4] * m[4] + m[5] * m[5]);
+    u_surf *= tpi_3V;
+    double u_pol = lpolar ? sc[S_UPOL] * 0.5 : 0.0;
+    double u_dir = sc[S_DIR], u_rec = sc[S_REC];
+    out->u_pol = u_pol;
+    out->u_coul = (u_dir + u_rec + (p.lsurf ? u_surf : 0.0) + u_self + u_pol) * cu;
+    double td[3][3], tr[3][3];
+    put6(td, sc + S_DIR + 1, inv_om * 0.5);
+    put6(tr, sc + S_REC + 1, 1.0);
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y) tc[x][y] = (td[x][y] + tr[x][y]) * cu / press_unit;
+    out->pvirial_coul = 1.0 / 3.0 * (tc[0][0] + tc[1][1] + tc[2][2]) * press_unit;
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y) t[x][y] += 2.0 * tc[x][y];
+  }
+  memcpy(out->tau_nonb, tn, sizeof(tn));
+  memcpy(out->tau_coul, tc, sizeof(tc));
+  memcpy(out->tau, t, sizeof(t));
+}
+
 }  // namespace mdff

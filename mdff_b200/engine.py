@@ -129,3 +129,115 @@ class ForceEngine:
         st = self._lib.mdff_gpu_verlet_half_list(self._h, int(which), dptr(rx), dptr(ry), dptr(rz),
                                                  iptr(point), iptr(lst), int(cap), ctypes.byref(nout))
         return st, point, lst[: min(nout.value, cap)].copy(), nout.value
+
+
+class BatchEngine:
+    """Many independent configurations per call (include/mdff_gpu.h batched
+    entry points): ``BatchEngine(psets, configs)`` with ``configs`` a list of
+    (pset index, natmi per type, cell 3x3); :meth:`engforce` takes the
+    concatenated positions and returns per-ion arrays plus one dict of
+    scalars per configuration.  Each configuration is one engforce with
+    calc = 'other'."""
+
+    def __init__(self, psets, configs):
+        self._lib = _abi.load_library()
+        self.nconf = len(configs)
+        np_ = len(psets)
+        arr = (_abi.MdffParams * np_)(*psets)
+        self._psets = arr
+        pset = np.array([c[0] for c in configs], dtype=np.int32)
+        natmi = np.zeros((self.nconf, _abi.NT), dtype=np.int32)
+        cells = np.zeros((self.nconf, 9))
+        for k, (_, ni, cell) in enumerate(configs):
+            natmi[k, : len(ni)] = ni
+            cells[k] = np.asarray(cell, dtype=np.float64).reshape(9)
+        self.natm = natmi.sum(1)
+        self.offsets = np.concatenate([[0], np.cumsum(self.natm)])
+        self.ntot = int(self.offsets[-1])
+        self._keep = (pset, natmi, cells)
+        d = _abi.MdffBatchDesc(self.nconf, pset.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                               natmi.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), dptr(cells))
+        h = ctypes.c_void_p()
+        st = self._lib.mdff_gpu_batch_create(arr, np_, ctypes.byref(d), ctypes.byref(h))
+        if st != 0:
+            msg = self._lib.mdff_gpu_batch_last_error(None).decode()
+            raise MdffError(st, f"batch_create: {self._lib.mdff_gpu_strerror(st).decode()} ({msg})")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.mdff_gpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st, what, allow=()):
+        if st != 0 and st not in allow:
+            msg = self._lib.mdff_gpu_batch_last_error(self._h).decode()
+            raise MdffError(st, f"{what}: {self._lib.mdff_gpu_strerror(st).decode()} {msg}")
+        return st
+
+    @staticmethod
+    def _conf_dicts(confs):
+        out = []
+        for c in confs:
+            d = {k: getattr(c, k) for k in ("u_lj", "vir_lj", "u_bmhft", "vir_bmhft", "u_coul",
+                                            "u_pol", "pvirial_coul", "rmsd", "n_pol_iter",
+                                            "converged", "catastrophe", "nk", "alphaES",
+                                            "cutlongrange")}
+            d["kES"] = list(c.kES)
+            for k in ("tau_nonb", "tau_coul", "tau"):
+                d[k] = _mat(getattr(c, k))
+            out.append(d)
+        return out
+
+    def engforce(self, rx, ry, rz, allow_status=()):
+        n = self.ntot
+        rx, ry, rz = (np.ascontiguousarray(a, dtype=np.float64) for a in (rx, ry, rz))
+        out = {k: np.zeros(n) for k in ("fx", "fy", "fz")}
+        out["mu"] = np.zeros((n, 3))
+        out["ef"] = np.zeros((n, 3))
+        confs = (_abi.MdffBatchConf * self.nconf)()
+        st = self._lib.mdff_gpu_batch_engforce(self._h, dptr(rx), dptr(ry), dptr(rz),
+                                               dptr(out["fx"]), dptr(out["fy"]), dptr(out["fz"]),
+                                               dptr(out["mu"]), dptr(out["ef"]), confs)
+        out["status"] = self._check(st, "batch_engforce", allow_status)
+        out["conf"] = self._conf_dicts(confs)
+        return out
+
+    def engforce_device(self, d_pos, d_force, d_mu=0, d_ef=0):
+        confs = (_abi.MdffBatchConf * self.nconf)()
+        st = self._lib.mdff_gpu_batch_engforce_device(self._h, ctypes.c_void_p(d_pos),
+                                                      ctypes.c_void_p(d_force),
+                                                      ctypes.c_void_p(d_mu or None),
+                                                      ctypes.c_void_p(d_ef or None), confs)
+        self._check(st, "batch_engforce_device")
+        return self._conf_dicts(confs)
+
+    def tune(self):
+        c, t, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        self._check(self._lib.mdff_gpu_batch_tune(self._h, ctypes.byref(c), ctypes.byref(t),
+                                                  ctypes.byref(ms)), "batch_tune")
+        return c.value, t.value, ms.value
+
+    def set_shape(self, cluster, threads):
+        self._check(self._lib.mdff_gpu_batch_set_shape(self._h, int(cluster), int(threads)),
+                    "batch_set_shape")
+
+    def info(self):
+        v = [ctypes.c_int() for _ in range(4)]
+        ms = ctypes.c_double()
+        self._check(self._lib.mdff_gpu_batch_info(self._h, *[ctypes.byref(x) for x in v],
+                                                  ctypes.byref(ms)), "batch_info")
+        return dict(ntot=v[0].value, nconf=v[1].value, cluster=v[2].value, threads=v[3].value,
+                    ms_last=ms.value)

@@ -310,3 +310,115 @@ def random_ionic(n_per_type=(20, 20), L=14.0, seed=7, q=(1.5, -1.5), pol=(0.0, 1
     mass = np.full(n, 20.0)
     vel = maxwell(rng, mass, 1000.0)
     return System("random_ionic", p, cell, pos, mass, vel, dict(L=L, seed=seed))
+
+
+# --------------------------------------------------------------------------
+# batched workloads: many small independent boxes
+
+FORMULA = {"nacl": (22.98977 + 35.453, 1.55), "mgo": (24.305 + 15.9994, 3.58)}
+
+
+def batch_psets(precision=_abi.PREC_MIXED, cg_tol=1e-8, epsw=1e-6, cg_max_iter=200):
+    """Parameter sets of the batched workloads.  0 = NaCl type: Tosi-Fumi BMH,
+    charges +1/-1, no polarisation.  1 = MgO type: Lewis-Catlow Buckingham,
+    charges +2/-2, O polarisability 1.6 A^3 with Tang-Toennies damping
+    (b 3.0, c 1.0, order 4) of the Mg charge field on O, as mgo().  Ewald
+    alpha and kmax per box from the ewald_param rule (lautoES, coulomb.f90:
+    363-410) at epsw; the real-space cutoff is clamped to half of each box.
+    Short-range cutoffs 6 A (NaCl) and 4 A (MgO) fit the smallest boxes."""
+    A, B, C, D = tosi_fumi_nacl()
+    common = dict(lcoulomb=1, lbmhft=1, cutlongrange=12.0, lautoES=1, epsw=epsw,
+                  precision=precision, solver=_abi.SOLVER_CG, cg_tol=cg_tol,
+                  cg_max_iter=cg_max_iter, conv_tol_ind=cg_tol, calc=_abi.CALC_OTHER)
+    nacl = make_params([1, 1], cutshortrange=6.0, qch=[1.0, -1.0], Abmhftd=A, Bbmhftd=B,
+                       Cbmhftd=C, Dbmhftd=D, **common)
+    Am, Bm, Cm = lewis_catlow_mgo()
+    mgo_p = make_params([1, 1], cutshortrange=4.0, qch=[2.0, -2.0], Abmhftd=Am, Bbmhftd=Bm,
+                        Cbmhftd=Cm, ldip_polar=[0, 1], poldip_iso={1: 1.6},
+                        ldip_damping={(1, 0, 1): 1}, pol_damp_b={(1, 0, 1): 3.0},
+                        pol_damp_c={(1, 0, 1): 1.0}, pol_damp_k={(1, 0, 1): 4}, **common)
+    return [nacl, mgo_p]
+
+
+# minimum separations enforced on the jittered MgO-type boxes (cation-anion,
+# anion-anion, cation-cation; A): with the O polarisability 1.6 A^3 the
+# undamped dipole-dipole coupling of O-O pairs below ~1.9 A, or a Mg charge
+# within ~1.3 A of an O, drives the reference's SCF into the polarisation
+# catastrophe (moment_from_pola.f90:176-216)
+DMIN = {"nacl": None, "mgo": (1.5, 2.0, 2.0)}
+
+
+def rocksalt_box(rng, n_ions, kind, density, jitter):
+    """n_ions (even) of a rock-salt compound in a cubic box: the smallest m^3
+    conventional-cell lattice with room for n_ions/2 cations and anions, its
+    lattice constant that of the full crystal at the given mass density, sites
+    drawn without replacement (equal numbers of vacancies on both
+    sublattices, so the ion density is the lattice's times the filled
+    fraction), positions jittered by U(-jitter, jitter) per component.  Where
+    DMIN gives minimum separations, an ion's jitter is redrawn (up to 200
+    times) until it keeps them to every ion placed before it.  Cations first,
+    then anions.  Returns (positions, box edge)."""
+    nf = n_ions // 2
+    fmass = FORMULA[kind][0]
+    m = 1
+    while 4 * m ** 3 < nf:
+        m += 1
+    L = m * box_length(4, fmass, density)
+    cat, ani = rocksalt(m, L / m)
+    ci = np.sort(rng.choice(len(cat), nf, replace=False))
+    ai = np.sort(rng.choice(len(ani), nf, replace=False))
+    sites = np.concatenate([cat[ci], ani[ai]])
+    dmin = DMIN[kind]
+    if dmin is None:
+        return sites + rng.uniform(-jitter, jitter, (2 * nf, 3)), L
+    pos = np.zeros_like(sites)
+    anion = np.arange(2 * nf) >= nf
+    for i in range(2 * nf):
+        for _ in range(200):
+            x = sites[i] + rng.uniform(-jitter, jitter, 3)
+            if i == 0:
+                break
+            d = pos[:i] - x
+            d -= L * np.round(d / L)
+            r = np.sqrt((d * d).sum(1))
+            lim = np.where(anion[:i] != anion[i], dmin[0], dmin[1] if anion[i] else dmin[2])
+            if (r >= lim).all():
+                break
+        else:
+            raise RuntimeError("rocksalt_box: jitter rejection failed")
+        pos[i] = x
+    return pos, L
+
+
+def batch(nconf=256, seed=99, nmin=64, nmax=1000, jitter=0.3, density_spread=0.1,
+          kinds=("nacl", "mgo"), precision=_abi.PREC_MIXED, cg_tol=1e-8, epsw=1e-6):
+    """Seeded batch of independent cubic rock-salt boxes: per box a kind
+    (uniform over kinds), an even ion count uniform in [nmin, nmax], a lattice
+    density uniform within +-density_spread of the kind's nominal (NaCl 1.55,
+    MgO 3.58 g/cm^3; vacancies fill the lattice up, rocksalt_box) and +-jitter
+    positions.  Returns (psets, configs, positions):
+    configs[c] = (pset index, [n_cation, n_anion], cell), positions a list of
+    (n_c, 3) arrays in the configuration order."""
+    rng = np.random.default_rng(seed)
+    psets = batch_psets(precision=precision, cg_tol=cg_tol, epsw=epsw)
+    index = {"nacl": 0, "mgo": 1}
+    configs, pos = [], []
+    for _ in range(nconf):
+        kind = kinds[int(rng.integers(len(kinds)))]
+        n = 2 * int(rng.integers(nmin // 2, nmax // 2 + 1))
+        dens = FORMULA[kind][1] * rng.uniform(1 - density_spread, 1 + density_spread)
+        p, L = rocksalt_box(rng, n, kind, dens, jitter)
+        configs.append((index[kind], [n // 2, n // 2], np.eye(3) * L))
+        pos.append(p)
+    return psets, configs, pos
+
+
+def config_params(psets, conf):
+    """The single-configuration parameters of one batch entry (for the
+    single engine or the oracle)."""
+    from .params import params_copy
+    p = params_copy(psets[conf[0]])
+    for t in range(_abi.NT):
+        p.natmi[t] = conf[1][t] if t < len(conf[1]) else 0
+    p.natm = int(sum(conf[1]))
+    return p

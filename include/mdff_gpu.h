@@ -309,6 +309,40 @@ int mdff_gpu_batch_info(mdff_batch_handle h, int* ntot, int* nconf, int* cluster
 const char* mdff_gpu_batch_last_error(mdff_batch_handle h);
 void mdff_gpu_batch_destroy(mdff_batch_handle h);
 
+/* ---- force-field gradients of a batch (differentiable fitting) -------------
+   No counterpart in the reference.  Fit parameters (at most MDFF_FIT_MAX),
+   each a kind and type indices, act on every parameter set of the batch:
+     MDFF_FIT_A / _RHO / _C   Buckingham A (eV), rho (A, B = 1/rho), C (eV A^6)
+                              of the type pair (t1, t2), both orders
+     MDFF_FIT_POL             isotropic polarisability of type t1 (A^3)
+     MDFF_FIT_TTB / _TTC      Tang-Toennies b (1/A), c of the charge field of
+                              type t2 on the dipoles of type t1: pol_damp
+                              (t1,t1,t2) and (t1,t2,t1)
+     MDFF_FIT_QSCALE          one factor s on every charge (qch * s)
+   mdff_gpu_batch_adjoint returns dJ/dtheta for J = sum_c [ gE_c U_c + gF . F
+   + gmu . mu_ind ] (U = u_lj + u_bmhft + u_coul, eV) at the positions of the
+   last evaluation: one adjoint linear solve per configuration with the
+   dipole solver's operator.  gE [nconf], gF SoA [3][ntot], gmu [ntot][3] or
+   NULL; host arrays (on_device = 0) or device arrays (1); grad [nparam] and
+   grad_conf [nconf][nparam] (optional) are host arrays.  The surface term
+   (lsurf) is not covered.  The call reuses the evaluation's device state and
+   overwrites its field buffer: fetch ef before calling it. */
+#define MDFF_FIT_MAX 16
+#define MDFF_FIT_A 0
+#define MDFF_FIT_RHO 1
+#define MDFF_FIT_C 2
+#define MDFF_FIT_POL 3
+#define MDFF_FIT_TTB 4
+#define MDFF_FIT_TTC 5
+#define MDFF_FIT_QSCALE 6
+int mdff_gpu_batch_fit_define(mdff_batch_handle h, int nparam, const int* kind, const int* t1,
+                              const int* t2);
+/* set the fit parameters' values (rebuilds every configuration's tables) */
+int mdff_gpu_batch_fit_set(mdff_batch_handle h, const double* theta);
+int mdff_gpu_batch_fit_get(mdff_batch_handle h, double* theta);
+int mdff_gpu_batch_adjoint(mdff_batch_handle h, const double* gE, const double* gF,
+                           const double* gmu, int on_device, double* grad, double* grad_conf);
+
 #ifdef __cplusplus
 }
 #endif

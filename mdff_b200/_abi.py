@@ -135,7 +135,14 @@ SIGNATURES = {
     "mdff_gpu_batch_info": (_i, [_P, _IP, _IP, _IP, _IP, _DP]),
     "mdff_gpu_batch_last_error": (ctypes.c_char_p, [_P]),
     "mdff_gpu_batch_destroy": (None, [_P]),
+    "mdff_gpu_batch_fit_define": (_i, [_P, _i, _IP, _IP, _IP]),
+    "mdff_gpu_batch_fit_set": (_i, [_P, _DP]),
+    "mdff_gpu_batch_fit_get": (_i, [_P, _DP]),
+    "mdff_gpu_batch_adjoint": (_i, [_P, _P, _P, _P, _i, _DP, _DP]),
 }
+
+FIT_A, FIT_RHO, FIT_C, FIT_POL, FIT_TTB, FIT_TTC, FIT_QSCALE = range(7)
+FIT_MAX = 16
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmdff_gpu.so")

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/mdff_gpu.h"
+#include "adjoint.cuh"
 #include "batch.cuh"
 #include "setup.h"
 
@@ -42,7 +43,7 @@ struct mdff_batch {
   std::vector<int> order;
   std::vector<mdff_params> pconf;   // processed parameters per configuration
   std::vector<double> omega, coul_unit, press_unit;
-  std::vector<int> lsr, lpolar;
+  std::vector<int> lsr, lpolar, pset_of;
   // device
   BConf* d_conf = nullptr;
   int *d_order = nullptr, *d_queue = nullptr, *d_typ = nullptr, *d_ipol = nullptr;
@@ -68,6 +69,17 @@ struct mdff_batch {
   double* graph_force = nullptr;
   double ms_last = 0.0;
   bool have_pos = false;
+  // fitting: parameter sets as given, fit parameters and their values
+  std::vector<mdff_params> base;
+  std::vector<double> cells;
+  int nparam = 0;
+  FitParam prm[kFitMax];
+  std::vector<double> theta;
+  double4 *d_w = nullptr, *d_rhs = nullptr, *d_lam = nullptr;
+  double2 *d_ch = nullptr;  // 5 structure-factor channels of sum nk
+  double *d_grad = nullptr, *d_info = nullptr, *d_gin = nullptr;
+  long long ktot = 0;
+  double ms_adjoint = 0.0;
 };
 
 namespace {
@@ -305,6 +317,8 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
     return MDFF_ERR_BAD_ARGS;
   }
   h->nconf = d->nconf;
+  h->base.assign(psets, psets + npsets);
+  h->cells.assign(d->cell_A, d->cell_A + 9 * (size_t)d->nconf);
   h->mixed = psets[0].precision == MDFF_PREC_MIXED ? 1 : 0;
   h->device = psets[0].device;
   int ndev = 0;
@@ -333,6 +347,7 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
       return MDFF_ERR_BAD_ARGS;
     }
     mdff_params p = psets[ps];
+    h->pset_of.push_back(ps);
     long n = 0;
     for (int t = 0; t < MDFF_NTYPEMAX; ++t) {
       p.natmi[t] = (t < p.ntype) ? d->natmi[(size_t)c * MDFF_NTYPEMAX + t] : 0;
@@ -429,6 +444,7 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
     h->nmax = std::max(h->nmax, (int)n);
   }
   h->ntot = ntot;
+  h->ktot = ktot;
   h->order.resize(h->nconf);
   std::iota(h->order.begin(), h->order.end(), 0);
   std::stable_sort(h->order.begin(), h->order.end(),
@@ -481,6 +497,65 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
   return MDFF_OK;
 }
 
+// the parameter set of configuration c with the fit parameters' values
+mdff_params fitted_pset(const mdff_batch* h, int ps) {
+  mdff_params p = h->base[ps];
+  for (int k = 0; k < h->nparam; ++k) {
+    const FitParam& f = h->prm[k];
+    double v = h->theta[k];
+    int a = f.t1, b = f.t2;
+    switch (f.kind) {
+      case FIT_A: p.Abmhftd[a][b] = p.Abmhftd[b][a] = v; break;
+      case FIT_RHO: p.Bbmhftd[a][b] = p.Bbmhftd[b][a] = 1.0 / v; break;
+      case FIT_C: p.Cbmhftd[a][b] = p.Cbmhftd[b][a] = v; break;
+      case FIT_POL:
+        for (int x = 0; x < 3; ++x)
+          for (int y = 0; y < 3; ++y) p.poldip[a][x][y] = (x == y) ? v : 0.0;
+        break;
+      // field on dipole type a from charges of type b: tables (a,a,b) and (a,b,a)
+      case FIT_TTB: p.pol_damp_b[a][a][b] = p.pol_damp_b[a][b][a] = v; break;
+      case FIT_TTC: p.pol_damp_c[a][a][b] = p.pol_damp_c[a][b][a] = v; break;
+      case FIT_QSCALE:
+        for (int t = 0; t < MDFF_NTYPEMAX; ++t) p.qch[t] = h->base[ps].qch[t] * v;
+        break;
+    }
+  }
+  return p;
+}
+
+// rebuild the value tables of every configuration for the current theta
+int refit_tables(mdff_batch* h) {
+  std::vector<double> q, pol, inv;
+  std::vector<NBPair> nb;
+  std::vector<ESPair> es;
+  for (int c = 0; c < h->nconf; ++c) {
+    mdff_params p = fitted_pset(h, h->pset_of[c]);
+    for (int t = 0; t < MDFF_NTYPEMAX; ++t) p.natmi[t] = h->pconf[c].natmi[t];
+    p.natm = h->pconf[c].natm;
+    p.calc = MDFF_CALC_OTHER;
+    Setup S;
+    const char* serr = nullptr;
+    int s = setup_system(&p, h->cells.data() + 9 * (size_t)c, S, &serr);
+    if (s) {
+      h->err = "configuration " + std::to_string(c) + ": " + serr;
+      return s;
+    }
+    h->pconf[c] = S.p;
+    nb.insert(nb.end(), S.nb.begin(), S.nb.end());
+    es.insert(es.end(), S.es.begin(), S.es.end());
+    q.insert(q.end(), S.q.begin(), S.q.end());
+    pol.insert(pol.end(), S.pol.begin(), S.pol.end());
+    inv.insert(inv.end(), S.inv.begin(), S.inv.end());
+  }
+  BCK(cudaMemcpyAsync(h->d_nb, nb.data(), sizeof(NBPair) * nb.size(), cudaMemcpyHostToDevice, h->st));
+  BCK(cudaMemcpyAsync(h->d_es, es.data(), sizeof(ESPair) * es.size(), cudaMemcpyHostToDevice, h->st));
+  BCK(cudaMemcpyAsync(h->d_q, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice, h->st));
+  BCK(cudaMemcpyAsync(h->d_pol, pol.data(), sizeof(double) * pol.size(), cudaMemcpyHostToDevice, h->st));
+  BCK(cudaMemcpyAsync(h->d_inv, inv.data(), sizeof(double) * inv.size(), cudaMemcpyHostToDevice, h->st));
+  BCK(cudaStreamSynchronize(h->st));
+  return MDFF_OK;
+}
+
 void destroy_impl(mdff_batch* h) {
   if (!h) return;
   if (h->device >= 0) cudaSetDevice(h->device);
@@ -490,7 +565,8 @@ void destroy_impl(mdff_batch* h) {
   void* bufs[] = {h->d_conf, h->d_order, h->d_queue, h->d_typ, h->d_ipol, h->d_pos, h->d_q,
                   h->d_pol, h->d_inv, h->d_dip, h->d_nb, h->d_es, h->d_rows, h->d_Ak, h->d_kvec,
                   h->d_s, h->d_Estat, h->d_x, h->d_r, h->d_z, h->d_p, h->d_mu, h->d_E,
-                  h->d_tab64, h->d_tab32, h->d_rho, h->d_force, h->d_part, h->d_out, h->d_pack};
+                  h->d_tab64, h->d_tab32, h->d_rho, h->d_force, h->d_part, h->d_out, h->d_pack,
+                  h->d_w, h->d_rhs, h->d_lam, h->d_ch, h->d_grad, h->d_info, h->d_gin};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (h->h_out) cudaFreeHost(h->h_out);
@@ -635,6 +711,169 @@ int mdff_gpu_batch_info(mdff_batch_handle h, int* ntot, int* nconf, int* cluster
   if (cluster) *cluster = h->shape.cluster;
   if (threads) *threads = h->shape.threads;
   if (ms_last) *ms_last = h->ms_last;
+  return MDFF_OK;
+}
+
+int mdff_gpu_batch_fit_define(mdff_batch_handle h, int nparam, const int* kind, const int* t1,
+                              const int* t2) {
+  if (!h || nparam < 0 || nparam > kFitMax || (nparam > 0 && (!kind || !t1 || !t2))) {
+    if (h) h->err = "0 <= nparam <= 16 and kind/t1/t2 arrays required";
+    return MDFF_ERR_BAD_ARGS;
+  }
+  for (int c = 0; c < h->nconf; ++c)
+    if (h->pconf[c].lsurf) {
+      h->err = "the fit gradient does not cover the surface term (lsurf)";
+      return MDFF_ERR_BAD_ARGS;
+    }
+  int ntmin = MDFF_NTYPEMAX;
+  for (const auto& p : h->base) ntmin = std::min(ntmin, p.ntype);
+  h->nparam = nparam;
+  h->theta.assign(nparam, 0.0);
+  // initial values from the parameter set of the first configuration
+  const mdff_params& p0 = h->base[h->pset_of[0]];
+  for (int k = 0; k < nparam; ++k) {
+    FitParam f{kind[k], t1[k], t2[k], 0};
+    bool types_ok = f.t1 >= 0 && f.t1 < ntmin && f.t2 >= 0 && f.t2 < ntmin;
+    if (f.kind < FIT_A || f.kind > FIT_QSCALE || (f.kind != FIT_QSCALE && !types_ok)) {
+      h->err = "fit parameter " + std::to_string(k) + ": unknown kind or type index";
+      h->nparam = 0;
+      return MDFF_ERR_BAD_ARGS;
+    }
+    h->prm[k] = f;
+    int a = f.t1, b = f.t2;
+    switch (f.kind) {
+      case FIT_A: h->theta[k] = p0.Abmhftd[a][b]; break;
+      case FIT_RHO: h->theta[k] = p0.Bbmhftd[a][b] != 0.0 ? 1.0 / p0.Bbmhftd[a][b] : 0.0; break;
+      case FIT_C: h->theta[k] = p0.Cbmhftd[a][b]; break;
+      case FIT_POL: h->theta[k] = p0.poldip[a][0][0]; break;
+      case FIT_TTB: h->theta[k] = p0.pol_damp_b[a][b][a]; break;
+      case FIT_TTC: h->theta[k] = p0.pol_damp_c[a][b][a]; break;
+      case FIT_QSCALE: h->theta[k] = 1.0; break;
+    }
+  }
+  BCK(cudaSetDevice(h->device));
+  if (!h->d_w) {
+    size_t nk = (size_t)std::max<long long>(h->ktot, 1);
+    BALLOC(h->d_w, h->ntot);
+    BALLOC(h->d_rhs, h->ntot);
+    BALLOC(h->d_lam, h->ntot);
+    BALLOC(h->d_ch, 5 * nk);
+    BALLOC(h->d_grad, (size_t)h->nconf * kFitMax);
+    BALLOC(h->d_info, (size_t)h->nconf * 4);
+    BALLOC(h->d_gin, (size_t)h->nconf + 6 * (size_t)h->ntot);
+  }
+  return MDFF_OK;
+}
+
+int mdff_gpu_batch_fit_set(mdff_batch_handle h, const double* theta) {
+  if (!h || !theta) return MDFF_ERR_BAD_ARGS;
+  for (int k = 0; k < h->nparam; ++k) {
+    if (!std::isfinite(theta[k]) || (h->prm[k].kind == FIT_RHO && theta[k] <= 0.0) ||
+        (h->prm[k].kind == FIT_POL && theta[k] <= 0.0)) {
+      h->err = "fit parameter " + std::to_string(k) + " out of its domain";
+      return MDFF_ERR_BAD_ARGS;
+    }
+  }
+  h->theta.assign(theta, theta + h->nparam);
+  BCK(cudaSetDevice(h->device));
+  return refit_tables(h);
+}
+
+int mdff_gpu_batch_fit_get(mdff_batch_handle h, double* theta) {
+  if (!h || !theta) return MDFF_ERR_BAD_ARGS;
+  for (int k = 0; k < h->nparam; ++k) theta[k] = h->theta[k];
+  return MDFF_OK;
+}
+
+int mdff_gpu_batch_adjoint(mdff_batch_handle h, const double* gE, const double* gF,
+                           const double* gmu, int on_device, double* grad, double* grad_conf) {
+  if (!h || !gE || !gF || !grad) return MDFF_ERR_BAD_ARGS;
+  if (!h->have_pos || h->nparam == 0) {
+    h->err = "adjoint needs fit_define and a forward evaluation first";
+    return MDFF_ERR_BAD_ARGS;
+  }
+  BCK(cudaSetDevice(h->device));
+  const double *dgE = gE, *dgF = gF, *dgmu = gmu;
+  if (!on_device) {
+    double* g0 = h->d_gin;
+    BCK(cudaMemcpyAsync(g0, gE, sizeof(double) * h->nconf, cudaMemcpyHostToDevice, h->st));
+    BCK(cudaMemcpyAsync(g0 + h->nconf, gF, sizeof(double) * 3 * h->ntot, cudaMemcpyHostToDevice, h->st));
+    dgE = g0;
+    dgF = g0 + h->nconf;
+    if (gmu) {
+      BCK(cudaMemcpyAsync(g0 + h->nconf + 3 * (size_t)h->ntot, gmu, sizeof(double) * 3 * h->ntot,
+                          cudaMemcpyHostToDevice, h->st));
+      dgmu = g0 + h->nconf + 3 * (size_t)h->ntot;
+    }
+  }
+  AdjArgs J;
+  J.gE = dgE;
+  J.gF = dgF;
+  J.gmu = dgmu;
+  J.w = h->d_w;
+  J.rhs = h->d_rhs;
+  J.lam = h->d_lam;
+  size_t nk = (size_t)std::max<long long>(h->ktot, 1);
+  J.rq = h->d_ch;
+  J.rm = h->d_ch + nk;
+  J.sq = h->d_ch + 2 * nk;
+  J.sm = h->d_ch + 3 * nk;
+  J.rl = h->d_ch + 4 * nk;
+  J.grad = h->d_grad;
+  J.info = h->d_info;
+  J.qscale = 1.0;
+  for (int k = 0; k < h->nparam; ++k)
+    if (h->prm[k].kind == FIT_QSCALE) J.qscale = h->theta[k];
+  J.tol_rel = 1e-12;
+  J.nparam = h->nparam;
+  for (int k = 0; k < kFitMax; ++k) J.prm[k] = (k < h->nparam) ? h->prm[k] : FitParam{-1, 0, 0, 0};
+  // launch: the forward's shape, persistent clusters
+  Shape sh = h->shape;
+  size_t smem = batch_smem_extra_offset(h->nmax) + sizeof(double4) * h->nmax;
+  if (smem > 227 * 1024) {
+    h->err = "configurations too large for the adjoint's shared-memory layout";
+    return MDFF_ERR_BAD_ARGS;
+  }
+  BCK(cudaFuncSetAttribute(k_batch_adjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = sh.cluster;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cfg.blockDim = dim3(sh.threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.gridDim = dim3(sh.cluster);
+  int ncl = 0;
+  BCK(cudaOccupancyMaxActiveClusters(&ncl, (void*)k_batch_adjoint, &cfg));
+  if (ncl <= 0) {
+    h->err = "adjoint launch shape does not fit on the device";
+    return MDFF_ERR_CUDA;
+  }
+  ncl = std::min(ncl, h->nconf);
+  cfg.gridDim = dim3(sh.cluster * ncl);
+  cfg.stream = h->st;
+  BatchArgs a = make_args(h, h->graph_pos, h->graph_force);
+  BCK(cudaMemsetAsync(h->d_queue, 0, sizeof(int), h->st));
+  BCK(cudaEventRecord(h->ev0, h->st));
+  BCK(cudaLaunchKernelEx(&cfg, k_batch_adjoint, a, J, h->nmax));
+  BCK(cudaEventRecord(h->ev1, h->st));
+  std::vector<double> gc((size_t)h->nconf * kFitMax);
+  BCK(cudaMemcpyAsync(gc.data(), h->d_grad, sizeof(double) * gc.size(), cudaMemcpyDeviceToHost, h->st));
+  BCK(cudaStreamSynchronize(h->st));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+  h->ms_adjoint = ms;
+  for (int k = 0; k < h->nparam; ++k) {
+    double s = 0.0;
+    for (int c = 0; c < h->nconf; ++c) s += gc[(size_t)c * kFitMax + k];
+    grad[k] = s;
+  }
+  if (grad_conf)
+    for (int c = 0; c < h->nconf; ++c)
+      for (int k = 0; k < h->nparam; ++k) grad_conf[(size_t)c * h->nparam + k] = gc[(size_t)c * kFitMax + k];
   return MDFF_OK;
 }
 

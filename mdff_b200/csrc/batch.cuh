@@ -125,6 +125,12 @@ __host__ __device__ inline size_t batch_smem_bytes(int nmax) {
   return b;
 }
 
+// offset of the adjoint's extra [nmax] double4 array after the layout
+// (rounded up to 16 bytes: vector loads need the alignment)
+__host__ __device__ inline size_t batch_smem_extra_offset(int nmax) {
+  return (batch_smem_bytes(nmax) + 15) & ~(size_t)15;
+}
+
 __device__ inline BShared batch_smem(unsigned char* base, int nmax) {
   BShared S;
   size_t o = 0;
@@ -688,6 +694,103 @@ __device__ void bmatvec(cgx::cluster_group& cl, const BatchArgs& a, BCtx& X, con
   __syncthreads();
 }
 
+// PCG on (alpha^-1 - T) x = b over the polarisable ions of the configuration,
+// x holding the first guess.  The true residual is formed with the FP64
+// operator; with MIXED the inner iterations use the FP32 operator and stop
+// at 1e-4 of that residual (iterative refinement), else they run to tol.
+// Stops on the reference's rmsd measure (get_rmsd_mu, moment_from_pola.f90:
+// 998-1027) <= tol, or after maxit inner iterations / 8 refinements.
+template <bool MIXED>
+__device__ void bsolve(cgx::cluster_group& cl, const BatchArgs& a, BCtx& X, const BShared& S,
+                       const double4* __restrict__ b, double4* __restrict__ x, double tol,
+                       int maxit, int& iters, double& rmsd) {
+  typedef typename std::conditional<MIXED, float, double>::type RM;
+  const BConf& c = *X.c;
+  const double npol = (double)max(c.npol, 1);
+  int outer = 0;
+  iters = 0;
+  while (true) {
+    // true residual with the FP64 operator
+    bmatvec<double>(cl, a, X, S, x, a.p);
+    double v2[2] = {0.0, 0.0};
+    for (int i = X.i0 + threadIdx.x; i < X.i1; i += blockDim.x) {
+      int gi = X.off + i;
+      double4 ri = make_double4(0, 0, 0, 0), zi = make_double4(0, 0, 0, 0);
+      if (a.ipol[gi]) {
+        double4 ax = bmat3(a.inv + 9 * (size_t)gi, x[gi]);
+        double4 bi = b[gi], tx = a.p[gi];
+        ri = make_double4(bi.x + tx.x - ax.x, bi.y + tx.y - ax.y, bi.z + tx.z - ax.z, 0.0);
+        zi = bmat3(a.pol + 9 * (size_t)gi, ri);
+        const double* pl = a.pol + 9 * (size_t)gi;
+        double rr[3] = {ri.x, ri.y, ri.z};
+        for (int d = 0; d < 3; ++d)
+          if (pl[4 * d] != 0.0) v2[1] += rr[d] * rr[d];
+      }
+      a.r[gi] = ri;
+      a.z[gi] = zi;
+      a.p[gi] = zi;
+      v2[0] += ri.x * zi.x + ri.y * zi.y + ri.z * zi.z;
+    }
+    cluster_sum<2>(cl, X, S, v2);
+    double rz = v2[0];
+    rmsd = sqrt(v2[1] / npol);
+    if (rmsd <= tol || iters >= maxit || outer >= 8) break;
+    ++outer;
+    const double tol_in = MIXED ? fmax(tol, 1e-4 * rmsd) : tol;
+    while (true) {
+      // Tp into Estat-free scratch: a.E (own rows) holds T p
+      bmatvec<RM>(cl, a, X, S, a.p, a.E);
+      double pq[1] = {0.0};
+      for (int i = X.i0 + threadIdx.x; i < X.i1; i += blockDim.x) {
+        int gi = X.off + i;
+        double4 qi = make_double4(0, 0, 0, 0);
+        if (a.ipol[gi]) {
+          double4 ap = bmat3(a.inv + 9 * (size_t)gi, a.p[gi]);
+          double4 tp = a.E[gi];
+          qi = make_double4(ap.x - tp.x, ap.y - tp.y, ap.z - tp.z, 0.0);
+        }
+        a.E[gi] = qi;  // q = A p
+        double4 pi = a.p[gi];
+        pq[0] += pi.x * qi.x + pi.y * qi.y + pi.z * qi.z;
+      }
+      cluster_sum<1>(cl, X, S, pq);
+      double alp = (pq[0] != 0.0) ? rz / pq[0] : 0.0;
+      double u2[2] = {0.0, 0.0};
+      for (int i = X.i0 + threadIdx.x; i < X.i1; i += blockDim.x) {
+        int gi = X.off + i;
+        if (!a.ipol[gi]) continue;
+        double4 xi = x[gi], ri = a.r[gi], pi = a.p[gi], qi = a.E[gi];
+        xi.x += alp * pi.x;
+        xi.y += alp * pi.y;
+        xi.z += alp * pi.z;
+        ri.x -= alp * qi.x;
+        ri.y -= alp * qi.y;
+        ri.z -= alp * qi.z;
+        double4 zi = bmat3(a.pol + 9 * (size_t)gi, ri);
+        x[gi] = xi;
+        a.r[gi] = ri;
+        a.z[gi] = zi;
+        u2[0] += ri.x * zi.x + ri.y * zi.y + ri.z * zi.z;
+        const double* pl = a.pol + 9 * (size_t)gi;
+        double rr[3] = {ri.x, ri.y, ri.z};
+        for (int d = 0; d < 3; ++d)
+          if (pl[4 * d] != 0.0) u2[1] += rr[d] * rr[d];
+      }
+      cluster_sum<2>(cl, X, S, u2);
+      ++iters;
+      double rms_in = sqrt(u2[1] / npol);
+      if (!(rms_in > tol_in && iters < maxit)) break;
+      double be = (rz != 0.0) ? u2[0] / rz : 0.0;
+      rz = u2[0];
+      for (int i = X.i0 + threadIdx.x; i < X.i1; i += blockDim.x) {
+        int gi = X.off + i;
+        double4 pi = a.p[gi], zi = a.z[gi];
+        a.p[gi] = make_double4(zi.x + be * pi.x, zi.y + be * pi.y, zi.z + be * pi.z, 0.0);
+      }
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // one configuration, whole cluster
 template <bool MIXED>
@@ -790,89 +893,7 @@ __device__ void bconfig(cgx::cluster_group& cl, const BatchArgs& a, BCtx& X, con
       a.x[gi] = a.ipol[gi] ? bmat3(a.pol + 9 * (size_t)gi, a.Estat[gi]) : make_double4(0, 0, 0, 0);
     }
     const double tol = c.tol;
-    const int maxit = c.maxit;
-    const double npol = (double)max(c.npol, 1);
-    int outer = 0;
-    while (true) {
-      // true residual with the FP64 operator
-      bmatvec<double>(cl, a, X, S, a.x, a.p);
-      double v2[2] = {0.0, 0.0};
-      for (int i = X.i0 + threadIdx.x; i < X.i1; i += blockDim.x) {
-        int gi = X.off + i;
-        double4 ri = make_double4(0, 0, 0, 0), zi = make_double4(0, 0, 0, 0);
-        if (a.ipol[gi]) {
-          double4 ax = bmat3(a.inv + 9 * (size_t)gi, a.x[gi]);
-          double4 b = a.Estat[gi], tx = a.p[gi];
-          ri = make_double4(b.x + tx.x - ax.x, b.y + tx.y - ax.y, b.z + tx.z - ax.z, 0.0);
-          zi = bmat3(a.pol + 9 * (size_t)gi, ri);
-          const double* pl = a.pol + 9 * (size_t)gi;
-          double rr[3] = {ri.x, ri.y, ri.z};
-          for (int d = 0; d < 3; ++d)
-            if (pl[4 * d] != 0.0) v2[1] += rr[d] * rr[d];
-        }
-        a.r[gi] = ri;
-        a.z[gi] = zi;
-        a.p[gi] = zi;
-        v2[0] += ri.x * zi.x + ri.y * zi.y + ri.z * zi.z;
-      }
-      cluster_sum<2>(cl, X, S, v2);
-      double rz = v2[0];
-      rmsd = sqrt(v2[1] / npol);
-      if (rmsd <= tol || iters >= maxit || outer >= 8) break;
-      ++outer;
-      const double tol_in = MIXED ? fmax(tol, 1e-4 * rmsd) : tol;
-      while (true) {
-        // Tp into Estat-free scratch: a.E (own rows) holds T p
-        bmatvec<RM>(cl, a, X, S, a.p, a.E);
-        double pq[1] = {0.0};
-        for (int i = X.i0 + threadIdx.x; i < X.i1; i += blockDim.x) {
-          int gi = X.off + i;
-          double4 qi = make_double4(0, 0, 0, 0);
-          if (a.ipol[gi]) {
-            double4 ap = bmat3(a.inv + 9 * (size_t)gi, a.p[gi]);
-            double4 tp = a.E[gi];
-            qi = make_double4(ap.x - tp.x, ap.y - tp.y, ap.z - tp.z, 0.0);
-          }
-          a.E[gi] = qi;  // q = A p
-          double4 pi = a.p[gi];
-          pq[0] += pi.x * qi.x + pi.y * qi.y + pi.z * qi.z;
-        }
-        cluster_sum<1>(cl, X, S, pq);
-        double alp = (pq[0] != 0.0) ? rz / pq[0] : 0.0;
-        double u2[2] = {0.0, 0.0};
-        for (int i = X.i0 + threadIdx.x; i < X.i1; i += blockDim.x) {
-          int gi = X.off + i;
-          if (!a.ipol[gi]) continue;
-          double4 xi = a.x[gi], ri = a.r[gi], pi = a.p[gi], qi = a.E[gi];
-          xi.x += alp * pi.x;
-          xi.y += alp * pi.y;
-          xi.z += alp * pi.z;
-          ri.x -= alp * qi.x;
-          ri.y -= alp * qi.y;
-          ri.z -= alp * qi.z;
-          double4 zi = bmat3(a.pol + 9 * (size_t)gi, ri);
-          a.x[gi] = xi;
-          a.r[gi] = ri;
-          a.z[gi] = zi;
-          u2[0] += ri.x * zi.x + ri.y * zi.y + ri.z * zi.z;
-          const double* pl = a.pol + 9 * (size_t)gi;
-          double rr[3] = {ri.x, ri.y, ri.z};
-          for (int d = 0; d < 3; ++d)
-            if (pl[4 * d] != 0.0) u2[1] += rr[d] * rr[d];
-        }
-        cluster_sum<2>(cl, X, S, u2);
-        ++iters;
-        double rms_in = sqrt(u2[1] / npol);
-        if (!(rms_in > tol_in && iters < maxit)) break;
-        double be = (rz != 0.0) ? u2[0] / rz : 0.0;
-        rz = u2[0];
-        for (int i = X.i0 + threadIdx.x; i < X.i1; i += blockDim.x) {
-          int gi = X.off + i;
-          double4 pi = a.p[gi], zi = a.z[gi];
-          a.p[gi] = make_double4(zi.x + be * pi.x, zi.y + be * pi.y, zi.z + be * pi.z, 0.0);
-        }
-      }
-    }
+    bsolve<MIXED>(cl, a, X, S, a.Estat, a.x, tol, c.maxit, iters, rmsd);
     conv = rmsd <= tol ? 1 : 0;
   }
   // ---- u_pol, total dipoles, catastrophe ---------------------------------

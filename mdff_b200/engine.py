@@ -241,3 +241,48 @@ class BatchEngine:
                                                   ctypes.byref(ms)), "batch_info")
         return dict(ntot=v[0].value, nconf=v[1].value, cluster=v[2].value, threads=v[3].value,
                     ms_last=ms.value)
+
+    # -- force-field gradients ---------------------------------------------
+    def fit_define(self, params):
+        """params: list of (kind, t1, t2) with kinds _abi.FIT_*; returns the
+        current values (theta) of those parameters."""
+        k = np.array([p[0] for p in params], dtype=np.int32)
+        t1 = np.array([p[1] for p in params], dtype=np.int32)
+        t2 = np.array([p[2] for p in params], dtype=np.int32)
+        self.nparam = len(params)
+        self._check(self._lib.mdff_gpu_batch_fit_define(self._h, self.nparam, iptr(k), iptr(t1),
+                                                        iptr(t2)), "batch_fit_define")
+        return self.fit_get()
+
+    def fit_set(self, theta):
+        th = np.ascontiguousarray(theta, dtype=np.float64)
+        self._check(self._lib.mdff_gpu_batch_fit_set(self._h, dptr(th)), "batch_fit_set")
+
+    def fit_get(self):
+        th = np.zeros(self.nparam)
+        self._check(self._lib.mdff_gpu_batch_fit_get(self._h, dptr(th)), "batch_fit_get")
+        return th
+
+    def adjoint(self, gE, gF, gmu=None, per_conf=False):
+        """dJ/dtheta for host arrays gE [nconf], gF [ntot, 3] (or SoA [3, ntot]),
+        gmu [ntot, 3] (optional), at the positions of the last engforce."""
+        gE = np.ascontiguousarray(gE, dtype=np.float64)
+        gF = np.asarray(gF, dtype=np.float64)
+        if gF.shape == (self.ntot, 3):
+            gF = gF.T
+        gF = np.ascontiguousarray(gF)
+        gm = None if gmu is None else np.ascontiguousarray(gmu, dtype=np.float64)
+        grad = np.zeros(self.nparam)
+        gc = np.zeros((self.nconf, self.nparam)) if per_conf else None
+        st = self._lib.mdff_gpu_batch_adjoint(self._h, gE.ctypes.data, gF.ctypes.data,
+                                              None if gm is None else gm.ctypes.data, 0,
+                                              dptr(grad), dptr(gc) if per_conf else None)
+        self._check(st, "batch_adjoint")
+        return (grad, gc) if per_conf else grad
+
+    def adjoint_device(self, d_gE, d_gF, d_gmu=0):
+        grad = np.zeros(self.nparam)
+        st = self._lib.mdff_gpu_batch_adjoint(self._h, ctypes.c_void_p(d_gE), ctypes.c_void_p(d_gF),
+                                              ctypes.c_void_p(d_gmu or None), 1, dptr(grad), None)
+        self._check(st, "batch_adjoint")
+        return grad

@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--relax", type=int, default=300, help="FIRE iterations before MD")
     ap.add_argument("--equil", type=int, default=50, help="rescaled MD steps before warm-up")
     ap.add_argument("--drift-steps", type=int, default=5000, help="NVE steps for the energy drift")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-evaluation measurement")
+    ap.add_argument("--no-fit", action="store_true", help="skip the fitting-gradient measurement")
     return ap.parse_args()
 
 
@@ -493,6 +495,127 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_batch_bench(local_rank, cpu=True):
+    """Batched evaluation: 256 independent rock-salt boxes (NaCl / MgO type,
+    64-1000 ions, seed 99) per call through the persistent cluster kernel;
+    mixed and FP64, launch shape from the autotuner, device time (CUDA events
+    in the library) and end to end with host arrays."""
+    import torch
+    from mdff_b200 import _abi, systems
+    from mdff_b200.engine import BatchEngine
+    out = {"workload": "256 cubic rock-salt boxes, NaCl/MgO type, 64-1000 ions (seed 99)"}
+    forces = {}
+    for prec, tag in ((_abi.PREC_MIXED, "mixed"), (_abi.PREC_FP64, "fp64")):
+        ps, cf, pos = systems.batch(nconf=256, seed=99, precision=prec)
+        P = np.concatenate(pos)
+        for p in ps:
+            p.device = local_rank
+        with BatchEngine(ps, cf) as eng:
+            r = eng.engforce(P[:, 0], P[:, 1], P[:, 2])
+            shape = eng.tune()
+            ms = []
+            for _ in range(10):
+                eng.engforce(P[:, 0], P[:, 1], P[:, 2])
+                ms.append(eng.info()["ms_last"])
+            # end to end: host positions in, host forces / dipoles / fields out
+            t0 = time.perf_counter()
+            for _ in range(5):
+                r = eng.engforce(P[:, 0], P[:, 1], P[:, 2])
+            e2e = (time.perf_counter() - t0) / 5
+            forces[tag] = np.stack([r["fx"], r["fy"], r["fz"]], 1)
+            its = [c["n_pol_iter"] for c in r["conf"] if c["n_pol_iter"] > 0]
+            out[tag] = {"ms": float(np.median(ms)), "configs_per_s": 256e3 / float(np.median(ms)),
+                        "ions_per_s": eng.ntot * 1e3 / float(np.median(ms)),
+                        "e2e_configs_per_s": 256 / e2e, "shape": {"cluster": shape[0],
+                                                                   "threads": shape[1]},
+                        "cg_iters_mean": float(np.mean(its)) if its else 0.0}
+            out["ntot"] = eng.ntot
+    f64 = forces["fp64"]
+    out["force_err_rms_rel_mixed_vs_fp64"] = float(np.sqrt(((forces["mixed"] - f64) ** 2).sum() /
+                                                           (f64 ** 2).sum()))
+    if cpu:
+        # CPU oracle on a sample of the same boxes (OpenMP, all host threads)
+        from oracle import oracle as orc
+        ps, cf, pos = systems.batch(nconf=256, seed=99, precision=_abi.PREC_FP64)
+        idx = list(range(0, 256, 32))
+        t0 = time.perf_counter()
+        nat = 0
+        for k in idx:
+            p = systems.config_params(ps, cf[k])
+            p.solver = _abi.SOLVER_SCF
+            orc.Oracle(p, cf[k][2]).engforce(pos[k][:, 0], pos[k][:, 1], pos[k][:, 2])
+            nat += pos[k].shape[0]
+        dt = time.perf_counter() - t0
+        out["cpu_oracle"] = {"configs_per_s": len(idx) / dt, "sample": f"{len(idx)} of the 256 boxes "
+                             f"({nat} ions), SCF to 1e-8", "cores": orc.lib().or_get_threads()}
+    torch.cuda.synchronize()
+    return out
+
+
+def run_fit_bench(local_rank):
+    """Differentiable fitting: 64 MgO-type boxes of 216-512 ions, 10 parameters,
+    force-matching loss against forces of the FP64 engine at parameters
+    perturbed by 5 % (seeded).  Times one loss + gradient (forward + adjoint),
+    checks the gradient against central differences (h = 1e-5 relative) and
+    runs a short L-BFGS fit from the unperturbed start."""
+    import torch
+    from mdff_b200 import fit
+    psets, configs, pos, theta_true = fit.fitting_workload()
+    for p in psets:
+        p.device = local_rank
+    ff = fit.BatchForceField(psets, configs, fit.MGO_FIT)
+    Fn = fit.EngForceFn()
+    P = torch.tensor(np.ascontiguousarray(np.concatenate(pos).T), dtype=torch.float64,
+                     device=f"cuda:{local_rank}")
+    with torch.no_grad():
+        Ft = Fn.apply(torch.tensor(theta_true), ff, P)[1].clone()
+    theta0 = ff.theta0.copy()
+
+    def loss_grad(th_np):
+        th = torch.tensor(th_np, dtype=torch.float64, requires_grad=True)
+        U, F, mu = Fn.apply(th, ff, P)
+        loss = ((F - Ft) ** 2).sum()
+        loss.backward()
+        return float(loss.detach()), th.grad.numpy().copy()
+
+    loss_grad(theta0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(5):
+        l0, g0 = loss_grad(theta0)
+    torch.cuda.synchronize()
+    t_lg = (time.perf_counter() - t0) / 5
+    info = ff.engine.info()
+    # central differences of the loss
+    fd = np.zeros_like(theta0)
+    for k in range(theta0.size):
+        h = 1e-5 * max(abs(theta0[k]), 1.0)
+        tp, tm = theta0.copy(), theta0.copy()
+        tp[k] += h
+        tm[k] -= h
+        with torch.no_grad():
+            lp = float(((Fn.apply(torch.tensor(tp), ff, P)[1] - Ft) ** 2).sum())
+            lm = float(((Fn.apply(torch.tensor(tm), ff, P)[1] - Ft) ** 2).sum())
+        fd[k] = (lp - lm) / (2 * h)
+    sc = np.maximum(np.abs(theta0), 1.0)
+    err = np.abs(sc * (g0 - fd)) / np.abs(sc * fd).max()
+    # short fit in scaled variables
+    from scipy.optimize import minimize
+    res = minimize(lambda z: (lambda lg: (lg[0], lg[1] * sc))(loss_grad(z * sc)), theta0 / sc,
+                   jac=True, method="L-BFGS-B", options={"maxiter": 40})
+    th_fit = res.x * sc
+    ff.close()
+    return {"workload": "64 MgO-type boxes, 216-512 ions, 10 parameters, FP64 (seed 2027)",
+            "ntot": int(P.shape[1]), "ms_loss_and_grad": 1e3 * t_lg,
+            "ms_forward_device": info["ms_last"], "loss0": l0,
+            "fd_check_max_scaled_err": float(err.max()),
+            "fd_check": dict(zip(fit.param_names(fit.MGO_FIT), [float(e) for e in err])),
+            "lbfgs": {"iterations": int(res.nit), "evaluations": int(res.nfev),
+                      "loss_final": float(res.fun),
+                      "max_rel_err_vs_true_params": float(np.max(np.abs(th_fit - theta_true) /
+                                                                 np.maximum(np.abs(theta_true), 1.0)))}}
+
+
 def main():
     args = parse()
     rank, world, local_rank = replicas.world()
@@ -538,6 +661,10 @@ def main():
                 "sample": f"one warm-start engforce (= one MD step, SCF to 1e-8, {nscf} iterations) "
                           f"of the {wl['natm']}-ion workload at the GPU run's last configuration; "
                           f"C restatement of the reference engforce, OpenMP {cores} threads"}
+        if world == 1 and not args.no_batch:
+            line["batch"] = run_batch_bench(local_rank, cpu=not args.no_cpu)
+        if world == 1 and not args.no_fit:
+            line["fitting"] = run_fit_bench(local_rank)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

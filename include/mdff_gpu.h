@@ -151,6 +151,9 @@ typedef struct mdff_stats {
   double cutlongrange;                    /* after the half-cell clamp           */
   int n_launches;                         /* kernels launched by last call       */
   double ms_last;                         /* device time of last call (ms)       */
+  double rmsd_initial;                    /* CG: rmsd of the first guess (e/A^2) */
+  int n_fp64_residuals;                   /* CG: FP64 residual evaluations       */
+  int pad;
 } mdff_stats;
 
 typedef struct mdff_ctx* mdff_handle;

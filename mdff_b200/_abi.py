@@ -78,7 +78,8 @@ class MdffStats(ctypes.Structure):
         ("n_pol_iter", _i), ("converged", _i), ("rmsd", _d),
         ("list_rebuilds", _i), ("list_capacity", _i), ("list_needed", _i),
         ("nk", _i), ("alphaES", _d), ("kES", _i * 3), ("cutlongrange", _d),
-        ("n_launches", _i), ("ms_last", _d),
+        ("n_launches", _i), ("ms_last", _d), ("rmsd_initial", _d), ("n_fp64_residuals", _i),
+        ("pad", _i),
     ]
 
 

@@ -736,7 +736,14 @@ __device__ void bsolve(cgx::cluster_group& cl, const BatchArgs& a, BCtx& X, cons
     rmsd = sqrt(v2[1] / npol);
     if (rmsd <= tol || iters >= maxit || outer >= 8) break;
     ++outer;
-    const double tol_in = MIXED ? fmax(tol, 1e-4 * rmsd) : tol;
+    // FP64 operator: the recurrence residual is final.  FP32 operator: trusted
+    // to half the tolerance when the starting residual is small (the drift from
+    // the true residual is ~ the FP32 matvec error times that start), else a
+    // 1e-4 reduction and a new FP64 residual (iterative refinement).
+    const double kGap = 3e-6;
+    const bool trust = !MIXED || kGap * rmsd <= 0.5 * tol;
+    const double tol_in = !MIXED ? tol : (trust ? 0.5 * tol : fmax(tol, 1e-4 * rmsd));
+    double rms_last = rmsd;
     while (true) {
       // Tp into Estat-free scratch: a.E (own rows) holds T p
       bmatvec<RM>(cl, a, X, S, a.p, a.E);
@@ -779,6 +786,7 @@ __device__ void bsolve(cgx::cluster_group& cl, const BatchArgs& a, BCtx& X, cons
       cluster_sum<2>(cl, X, S, u2);
       ++iters;
       double rms_in = sqrt(u2[1] / npol);
+      rms_last = rms_in;
       if (!(rms_in > tol_in && iters < maxit)) break;
       double be = (rz != 0.0) ? u2[0] / rz : 0.0;
       rz = u2[0];
@@ -787,6 +795,10 @@ __device__ void bsolve(cgx::cluster_group& cl, const BatchArgs& a, BCtx& X, cons
         double4 pi = a.p[gi], zi = a.z[gi];
         a.p[gi] = make_double4(zi.x + be * pi.x, zi.y + be * pi.y, zi.z + be * pi.z, 0.0);
       }
+    }
+    if (trust && (rms_last <= tol_in || iters >= maxit)) {
+      rmsd = rms_last;
+      break;
     }
   }
 }

@@ -106,6 +106,11 @@ struct mdff_ctx {
   double4 *d_mu_tot = nullptr, *d_hist = nullptr, *d_E = nullptr;
   double4 *d_r = nullptr, *d_z = nullptr, *d_pv = nullptr, *d_qv = nullptr, *d_Tp = nullptr;
   float4* d_mu32 = nullptr;      // FP32 copy of the dipoles of an FP32 pass
+  // FP32 dipole-field pair cache of the mixed mode (k_static_cache), ELL [natm][cap]
+  float4* d_ddr = nullptr;
+  float* d_ddb1 = nullptr;
+  int *d_ddj = nullptr, *d_ddn = nullptr;
+  bool dd_cache_ok = false;
   // outputs / reductions
   double* d_force = nullptr;     // [3][natm]
   double* d_part = nullptr;
@@ -375,6 +380,19 @@ static int alloc_list(mdff_ctx* h, int cap) {
   h->L.nbr = nullptr;
   DALLOC(h->L.nbr, (size_t)h->natm * cap);
   h->L.cap = cap;
+  h->dd_cache_ok = false;
+  if (h->p.precision == MDFF_PREC_MIXED && h->lpolar) {
+    cudaFree(h->d_ddr);
+    cudaFree(h->d_ddb1);
+    cudaFree(h->d_ddj);
+    h->d_ddr = nullptr;
+    h->d_ddb1 = nullptr;
+    h->d_ddj = nullptr;
+    DALLOC(h->d_ddr, (size_t)h->natm * cap);
+    DALLOC(h->d_ddb1, (size_t)h->natm * cap);
+    DALLOC(h->d_ddj, (size_t)h->natm * cap);
+    if (!h->d_ddn) DALLOC(h->d_ddn, h->natm);
+  }
   h->stats.list_capacity = cap * h->natm;
   return MDFF_OK;
 }
@@ -585,7 +603,9 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   int s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, fp32 ? h->d_mu32 : nullptr);
   if (s) return s;
   int pr = prof_begin(h, KC_ESFIELD, 0);
-  if (fp32)
+  if (fp32 && dd_mask == 1 && h->dd_cache_ok)
+    k_dd_cached<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n, E);
+  else if (fp32)
     k_es_field<float, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu32, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
   else
     k_es_field<double, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
@@ -619,7 +639,15 @@ static int static_field(mdff_ctx* h, bool fp32) {
     k_to_float4<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_dipia, n, h->d_mu32);
     LAUNCH_CHECK();
   }
-  if (qq || dd) {
+  h->dd_cache_ok = false;
+  if (fp32 && !dd && h->lpolar && h->d_ddr) {
+    // damped charge field + the pair cache of the FP32 solver iterations
+    int pr = prof_begin(h, KC_ESFIELD, 0);
+    k_static_cache<<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, qq ? 1 : 0, E, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn);
+    LAUNCH_CHECK();
+    prof_end(h, pr);
+    h->dd_cache_ok = true;
+  } else if (qq || dd) {
     int pr = prof_begin(h, KC_ESFIELD, 0);
     if (fp32) {
       if (qq && dd) ESF(float, true, true, h->d_mu32);
@@ -1466,7 +1494,8 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_rchunk, h->d_tab64, h->d_tab32, h->d_w, h->d_w32, h->d_rho_part, h->d_rhoA, h->d_str,
                   h->d_G, h->d_H, h->d_Estat, h->d_Eind, h->d_Efield, h->d_mu_ind, h->d_mu_tot,
                   h->d_hist, h->d_E, h->d_r, h->d_z, h->d_pv, h->d_qv, h->d_Tp, h->d_mu32, h->d_force,
-                  h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part};
+                  h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
+                  h->d_ddb1, h->d_ddj, h->d_ddn};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);

@@ -390,6 +390,127 @@ static __global__ void __launch_bounds__(256) k_es_field(
 }
 
 // --------------------------------------------------------------------------
+// FP32 static pass with a pair cache.  Same damped charge field as
+// k_es_field<float, true, false>, and in the same sweep the rows of the
+// polarisable ions keep, for every polarisable partner within rc, the FP32
+// terms of the undamped dipole field T2(r) mu = B2 r (r.mu) - B1 mu:
+//   cr[i][m] = (rx, ry, rz, B2), cb1[i][m] = B1, cj[i][m] = j,  cn[i] = count
+// (compacted with a warp ballot, row order kept).  The FP32 iterations of the
+// dipole solve then read these instead of recomputing erfc / exp per pair
+// (positions are fixed within a call).
+static __global__ void __launch_bounds__(256) k_static_cache(
+    const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
+    const int* __restrict__ ipolar, const int* __restrict__ nbr, const int* __restrict__ nnb,
+    int cap, int natm, const CellC* __restrict__ cell, const ESPair* __restrict__ tab, int ntype,
+    double alpha, double cutsq, int has_q, double4* __restrict__ E, float4* __restrict__ cr,
+    float* __restrict__ cb1, int* __restrict__ cj, int* __restrict__ cn) {
+  __shared__ ESPair stab[MDFF_NT * MDFF_NT];
+  __shared__ double cA[9];
+  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
+  if (threadIdx.x < 9) cA[threadIdx.x] = cell->A[threadIdx.x];
+  __syncthreads();
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= natm) return;
+  double4 si = s[i];
+  int ti = itype[i];
+  bool pol_i = ipolar[i] != 0;
+  int n = nnb[i];
+  const int* row = nbr + (size_t)i * cap;
+  size_t cbase = (size_t)i * cap;
+  float ex = 0.f, ey = 0.f, ez = 0.f;
+  const float rc2 = (float)cutsq;
+  int m = 0;
+  for (int k0 = 0; k0 < n; k0 += 32) {
+    int k = k0 + lane;
+    bool keep = false;
+    float rx = 0.f, ry = 0.f, rz = 0.f, B1 = 0.f, B2 = 0.f;
+    int j = 0;
+    if (k < n) {
+      j = row[k];
+      double4 sj = s[j];
+      float r2 = pair_vec<float>(cA, si, sj, rx, ry, rz);
+      if (r2 <= rc2) {  // ewald_dir.f90:202
+        double qj = has_q ? q[j] : 0.0;
+        bool pp = pol_i && ipolar[j] != 0;
+        if (pp || qj != 0.0) {
+          Radial<float> g;
+          radial<float, false>(r2, (float)alpha, g);
+          if (qj != 0.0) {
+            float F1d = 0.f;
+            int tj = itype[j];
+            bool i_is_a = half_mask(i, j);
+            int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
+            const ESPair& P = stab[ta * ntype + tb];
+            if (P.ldamp) {
+              float fdm, fdd;
+              if (i_is_a)
+                tt_damp<float>((float)P.ba, (float)P.ca, g.d, P.ka, fdm, fdd);
+              else
+                tt_damp<float>((float)P.bb, (float)P.cb, g.d, P.kb, fdm, fdd);
+              F1d = 1.f - fdm;
+            }
+            float c = (float)qj * g.dm3 * (g.F1 - F1d);
+            ex += c * rx;
+            ey += c * ry;
+            ez += c * rz;
+          }
+          if (pp) {
+            keep = true;
+            B1 = g.F1 * g.dm3;
+            B2 = 3.f * g.F2 * g.dm5;
+          }
+        }
+      }
+    }
+    unsigned bal = __ballot_sync(FULL_MASK, keep);
+    if (keep) {
+      int pos = m + __popc(bal & ((1u << lane) - 1u));
+      cr[cbase + pos] = make_float4(rx, ry, rz, B2);
+      cb1[cbase + pos] = B1;
+      cj[cbase + pos] = j;
+    }
+    m += __popc(bal);
+  }
+  double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
+  if (lane == 0) {
+    double4 o = E[i];
+    E[i] = make_double4(o.x + dx, o.y + dy, o.z + dz, 0.0);
+    cn[i] = m;
+  }
+}
+
+// FP32 dipole field of mu (float4) from the pair cache of k_static_cache:
+// E_i += sum_m T2(r_im) mu_j over the polarisable partners (k_es_field<float,
+// false, true> with dd_mask = 1, without the per-pair radial functions)
+static __global__ void __launch_bounds__(256) k_dd_cached(
+    const float4* __restrict__ mu, const float4* __restrict__ cr, const float* __restrict__ cb1,
+    const int* __restrict__ cj, const int* __restrict__ cn, int cap, int natm,
+    double4* __restrict__ E) {
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= natm) return;
+  int n = cn[i];
+  if (n == 0) return;
+  size_t base = (size_t)i * cap;
+  float ex = 0.f, ey = 0.f, ez = 0.f;
+  for (int k = lane; k < n; k += 32) {
+    float4 r = cr[base + k];
+    float B1 = cb1[base + k];
+    float4 m = mu[cj[base + k]];
+    float rm = r.x * m.x + r.y * m.y + r.z * m.z;
+    ex += r.w * r.x * rm - B1 * m.x;
+    ey += r.w * r.y * rm - B1 * m.y;
+    ez += r.w * r.z * rm - B1 * m.z;
+  }
+  double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
+  if (lane == 0) {
+    double4 o = E[i];
+    E[i] = make_double4(o.x + dx, o.y + dy, o.z + dz, 0.0);
+  }
+}
+
+// --------------------------------------------------------------------------
 // final real-space pass: qq + qd + dd with damping; energy, field, force,
 // stress.  Partials per block: [u, tau xx yy zz xy xz yz] -> 7 doubles
 // (tau is the reference's  - sum (r_j f_k + r_k f_j)  before *0.5/omega).

@@ -1,0 +1,410 @@
+"""The reference's input formats: POSFF configurations and control files of
+Fortran namelists, so that the engine runs the reference's own decks and
+writes decks the reference binary reads.
+
+* POSFF (read_pos.f90:36-158): natm, system name, the three lattice vectors
+  (one per line; columns of simu_cell%A), ntype, type names, ions per type,
+  'Direct'/'D' or 'Cartesian'/'C', then one line per ion: type name and
+  position (+ velocity (+ force) for posff_data 'rvn' / 'rvf').  Positions are
+  wrapped as the reader does: kardir, periodicbc (s - NINT(s)), dirkar
+  (read_pos.f90:148-150, lattice.f90:276-295).
+* Control files: namelist groups &controltag, &fieldtag, &non_bondedtag,
+  &coulombtag, &pimtag, &mdtag, ... (control.f90:128-161, field.f90:126-130,
+  non_bonded.f90:135-150, coulomb.f90:97-106, pim.f90:258-279), with the
+  reference's defaults (the *_default_tag routines).  '!INCLUDE <file>' lines
+  are replaced by the file, as the examples' deck generator does
+  (examples/ex09/config/gen_tests, include()).
+"""
+import os
+import re
+
+import numpy as np
+
+from . import _abi
+from .params import make_params
+
+# ---------------------------------------------------------------------------
+# POSFF
+
+
+def read_posff(path, posff_data="rnn"):
+    """Returns dict(natm, system, cell (3x3, columns = lattice vectors), ntype,
+    names, natmi, pos (natm, 3) Cartesian, wrapped), plus vel / force for
+    posff_data 'rvn' / 'rvf'."""
+    with open(path) as f:
+        lines = [ln for ln in f.read().splitlines()]
+    k = 0
+
+    def nxt():
+        nonlocal k
+        while k < len(lines) and not lines[k].strip():
+            k += 1
+        ln = lines[k]
+        k += 1
+        return ln.split()
+
+    natm = int(nxt()[0])
+    system = " ".join(nxt())
+    cols = [[float(x.replace("d", "e").replace("D", "e")) for x in nxt()[:3]] for _ in range(3)]
+    A = np.array(cols).T  # A(:, j) = lattice vector j
+    ntype = int(nxt()[0])
+    names = nxt()[:ntype]
+    natmi = [int(x) for x in nxt()[:ntype]]
+    cpos = nxt()[0]
+    if cpos not in ("Direct", "D", "Cartesian", "C"):
+        raise ValueError(f"POSFF coordinate tag {cpos!r} (read_pos.f90:80)")
+    ncol = {"rnn": 3, "rvn": 6, "rvf": 9}[posff_data]
+    typ, data = [], []
+    for _ in range(natm):
+        t = nxt()
+        typ.append(t[0])
+        data.append([float(x.replace("d", "e").replace("D", "e")) for x in t[1:1 + ncol]])
+    data = np.array(data, dtype=np.float64)
+    pos = data[:, :3].copy()
+    if cpos in ("Direct", "D"):
+        pos = pos @ A.T
+    B = np.linalg.inv(A)
+    s = pos @ B.T
+    s = s - np.where(s >= 0, np.floor(s + 0.5), np.ceil(s - 0.5))  # Fortran NINT
+    pos = s @ A.T
+    out = dict(natm=natm, system=system, cell=A, ntype=ntype, names=names, natmi=natmi,
+               pos=pos, types=typ)
+    if ncol >= 6:
+        out["vel"] = data[:, 3:6].copy()
+    if ncol == 9:
+        out["force"] = data[:, 6:9].copy()
+    return out
+
+
+def write_posff(path, system, cell, names, natmi, pos, vel=None, force=None):
+    """POSFF in Cartesian coordinates (ions grouped by type in names order)."""
+    A = np.asarray(cell, dtype=np.float64)
+    pos = np.asarray(pos, dtype=np.float64)
+    natm = pos.shape[0]
+    typ = np.repeat(np.arange(len(names)), natmi)
+    with open(path, "w") as f:
+        f.write(f"{natm}\n{system}\n")
+        for j in range(3):
+            f.write(" ".join(f"{A[a, j]:20.12f}" for a in range(3)) + "\n")
+        f.write(f"{len(names)}\n{' '.join(names)}\n{' '.join(str(n) for n in natmi)}\nCartesian\n")
+        for i in range(natm):
+            cols = list(pos[i])
+            if vel is not None:
+                cols += list(vel[i])
+            if force is not None:
+                cols += list(force[i])
+            f.write(f"{names[typ[i]]:>3s} " + " ".join(f"{x:22.14e}" for x in cols) + "\n")
+
+
+# ---------------------------------------------------------------------------
+# Fortran namelists
+
+
+def expand_includes(text, directory):
+    """Replace every line containing '!INCLUDE <file>' by the file's text
+    (the deck generator's sed include of examples/ex09/config/gen_tests)."""
+    out = []
+    for ln in text.splitlines():
+        m = re.search(r"!INCLUDE\s*<([^>]+)>", ln)
+        if m:
+            with open(os.path.join(directory, m.group(1))) as f:
+                out.extend(f.read().splitlines())
+        else:
+            out.append(ln)
+    return "\n".join(out)
+
+
+def _strip_comment(ln):
+    q = None
+    for i, ch in enumerate(ln):
+        if q:
+            if ch == q:
+                q = None
+        elif ch in "'\"":
+            q = ch
+        elif ch == "!":
+            return ln[:i]
+    return ln
+
+
+def _value(tok):
+    t = tok.strip()
+    if not t:
+        return None
+    if t[0] in "'\"":
+        return t[1:-1]
+    low = t.lower()
+    if low in (".true.", "t", ".t."):
+        return True
+    if low in (".false.", "f", ".f."):
+        return False
+    try:
+        if re.fullmatch(r"[+-]?\d+", t):
+            return int(t)
+        return float(low.replace("d", "e"))
+    except ValueError:
+        return t
+
+
+def _split_values(s):
+    vals, cur, q = [], "", None
+    for ch in s:
+        if q:
+            cur += ch
+            if ch == q:
+                q = None
+            continue
+        if ch in "'\"":
+            q = ch
+            cur += ch
+        elif ch in ", \t\n":
+            if cur:
+                vals.append(cur)
+            cur = ""
+        else:
+            cur += ch
+    if cur:
+        vals.append(cur)
+    out = []
+    for v in vals:
+        m = re.fullmatch(r"(\d+)\*(.+)", v)
+        if m:
+            out.extend([_value(m.group(2))] * int(m.group(1)))
+        else:
+            out.append(_value(v))
+    return out
+
+
+def read_namelists(text):
+    """Parse every namelist group of a control file.  Returns {group:
+    {name: value}} with names lower case; a plain assignment gives a value or
+    a list (list-directed fill from element 1), an indexed one gives
+    {(i, j, ...): value} entries (1-based indices as written)."""
+    groups = {}
+    clean = "\n".join(_strip_comment(ln) for ln in text.splitlines())
+    for m in re.finditer(r"&(\w+)(.*?)(?:&end\b|^\s*/\s*$)", clean, re.S | re.I | re.M):
+        name = m.group(1).lower()
+        if name == "end":
+            continue
+        body = m.group(2)
+        g = groups.setdefault(name, {})
+        asg = list(re.finditer(r"([A-Za-z_]\w*)\s*(\(([^)]*)\))?\s*=", body))
+        for a, b in zip(asg, asg[1:] + [None]):
+            key = a.group(1).lower()
+            seg = body[a.end(): b.start() if b else len(body)]
+            vals = _split_values(seg)
+            if a.group(2):
+                idx = tuple(int(x) for x in a.group(3).split(","))
+                ent = g.setdefault(key, {})
+                if not isinstance(ent, dict):
+                    ent = g[key] = {(i + 1,): v for i, v in enumerate(ent)}
+                if len(vals) == 1:
+                    ent[idx] = vals[0]
+                else:  # list-directed fill along the first index
+                    for k, v in enumerate(vals):
+                        ent[(idx[0] + k,) + idx[1:]] = v
+            else:
+                g[key] = vals[0] if len(vals) == 1 else vals
+    return groups
+
+
+def read_control(path, include_dir=None):
+    with open(path) as f:
+        text = f.read()
+    return read_namelists(expand_includes(text, include_dir or os.path.dirname(path) or "."))
+
+
+# ---------------------------------------------------------------------------
+# namelists -> mdff_params
+
+_CALC = {"md": _abi.CALC_MD, "opt": _abi.CALC_OPT}
+_TRUNC = {"notrunc": _abi.TRUNC_NONE, "linear": _abi.TRUNC_LINEAR, "quadratic": _abi.TRUNC_QUADRATIC}
+
+
+def _table(v, ndim, ntype):
+    """A per-type namelist entry as a {0-based index tuple: value} table."""
+    if v is None:
+        return None
+    if isinstance(v, dict):
+        return {tuple(i - 1 for i in k): x for k, x in v.items()}
+    vals = v if isinstance(v, list) else [v]
+    if ndim == 1:
+        return {(i,): x for i, x in enumerate(vals)}
+    raise ValueError("multi-index table given as a plain list")
+
+
+def params_from_namelists(nl, natmi, **extra):
+    """mdff_params for the ions per type natmi from parsed namelists, with the
+    reference's defaults for everything not given.  Unsupported switches of
+    the path (Morse, direct Coulomb, quadrupoles, Thole) raise ValueError."""
+    ntype = len(natmi)
+    c = nl.get("controltag", {})
+    fd = nl.get("fieldtag", {})
+    nb = nl.get("non_bondedtag", {})
+    cl = nl.get("coulombtag", {})
+    pm = nl.get("pimtag", {})
+    if c.get("lmorse", False):
+        raise ValueError("lmorse: Morse is never dispatched by engforce")
+    if str(c.get("longrange", "ewald")).lower() != "ewald":
+        raise ValueError("longrange must be 'ewald'")
+    if cl.get("thole_functions", False):
+        raise ValueError("thole_functions are not built")
+    kw = {}
+    for k in ("lcoulomb", "lbmhft", "lbmhftd", "lnmlj", "lsurf", "lreduced"):
+        if k in c:
+            kw[k] = int(bool(c[k]))
+    for k in ("cutshortrange", "cutlongrange", "skindiff"):
+        if k in c:
+            kw[k] = float(c[k])
+    calc = str(c.get("calc", "md")).lower()
+    kw["calc"] = _CALC.get(calc, _abi.CALC_OTHER)
+    if "ctrunc" in nb:
+        kw["trunc"] = _TRUNC[str(nb["ctrunc"]).lower()]
+    if "symmetric_pot" in nb:
+        kw["symmetric_pot_nb"] = int(bool(nb["symmetric_pot"]))
+    for k in ("epslj", "sigmalj", "plj", "qlj", "abmhftd", "bbmhftd", "cbmhftd", "dbmhftd",
+              "bdbmhftd"):
+        if k in nb:
+            name = {"abmhftd": "Abmhftd", "bbmhftd": "Bbmhftd", "cbmhftd": "Cbmhftd",
+                    "dbmhftd": "Dbmhftd", "bdbmhftd": "BDbmhftd"}.get(k, k)
+            kw[name] = _table(nb[k], 2, ntype)
+    if "qch" in fd:
+        q = fd["qch"]
+        q = q if isinstance(q, list) else [q] if not isinstance(q, dict) else \
+            [q.get((i + 1,), 0.0) for i in range(ntype)]
+        kw["qch"] = [float(x) for x in q]
+    if "dip" in fd:
+        t = _table(fd["dip"], 2, ntype)
+        dip = np.zeros((_abi.NT, 3))
+        for (it, a), v in t.items():
+            dip[it, a] = v
+        kw["dip"] = dip
+    for k in ("quad",):
+        if k in fd and any(float(v) != 0.0 for v in (_table(fd[k], 3, ntype) or {}).values()):
+            raise ValueError("quadrupoles are not built")
+    if "lautoes" in cl:
+        kw["lautoES"] = int(bool(cl["lautoes"]))
+    if "epsw" in cl:
+        kw["epsw"] = float(cl["epsw"])
+    if "alphaes" in cl:
+        kw["alphaES"] = float(cl["alphaes"])
+    if "kes" in cl:
+        k3 = cl["kes"]
+        kw["kES"] = tuple(int(x) for x in (k3 if isinstance(k3, list) else [k3] * 3))
+    if "symmetric_pot" in pm:
+        kw["symmetric_pot_pim"] = int(bool(pm["symmetric_pot"]))
+    for k in ("conv_tol_ind",):
+        if k in pm:
+            kw[k] = float(pm[k])
+    for k in ("min_scf_pol_iter", "max_scf_pol_iter", "extrapolate_order"):
+        if k in pm:
+            kw[k] = int(pm[k])
+    if "ldip_polar" in pm:
+        t = _table(pm["ldip_polar"], 1, ntype)
+        kw["ldip_polar"] = [int(bool(t.get((i,), False))) for i in range(ntype)]
+    if "poldip" in pm:
+        t = _table(pm["poldip"], 3, ntype)
+        pol = np.zeros((_abi.NT, 3, 3))
+        for (it, a, b), v in t.items():
+            pol[it, a, b] = v
+        kw["poldip"] = pol
+    if "poldip_iso" in pm:  # pim.f90:222-226
+        t = _table(pm["poldip_iso"], 1, ntype)
+        pol = kw.get("poldip", np.zeros((_abi.NT, 3, 3)))
+        for (it,), v in t.items():
+            if float(v) != 0.0:
+                pol[it] = np.eye(3) * float(v)
+        kw["poldip"] = pol
+    for k in ("ldip_damping", "pol_damp_b", "pol_damp_c", "pol_damp_k"):
+        if k in pm:
+            t = _table(pm[k], 3, ntype)
+            if k == "ldip_damping":
+                t = {i: int(bool(v)) for i, v in t.items()}
+            kw[k] = t
+    kw.update(extra)
+    return make_params(list(natmi), **kw)
+
+
+# ---------------------------------------------------------------------------
+# mdff_params -> control file
+
+
+def _f(x):
+    return f"{float(x):.16e}".replace("e", "d")
+
+
+def write_control(path, p, names, masses=None, calc="md", extra_md=None):
+    """A control file the reference reads for the parameters p (types named
+    names): &controltag, &mdtag, &fieldtag, &non_bondedtag, &coulombtag,
+    &pimtag with every non-default entry written explicitly."""
+    nt = p.ntype
+    L = []
+    L.append("&controltag")
+    L.append(f"  calc = '{calc}'")
+    for k in ("lcoulomb", "lbmhft", "lbmhftd", "lnmlj", "lsurf", "lreduced"):
+        L.append(f"  {k} = {'.true.' if getattr(p, k) else '.false.'}")
+    for k in ("cutshortrange", "cutlongrange", "skindiff"):
+        L.append(f"  {k} = {_f(getattr(p, k))}")
+    L.append("  longrange = 'ewald'")
+    L.append("&end")
+    L.append("&mdtag")
+    for k, v in (extra_md or {}).items():
+        L.append(f"  {k} = {v}")
+    L.append("&end")
+    L.append("&fieldtag")
+    if masses is not None:
+        L.append("  mass = " + " ".join(_f(m) for m in masses))
+    L.append("  qch = " + " ".join(_f(p.qch[i]) for i in range(nt)))
+    for it in range(nt):
+        for a in range(3):
+            if p.dip[it][a] != 0.0:
+                L.append(f"  dip({it + 1},{a + 1}) = {_f(p.dip[it][a])}")
+    L.append("&end")
+    L.append("&non_bondedtag")
+    L.append("  ctrunc = '" + {0: "notrunc", 1: "linear", 2: "quadratic"}[p.trunc] + "'")
+    L.append(f"  symmetric_pot = {'.true.' if p.symmetric_pot_nb else '.false.'}")
+    for name in ("epslj", "sigmalj", "Abmhftd", "Bbmhftd", "Cbmhftd", "Dbmhftd", "BDbmhftd"):
+        tab = getattr(p, name)
+        for i in range(nt):
+            for j in range(nt):
+                if tab[i][j] != 0.0:
+                    L.append(f"  {name}({i + 1},{j + 1}) = {_f(tab[i][j])}")
+    for name, dflt in (("plj", 6.0), ("qlj", 12.0)):
+        tab = getattr(p, name)
+        for i in range(nt):
+            for j in range(nt):
+                if tab[i][j] != dflt:
+                    L.append(f"  {name}({i + 1},{j + 1}) = {_f(tab[i][j])}")
+    L.append("&end")
+    L.append("&coulombtag")
+    L.append(f"  lautoES = {'.true.' if p.lautoES else '.false.'}")
+    L.append(f"  epsw = {_f(p.epsw)}")
+    L.append(f"  alphaES = {_f(p.alphaES)}")
+    L.append(f"  kES = {p.kES[0]} {p.kES[1]} {p.kES[2]}")
+    L.append("&end")
+    L.append("&pimtag")
+    L.append(f"  symmetric_pot = {'.true.' if p.symmetric_pot_pim else '.false.'}")
+    L.append(f"  conv_tol_ind = {_f(p.conv_tol_ind)}")
+    L.append(f"  min_scf_pol_iter = {p.min_scf_pol_iter}")
+    L.append(f"  max_scf_pol_iter = {p.max_scf_pol_iter}")
+    L.append(f"  extrapolate_order = {p.extrapolate_order}")
+    L.append("  algo_moment_from_pola = 'scf'")
+    L.append("  algo_ext_dipole = 'aspc'")
+    for it in range(nt):
+        if p.ldip_polar[it]:
+            L.append(f"  ldip_polar({it + 1}) = .true.")
+        for a in range(3):
+            for b in range(3):
+                if p.poldip[it][a][b] != 0.0:
+                    L.append(f"  poldip({it + 1},{a + 1},{b + 1}) = {_f(p.poldip[it][a][b])}")
+    for i in range(nt):
+        for j in range(nt):
+            for k in range(nt):
+                if p.ldip_damping[i][j][k]:
+                    L.append(f"  ldip_damping({i + 1},{j + 1},{k + 1}) = .true.")
+                    L.append(f"  pol_damp_b({i + 1},{j + 1},{k + 1}) = {_f(p.pol_damp_b[i][j][k])}")
+                    L.append(f"  pol_damp_c({i + 1},{j + 1},{k + 1}) = {_f(p.pol_damp_c[i][j][k])}")
+                    L.append(f"  pol_damp_k({i + 1},{j + 1},{k + 1}) = {p.pol_damp_k[i][j][k]}")
+    L.append("&end")
+    with open(path, "w") as f:
+        f.write("\n".join(L) + "\n")

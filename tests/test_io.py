@@ -1,0 +1,105 @@
+"""POSFF / control-file IO (mdff_b200.mdffio): round trips, the namelist
+features the reference's decks use, and -- where the reference is mounted --
+the ex09 decks re-read from its own files must equal the committed fixture."""
+import os
+
+import numpy as np
+import pytest
+
+from mdff_b200 import _abi, mdffio, systems
+from mdff_b200.params import make_params
+
+REF = "/root/reference"
+
+
+def test_posff_round_trip(tmp_path):
+    rng = np.random.default_rng(3)
+    A = np.array([[10.0, 0.5, 0.0], [0.0, 11.0, 0.3], [0.0, 0.0, 12.0]])
+    s = rng.uniform(-0.5, 0.5, (7, 3))
+    pos = s @ A.T
+    f = tmp_path / "POSFF"
+    mdffio.write_posff(f, "test", A, ["Na", "Cl"], [3, 4], pos)
+    r = mdffio.read_posff(f)
+    assert r["natm"] == 7 and r["names"] == ["Na", "Cl"] and r["natmi"] == [3, 4]
+    assert np.allclose(r["cell"], A)
+    assert np.allclose(r["pos"], pos, atol=1e-12)
+
+
+def test_posff_direct_and_wrap(tmp_path):
+    f = tmp_path / "POSFF"
+    f.write_text("2\nx\n10 0 0\n0 10 0\n0 0 10\n1\nA\n2\nDirect\nA 0.25 0.75 0.5\nA 1.1 -0.6 0.0\n")
+    r = mdffio.read_posff(f)
+    # kardir / periodicbc (s - NINT(s)) / dirkar: 0.75 -> -0.25, 0.5 -> -0.5, 1.1 -> 0.1, -0.6 -> 0.4
+    assert np.allclose(r["pos"], [[2.5, -2.5, -5.0], [1.0, 4.0, 0.0]])
+
+
+def test_namelist_features():
+    txt = """
+    ! comment line
+    &controltag
+        calc = 'md'   ! trailing comment
+        lcoulomb = .true. , lbmhft=.false.
+        cutlongrange = 7.2d0
+    &end
+    &fieldtag
+        qch = -2.0d0 4.0 3*0.5
+        kES = 11 11 11,
+    &end
+    &pimtag
+        ldip_polar(1) = .true.
+        poldip(1,2,2) = 0.9397d0
+        pol_damp_k(1,1,2) = 4
+    /
+    """
+    nl = mdffio.read_namelists(txt)
+    assert nl["controltag"]["calc"] == "md"
+    assert nl["controltag"]["lcoulomb"] is True and nl["controltag"]["lbmhft"] is False
+    assert nl["controltag"]["cutlongrange"] == 7.2
+    assert nl["fieldtag"]["qch"] == [-2.0, 4.0, 0.5, 0.5, 0.5]
+    assert nl["fieldtag"]["kes"] == [11, 11, 11]
+    assert nl["pimtag"]["ldip_polar"] == {(1,): True}
+    assert nl["pimtag"]["poldip"] == {(1, 2, 2): 0.9397}
+    assert nl["pimtag"]["pol_damp_k"] == {(1, 1, 2): 4}
+
+
+def test_control_round_trip(tmp_path):
+    s = systems.mgo(ncell=2)
+    p = s.params
+    f = tmp_path / "control.F"
+    mdffio.write_control(f, p, ["Mg", "O"], masses=[24.305, 15.9994])
+    q = mdffio.params_from_namelists(mdffio.read_control(f), [p.natmi[0], p.natmi[1]])
+    for k in ("lcoulomb", "lbmhft", "cutshortrange", "cutlongrange", "skindiff", "alphaES",
+              "epsw", "conv_tol_ind", "extrapolate_order", "trunc", "calc"):
+        assert getattr(q, k) == getattr(p, k), k
+    assert list(q.kES) == list(p.kES)
+    for name in ("Abmhftd", "Bbmhftd", "Cbmhftd", "pol_damp_b", "pol_damp_c", "pol_damp_k",
+                 "ldip_damping", "poldip", "qch", "ldip_polar"):
+        assert np.array_equal(np.ctypeslib.as_array(getattr(q, name)),
+                              np.ctypeslib.as_array(getattr(p, name))), name
+
+
+def test_unsupported_switches_raise():
+    with pytest.raises(ValueError):
+        mdffio.params_from_namelists({"controltag": {"lmorse": True}}, [1, 1])
+    with pytest.raises(ValueError):
+        mdffio.params_from_namelists({"controltag": {"longrange": "direct"}}, [1, 1])
+
+
+@pytest.mark.skipif(not os.path.isdir(REF), reason="reference not mounted")
+def test_ex09_decks_match_fixture():
+    import importlib.util
+    here = os.path.dirname(os.path.abspath(__file__))
+    spec = importlib.util.spec_from_file_location("mk", os.path.join(here, "golden",
+                                                                     "make_ex09_decks.py"))
+    mk = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mk)
+    cfgdir = os.path.join(REF, "examples", "ex09", "config")
+    glob, rows = mk.read_table(os.path.join(cfgdir, "test.config"))
+    fx = np.load(os.path.join(here, "golden", "ex09_decks.npz"))
+    posff = mdffio.read_posff(os.path.join(cfgdir, "POSFF"))
+    assert np.array_equal(posff["pos"], fx["pos"])
+    assert len(rows) == 11
+    for row in rows:
+        nl = mdffio.read_namelists(mk.assemble(os.path.join(cfgdir, "pot_mdff"), glob, row))
+        p = mdffio.params_from_namelists(nl, posff["natmi"])
+        assert bytes(p) == fx[f"params_{row[0]}"].tobytes()

@@ -234,6 +234,13 @@ int mdff_gpu_md_nve(mdff_handle h, double* d_pos, double* d_vel,
                     const double* d_invmass, double dt, int nsteps, int itime0,
                     double* ekin_pot);
 
+/* Electric field gradient efg_t (doefg; ewald_dir.f90:543-582,
+   ewald_rec.f90:209-217, ewald.f90 self term) at every ion for the state of
+   the last engforce call (its positions and total dipoles): efg [natm][3][3]
+   host array, eV/(e A^2) (x coul_unit as the reference).  The reciprocal part
+   fills the upper triangle only, as the reference does.  FP64. */
+int mdff_gpu_efg(mdff_handle h, double* efg);
+
 /* Per-kernel-class device timing with CUDA events on the handle's stream
    (for roofline figures).  Classes: 0 list build, 1 short range, 2 real-space
    field, 3 real-space force, 4 structure factor, 5 reciprocal field/force,

@@ -125,6 +125,7 @@ SIGNATURES = {
     "mdff_gpu_profile": (_i, [_P, _i]),
     "mdff_gpu_kernel_times": (_i, [_P, _DP, ctypes.POINTER(ctypes.c_longlong), _DP]),
     "mdff_gpu_peak_flops": (_i, [_i, _i, _DP]),
+    "mdff_gpu_efg": (_i, [_P, _DP]),
     "mdff_gpu_destroy": (None, [_P]),
     "mdff_gpu_batch_create": (_i, [ctypes.POINTER(MdffParams), _i, ctypes.POINTER(MdffBatchDesc),
                                    ctypes.POINTER(_P)]),

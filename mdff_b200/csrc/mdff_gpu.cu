@@ -111,6 +111,8 @@ struct mdff_ctx {
   float* d_ddb1 = nullptr;
   int *d_ddj = nullptr, *d_ddn = nullptr;
   bool dd_cache_ok = false;
+  double* d_efg = nullptr;       // [natm][9] electric field gradient (mdff_gpu_efg)
+  bool have_state = false;       // an engforce has run: positions, list, dipoles valid
   // outputs / reductions
   double* d_force = nullptr;     // [3][natm]
   double* d_part = nullptr;
@@ -1017,6 +1019,7 @@ static int engforce_retry(mdff_ctx* h, int itime) {
     s = run_engforce(h, itime);
     h->launches_call += h->launches;
   }
+  h->have_state = (s == MDFF_OK || s == MDFF_ERR_NOT_CONVERGED);
   return s;
 }
 
@@ -1423,6 +1426,71 @@ int mdff_gpu_md_nve(mdff_handle h, double* d_pos, double* d_vel, const double* d
   return MDFF_OK;
 }
 
+// efg = (efg + diag(-2 selfa2 q_i)) * coul_unit  (ewald.f90 self term of the gradient)
+__global__ void k_efg_finish(const double* __restrict__ q, int natm, double selfa2, double cu,
+                             double* __restrict__ efg) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natm) return;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double s = (a == b) ? -2.0 * selfa2 * q[i] : 0.0;
+      efg[9 * (size_t)i + 3 * a + b] = (efg[9 * (size_t)i + 3 * a + b] + s) * cu;
+    }
+}
+
+int mdff_gpu_efg(mdff_handle h, double* efg) {
+  if (!h || !efg) return MDFF_ERR_BAD_ARGS;
+  if (!h->p.lcoulomb || !h->have_state) {
+    h->err = "efg needs lcoulomb and a completed engforce call";
+    return MDFF_ERR_BAD_ARGS;
+  }
+  CK(cudaSetDevice(h->device));
+  int n = h->natm;
+  if (!h->d_efg) DALLOC(h->d_efg, 9 * (size_t)n);
+  double cutsq = h->p.cutlongrange * h->p.cutlongrange;
+  k_es_efg<<<cdiv((long)n * 32, 256), 256, 0, h->st>>>(h->d_s, h->d_q, h->d_mu_tot, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->p.alphaES, cutsq, h->task_qq, h->task_dd, h->d_efg);
+  LAUNCH_CHECK();
+  if (h->nk > 0) {
+    // FP64 structure factor of the final charges and dipoles
+    RecMesh M;
+    M.kmax[0] = h->p.kES[0];
+    M.kmax[1] = h->p.kES[1];
+    M.kmax[2] = h->p.kES[2];
+    M.nrows = (int)h->rows.size();
+    M.rows = h->d_rows;
+    M.nk = h->nk;
+    M.Ak = h->d_Ak;
+    M.kvec = h->d_kvec;
+    int has_q = h->task_qq ? 1 : 0, has_mu = (h->task_qd || h->task_dd) ? 1 : 0;
+    k_rec_weights<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_q, h->d_mu_tot, n, h->d_cell, has_q, has_mu, h->d_w, nullptr, nullptr);
+    LAUNCH_CHECK();
+    int nzt = pick_nzt(2 * M.kmax[2] + 1);
+    int ntiles = cdiv(2 * M.kmax[2] + 1, nzt);
+    dim3 gr((unsigned)(M.nrows * ntiles), (unsigned)h->n_rho_chunks);
+    switch (nzt) {
+      case 8: launch_rho<double, 8>(h, gr, h->d_tab64, n, kRhoChunk, M, ntiles, has_q, has_mu); break;
+      case 11: launch_rho<double, 11>(h, gr, h->d_tab64, n, kRhoChunk, M, ntiles, has_q, has_mu); break;
+      case 13: launch_rho<double, 13>(h, gr, h->d_tab64, n, kRhoChunk, M, ntiles, has_q, has_mu); break;
+      case 21: launch_rho<double, 21>(h, gr, h->d_tab64, n, kRhoChunk, M, ntiles, has_q, has_mu); break;
+      case 25: launch_rho<double, 25>(h, gr, h->d_tab64, n, kRhoChunk, M, ntiles, has_q, has_mu); break;
+      default: launch_rho<double, 16>(h, gr, h->d_tab64, n, kRhoChunk, M, ntiles, has_q, has_mu); break;
+    }
+    LAUNCH_CHECK();
+    k_rec_sum<<<cdiv(h->nk, 256), 256, 0, h->st>>>(h->d_rho_part, h->n_rho_chunks, M, h->d_rhoA, h->d_str);
+    LAUNCH_CHECK();
+    double fpi_V = 2.0 * (kTwoPi / h->omega);
+    k_rec_efg<<<cdiv(n, 128), 128, 0, h->st>>>(h->d_tab64, n, M, h->d_rhoA, h->d_cell, 2.0 * fpi_V, h->d_efg);
+    LAUNCH_CHECK();
+  }
+  double a = h->p.alphaES;
+  double selfa2 = 2.0 * (a / std::sqrt(kPi)) * a * a / 3.0;
+  k_efg_finish<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_q, n, selfa2, h->coul_unit, h->d_efg);
+  LAUNCH_CHECK();
+  CK(cudaMemcpyAsync(efg, h->d_efg, sizeof(double) * 9 * n, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return MDFF_OK;
+}
+
 int mdff_gpu_profile(mdff_handle h, int enable) {
   if (!h) return MDFF_ERR_BAD_ARGS;
   h->prof = enable != 0;
@@ -1495,7 +1563,7 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_G, h->d_H, h->d_Estat, h->d_Eind, h->d_Efield, h->d_mu_ind, h->d_mu_tot,
                   h->d_hist, h->d_E, h->d_r, h->d_z, h->d_pv, h->d_qv, h->d_Tp, h->d_mu32, h->d_force,
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
-                  h->d_ddb1, h->d_ddj, h->d_ddn};
+                  h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);

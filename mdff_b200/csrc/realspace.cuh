@@ -663,6 +663,64 @@ static __global__ void __launch_bounds__(256) k_es_force(
     for (int k = 0; k < kESPart; ++k) part[(size_t)blockIdx.x * kESPart + k] = acc[k];
 }
 
+// --------------------------------------------------------------------------
+// real-space electric field gradient (multipole_ES_dir with do_efg,
+// ewald_dir.f90:543-545, 577-582), FP64, full list, warp per ion:
+//   efg_i -= q_j T2(r_ij)            (charges; undamped)
+//   efg_i += T3(r_ij) . mu_j         (both dipoles non-zero)
+// T2 and T3 are even / odd in r, so the reference's ia / ja updates are the
+// same expression from either side.  Out: efg[i][9] (overwritten).
+static __global__ void __launch_bounds__(256) k_es_efg(
+    const double4* __restrict__ s, const double* __restrict__ q, const double4* __restrict__ mu,
+    const int* __restrict__ nbr, const int* __restrict__ nnb, int cap, int natm,
+    const CellC* __restrict__ cell, double alpha, double cutsq, int task_qq, int task_dd,
+    double* __restrict__ efg) {
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= natm) return;
+  double4 si = s[i];
+  double4 mi = mu[i];
+  bool dip_i = mi.x != 0.0 || mi.y != 0.0 || mi.z != 0.0;
+  int n = nnb[i];
+  const int* row = nbr + (size_t)i * cap;
+  double e[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) e[k] = 0.0;
+  for (int k = lane; k < n; k += 32) {
+    int j = row[k];
+    double4 sj = s[j];
+    double r[3];
+    double r2 = min_image_exact(cell->A, xsub(si.x, sj.x), xsub(si.y, sj.y), xsub(si.z, sj.z),
+                                r[0], r[1], r[2]);
+    if (r2 > cutsq) continue;
+    Radial<double> g;
+    radial<double, true>(r2, alpha, g);
+    double F2 = 3.0 * g.F2 * g.dm5, F1 = g.F1 * g.dm3, F3 = 15.0 * g.F3 * g.dm7;
+    if (task_qq) {
+      double qj = q[j];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) e[3 * a + b] -= qj * (r[a] * r[b] * F2 - (a == b ? F1 : 0.0));
+    }
+    double4 mj = mu[j];
+    if (task_dd && dip_i && (mj.x != 0.0 || mj.y != 0.0 || mj.z != 0.0)) {
+      double m[3] = {mj.x, mj.y, mj.z};
+      double rm = r[0] * m[0] + r[1] * m[1] + r[2] * m[2];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+          e[3 * a + b] += -r[a] * r[b] * rm * F3 +
+                          F2 * ((a == b ? rm : 0.0) + r[b] * m[a] + r[a] * m[b]);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) e[k] = warp_sum(e[k]);
+  if (lane == 0)
+    for (int k = 0; k < 9; ++k) efg[9 * (size_t)i + k] = e[k];
+}
+
 // fixed-order reduction of per-block partials: out[v] = sum_b part[b*nv+v]
 static __global__ void k_reduce_partials(const double* __restrict__ part, int nblk, int nv,
                                   double* __restrict__ out) {

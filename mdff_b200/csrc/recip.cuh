@@ -345,6 +345,56 @@ static __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>
   if (HAS_MU_FORCE) Hpart[(size_t)blockIdx.y * natm + i] = make_double4(H[0], H[1], H[2], 0.0);
 }
 
+// reciprocal electric field gradient (ewald_rec.f90:209-217): per ion
+// sum_k k_a k_b recarg2 on the upper triangle only (the reference never
+// fills the lower one), scaled by 2 fpi_V and added into efg[i][9].  FP64,
+// ion-major over all k rows; rho' = A_k rho of the final pass.
+// N_pq = sum_k n_p n_q recarg2 per row from sums over nz, k_a k_b =
+// 4 pi^2 sum_pq B_ap B_bq n_p n_q.
+static __global__ void __launch_bounds__(128) k_rec_efg(const double2* __restrict__ tab, int natm,
+                                                      RecMesh M, const double2* __restrict__ rhoA,
+                                                      const CellC* __restrict__ cell, double scale,
+                                                      double* __restrict__ efg) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natm) return;
+  const int kx = M.kmax[0], ky = M.kmax[1], kz = M.kmax[2];
+  double2 Z1 = tab[(size_t)(kx + 1 + ky + 1 + 1) * natm + i];
+  double N[6] = {0, 0, 0, 0, 0, 0};  // xx yy zz xy xz yz
+  for (int r = 0; r < M.nrows; ++r) {
+    int4 ri = M.rows[r];
+    int nx = ri.x, ny = ri.y, nz_lo = ri.z;
+    double2 XY = phase_xyz<double>(tab, natm, i, nx, ny, 0, kx, ky);
+    double2 P = phase_z<double>(tab, natm, i, XY, nz_lo, kx, ky);
+    double S0 = 0.0, S1 = 0.0, S2 = 0.0;
+    int nn = kz - nz_lo + 1;
+    const double2* rr = rhoA + ri.w;
+    for (int t = 0; t < nn; ++t) {
+      double2 rho = rr[t];
+      double v = rho.x * P.x + rho.y * P.y;  // recarg2
+      double nz = (double)(nz_lo + t);
+      S0 += v;
+      S1 += nz * v;
+      S2 += nz * nz * v;
+      P = cmul(P, Z1);
+    }
+    N[0] += (double)nx * nx * S0;
+    N[1] += (double)ny * ny * S0;
+    N[2] += S2;
+    N[3] += (double)nx * ny * S0;
+    N[4] += (double)nx * S1;
+    N[5] += (double)ny * S1;
+  }
+  const double* B = cell->B;
+  double Nm[3][3] = {{N[0], N[3], N[4]}, {N[3], N[1], N[5]}, {N[4], N[5], N[2]}};
+  for (int a = 0; a < 3; ++a)
+    for (int b = a; b < 3; ++b) {
+      double v = 0.0;
+      for (int p = 0; p < 3; ++p)
+        for (int qq = 0; qq < 3; ++qq) v += B[3 * a + p] * B[3 * b + qq] * Nm[p][qq];
+      efg[9 * (size_t)i + 3 * a + b] += kTwoPi * kTwoPi * v * scale;
+    }
+}
+
 // chunk sum and scaling.  E += -(2 pi B G) * 2 fpi_V (ewald_rec.f90:193-198,
 // 300-352); with do_forces, F += [q (-2 pi B G) + 2 pi B H] * 2 fpi_V * coul_unit.
 // Four threads per ion split the chunk partials (fixed order, shuffle sum).

@@ -105,6 +105,13 @@ class ForceEngine:
         self._check(st, "md_nve")
         return e
 
+    def efg(self):
+        """Electric field gradient [natm, 3, 3] for the state of the last
+        engforce (the reference's efg_t)."""
+        e = np.zeros((self.natm, 3, 3))
+        self._check(self._lib.mdff_gpu_efg(self._h, dptr(e)), "efg")
+        return e
+
     def stats(self):
         s = _abi.MdffStats()
         self._check(self._lib.mdff_gpu_get_stats(self._h, ctypes.byref(s)), "stats")

@@ -29,7 +29,7 @@ namespace {
 
 constexpr int NT = MDFF_NTYPEMAX;
 constexpr int kRhoThreads = 128;
-constexpr int kRhoChunk = 4096;    // ions per structure-factor block
+constexpr int kRhoChunk = 3072;    // ions per structure-factor block (4 chunks at 12k ions: fuller waves)
 constexpr int kFieldThreads = 128;
 
 // scalar slots (device doubles, copied to the host at the end of a call)

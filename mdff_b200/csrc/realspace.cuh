@@ -512,6 +512,7 @@ static __global__ void __launch_bounds__(256) k_dd_cached(
 
 // --------------------------------------------------------------------------
 // final real-space pass: qq + qd + dd with damping; energy, field, force,
+// (FP32: three blocks per SM, 80 registers, measured 14% faster than two)
 // stress.  Partials per block: [u, tau xx yy zz xy xz yz] -> 7 doubles
 // (tau is the reference's  - sum (r_j f_k + r_k f_j)  before *0.5/omega).
 constexpr int kESPart = 7;
@@ -585,7 +586,7 @@ __device__ __forceinline__ void es_force_pair(const ESPair& P, int damp_ind, R d
 }
 
 template <typename R>
-static __global__ void __launch_bounds__(256) k_es_force(
+static __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_es_force(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
     const double4* __restrict__ mu, const int* __restrict__ nbr, const int* __restrict__ nnb,
     int cap, int natm, const CellC* __restrict__ cell, const ESPair* __restrict__ tab, int ntype,

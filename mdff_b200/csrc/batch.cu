@@ -827,8 +827,15 @@ int mdff_gpu_batch_adjoint(mdff_batch_handle h, const double* gE, const double* 
   J.tol_rel = 1e-12;
   J.nparam = h->nparam;
   for (int k = 0; k < kFitMax; ++k) J.prm[k] = (k < h->nparam) ? h->prm[k] : FitParam{-1, 0, 0, 0};
-  // launch: the forward's shape, persistent clusters
+  // launch: persistent clusters of the forward's block size; the cluster is
+  // widened until the clusters of all configurations cover the SMs twice (a
+  // fitting batch of tens of boxes would otherwise leave most SMs idle)
   Shape sh = h->shape;
+  {
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+    while (sh.cluster < kBMaxC && (long)h->nconf * sh.cluster < 2L * nsm) sh.cluster *= 2;
+  }
   size_t smem = batch_smem_extra_offset(h->nmax) + sizeof(double4) * h->nmax;
   if (smem > 227 * 1024) {
     h->err = "configurations too large for the adjoint's shared-memory layout";

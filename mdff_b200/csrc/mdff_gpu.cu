@@ -448,7 +448,7 @@ static int list_update(mdff_ctx* h) {
 }
 
 static int reduce_into(mdff_ctx* h, int nblk, int nv, double* out) {
-  k_reduce_partials<<<1, 256, 0, h->st>>>(h->d_part, nblk, nv, out);
+  k_reduce_partials<<<nv, 256, 0, h->st>>>(h->d_part, nblk, nv, out);
   LAUNCH_CHECK();
   return MDFF_OK;
 }
@@ -503,13 +503,21 @@ static void launch_rho(mdff_ctx* h, dim3 g, const typename cplx<R>::T* tab, int 
     k_rec_rho<R, false, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
 }
 
-// reciprocal pass: E += rec field; force += rec force * coul_unit (if forces);
-// energy (7 doubles) into e_out (if non-null)
+// reciprocal pass: E += rec field (+ the self / surface field sf, when on);
+// force += rec force * coul_unit (if forces); energy (7 doubles) into e_out
+// (if non-null)
 template <typename R>
 static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4* mu, int has_q,
-                      int has_mu, int forces, double4* E, double* e_out, float4* mu32) {
+                      int has_mu, int forces, double4* E, double* e_out, float4* mu32,
+                      SelfField sf) {
   int n = h->natm;
-  if (h->nk == 0) return MDFF_OK;
+  if (h->nk == 0) {
+    if (sf.on) {
+      k_self_surf_field<<<cdiv(n, 256), 256, 0, h->st>>>(sf.mu, n, sf.selfa2, sf.lsurf, sf.fpi_3V, sf.mom, E);
+      LAUNCH_CHECK();
+    }
+    return MDFF_OK;
+  }
   RecMesh M;
   M.kmax[0] = h->p.kES[0];
   M.kmax[1] = h->p.kES[1];
@@ -543,12 +551,16 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   }
   LAUNCH_CHECK();
   prof_end(h, pr);
-  k_rec_sum<<<cdiv(h->nk, 256), 256, 0, h->st>>>(h->d_rho_part, h->n_rho_chunks, M, h->d_rhoA, h->d_str);
-  LAUNCH_CHECK();
   double tpi_V = kTwoPi / h->omega;
+  // without energy the field kernels sum the chunk partials while staging rho'
+  int npart = 0;
   if (e_out) {
+    k_rec_sum<<<cdiv(h->nk, 256), 256, 0, h->st>>>(h->d_rho_part, h->n_rho_chunks, M, h->d_rhoA, h->d_str);
+    LAUNCH_CHECK();
     k_rec_energy<<<1, 1024, 0, h->st>>>(h->d_str, M, tpi_V, h->omega, 1, e_out);
     LAUNCH_CHECK();
+  } else {
+    npart = h->n_rho_chunks;
   }
   int nch = (int)h->rchunk.size() - 1;
   dim3 gf((unsigned)cdiv(n, kFieldThreads), (unsigned)nch);
@@ -558,27 +570,41 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   if constexpr (std::is_same<R, float>::value) {
     dim3 gx((unsigned)cdiv(n, 2 * kFieldThreads), (unsigned)nch);
     if (muf)
-      k_rec_field_x2<true><<<gx, kFieldThreads, smem, h->st>>>(tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_G, h->d_H);
+      k_rec_field_x2<true><<<gx, kFieldThreads, smem, h->st>>>(tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
     else
-      k_rec_field_x2<false><<<gx, kFieldThreads, smem, h->st>>>(tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_G, h->d_H);
+      k_rec_field_x2<false><<<gx, kFieldThreads, smem, h->st>>>(tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
   } else if (muf)
-    k_rec_field<R, true><<<gf, kFieldThreads, smem, h->st>>>(tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_G, h->d_H);
+    k_rec_field<R, true><<<gf, kFieldThreads, smem, h->st>>>(tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
   else
-    k_rec_field<R, false><<<gf, kFieldThreads, smem, h->st>>>(tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_G, h->d_H);
+    k_rec_field<R, false><<<gf, kFieldThreads, smem, h->st>>>(tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
   LAUNCH_CHECK();
   prof_end(h, pr);
   double fpi_V = 2.0 * tpi_V;
   k_rec_field_sum<<<cdiv((long)n * 4, 256), 256, 0, h->st>>>(h->d_G, h->d_H, nch, n, h->d_cell, h->d_q,
                                                    2.0 * fpi_V, muf ? 1 : 0, forces, h->coul_unit, E,
-                                                   h->d_force);
+                                                   h->d_force, sf);
   LAUNCH_CHECK();
   return MDFF_OK;
 }
 
 static int rec_pass(mdff_ctx* h, bool fp32, const double4* mu, int has_q, int has_mu, int forces,
-                    double4* E, double* e_out, float4* mu32 = nullptr) {
-  if (fp32) return rec_pass_t<float>(h, h->d_tab32, mu, has_q, has_mu, forces, E, e_out, mu32);
-  return rec_pass_t<double>(h, h->d_tab64, mu, has_q, has_mu, forces, E, e_out, mu32);
+                    double4* E, double* e_out, SelfField sf, float4* mu32 = nullptr) {
+  if (fp32) return rec_pass_t<float>(h, h->d_tab32, mu, has_q, has_mu, forces, E, e_out, mu32, sf);
+  return rec_pass_t<double>(h, h->d_tab64, mu, has_q, has_mu, forces, E, e_out, mu32, sf);
+}
+
+// the self field 2 selfa2 mu (+ surface field of the reduced moments in mom
+// when lsurf) of one moment set (field_dipole_ES_self / surface, coulomb.f90)
+static SelfField self_field(mdff_ctx* h, const double4* mu, const double* mom) {
+  double a = h->p.alphaES;
+  SelfField sf;
+  sf.on = 1;
+  sf.lsurf = h->p.lsurf;
+  sf.mu = mu;
+  sf.selfa2 = 2.0 * (a / std::sqrt(kPi)) * a * a / 3.0;
+  sf.fpi_3V = 2.0 * (kTwoPi / h->omega / 3.0);
+  sf.mom = mom;
+  return sf;
 }
 
 static int build_tables(mdff_ctx* h) {
@@ -601,8 +627,15 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   CK(cudaMemsetAsync(E, 0, sizeof(double4) * n, h->st));
   double cutsq = h->p.cutlongrange * h->p.cutlongrange;
   int nb = cdiv((long)n * 32, 256);
-  // reciprocal first: its weights kernel also writes the FP32 dipoles
-  int s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, fp32 ? h->d_mu32 : nullptr);
+  int s;
+  if (h->p.lsurf) {
+    s = moments(h, mu, 0, h->d_scal + S_MOM2);
+    if (s) return s;
+  }
+  // reciprocal first: its weights kernel also writes the FP32 dipoles; its
+  // final kernel adds the self / surface field
+  s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, self_field(h, mu, h->d_scal + S_MOM2),
+               fp32 ? h->d_mu32 : nullptr);
   if (s) return s;
   int pr = prof_begin(h, KC_ESFIELD, 0);
   if (fp32 && dd_mask == 1 && h->dd_cache_ok)
@@ -613,15 +646,6 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
     k_es_field<double, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
   LAUNCH_CHECK();
   prof_end(h, pr);
-  double a = h->p.alphaES;
-  double selfa2 = 2.0 * (a / std::sqrt(kPi)) * a * a / 3.0;
-  double fpi_3V = 2.0 * (kTwoPi / h->omega / 3.0);
-  if (h->p.lsurf) {
-    s = moments(h, mu, 0, h->d_scal + S_MOM2);
-    if (s) return s;
-  }
-  k_self_surf_field<<<cdiv(n, 256), 256, 0, h->st>>>(mu, n, selfa2, h->p.lsurf, fpi_3V, h->d_scal + S_MOM2, E);
-  LAUNCH_CHECK();
   return MDFF_OK;
 }
 
@@ -664,17 +688,14 @@ static int static_field(mdff_ctx* h, bool fp32) {
     prof_end(h, pr);
   }
 #undef ESF
-  int s = rec_pass(h, fp32, h->d_dipia, h->task_qq ? 1 : 0, dd ? 1 : 0, 0, E, nullptr);
-  if (s) return s;
-  double a = h->p.alphaES;
-  double selfa2 = 2.0 * (a / std::sqrt(kPi)) * a * a / 3.0;
-  double fpi_3V = 2.0 * (kTwoPi / h->omega / 3.0);
+  int s;
   if (h->p.lsurf) {
     s = moments(h, h->d_dipia, 1, h->d_scal + S_MOM2);
     if (s) return s;
   }
-  k_self_surf_field<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_dipia, n, selfa2, h->p.lsurf, fpi_3V, h->d_scal + S_MOM2, E);
-  LAUNCH_CHECK();
+  s = rec_pass(h, fp32, h->d_dipia, h->task_qq ? 1 : 0, dd ? 1 : 0, 0, E, nullptr,
+               self_field(h, h->d_dipia, h->d_scal + S_MOM2));
+  if (s) return s;
   return MDFF_OK;
 }
 
@@ -983,13 +1004,10 @@ static int run_engforce(mdff_ctx* h, int itime) {
     prof_end(h, prf);
     if ((s = reduce_into(h, nbw, kESPart, h->d_scal + S_DIR))) return s;
     int has_mu = (h->task_qd || h->task_dd) ? 1 : 0;
-    if ((s = rec_pass(h, fp32, h->d_mu_tot, h->task_qq ? 1 : 0, has_mu, 1, h->d_E, h->d_scal + S_REC))) return s;
     if ((s = moments(h, h->d_mu_tot, 1, h->d_scal + S_MOM))) return s;
-    double a = h->p.alphaES;
-    double selfa2 = 2.0 * (a / std::sqrt(kPi)) * a * a / 3.0;
-    double fpi_3V = 2.0 * (kTwoPi / h->omega / 3.0);
-    k_self_surf_field<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_mu_tot, n, selfa2, h->p.lsurf, fpi_3V, h->d_scal + S_MOM, h->d_E);
-    LAUNCH_CHECK();
+    if ((s = rec_pass(h, fp32, h->d_mu_tot, h->task_qq ? 1 : 0, has_mu, 1, h->d_E, h->d_scal + S_REC,
+                      self_field(h, h->d_mu_tot, h->d_scal + S_MOM))))
+      return s;
   }
   CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(h->h_flags, h->L.flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, h->st));

@@ -722,22 +722,21 @@ static __global__ void __launch_bounds__(256) k_es_efg(
     for (int k = 0; k < 9; ++k) efg[9 * (size_t)i + k] = e[k];
 }
 
-// fixed-order reduction of per-block partials: out[v] = sum_b part[b*nv+v]
+// fixed-order reduction of per-block partials: out[v] = sum_b part[b*nv+v];
+// one block per value (grid = nv), the same order for every launch
 static __global__ void k_reduce_partials(const double* __restrict__ part, int nblk, int nv,
-                                  double* __restrict__ out) {
+                                         double* __restrict__ out) {
   __shared__ double sh[256];
-  for (int v = 0; v < nv; ++v) {
-    double acc = 0.0;
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc += part[(size_t)b * nv + v];
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int w = blockDim.x >> 1; w > 0; w >>= 1) {
-      if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) out[v] = sh[0];
+  const int v = blockIdx.x;
+  double acc = 0.0;
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc += part[(size_t)b * nv + v];
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x >> 1; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
     __syncthreads();
   }
+  if (threadIdx.x == 0) out[v] = sh[0];
 }
 
 }  // namespace mdff

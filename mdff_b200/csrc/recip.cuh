@@ -31,6 +31,16 @@ struct cplx<float> {
   typedef float2 T;
 };
 
+// self field 2 selfa2 mu_i (+ the surface field -fpi_3V (qtot + mutot) of the
+// reduced moments mom[0..5] when lsurf), added to E by k_rec_field_sum when on;
+// the same sums as k_self_surf_field
+struct SelfField {
+  int on, lsurf;
+  const double4* mu;
+  double selfa2, fpi_3V;
+  const double* mom;
+};
+
 struct RecMesh {
   int kmax[3];
   int nrows;
@@ -206,6 +216,20 @@ static __global__ void __launch_bounds__(128) k_rec_rho(const typename cplx<R>::
   }
 }
 
+// rho' (k) = A_k sum over ion chunks of the structure-factor partials, the
+// chunks in order (k_rec_sum and the field kernels' staging give the same bits)
+static __device__ __forceinline__ double2 rho_prime(const double2* __restrict__ part, int nchunk,
+                                                    const double* __restrict__ Ak, int nk, int k) {
+  double r = 0.0, im = 0.0;
+  for (int c = 0; c < nchunk; ++c) {
+    double2 v = part[(size_t)c * nk + k];
+    r += v.x;
+    im += v.y;
+  }
+  double A = Ak[k];
+  return make_double2(A * r, A * im);
+}
+
 // rho = sum over chunks; rhoA = A_k rho; str = A_k |rho|^2
 static __global__ void k_rec_sum(const double2* __restrict__ part, int nchunk, RecMesh M,
                           double2* __restrict__ rhoA, double* __restrict__ str) {
@@ -256,6 +280,7 @@ static __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>
                                                    const double4* __restrict__ w, int natm,
                                                    RecMesh M, const int* __restrict__ rchunk,
                                                    const double2* __restrict__ rhoA,
+                                                   const double2* __restrict__ part, int npart,
                                                    double4* __restrict__ Gpart,
                                                    double4* __restrict__ Hpart) {
   typedef typename cplx<R>::T C;
@@ -265,7 +290,7 @@ static __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>
   int k0 = M.rows[r0].w;
   int k1 = (r1 < M.nrows) ? M.rows[r1].w : M.nk;
   for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-    double2 v = rhoA[k];
+    double2 v = npart ? rho_prime(part, npart, M.Ak, M.nk, k) : rhoA[k];
     C c;
     c.x = (R)v.x;
     c.y = (R)v.y;
@@ -402,7 +427,8 @@ static __global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const 
                                 int nchunk, int natm, const CellC* __restrict__ cell,
                                 const double* __restrict__ q, double scale /* 2 fpi_V */,
                                 int has_mu_force, int do_forces, double coul_unit,
-                                double4* __restrict__ E, double* __restrict__ force) {
+                                double4* __restrict__ E, double* __restrict__ force,
+                                SelfField sf) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int i = t >> 2, sub = t & 3;
   double g[3] = {0, 0, 0}, h[3] = {0, 0, 0};
@@ -434,8 +460,21 @@ static __global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const 
     e[a] = -kTwoPi * (B[3 * a + 0] * g[0] + B[3 * a + 1] * g[1] + B[3 * a + 2] * g[2]) * scale;
     fm[a] = kTwoPi * (B[3 * a + 0] * h[0] + B[3 * a + 1] * h[1] + B[3 * a + 2] * h[2]) * scale;
   }
+  // self (+ surface) field of the same moments, field only (no force)
+  double s[3] = {0.0, 0.0, 0.0};
+  if (sf.on) {
+    double4 m = sf.mu ? sf.mu[i] : make_double4(0, 0, 0, 0);
+    if (sf.lsurf) {
+      s[0] = -(sf.mom[0] + sf.mom[3]) * sf.fpi_3V;
+      s[1] = -(sf.mom[1] + sf.mom[4]) * sf.fpi_3V;
+      s[2] = -(sf.mom[2] + sf.mom[5]) * sf.fpi_3V;
+    }
+    s[0] += 2.0 * sf.selfa2 * m.x;
+    s[1] += 2.0 * sf.selfa2 * m.y;
+    s[2] += 2.0 * sf.selfa2 * m.z;
+  }
   double4 o = E[i];
-  E[i] = make_double4(o.x + e[0], o.y + e[1], o.z + e[2], 0.0);
+  E[i] = make_double4(o.x + e[0] + s[0], o.y + e[1] + s[1], o.z + e[2] + s[2], 0.0);
   if (do_forces) {
     double qi = q[i];
     force[i] += (qi * e[0] + (has_mu_force ? fm[0] : 0.0)) * coul_unit;
@@ -565,6 +604,7 @@ static __global__ void __launch_bounds__(128) k_rec_field_x2(const float2* __res
                                                       const float4* __restrict__ w, int natm,
                                                       RecMesh M, const int* __restrict__ rchunk,
                                                       const double2* __restrict__ rhoA,
+                                                      const double2* __restrict__ part, int npart,
                                                       double4* __restrict__ Gpart,
                                                       double4* __restrict__ Hpart) {
   extern __shared__ unsigned char shraw[];
@@ -573,7 +613,7 @@ static __global__ void __launch_bounds__(128) k_rec_field_x2(const float2* __res
   int k0 = M.rows[r0].w;
   int k1 = (r1 < M.nrows) ? M.rows[r1].w : M.nk;
   for (int k = k0 + threadIdx.x; k < k1; k += blockDim.x) {
-    double2 v = rhoA[k];
+    double2 v = npart ? rho_prime(part, npart, M.Ak, M.nk, k) : rhoA[k];
     sh[k - k0] = make_float2((float)v.x, (float)v.y);
   }
   __syncthreads();

@@ -99,6 +99,7 @@ struct mdff_ctx {
   double2* d_rhoA = nullptr;
   double* d_str = nullptr;
   int n_rho_chunks = 0;
+  int nsm = 0;  // SMs of the device
   double4* d_G = nullptr;
   double4* d_H = nullptr;
   // pim
@@ -432,11 +433,14 @@ static int list_update(mdff_ctx* h) {
   LAUNCH_CHECK();
   k_cell_scatter<<<cdiv(n, 256), 256, 0, h->st>>>(n, h->L);
   LAUNCH_CHECK();
-  k_build_rows<<<cdiv((long)n * 32, 256), 256, 0, h->st>>>(h->d_s, n, h->d_cell, h->L);
+  // grid-stride build and sort: a step without a rebuild launches a few
+  // blocks per SM that read the flag and leave
+  int nsm = h->nsm > 0 ? h->nsm : 148;
+  k_build_rows<<<std::min(cdiv((long)n * 32, 256), 8 * nsm), 256, 0, h->st>>>(h->d_s, n, h->d_cell, h->L);
   LAUNCH_CHECK();
   int P = 1;
   while (P < h->L.cap) P <<= 1;
-  k_sort_rows<<<n, 256, P * sizeof(int), h->st>>>(h->L, n);
+  k_sort_rows<<<std::min(n, 8 * nsm), 256, P * sizeof(int), h->st>>>(h->L, n);
   LAUNCH_CHECK();
   k_build_done<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_s, n, h->L);
   LAUNCH_CHECK();
@@ -969,10 +973,14 @@ static int run_engforce(mdff_ctx* h, int itime) {
     // short range stays FP64 in the mixed mode too: BKS-type pair forces of
     // tens of eV/A cancel to net forces of a few eV/A, and FP32 rounding of the
     // pair terms alone gives ~1e-5 relative force error
-    if (false)
-      k_shortrange<float><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_itype, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_nbtab, h->ntype, do_bmh, h->p.lbmhftd, h->p.lnmlj, h->p.trunc, h->d_force, h->d_part);
-    else
-      k_shortrange<double><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_itype, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_nbtab, h->ntype, do_bmh, h->p.lbmhftd, h->p.lnmlj, h->p.trunc, h->d_force, h->d_part);
+#define SRK(MODE)                                                                              \
+  k_shortrange<double, MODE><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_itype, h->L.nbr, h->L.nnb,     \
+                                                     h->L.cap, n, h->d_cell, h->d_nbtab, h->ntype, \
+                                                     h->p.lbmhftd, h->p.trunc, h->d_force, h->d_part)
+    if (do_bmh && h->p.lnmlj) SRK(3);
+    else if (do_bmh) SRK(1);
+    else SRK(2);
+#undef SRK
     LAUNCH_CHECK();
     prof_end(h, pr);
     if ((s = reduce_into(h, nbw, kSRPart, h->d_scal + S_SR))) return s;
@@ -1144,6 +1152,7 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   }
   h->device = p.device;
   CK(cudaSetDevice(h->device));
+  CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
   CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
   CK(cudaEventCreate(&h->ev0));
   CK(cudaEventCreate(&h->ev1));

@@ -159,14 +159,9 @@ __global__ void k_cell_scatter(int natm, ListDev L) {
   L.cell_atoms[L.cell_start[c] + slot] = i;
 }
 
-// warp per atom: enumerate neighbour cells, exact distance test, append.
-__global__ void k_build_rows(const double4* __restrict__ s, int natm, const CellC* __restrict__ cell,
-                             ListDev L) {
-  if (L.flags[0] == 0) return;
-  int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  int lane = threadIdx.x & 31;
-  if (warp >= natm) return;
-  int i = warp;
+// one row of the list: warp-cooperative over the 27 (or fewer) neighbour cells
+__device__ __forceinline__ void build_row(const double4* __restrict__ s, int i, int lane,
+                                          const CellC* __restrict__ cell, ListDev L) {
   double4 si = s[i];
   int ci = L.cell_of[i];
   int cz0 = ci % L.nc[2], cy0 = (ci / L.nc[2]) % L.nc[1], cx0 = ci / (L.nc[2] * L.nc[1]);
@@ -222,35 +217,47 @@ __global__ void k_build_rows(const double4* __restrict__ s, int natm, const Cell
   }
 }
 
-// block per row: bitonic sort of the row into ascending j (the reference's
-// row order); P = power of two >= cap, smem P ints.
+// warp per atom (grid-stride over atoms, so that a launch without a rebuild
+// costs a few blocks): enumerate neighbour cells, exact distance test, append.
+__global__ void k_build_rows(const double4* __restrict__ s, int natm, const CellC* __restrict__ cell,
+                             ListDev L) {
+  if (L.flags[0] == 0) return;
+  int lane = threadIdx.x & 31;
+  int nwarp = (gridDim.x * blockDim.x) >> 5;
+  for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < natm; i += nwarp)
+    build_row(s, i, lane, cell, L);
+}
+
+// block per row (grid-stride over rows): bitonic sort of the row into
+// ascending j (the reference's row order); P = power of two >= cap, smem P ints.
 __global__ void k_sort_rows(ListDev L, int natm) {
   if (L.flags[0] == 0) return;
   extern __shared__ int sh[];
-  int i = blockIdx.x;
-  if (i >= natm) return;
-  int n = L.nnb[i];
-  int P = 1;
-  while (P < n) P <<= 1;
-  int* row = L.nbr + (size_t)i * L.cap;
-  for (int k = threadIdx.x; k < P; k += blockDim.x) sh[k] = (k < n) ? row[k] : 0x7fffffff;
-  __syncthreads();
-  for (int size = 2; size <= P; size <<= 1) {
-    for (int stride = size >> 1; stride > 0; stride >>= 1) {
-      for (int t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
-        int lo = 2 * stride * (t / stride) + (t % stride);
-        int hi = lo + stride;
-        bool up = ((lo & size) == 0);
-        int a = sh[lo], b = sh[hi];
-        if ((a > b) == up) {
-          sh[lo] = b;
-          sh[hi] = a;
+  for (int i = blockIdx.x; i < natm; i += gridDim.x) {
+    int n = L.nnb[i];
+    int P = 1;
+    while (P < n) P <<= 1;
+    int* row = L.nbr + (size_t)i * L.cap;
+    for (int k = threadIdx.x; k < P; k += blockDim.x) sh[k] = (k < n) ? row[k] : 0x7fffffff;
+    __syncthreads();
+    for (int size = 2; size <= P; size <<= 1) {
+      for (int stride = size >> 1; stride > 0; stride >>= 1) {
+        for (int t = threadIdx.x; t < (P >> 1); t += blockDim.x) {
+          int lo = 2 * stride * (t / stride) + (t % stride);
+          int hi = lo + stride;
+          bool up = ((lo & size) == 0);
+          int a = sh[lo], b = sh[hi];
+          if ((a > b) == up) {
+            sh[lo] = b;
+            sh[hi] = a;
+          }
         }
+        __syncthreads();
       }
-      __syncthreads();
     }
+    for (int k = threadIdx.x; k < n; k += blockDim.x) row[k] = sh[k];
+    __syncthreads();  // sh is reused by the next row
   }
-  for (int k = threadIdx.x; k < n; k += blockDim.x) row[k] = sh[k];
 }
 
 // after a build: remember positions for the next check, clear the request

@@ -91,12 +91,15 @@ __device__ __forceinline__ void sr_pair_lj(const NBPair& P, int trunc, R rijsq, 
   wij = (R)P.fc * (srq - srp) * sr2;
 }
 
-template <typename R>
-static __global__ void __launch_bounds__(256) k_shortrange(
+// MODE bit 0: BMH / BMHFTD (+ wall), bit 1: n-m LJ.  One instantiation per
+// mode keeps the accumulators of the absent potential out of the registers.
+template <typename R, int MODE>
+static __global__ void __launch_bounds__(256, MODE == 3 ? 2 : 3) k_shortrange(
     const double4* __restrict__ s, const int* __restrict__ itype, const int* __restrict__ nbr,
     const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
-    const NBPair* __restrict__ tab, int ntype, int do_bmh, int lbmhftd, int do_lj, int trunc,
+    const NBPair* __restrict__ tab, int ntype, int lbmhftd, int trunc,
     double* __restrict__ force /* SoA [3][natm] */, double* __restrict__ part) {
+  constexpr bool do_bmh = (MODE & 1) != 0, do_lj = (MODE & 2) != 0;
   __shared__ NBPair stab[MDFF_NT * MDFF_NT];
   __shared__ double red[kSRPart * 8];
   for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];

@@ -11,12 +11,14 @@
 #include <type_traits>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/mdff_gpu.h"
 #include "common.cuh"
+#include "recip_tc.cuh"
 #include "nlist.cuh"
 #include "pim.cuh"
 #include "realspace.cuh"
@@ -100,6 +102,11 @@ struct mdff_ctx {
   double* d_str = nullptr;
   int n_rho_chunks = 0;
   int nsm = 0;  // SMs of the device
+  // FP32 structure factor of the CG operator on the tensor cores
+  // (k_rec_rho_tc): ion chunk size and count; off when kz > 31 or
+  // MDFF_REC_TC=0 in the environment
+  bool rho_tc = false;
+  int tc_chunk = 0, n_tc_chunks = 0;
   double4* d_G = nullptr;
   double4* d_H = nullptr;
   // pim
@@ -339,7 +346,28 @@ static int build_mesh(mdff_ctx* h) {
   DALLOC(h->d_kvec, std::max(nk, 1));
   DALLOC(h->d_rchunk, h->rchunk.size());
   h->n_rho_chunks = cdiv(h->natm, kRhoChunk);
-  DALLOC(h->d_rho_part, (size_t)h->n_rho_chunks * std::max(nk, 1));
+  {
+    // tensor-core structure factor: about two CTAs per SM over (row tiles x ion chunks)
+    const char* env = std::getenv("MDFF_REC_TC");
+    h->rho_tc = rho_tc_nb(h->p.kES[2]) > 0 && nrows > 0 && !(env && env[0] == '0') &&
+                rho_tc_smem(h->p.kES[0], h->p.kES[1], h->p.kES[2]) <= 227 * 1024;
+    int tiles = cdiv(nrows, 32);
+    int nchunk = std::max(1, (2 * (h->nsm > 0 ? h->nsm : 148)) / std::max(tiles, 1));
+    h->tc_chunk = std::max(tc::KB, cdiv(cdiv(h->natm, nchunk), tc::KB) * tc::KB);
+    h->n_tc_chunks = cdiv(h->natm, h->tc_chunk);
+  }
+  DALLOC(h->d_rho_part, (size_t)std::max(h->n_rho_chunks, h->n_tc_chunks) * std::max(nk, 1));
+  if (h->rho_tc) {
+    int smem = (int)rho_tc_smem(h->p.kES[0], h->p.kES[1], h->p.kES[2]);
+#define TC_ATTR(Q, MU, NB) \
+  CK(cudaFuncSetAttribute(k_rec_rho_tc<Q, MU, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))
+    if (rho_tc_nb(h->p.kES[2]) == 32) {
+      TC_ATTR(true, true, 32); TC_ATTR(false, true, 32); TC_ATTR(true, false, 32);
+    } else {
+      TC_ATTR(true, true, 64); TC_ATTR(false, true, 64); TC_ATTR(true, false, 64);
+    }
+#undef TC_ATTR
+  }
   DALLOC(h->d_rhoA, std::max(nk, 1));
   DALLOC(h->d_str, std::max(nk, 1));
   DALLOC(h->d_G, (size_t)(h->rchunk.size() - 1) * h->natm);
@@ -507,6 +535,30 @@ static void launch_rho(mdff_ctx* h, dim3 g, const typename cplx<R>::T* tab, int 
     k_rec_rho<R, false, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
 }
 
+// FP32 structure factor on the tensor cores into d_rho_part (n_tc_chunks chunks)
+template <int NB>
+static void launch_rho_tc_n(mdff_ctx* h, const RecMesh& M, int n, int has_q, int has_mu) {
+  size_t smem = rho_tc_smem_n(NB, M.kmax[0], M.kmax[1], M.kmax[2]);
+  int* err = h->d_cata + 1;
+  if (has_mu) {
+    dim3 g((unsigned)cdiv(M.nrows, 32), (unsigned)h->n_tc_chunks);
+    if (has_q)
+      k_rec_rho_tc<true, true, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err);
+    else
+      k_rec_rho_tc<false, true, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err);
+  } else {
+    dim3 g((unsigned)cdiv(M.nrows, 64), (unsigned)h->n_tc_chunks);
+    k_rec_rho_tc<true, false, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err);
+  }
+}
+
+static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n, int has_q, int has_mu) {
+  if (rho_tc_nb(M.kmax[2]) == 32)
+    launch_rho_tc_n<32>(h, M, n, has_q, has_mu);
+  else
+    launch_rho_tc_n<64>(h, M, n, has_q, has_mu);
+}
+
 // reciprocal pass: E += rec field (+ the self / surface field sf, when on);
 // force += rec force * coul_unit (if forces); energy (7 doubles) into e_out
 // (if non-null)
@@ -545,26 +597,39 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   double ops_rho = (has_q && has_mu) ? 20.0 : (has_mu ? 16.0 : 11.0);
   double ops_fld = (forces && has_mu) ? 32.0 : (forces ? 17.0 : 20.0);
   int pr = prof_begin(h, KC_RHO, (double)h->nk * n * ops_rho);
-  switch (nzt) {
-    case 8: launch_rho<R, 8>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
-    case 11: launch_rho<R, 11>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
-    case 13: launch_rho<R, 13>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
-    case 21: launch_rho<R, 21>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
-    case 25: launch_rho<R, 25>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
-    default: launch_rho<R, 16>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+  int nparts = h->n_rho_chunks;
+  // the tensor-core structure factor serves the FP32 CG operator (dipoles
+  // alone, no forces), whose error the FP64 residual refinement removes; the
+  // static field and the force pass keep the CUDA-core kernels (FP32 sums
+  // with round-to-nearest)
+  if (F32 && h->rho_tc && !has_q && has_mu && !forces) {
+    nparts = h->n_tc_chunks;
+    launch_rho_tc(h, M, n, has_q, has_mu);
+  } else {
+    switch (nzt) {
+      case 8: launch_rho<R, 8>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+      case 11: launch_rho<R, 11>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+      case 13: launch_rho<R, 13>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+      case 21: launch_rho<R, 21>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+      case 25: launch_rho<R, 25>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+      default: launch_rho<R, 16>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;
+    }
   }
   LAUNCH_CHECK();
   prof_end(h, pr);
   double tpi_V = kTwoPi / h->omega;
-  // without energy the field kernels sum the chunk partials while staging rho'
+  // without energy and with few chunks the field kernels sum the chunk
+  // partials while staging rho'
   int npart = 0;
-  if (e_out) {
-    k_rec_sum<<<cdiv(h->nk, 256), 256, 0, h->st>>>(h->d_rho_part, h->n_rho_chunks, M, h->d_rhoA, h->d_str);
-    LAUNCH_CHECK();
-    k_rec_energy<<<1, 1024, 0, h->st>>>(h->d_str, M, tpi_V, h->omega, 1, e_out);
+  if (e_out || nparts > 4) {
+    k_rec_sum<<<cdiv(h->nk, 256), 256, 0, h->st>>>(h->d_rho_part, nparts, M, h->d_rhoA, h->d_str);
     LAUNCH_CHECK();
   } else {
-    npart = h->n_rho_chunks;
+    npart = nparts;
+  }
+  if (e_out) {
+    k_rec_energy<<<1, 1024, 0, h->st>>>(h->d_str, M, tpi_V, h->omega, 1, e_out);
+    LAUNCH_CHECK();
   }
   int nch = (int)h->rchunk.size() - 1;
   dim3 gf((unsigned)cdiv(n, kFieldThreads), (unsigned)nch);
@@ -1019,12 +1084,17 @@ static int run_engforce(mdff_ctx* h, int itime) {
   }
   CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(h->h_flags, h->L.flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, h->st));
-  CK(cudaMemcpyAsync(h->h_cata, h->d_cata, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(h->h_cata, h->d_cata, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   prof_collect(h);
   h->stats.list_rebuilds = h->h_flags[3];
   h->stats.list_needed = h->h_flags[2] * n;
   if (h->h_flags[1]) return MDFF_ERR_LIST_OVERFLOW;
+  if (h->h_cata[1]) {
+    h->err = h->h_cata[1] == 2 ? "tensor-core structure factor launched with too little shared memory"
+                               : "a tensor-core structure-factor wait gave up";
+    return MDFF_ERR_TIMEOUT;
+  }
   if (h->h_cata[0]) return MDFF_ERR_CATASTROPHE;
   if (h->lpolar && !h->stats.converged && h->p.fail_on_nonconvergence) return MDFF_ERR_NOT_CONVERGED;
   return MDFF_OK;
@@ -1229,10 +1299,10 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   h->part_cap = (size_t)std::max(cdiv((long)n * 32, 256), cdiv(n, 256)) * 16 + 64;
   DALLOC(h->d_part, h->part_cap);
   DALLOC(h->d_scal, S_NSCAL);
-  DALLOC(h->d_cata, 1);
+  DALLOC(h->d_cata, 2);  // [0] catastrophe, [1] a tensor-core wait gave up
   DALLOC(h->d_ekin_part, cdiv(n, 256));
   CK(cudaMallocHost((void**)&h->h_scal, sizeof(double) * S_NSCAL));
-  CK(cudaMallocHost((void**)&h->h_cata, sizeof(int)));
+  CK(cudaMallocHost((void**)&h->h_cata, 2 * sizeof(int)));
   CK(cudaStreamSynchronize(h->st));
   return MDFF_OK;
 }

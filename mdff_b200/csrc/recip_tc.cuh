@@ -44,9 +44,10 @@ __device__ __forceinline__ uint32_t tf32_rna(float x) {
 }
 
 // x = hi + lo with hi, lo TF32 (|x - hi - lo| <= 2^-22 |x|)
+__device__ __forceinline__ uint32_t tf32_round(uint32_t b) { return (b + 0x1000u) & 0xFFFFE000u; }
 __device__ __forceinline__ void tf32_split(float x, uint32_t& hi, uint32_t& lo) {
-  hi = tf32_rna(x);
-  lo = tf32_rna(x - __uint_as_float(hi));
+  hi = tf32_round(__float_as_uint(x));
+  lo = tf32_round(__float_as_uint(x - __uint_as_float(hi)));
 }
 
 // shared-memory matrix descriptor: no swizzle, K-major; lbo = byte distance of

@@ -107,6 +107,11 @@ struct mdff_ctx {
   // MDFF_REC_TC=0 in the environment
   bool rho_tc = false;
   int tc_chunk = 0, n_tc_chunks = 0;
+  // FP32 reciprocal field / force partials on the tensor cores
+  // (k_rec_field_tc, B tiles in d_fb); off when kz > 31 or MDFF_FIELD_TC=0
+  // in the environment
+  bool field_tc = false;
+  uint32_t* d_fb = nullptr;
   double4* d_G = nullptr;
   double4* d_H = nullptr;
   // pim
@@ -368,6 +373,25 @@ static int build_mesh(mdff_ctx* h) {
     }
 #undef TC_ATTR
   }
+  {
+    const char* env = std::getenv("MDFF_FIELD_TC");
+    int kf = field_tc_kf(h->p.kES[2]);
+    h->field_tc = kf > 0 && nrows > 0 && !(env && env[0] == '0');
+    cudaFree(h->d_fb);
+    h->d_fb = nullptr;
+    if (h->field_tc) {
+      // B tiles for the smaller row tile (with dipole forces): hi + lo per tile
+      DALLOC(h->d_fb, (size_t)cdiv(nrows, field_tc_rpt(true)) * 2 * 128 * kf);
+      int smem = (int)field_tc_smem(kf);
+      if (kf == 32) {
+        CK(cudaFuncSetAttribute(k_rec_field_tc<true, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CK(cudaFuncSetAttribute(k_rec_field_tc<false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      } else {
+        CK(cudaFuncSetAttribute(k_rec_field_tc<true, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        CK(cudaFuncSetAttribute(k_rec_field_tc<false, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      }
+    }
+  }
   DALLOC(h->d_rhoA, std::max(nk, 1));
   DALLOC(h->d_str, std::max(nk, 1));
   DALLOC(h->d_G, (size_t)(h->rchunk.size() - 1) * h->natm);
@@ -552,6 +576,36 @@ static void launch_rho_tc_n(mdff_ctx* h, const RecMesh& M, int n, int has_q, int
   }
 }
 
+// FP32 field / force partials on the tensor cores into d_G / d_H (B tiles
+// built first into d_fb); returns the number of partial chunks written
+template <int KF>
+static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf) {
+  int rpt = field_tc_rpt(muf);
+  int ntile = cdiv(M.nrows, rpt);
+  int ion_tiles = cdiv(n, 128);
+  int nalloc = (int)h->rchunk.size() - 1;
+  int ng = std::max(1, std::min({(2 * (h->nsm > 0 ? h->nsm : 148)) / std::max(ion_tiles, 1), ntile, nalloc}));
+  int tpg = cdiv(ntile, ng);
+  ng = cdiv(ntile, tpg);
+  dim3 g((unsigned)ion_tiles, (unsigned)ng);
+  size_t smem = field_tc_smem(KF);
+  size_t bsmem = (size_t)rpt * (2 * M.kmax[2] + 1) * sizeof(double2);
+  int* err = h->d_cata + 1;
+  if (muf) {
+    k_rec_field_btiles<true, KF><<<ntile, 256, bsmem, h->st>>>(M, h->d_rhoA, h->d_fb);
+    k_rec_field_tc<true, KF><<<g, kFieldTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, M, h->d_fb, tpg, h->d_G, h->d_H, err);
+  } else {
+    k_rec_field_btiles<false, KF><<<ntile, 256, bsmem, h->st>>>(M, h->d_rhoA, h->d_fb);
+    k_rec_field_tc<false, KF><<<g, kFieldTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, M, h->d_fb, tpg, h->d_G, h->d_H, err);
+  }
+  return ng;
+}
+
+static int launch_field_tc(mdff_ctx* h, const RecMesh& M, int n, bool muf) {
+  if (field_tc_kf(M.kmax[2]) == 32) return launch_field_tc_k<32>(h, M, n, muf);
+  return launch_field_tc_k<64>(h, M, n, muf);
+}
+
 static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n, int has_q, int has_mu) {
   if (rho_tc_nb(M.kmax[2]) == 32)
     launch_rho_tc_n<32>(h, M, n, has_q, has_mu);
@@ -621,7 +675,8 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   // without energy and with few chunks the field kernels sum the chunk
   // partials while staging rho'
   int npart = 0;
-  if (e_out || nparts > 4) {
+  const bool field_tc = F32 && h->field_tc;
+  if (e_out || nparts > 4 || field_tc) {
     k_rec_sum<<<cdiv(h->nk, 256), 256, 0, h->st>>>(h->d_rho_part, nparts, M, h->d_rhoA, h->d_str);
     LAUNCH_CHECK();
   } else {
@@ -636,7 +691,9 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   size_t smem = (size_t)h->max_chunk_k * sizeof(typename cplx<R>::T);
   bool muf = forces && has_mu;
   pr = prof_begin(h, KC_RECF, (double)h->nk * n * ops_fld);
-  if constexpr (std::is_same<R, float>::value) {
+  if (field_tc) {
+    nch = launch_field_tc(h, M, n, muf);
+  } else if constexpr (std::is_same<R, float>::value) {
     dim3 gx((unsigned)cdiv(n, 2 * kFieldThreads), (unsigned)nch);
     if (muf)
       k_rec_field_x2<true><<<gx, kFieldThreads, smem, h->st>>>(tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
@@ -1091,8 +1148,8 @@ static int run_engforce(mdff_ctx* h, int itime) {
   h->stats.list_needed = h->h_flags[2] * n;
   if (h->h_flags[1]) return MDFF_ERR_LIST_OVERFLOW;
   if (h->h_cata[1]) {
-    h->err = h->h_cata[1] == 2 ? "tensor-core structure factor launched with too little shared memory"
-                               : "a tensor-core structure-factor wait gave up";
+    h->err = h->h_cata[1] == 2 ? "tensor-core reciprocal kernel launched with too little shared memory"
+                               : "a tensor-core reciprocal-kernel wait gave up";
     return MDFF_ERR_TIMEOUT;
   }
   if (h->h_cata[0]) return MDFF_ERR_CATASTROPHE;
@@ -1660,7 +1717,7 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_G, h->d_H, h->d_Estat, h->d_Eind, h->d_Efield, h->d_mu_ind, h->d_mu_tot,
                   h->d_hist, h->d_E, h->d_r, h->d_z, h->d_pv, h->d_qv, h->d_Tp, h->d_mu32, h->d_force,
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
-                  h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg};
+                  h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);

@@ -412,3 +412,323 @@ static __global__ void __launch_bounds__(kRhoTcThreads) k_rec_rho_tc(
 }
 
 }  // namespace mdff
+
+namespace mdff {
+
+// ===========================================================================
+// Field / force partials of the FP32 reciprocal pass on the tensor cores.
+//
+// For ion i and mesh row (nx, ny) with P = X_nx Y_ny (ewald_rec.f90:181-250):
+//   a(k) = Im(rho'_k conj(e^{i k.r_i})),  G_i = sum_k n_k a(k),
+//   H_i  = sum_k n_k (k.mu_i) Re(rho'_k conj(e^{i k.r_i})).
+// Over the nz of a row, with conj(Z_-n) = Z_n:
+//   T  = sum_nz rho'(nz) conj(Z_nz),  T1 = sum_nz nz rho'(nz) conj(Z_nz),
+//   T2 = sum_nz nz^2 rho'(nz) conj(Z_nz),
+// linear in the ion features f = (Re Z_0..Re Z_kz, Im Z_0..Im Z_kz): a GEMM
+//   D[i][c] = sum_f A[i][f] B[c][f]
+// with A = ion features (M = 128 ions per tile, K = KF), B = per-row
+// coefficients of Re T, Im T, Re T1, Im T1 (+ Re T2, Im T2 for the dipole
+// force) from rho'(+n), rho'(-n).  Then per (ion, row), in FP32 from D and P:
+//   S0 = Im(conj(P) T), Sz = Im(conj(P) T1)  ->  G += (nx S0, ny S0, Sz) in FP64
+// and for H, with km = nx m1 + ny m2:
+//   T0 = km Re(conj(P) T) + m3 Re(conj(P) T1),  Tz = km Re(conj(P) T1) + m3 Re(conj(P) T2)
+//   -> H += (nx T0, ny T0, Tz).
+// K is only 2 (kz + 1) features, so the FP32 accumulation in the tensor core
+// is short; operands are split TF32 (A_hi B_hi + A_hi B_lo + A_lo B_hi).
+//
+// B tiles are built once per pass (k_rec_field_btiles).  CTA = 128 ions x a
+// group of row tiles (128 columns each), 256 threads: the next B tile is copied
+// in (cp.async) while the tensor core multiplies the current one into one half
+// of a double-buffered tensor-memory accumulator and the threads reduce the
+// previous one from the other half.
+constexpr int kFieldTcThreads = 256;
+
+// features per ion (K), 32 or 64 (0: kz too large for this kernel)
+__host__ __device__ constexpr int field_tc_kf(int kz) {
+  return 2 * (kz + 1) <= 32 ? 32 : (2 * (kz + 1) <= 64 ? 64 : 0);
+}
+// rows per 128-column tile
+__host__ __device__ constexpr int field_tc_rpt(bool has_h) { return has_h ? 16 : 32; }
+// A hi + lo and two B buffers (hi + lo), each 128 x KF TF32, + alignment slack
+__host__ __device__ constexpr size_t field_tc_smem(int KF) { return (size_t)6 * 128 * KF * 4 + 1024; }
+
+// B tiles of the field GEMM, once per pass: tile t = [hi | lo], each 128
+// columns x KF features in the canonical K-major layout (the shared-memory
+// image the field kernel copies).  One CTA per tile; rho' of the tile's rows
+// is staged in shared memory as rho'(row, nz), zero outside the row's range.
+template <bool HAS_H, int KF>
+static __global__ void __launch_bounds__(256) k_rec_field_btiles(RecMesh M, const double2* __restrict__ rhoA,
+                                                                 uint32_t* __restrict__ fb) {
+  constexpr int CPR = HAS_H ? 8 : 4, RPT = 128 / CPR;
+  constexpr int TILE = 128 * KF * 4;
+  const int kz = M.kmax[2], nzc = kz + 1, nzs = 2 * kz + 1;
+  extern __shared__ double2 rs[];  // [RPT][nzs]
+  const int t = blockIdx.x;
+  for (int e = threadIdx.x; e < RPT * nzs; e += blockDim.x) {
+    int lr = e / nzs, nz = e % nzs - kz;
+    int row = t * RPT + lr;
+    double2 v = make_double2(0.0, 0.0);
+    if (row < M.nrows) {
+      int4 ri = M.rows[row];
+      if (nz >= ri.z) v = rhoA[ri.w + nz - ri.z];
+    }
+    rs[e] = v;
+  }
+  __syncthreads();
+  unsigned char* Bh = reinterpret_cast<unsigned char*>(fb) + (size_t)t * 2 * TILE;
+  unsigned char* Bl = Bh + TILE;
+  for (int it = threadIdx.x; it < 128 * (KF / 4); it += blockDim.x) {
+    int c = it & 127, fc = it >> 7;
+    int lr = c / CPR, type = c % CPR;
+    bool ok = t * RPT + lr < M.nrows && type < 6;
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      int f = fc * 4 + u;
+      float x = 0.f;
+      if (ok && f < 2 * nzc) {
+        bool zi = f >= nzc;
+        int n = zi ? f - nzc : f;
+        double2 rp = rs[lr * nzs + kz + n];
+        double2 rm = n > 0 ? rs[lr * nzs + kz - n] : make_double2(0.0, 0.0);
+        double sr = rp.x + rm.x, si = rp.y + rm.y, dr = rp.x - rm.x, di = rp.y - rm.y;
+        double fn = (double)n, c0;
+        switch (type) {
+          case 0: c0 = zi ? di : sr; break;
+          case 1: c0 = zi ? -dr : si; break;
+          case 2: c0 = fn * (zi ? si : dr); break;
+          case 3: c0 = fn * (zi ? -sr : di); break;
+          case 4: c0 = fn * fn * (zi ? di : sr); break;
+          default: c0 = fn * fn * (zi ? -dr : si); break;
+        }
+        x = (float)c0;
+      }
+      tc::tf32_split(x, hi[u], lo[u]);
+    }
+    uint32_t o = tc::canon(c, fc * 4, 128);
+    *reinterpret_cast<uint4*>(Bh + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4*>(Bl + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  }
+}
+
+template <bool HAS_H, int KF>
+static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
+    const float2* __restrict__ tab, const float4* __restrict__ w, int natm, RecMesh M,
+    const uint32_t* __restrict__ fb, int tiles_per_group, double4* __restrict__ Gpart,
+    double4* __restrict__ Hpart, int* __restrict__ err) {
+  constexpr int NT = kFieldTcThreads;
+  constexpr int CPR = HAS_H ? 8 : 4;     // columns per mesh row (6 used with H)
+  constexpr int RPT = 128 / CPR;         // mesh rows per tile
+  constexpr int RPC = 32 / CPR;          // mesh rows per 32-column chunk
+  constexpr int TILE = 128 * KF * 4;     // bytes of one 128-row operand
+  constexpr uint32_t LBO = (128 / 8) * 128, SBO = 128;
+  extern __shared__ unsigned char smraw[];
+  unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tslot;
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int kx = M.kmax[0], ky = M.kmax[1], kz = M.kmax[2];
+  const int nzc = kz + 1;
+  const size_t zoff = (size_t)(kx + 1 + ky + 1);
+  {
+    uint32_t dyn;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
+    if (dyn < field_tc_smem(KF) || field_tc_kf(kz) != KF) {
+      if (tid == 0) atomicExch(err, 2);
+      return;
+    }
+  }
+  const int ntile = (M.nrows + RPT - 1) / RPT;
+  const int tbeg = blockIdx.y * tiles_per_group;
+  const int tend = min(tbeg + tiles_per_group, ntile);
+  const int i0 = blockIdx.x * 128;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32(&tslot)),
+                 "r"(256));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    abort_flag = 0;
+    tc::mbar_init(tc::smem_u32(&mbar[0]));
+    tc::mbar_init(tc::smem_u32(&mbar[1]));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tmem = tslot;
+  unsigned char* Ahi = sm;
+  unsigned char* Alo = sm + TILE;
+  auto Bbuf = [&](int b) { return sm + 2 * TILE + b * 2 * TILE; };
+  const int T = tend - tbeg;
+  // B tile t (hi | lo, 2 TILE bytes) -> buffer b, 16-byte copies
+  auto load_b = [&](int t, int b) {
+    const uint4* src = reinterpret_cast<const uint4*>(fb) + (size_t)t * (2 * TILE / 16);
+    uint32_t dst = tc::smem_u32(Bbuf(b));
+    for (int e = tid; e < 2 * TILE / 16; e += NT) cp_async16(dst + e * 16, src + e, 16);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  if (T > 0) load_b(tbeg, 0);
+
+  // A: ion features, items (ion m, 4 features) with m = it % 128
+  for (int it = tid; it < 128 * (KF / 4); it += NT) {
+    int m = it & 127, fc = it >> 7;
+    int i = i0 + m;
+    uint32_t hi[4], lo[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      int f = fc * 4 + u;
+      float x = 0.f;
+      if (i < natm && f < 2 * nzc) {
+        float2 Z = tab[(zoff + (f < nzc ? f : f - nzc)) * natm + i];
+        x = f < nzc ? Z.x : Z.y;
+      }
+      tc::tf32_split(x, hi[u], lo[u]);
+    }
+    uint32_t o = tc::canon(m, fc * 4, 128);
+    *reinterpret_cast<uint4*>(Ahi + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+    *reinterpret_cast<uint4*>(Alo + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+  }
+  // per-thread sums: ion m = 32 (warp & 3) + lane, column chunks (warp >> 2) and +2
+  const int q = warp & 3, hh = warp >> 2;
+  const int m = q * 32 + lane, ion = i0 + m;
+  const bool ion_ok = ion < natm;
+  const int ionc = ion_ok ? ion : 0;
+  float4 wi = ion_ok ? w[ion] : make_float4(0.f, 0.f, 0.f, 0.f);
+  double G[3] = {0.0, 0.0, 0.0}, H[3] = {0.0, 0.0, 0.0};
+  auto epilogue = [&](int t, int b) {
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc) {
+      int ch = hh + 2 * cc;
+      // the chunk's rows and this ion's phases X_nx Y_ny first (loads in flight together)
+      int nxr[RPC], nyr[RPC];
+      float okr[RPC];
+      float2 X[RPC], Y[RPC];
+#pragma unroll
+      for (int jj = 0; jj < RPC; ++jj) {
+        int row = t * RPT + ch * RPC + jj;
+        bool ok = row < M.nrows;
+        int4 ri = M.rows[ok ? row : 0];
+        nxr[jj] = ri.x;
+        nyr[jj] = ri.y;
+        okr[jj] = (ok && ion_ok) ? 1.f : 0.f;
+        int ay = ri.y < 0 ? -ri.y : ri.y;
+        X[jj] = tab[(size_t)ri.x * natm + ionc];
+        Y[jj] = tab[(size_t)(kx + 1 + ay) * natm + ionc];
+      }
+      float v[32];
+      tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 128 + ch * 32), v);
+#pragma unroll
+      for (int jj = 0; jj < RPC; ++jj) {
+        int nx = nxr[jj], ny = nyr[jj];
+        float Yi = ny < 0 ? -Y[jj].y : Y[jj].y;
+        float Pr = okr[jj] * (X[jj].x * Y[jj].x - X[jj].y * Yi);
+        float Pi = okr[jj] * (X[jj].x * Yi + X[jj].y * Y[jj].x);
+        const float* d = v + jj * CPR;
+        float s0 = Pr * d[1] - Pi * d[0];
+        float sz = Pr * d[3] - Pi * d[2];
+        G[0] += (double)nx * (double)s0;
+        G[1] += (double)ny * (double)s0;
+        G[2] += (double)sz;
+        if (HAS_H) {
+          float reA = Pr * d[0] + Pi * d[1], reB = Pr * d[2] + Pi * d[3], reC = Pr * d[4] + Pi * d[5];
+          float km = (float)nx * wi.y + (float)ny * wi.z;
+          float t0 = km * reA + wi.w * reB, tz = km * reB + wi.w * reC;
+          H[0] += (double)nx * (double)t0;
+          H[1] += (double)ny * (double)t0;
+          H[2] += (double)tz;
+        }
+      }
+    }
+  };
+
+  const uint32_t idesc = tc::idesc_tf32(128, 128);
+  int issued = 0, done = 0;  // tiles multiplied / tiles whose MMA completion was seen
+  for (int k = 0; k < T; ++k) {
+    const int b = k & 1;
+    if (k >= 1) {
+      // tile k - 1 multiplied: B buffer (k + 1) & 1 is free, its D is ready
+      if (tid == 0 && !tc::mbar_wait(tc::smem_u32(&mbar[(k - 1) & 1]), ((k - 1) >> 1) & 1, tc::kWaitLimit))
+        abort_flag = 1;
+      __syncthreads();
+      if (abort_flag) break;
+      done = k;
+    }
+    if (k + 1 < T) {
+      load_b(tbeg + k + 1, (k + 1) & 1);
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+    } else {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+    }
+    tc::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      const uint32_t aH = tc::smem_u32(Ahi), aL = tc::smem_u32(Alo);
+      const uint32_t bH = tc::smem_u32(Bbuf(b)), bL = bH + TILE;
+      const uint32_t d = tmem + (uint32_t)(b * 128);
+#pragma unroll
+      for (int s = 0; s < KF / 8; ++s) {
+        uint32_t o = (uint32_t)s * 2 * LBO;
+        uint64_t dAH = tc::smem_desc(aH + o, LBO, SBO), dAL = tc::smem_desc(aL + o, LBO, SBO);
+        uint64_t dBH = tc::smem_desc(bH + o, LBO, SBO), dBL = tc::smem_desc(bL + o, LBO, SBO);
+        tc::mma_tf32(d, dAH, dBH, idesc, s > 0 ? 1u : 0u);
+        tc::mma_tf32(d, dAH, dBL, idesc, 1u);
+        tc::mma_tf32(d, dAL, dBH, idesc, 1u);
+      }
+      tc::mma_commit(tc::smem_u32(&mbar[b]));
+    }
+    issued = k + 1;
+    if (k >= 1) {
+      tc::fence_after_sync();
+      epilogue(tbeg + k - 1, (k - 1) & 1);
+    }
+    tc::fence_before_sync();
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  if (!abort_flag && issued > done) {
+    if (tid == 0 && !tc::mbar_wait(tc::smem_u32(&mbar[(issued - 1) & 1]), ((issued - 1) >> 1) & 1, tc::kWaitLimit))
+      abort_flag = 1;
+    __syncthreads();
+    if (!abort_flag) {
+      tc::fence_after_sync();
+      epilogue(tbeg + issued - 1, (issued - 1) & 1);
+      done = issued;
+    }
+  } else if (abort_flag && issued > done && tid == 0) {
+    // stopped early: let the last issued MMA finish before freeing its memory
+    tc::mbar_wait(tc::smem_u32(&mbar[(issued - 1) & 1]), ((issued - 1) >> 1) & 1, tc::kWaitLimit);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after_sync();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256));
+  }
+  if (abort_flag) {
+    if (tid == 0) atomicExch(err, 1);
+    return;
+  }
+  // combine the two column halves of each ion (A is free: every MMA is done)
+  double* red = reinterpret_cast<double*>(sm);
+  if (hh == 1) {
+    red[m * 6 + 0] = G[0];
+    red[m * 6 + 1] = G[1];
+    red[m * 6 + 2] = G[2];
+    red[m * 6 + 3] = H[0];
+    red[m * 6 + 4] = H[1];
+    red[m * 6 + 5] = H[2];
+  }
+  __syncthreads();
+  if (hh == 0 && ion_ok) {
+    Gpart[(size_t)blockIdx.y * natm + ion] =
+        make_double4(G[0] + red[m * 6 + 0], G[1] + red[m * 6 + 1], G[2] + red[m * 6 + 2], 0.0);
+    if (HAS_H)
+      Hpart[(size_t)blockIdx.y * natm + ion] =
+          make_double4(H[0] + red[m * 6 + 3], H[1] + red[m * 6 + 4], H[2] + red[m * 6 + 5], 0.0);
+  }
+}
+
+}  // namespace mdff

@@ -424,6 +424,17 @@ def cpu_baseline_sample(s, hist, itime, pos_soa):
 KCLS = ("list_build", "short_range", "real_space_field", "real_space_force",
         "structure_factor", "reciprocal_field", "other")
 
+# DRAM bytes (read + write) per launch of each class's main kernel on the 12k
+# SiO2 workload, from one ncu capture (profiles/k_rec_rho_tc_k_rec_field_tc_sio2_12000.md,
+# profiles/realspace_kernels_sio2_12000.md); the working set is L2-resident
+TRAFFIC = {
+    "structure_factor": {"kernel": "k_rec_rho_tc<0, 1, 32>", "bytes": 3.968e6},
+    "reciprocal_field": {"kernel": "k_rec_field_tc<0, 32>", "bytes": 4.118e6},
+    "real_space_force": {"kernel": "k_es_force<float>", "bytes": 20.09e6},
+    "short_range": {"kernel": "k_shortrange<double, 1>", "bytes": 18.96e6},
+    "real_space_field": {"kernel": "k_static_cache", "bytes": 20.27e6},
+}
+
 
 def roofline_block(res, extra):
     kms, kl, kw = res["kms"], res["kl"], res["kw"]
@@ -436,15 +447,17 @@ def roofline_block(res, extra):
     achieved = ops_per_launch / (avg_ms * 1e-3) / 1e12
     peak = extra["peak_fp32_tflops"]
     share = {KCLS[i]: round(float(kms[i] / kms.sum()), 4) for i in range(len(KCLS)) if kms[i] > 0}
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tf):
-        traffic = json.load(open(tf)).get(KCLS[c])
+    tr = TRAFFIC.get(KCLS[c])
     return {"kernel": KCLS[c], "bound": "fp32_fma", "achieved": round(achieved, 3),
             "peak": round(peak, 3), "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
-            "traffic": traffic, "launches": int(kl[c]), "avg_launch_ms": round(avg_ms, 5),
+            "traffic": tr["bytes"] if tr else None,
+            "traffic_kernel": tr["kernel"] if tr else None,
+            "launches": int(kl[c]), "avg_launch_ms": round(avg_ms, 5),
             "peak_source": "measured live: register-resident FP32 FMA loop on all SMs (mdff_gpu_peak_flops); "
                            "MEASURED_PEAKS.json has HBM and bf16 tensor peaks only",
+            "note": "achieved counts algorithmic ops of the class (all its launches); the FP32 CG-operator "
+                    "launches of the reciprocal classes run on the tcgen05 tensor cores (split TF32), so "
+                    "frac compares with the CUDA-core FP32 ceiling",
             "time_share": share}
 
 

@@ -579,7 +579,7 @@ static void launch_rho_tc_n(mdff_ctx* h, const RecMesh& M, int n, int has_q, int
 // FP32 field / force partials on the tensor cores into d_G / d_H (B tiles
 // built first into d_fb); returns the number of partial chunks written
 template <int KF>
-static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf) {
+static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int npart) {
   int rpt = field_tc_rpt(muf);
   int ntile = cdiv(M.nrows, rpt);
   int ion_tiles = cdiv(n, 128);
@@ -589,21 +589,22 @@ static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf) {
   ng = cdiv(ntile, tpg);
   dim3 g((unsigned)ion_tiles, (unsigned)ng);
   size_t smem = field_tc_smem(KF);
-  size_t bsmem = (size_t)rpt * (2 * M.kmax[2] + 1) * sizeof(double2);
+  size_t bsmem = (size_t)kBtRows * (2 * M.kmax[2] + 1) * sizeof(double2);
+  dim3 gb((unsigned)ntile, (unsigned)(rpt / kBtRows));
   int* err = h->d_cata + 1;
   if (muf) {
-    k_rec_field_btiles<true, KF><<<ntile, 256, bsmem, h->st>>>(M, h->d_rhoA, h->d_fb);
+    k_rec_field_btiles<true, KF><<<gb, 128, bsmem, h->st>>>(M, h->d_rhoA, h->d_rho_part, npart, h->d_fb);
     k_rec_field_tc<true, KF><<<g, kFieldTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, M, h->d_fb, tpg, h->d_G, h->d_H, err);
   } else {
-    k_rec_field_btiles<false, KF><<<ntile, 256, bsmem, h->st>>>(M, h->d_rhoA, h->d_fb);
+    k_rec_field_btiles<false, KF><<<gb, 128, bsmem, h->st>>>(M, h->d_rhoA, h->d_rho_part, npart, h->d_fb);
     k_rec_field_tc<false, KF><<<g, kFieldTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, M, h->d_fb, tpg, h->d_G, h->d_H, err);
   }
   return ng;
 }
 
-static int launch_field_tc(mdff_ctx* h, const RecMesh& M, int n, bool muf) {
-  if (field_tc_kf(M.kmax[2]) == 32) return launch_field_tc_k<32>(h, M, n, muf);
-  return launch_field_tc_k<64>(h, M, n, muf);
+static int launch_field_tc(mdff_ctx* h, const RecMesh& M, int n, bool muf, int npart) {
+  if (field_tc_kf(M.kmax[2]) == 32) return launch_field_tc_k<32>(h, M, n, muf, npart);
+  return launch_field_tc_k<64>(h, M, n, muf, npart);
 }
 
 static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n, int has_q, int has_mu) {
@@ -672,11 +673,12 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   LAUNCH_CHECK();
   prof_end(h, pr);
   double tpi_V = kTwoPi / h->omega;
-  // without energy and with few chunks the field kernels sum the chunk
-  // partials while staging rho'
+  // without energy the field pass sums the chunk partials while staging rho'
+  // (the CUDA-core field kernels when there are few chunks; the tensor-core
+  // B-tile builder always)
   int npart = 0;
   const bool field_tc = F32 && h->field_tc;
-  if (e_out || nparts > 4 || field_tc) {
+  if (e_out || (nparts > 4 && !field_tc)) {
     k_rec_sum<<<cdiv(h->nk, 256), 256, 0, h->st>>>(h->d_rho_part, nparts, M, h->d_rhoA, h->d_str);
     LAUNCH_CHECK();
   } else {
@@ -692,7 +694,7 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   bool muf = forces && has_mu;
   pr = prof_begin(h, KC_RECF, (double)h->nk * n * ops_fld);
   if (field_tc) {
-    nch = launch_field_tc(h, M, n, muf);
+    nch = launch_field_tc(h, M, n, muf, npart);
   } else if constexpr (std::is_same<R, float>::value) {
     dim3 gx((unsigned)cdiv(n, 2 * kFieldThreads), (unsigned)nch);
     if (muf)

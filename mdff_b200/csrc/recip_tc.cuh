@@ -436,7 +436,8 @@ namespace mdff {
 // K is only 2 (kz + 1) features, so the FP32 accumulation in the tensor core
 // is short; operands are split TF32 (A_hi B_hi + A_hi B_lo + A_lo B_hi).
 //
-// B tiles are built once per pass (k_rec_field_btiles).  CTA = 128 ions x a
+// B tiles are built once per pass (k_rec_field_btiles, which also sums the
+// structure-factor chunks when no energy is needed).  CTA = 128 ions x a
 // group of row tiles (128 columns each), 256 threads: the next B tile is copied
 // in (cp.async) while the tensor core multiplies the current one into one half
 // of a double-buffered tensor-memory accumulator and the threads reduce the
@@ -454,33 +455,43 @@ __host__ __device__ constexpr size_t field_tc_smem(int KF) { return (size_t)6 * 
 
 // B tiles of the field GEMM, once per pass: tile t = [hi | lo], each 128
 // columns x KF features in the canonical K-major layout (the shared-memory
-// image the field kernel copies).  One CTA per tile; rho' of the tile's rows
-// is staged in shared memory as rho'(row, nz), zero outside the row's range.
+// image the field kernel copies).  grid = (tiles, RPT / kBtRows): each CTA
+// builds the columns of kBtRows mesh rows.  rho'(row, nz) is staged in shared
+// memory, zero outside the row's nz range: from rhoA, or (npart > 0) summed
+// from the structure-factor chunk partials in chunk order (rho_prime, the same
+// sums as k_rec_sum), which saves that pass when no energy is needed.
+constexpr int kBtRows = 4;
+
 template <bool HAS_H, int KF>
-static __global__ void __launch_bounds__(256) k_rec_field_btiles(RecMesh M, const double2* __restrict__ rhoA,
+static __global__ void __launch_bounds__(128) k_rec_field_btiles(RecMesh M, const double2* __restrict__ rhoA,
+                                                                 const double2* __restrict__ part, int npart,
                                                                  uint32_t* __restrict__ fb) {
   constexpr int CPR = HAS_H ? 8 : 4, RPT = 128 / CPR;
   constexpr int TILE = 128 * KF * 4;
   const int kz = M.kmax[2], nzc = kz + 1, nzs = 2 * kz + 1;
-  extern __shared__ double2 rs[];  // [RPT][nzs]
-  const int t = blockIdx.x;
-  for (int e = threadIdx.x; e < RPT * nzs; e += blockDim.x) {
+  extern __shared__ double2 rs[];  // [kBtRows][nzs]
+  const int t = blockIdx.x, lr0 = blockIdx.y * kBtRows;
+  for (int e = threadIdx.x; e < kBtRows * nzs; e += blockDim.x) {
     int lr = e / nzs, nz = e % nzs - kz;
-    int row = t * RPT + lr;
+    int row = t * RPT + lr0 + lr;
     double2 v = make_double2(0.0, 0.0);
     if (row < M.nrows) {
       int4 ri = M.rows[row];
-      if (nz >= ri.z) v = rhoA[ri.w + nz - ri.z];
+      if (nz >= ri.z) {
+        int k = ri.w + nz - ri.z;
+        v = npart ? rho_prime(part, npart, M.Ak, M.nk, k) : rhoA[k];
+      }
     }
     rs[e] = v;
   }
   __syncthreads();
   unsigned char* Bh = reinterpret_cast<unsigned char*>(fb) + (size_t)t * 2 * TILE;
   unsigned char* Bl = Bh + TILE;
-  for (int it = threadIdx.x; it < 128 * (KF / 4); it += blockDim.x) {
-    int c = it & 127, fc = it >> 7;
-    int lr = c / CPR, type = c % CPR;
-    bool ok = t * RPT + lr < M.nrows && type < 6;
+  for (int it = threadIdx.x; it < kBtRows * CPR * (KF / 4); it += blockDim.x) {
+    int cl = it % (kBtRows * CPR), fc = it / (kBtRows * CPR);
+    int lr = cl / CPR, type = cl % CPR;
+    int c = lr0 * CPR + cl;  // column in the tile
+    bool ok = t * RPT + lr0 + lr < M.nrows && type < 6;
     uint32_t hi[4], lo[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {

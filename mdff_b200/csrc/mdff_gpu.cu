@@ -620,7 +620,7 @@ static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n, int has_q, int h
 template <typename R>
 static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4* mu, int has_q,
                       int has_mu, int forces, double4* E, double* e_out, float4* mu32,
-                      SelfField sf) {
+                      SelfField sf, int* defer_nch, bool weights_ready) {
   int n = h->natm;
   if (h->nk == 0) {
     if (sf.on) {
@@ -639,9 +639,12 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   M.Ak = h->d_Ak;
   M.kvec = h->d_kvec;
   constexpr bool F32 = std::is_same<R, float>::value;
-  k_rec_weights<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_q, mu, n, h->d_cell, has_q, has_mu, h->d_w,
-                                                 F32 ? h->d_w32 : nullptr, mu32);
-  LAUNCH_CHECK();
+  // (the FP32 CG direction kernels write the FP32 weights themselves)
+  if (!(F32 && weights_ready)) {
+    k_rec_weights<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_q, mu, n, h->d_cell, has_q, has_mu, h->d_w,
+                                                   F32 ? h->d_w32 : nullptr, mu32);
+    LAUNCH_CHECK();
+  }
   int nzt = pick_nzt(2 * M.kmax[2] + 1);
   int ntiles = cdiv(2 * M.kmax[2] + 1, nzt);
   dim3 g((unsigned)(M.nrows * ntiles), (unsigned)h->n_rho_chunks);
@@ -708,6 +711,11 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   LAUNCH_CHECK();
   prof_end(h, pr);
   double fpi_V = 2.0 * tpi_V;
+  if (defer_nch) {
+    // the caller's kernel sums the field partials (k_dd_cached_rec)
+    *defer_nch = nch;
+    return MDFF_OK;
+  }
   k_rec_field_sum<<<cdiv((long)n * 4, 256), 256, 0, h->st>>>(h->d_G, h->d_H, nch, n, h->d_cell, h->d_q,
                                                    2.0 * fpi_V, muf ? 1 : 0, forces, h->coul_unit, E,
                                                    h->d_force, sf);
@@ -716,9 +724,10 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
 }
 
 static int rec_pass(mdff_ctx* h, bool fp32, const double4* mu, int has_q, int has_mu, int forces,
-                    double4* E, double* e_out, SelfField sf, float4* mu32 = nullptr) {
-  if (fp32) return rec_pass_t<float>(h, h->d_tab32, mu, has_q, has_mu, forces, E, e_out, mu32, sf);
-  return rec_pass_t<double>(h, h->d_tab64, mu, has_q, has_mu, forces, E, e_out, mu32, sf);
+                    double4* E, double* e_out, SelfField sf, float4* mu32 = nullptr,
+                    int* defer_nch = nullptr, bool weights_ready = false) {
+  if (fp32) return rec_pass_t<float>(h, h->d_tab32, mu, has_q, has_mu, forces, E, e_out, mu32, sf, defer_nch, weights_ready);
+  return rec_pass_t<double>(h, h->d_tab64, mu, has_q, has_mu, forces, E, e_out, mu32, sf, defer_nch, false);
 }
 
 // the self field 2 selfa2 mu (+ surface field of the reduced moments in mom
@@ -750,9 +759,15 @@ static int build_tables(mdff_ctx* h) {
 
 // field of a dipole set alone (charges zeroed, dd task, undamped): the SCF
 // induced pass / the CG operator.  E = T mu.
-static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, double4* E) {
+// weights_ready: d_w32 / d_mu32 already hold the FP32 operands of mu (written
+// by the CG direction kernels)
+static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, double4* E,
+                       bool weights_ready = false) {
   int n = h->natm;
-  CK(cudaMemsetAsync(E, 0, sizeof(double4) * n, h->st));
+  // FP32 CG operator with the pair cache: one kernel writes E (reciprocal +
+  // self + cached real-space dipole field)
+  const bool fused = fp32 && dd_mask == 1 && h->dd_cache_ok && h->nk > 0;
+  if (!fused) CK(cudaMemsetAsync(E, 0, sizeof(double4) * n, h->st));
   double cutsq = h->p.cutlongrange * h->p.cutlongrange;
   int nb = cdiv((long)n * 32, 256);
   int s;
@@ -762,11 +777,16 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   }
   // reciprocal first: its weights kernel also writes the FP32 dipoles; its
   // final kernel adds the self / surface field
-  s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, self_field(h, mu, h->d_scal + S_MOM2),
-               fp32 ? h->d_mu32 : nullptr);
+  int nch = 0;
+  SelfField sf = self_field(h, mu, h->d_scal + S_MOM2);
+  s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, sf, fp32 ? h->d_mu32 : nullptr,
+               fused ? &nch : nullptr, fp32 && weights_ready);
   if (s) return s;
   int pr = prof_begin(h, KC_ESFIELD, 0);
-  if (fp32 && dd_mask == 1 && h->dd_cache_ok)
+  if (fused)
+    k_dd_cached_rec<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n,
+                                           h->d_G, nch, h->d_cell, 2.0 * (2.0 * (kTwoPi / h->omega)), sf, E);
+  else if (fp32 && dd_mask == 1 && h->dd_cache_ok)
     k_dd_cached<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n, E);
   else if (fp32)
     k_es_field<float, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu32, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
@@ -934,14 +954,15 @@ static int cg_iteration(mdff_ctx* h, bool fp32, int in_graph, cudaGraphCondition
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
   double* sc = h->d_scal + S_CG;
-  if ((s = field_of_mu(h, h->d_pv, 1, fp32, h->d_Tp))) return s;
+  if ((s = field_of_mu(h, h->d_pv, 1, fp32, h->d_Tp, fp32))) return s;
   k_cg_Ap<<<nb, 256, 0, h->st>>>(h->d_pv, h->d_Tp, P, n, h->d_qv, h->d_part);
   LAUNCH_CHECK();
   if ((s = reduce_into(h, nb, 1, sc + 2))) return s;
   k_cg_update<<<nb, 256, 0, h->st>>>(sc + 0, sc + 2, P, n, h->d_pv, h->d_qv, h->d_mu_ind, h->d_r, h->d_z, h->d_part);
   LAUNCH_CHECK();
   if ((s = reduce_into(h, nb, 2, sc + 3))) return s;
-  k_cg_dir<<<nb, 256, 0, h->st>>>(sc + 0, sc + 3, n, h->d_z, h->d_pv);
+  k_cg_dir<<<nb, 256, 0, h->st>>>(sc + 0, sc + 3, n, h->d_z, h->d_pv, h->d_cell,
+                                  fp32 ? h->d_w32 : nullptr, h->d_mu32);
   LAUNCH_CHECK();
   k_cg_inner_check<<<1, 32, 0, h->st>>>(sc, h->npol, in_graph, hc);
   LAUNCH_CHECK();
@@ -1017,7 +1038,8 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
     if (need_residual) {
       // true residual (FP64 matvec)
       if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp))) return s;
-      k_cg_init<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part);
+      k_cg_init<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
+                                       h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32);
       LAUNCH_CHECK();
       if ((s = reduce_into(h, nb, 2, sc))) return s;
       CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * 9, cudaMemcpyDeviceToHost, h->st));

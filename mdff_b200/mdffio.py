@@ -14,6 +14,14 @@ writes decks the reference binary reads.
   reference's defaults (the *_default_tag routines).  '!INCLUDE <file>' lines
   are replaced by the file, as the examples' deck generator does
   (examples/ex09/config/gen_tests, include()).
+* Outputs: CONTFF (config.f90:208-252: the POSFF header with fixed formats,
+  positions wrapped, then type, position, velocity, force per ion), DIPFF
+  (field.f90:300-337: list-directed header, then ion number, type and the
+  three dipole components) and EFGALL (field.f90:392-448, formatted variant:
+  the six independent components vxx vyy vzz vxy vxz vyz per ion).  Fixed
+  formats (i8, 3f20.12, e24.16, ...) are written as Fortran writes them;
+  list-directed lines follow gfortran's layout (their widths differ between
+  compilers; the readers here and the reference's parse them by blanks).
 """
 import os
 import re
@@ -94,6 +102,130 @@ def write_posff(path, system, cell, names, natmi, pos, vel=None, force=None):
             if force is not None:
                 cols += list(force[i])
             f.write(f"{names[typ[i]]:>3s} " + " ".join(f"{x:22.14e}" for x in cols) + "\n")
+
+
+def fortran_e(x, w=24, d=16):
+    """Fortran Ew.d: 0.<d digits>E<sign><2 digits>, right-justified in w."""
+    x = float(x)
+    if x == 0.0:
+        body, ex = "0." + "0" * d, 0
+    else:
+        m, e = f"{abs(x):.{d - 1}e}".split("e")
+        body, ex = "0." + m.replace(".", ""), int(e) + 1
+    sgn = "-" if x < 0 or (x == 0.0 and str(x).startswith("-")) else ""
+    es = f"E{ex:+03d}" if abs(ex) < 100 else f"{ex:+04d}"
+    return f"{sgn}{body}{es}".rjust(w)
+
+
+def _ld_real(x):
+    # list-directed REAL(8) as gfortran writes it (17 significant digits)
+    return f"{float(x):26.17G}"
+
+
+def _ld_int(n):
+    return f"{int(n):12d}"
+
+
+def _wrap(A, pos):
+    B = np.linalg.inv(A)
+    s = np.asarray(pos, dtype=np.float64) @ B.T
+    s = s - np.where(s >= 0, np.floor(s + 0.5), np.ceil(s - 0.5))  # Fortran NINT
+    return s @ A.T
+
+
+def _ld_header(f, natm, system, A, names, natmi):
+    f.write(_ld_int(natm) + "\n")
+    f.write(" " + system + "\n")
+    for j in range(3):
+        f.write("".join(_ld_real(A[a, j]) for a in range(3)) + "\n")
+    f.write(_ld_int(len(names)) + "\n")
+    f.write(" " + " ".join(f"{n:3s}" for n in names) + "\n")
+    f.write("".join(_ld_int(n) for n in natmi) + "\n")
+
+
+def write_contff(path, system, cell, names, natmi, pos, vel, force):
+    """CONTFF: last configuration with velocities and forces (config.f90:208-252);
+    positions wrapped by kardir / periodicbc / dirkar as the writer does."""
+    A = np.asarray(cell, dtype=np.float64)
+    pos = _wrap(A, pos)
+    vel = np.asarray(vel, dtype=np.float64)
+    force = np.asarray(force, dtype=np.float64)
+    natm = pos.shape[0]
+    typ = np.repeat(np.arange(len(names)), natmi)
+    with open(path, "w") as f:
+        f.write(f"{natm:8d}\n{system}\n")
+        for j in range(3):
+            f.write("".join(f"{A[a, j]:20.12f}" for a in range(3)) + "\n")
+        f.write(f"{len(names):4d}\n")
+        f.write(" " + " ".join(f"{n:3s}" for n in names) + "\n")
+        f.write("".join(_ld_int(n) for n in natmi) + "\n")
+        f.write("Cartesian\n")
+        for i in range(natm):
+            vals = list(pos[i]) + list(vel[i]) + list(force[i])
+            f.write(f"{names[typ[i]]:3s}" + "".join(fortran_e(v) for v in vals) + "\n")
+
+
+def write_dipff(path, system, cell, names, natmi, mu):
+    """DIPFF: dipoles at the ions (field.f90:300-337)."""
+    A = np.asarray(cell, dtype=np.float64)
+    mu = np.asarray(mu, dtype=np.float64).reshape(-1, 3)
+    typ = np.repeat(np.arange(len(names)), natmi)
+    with open(path, "w") as f:
+        _ld_header(f, mu.shape[0], system, A, names, natmi)
+        f.write("      ia type                   mux                  muy                 muz\n")
+        for i in range(mu.shape[0]):
+            f.write(f"{i + 1:8d}  {names[typ[i]]:3s}" + "".join(fortran_e(v) for v in mu[i]) + "\n")
+
+
+def write_efgall(path, system, cell, names, natmi, efg):
+    """EFGALL, formatted variant (iefgall_format /= 0, field.f90:392-448):
+    vxx vyy vzz vxy vxz vyz per ion; efg is (natm, 3, 3) or (natm, 9)."""
+    A = np.asarray(cell, dtype=np.float64)
+    v = np.asarray(efg, dtype=np.float64).reshape(-1, 3, 3)
+    typ = np.repeat(np.arange(len(names)), natmi)
+    with open(path, "w") as f:
+        _ld_header(f, v.shape[0], system, A, names, natmi)
+        f.write("      ia type                   vxx                     vyy                     vzz"
+                "                     vxy                     vxz                     vyz\n")
+        for i in range(v.shape[0]):
+            e = v[i]
+            vals = (e[0, 0], e[1, 1], e[2, 2], e[0, 1], e[0, 2], e[1, 2])
+            f.write(f"{i + 1:8d}  {names[typ[i]]:3s}" + "".join(fortran_e(x) for x in vals) + "\n")
+
+
+def _read_ld_table(path, ncol):
+    with open(path) as f:
+        lines = [ln for ln in f.read().splitlines() if ln.strip()]
+    natm = int(lines[0].split()[0])
+    system = lines[1].strip()
+    A = np.array([[float(x) for x in lines[2 + j].split()[:3]] for j in range(3)]).T
+    ntype = int(lines[5].split()[0])
+    names = lines[6].split()[:ntype]
+    natmi = [int(x) for x in lines[7].split()[:ntype]]
+    rows = [ln.split() for ln in lines[9:9 + natm]]
+    data = np.array([[float(x) for x in r[2:2 + ncol]] for r in rows], dtype=np.float64)
+    return dict(natm=natm, system=system, cell=A, names=names, natmi=natmi,
+                types=[r[1] for r in rows], data=data)
+
+
+def read_dipff(path):
+    """Returns the header fields and mu (natm, 3)."""
+    d = _read_ld_table(path, 3)
+    d["mu"] = d.pop("data")
+    return d
+
+
+def read_efgall(path):
+    """Returns the header fields and efg (natm, 3, 3), symmetric."""
+    d = _read_ld_table(path, 6)
+    x = d.pop("data")
+    v = np.zeros((x.shape[0], 3, 3))
+    v[:, 0, 0], v[:, 1, 1], v[:, 2, 2] = x[:, 0], x[:, 1], x[:, 2]
+    v[:, 0, 1] = v[:, 1, 0] = x[:, 3]
+    v[:, 0, 2] = v[:, 2, 0] = x[:, 4]
+    v[:, 1, 2] = v[:, 2, 1] = x[:, 5]
+    d["efg"] = v
+    return d
 
 
 # ---------------------------------------------------------------------------

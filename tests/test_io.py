@@ -103,3 +103,52 @@ def test_ex09_decks_match_fixture():
         nl = mdffio.read_namelists(mk.assemble(os.path.join(cfgdir, "pot_mdff"), glob, row))
         p = mdffio.params_from_namelists(nl, posff["natmi"])
         assert bytes(p) == fx[f"params_{row[0]}"].tobytes()
+
+
+def test_fortran_e_format():
+    from mdff_b200.mdffio import fortran_e
+    assert fortran_e(1.0) == "  0.1000000000000000E+01"
+    assert fortran_e(-12.5366) == " -0.1253660000000000E+02"
+    assert fortran_e(0.0) == "  0.0000000000000000E+00"
+    assert fortran_e(3.2e-8) == "  0.3200000000000000E-07"
+    assert len(fortran_e(1e-120)) == 24 and fortran_e(1e-120).endswith("-119")
+
+
+def test_contff_reads_back_as_posff(tmp_path):
+    # CONTFF is the POSFF layout with velocities and forces (posff_data 'rvf')
+    from mdff_b200.mdffio import write_contff
+    rng = np.random.default_rng(3)
+    cell = np.array([[12.0, 1.0, 0.5], [0.0, 11.0, -0.4], [0.0, 0.0, 13.0]])
+    pos = rng.uniform(-20, 20, (7, 3))
+    vel, force = rng.standard_normal((7, 3)), rng.standard_normal((7, 3)) * 10
+    p = tmp_path / "CONTFF"
+    write_contff(p, "box", cell, ["Si", "O"], [3, 4], pos, vel, force)
+    lines = p.read_text().splitlines()
+    assert lines[0] == "       7" and lines[8] == "Cartesian"
+    assert all(len(ln) == 3 + 9 * 24 for ln in lines[9:])
+    d = mdffio.read_posff(p, "rvf")
+    B = np.linalg.inv(cell)
+    s = pos @ B.T
+    s -= np.where(s >= 0, np.floor(s + 0.5), np.ceil(s - 0.5))
+    np.testing.assert_allclose(d["pos"], s @ cell.T, rtol=0, atol=1e-12)
+    np.testing.assert_allclose(d["vel"], vel, rtol=1e-15)
+    np.testing.assert_allclose(d["force"], force, rtol=1e-15)
+    assert d["names"] == ["Si", "O"] and d["natmi"] == [3, 4]
+    np.testing.assert_allclose(d["cell"], cell, atol=1e-12)
+
+
+def test_dipff_efgall_round_trip(tmp_path):
+    from mdff_b200.mdffio import read_dipff, read_efgall, write_dipff, write_efgall
+    rng = np.random.default_rng(4)
+    cell = np.diag([10.0, 11.0, 12.0])
+    mu = rng.standard_normal((5, 3)) * 0.3
+    a = rng.standard_normal((5, 3, 3))
+    efg = a + a.transpose(0, 2, 1)
+    write_dipff(tmp_path / "DIPFF", "b", cell, ["Na", "Cl"], [2, 3], mu)
+    write_efgall(tmp_path / "EFGALL", "b", cell, ["Na", "Cl"], [2, 3], efg)
+    d = read_dipff(tmp_path / "DIPFF")
+    e = read_efgall(tmp_path / "EFGALL")
+    np.testing.assert_allclose(d["mu"], mu, rtol=1e-15)
+    np.testing.assert_allclose(e["efg"], efg, rtol=1e-15)
+    assert d["types"] == ["Na", "Na", "Cl", "Cl", "Cl"] and e["natmi"] == [2, 3]
+    np.testing.assert_allclose(d["cell"], cell)

@@ -24,6 +24,8 @@ def _cases():
         systems.random_ionic((24, 24), L=13.0, seed=51, calc=_abi.CALC_OTHER),
         systems.random_ionic((10, 10), L=10.0, seed=3, triclinic=True, calc=_abi.CALC_OTHER),
         systems.random_ionic((8, 8), L=9.0, seed=4, calc=_abi.CALC_OTHER),
+        # odd ion count: table rows of odd stride, a partial last K block
+        systems.random_ionic((19, 18), L=12.0, seed=8, q=(1.2, -1.2), calc=_abi.CALC_OTHER),
         systems.mgo(ncell=2, kmax=16, calc=_abi.CALC_OTHER),
         systems.sio2(nsio2=150, seed=9, calc=_abi.CALC_OTHER),
     ]
@@ -43,7 +45,7 @@ def _run(s, tc, monkeypatch):
     return r
 
 
-@pytest.mark.parametrize("case", range(5))
+@pytest.mark.parametrize("case", range(6))
 def test_tensor_core_operator_matches_cuda_core(oracle, case, monkeypatch):
     s = _cases()[case]
     a = _run(s, True, monkeypatch)

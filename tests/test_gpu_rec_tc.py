@@ -5,8 +5,8 @@ the FP32 CG operator (k_rec_rho_tc) and the FP32 field / force partials
 The mixed engine on the tensor cores (default) must agree with the same
 engine on the CUDA-core kernels (MDFF_REC_TC=0, MDFF_FIELD_TC=0) to the CG
 tolerance, on boxes that reach both B-tile widths (kz 7 -> 32 rows, kz 16
--> 64 rows), a triclinic cell and a box with fewer ions than one K block; both
-must meet the 1e-5 force bar against the CPU oracle."""
+-> 64 rows), a triclinic cell, a box with fewer ions than one K block and an
+odd ion count; both must meet the 1e-5 force bar against the CPU oracle."""
 import numpy as np
 import pytest
 

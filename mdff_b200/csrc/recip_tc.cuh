@@ -68,14 +68,18 @@ __host__ __device__ constexpr uint32_t idesc_tf32(int M, int N) {
          ((uint32_t)(M >> 4) << 24);
 }
 
+// bounded wait on an mbarrier phase: each try_wait may suspend the thread for
+// up to kSuspendNs before it reports, so a pending phase costs few issue slots;
+// the whole wait gives up after limit tries (about limit x kSuspendNs at most)
+constexpr uint32_t kSuspendNs = 1000;
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long limit) {
   for (long it = 0; it < limit; ++it) {
     uint32_t ok;
     asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; "
         "selp.b32 %0, 1, 0, p; }"
         : "=r"(ok)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "r"(kSuspendNs)
         : "memory");
     if (ok) return true;
   }

@@ -1131,8 +1131,8 @@ static int run_engforce(mdff_ctx* h, int itime) {
     prof_end(h, pr);
     if ((s = reduce_into(h, nbw, kSRPart, h->d_scal + S_SR))) return s;
   }
-  k_seti<<<1, 32, 0, h->st>>>(h->d_cata, 0);
-  LAUNCH_CHECK();
+  // per-call flags: [0] catastrophe, [1] a tensor-core wait gave up
+  CK(cudaMemsetAsync(h->d_cata, 0, 2 * sizeof(int), h->st));
   if (h->p.lcoulomb) {
     if ((s = build_tables(h))) return s;
     CK(cudaMemsetAsync(h->d_mu_ind, 0, sizeof(double4) * n, h->st));

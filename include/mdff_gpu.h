@@ -61,6 +61,9 @@ enum { MDFF_TRUNC_NONE = 0, MDFF_TRUNC_LINEAR = 1, MDFF_TRUNC_QUADRATIC = 2 };
 /* &gputag keywords (new; not in the reference) */
 enum { MDFF_PREC_FP64 = 0, MDFF_PREC_MIXED = 1 };
 enum { MDFF_SOLVER_SCF = 0, MDFF_SOLVER_CG = 1 };
+/* thole_function_type (coulomb.f90:72) */
+enum { MDFF_THOLE_NONE = 0, MDFF_THOLE_LINEAR = 1, MDFF_THOLE_EXPON1 = 2, MDFF_THOLE_EXPON2 = 3,
+       MDFF_THOLE_GAUSS = 4 };
 
 typedef struct mdff_params {
   int natm;                               /* config%natm                        */
@@ -120,6 +123,15 @@ typedef struct mdff_params {
   double wall24[MDFF_NTYPEMAX][MDFF_NTYPEMAX]; /* optional W/r^24 repulsive wall
                                              added to BMH pairs (eV A^24);
                                              0 = reference behaviour           */
+
+  /* &coulombtag Thole functions (coulomb.f90:65-72, 173-175, 228-234): the
+     dipole-dipole field and energy of pairs of polarisable ions use damped
+     radial functions (ewald_dir.f90:305-430); forces keep the plain tensor,
+     as in the reference.  thole_param[ta][tb] is used as given (ta = type of
+     the pair's "ia"); mdff_b200.mdffio applies the reference's fixed values
+     for expon1 / expon2 / gauss.  A = (alpha_xx(ta) alpha_xx(tb))^(1/6).     */
+  int thole_type;                         /* MDFF_THOLE_*; NONE = off          */
+  double thole_param[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
 } mdff_params;
 
 /* Results of one engforce call; pointer members are caller-owned host arrays

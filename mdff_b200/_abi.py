@@ -31,6 +31,7 @@ CALC_MD, CALC_OPT, CALC_OTHER = 0, 1, 2
 TRUNC_NONE, TRUNC_LINEAR, TRUNC_QUADRATIC = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 SOLVER_SCF, SOLVER_CG = 0, 1
+THOLE_NONE, THOLE_LINEAR, THOLE_EXPON1, THOLE_EXPON2, THOLE_GAUSS = 0, 1, 2, 3, 4
 
 _d = ctypes.c_double
 _i = ctypes.c_int
@@ -60,6 +61,7 @@ class MdffParams(ctypes.Structure):
         ("precision", _i), ("solver", _i), ("cg_tol", _d), ("cg_max_iter", _i),
         ("fail_on_nonconvergence", _i), ("device", _i),
         ("wall24", (_d * NT) * NT),
+        ("thole_type", _i), ("thole_param", (_d * NT) * NT),
     ]
 
 

@@ -347,6 +347,10 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
       return MDFF_ERR_BAD_ARGS;
     }
     mdff_params p = psets[ps];
+    if (p.thole_type != MDFF_THOLE_NONE) {
+      h->err = "Thole functions are not built into the batched engine (use mdff_gpu_create)";
+      return MDFF_ERR_UNSUPPORTED;
+    }
     h->pset_of.push_back(ps);
     long n = 0;
     for (int t = 0; t < MDFF_NTYPEMAX; ++t) {

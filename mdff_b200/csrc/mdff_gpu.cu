@@ -789,9 +789,9 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   else if (fp32 && dd_mask == 1 && h->dd_cache_ok)
     k_dd_cached<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n, E);
   else if (fp32)
-    k_es_field<float, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu32, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
+    k_es_field<float, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu32, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E, h->p.thole_type);
   else
-    k_es_field<double, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E);
+    k_es_field<double, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E, h->p.thole_type);
   LAUNCH_CHECK();
   prof_end(h, pr);
   return MDFF_OK;
@@ -808,7 +808,7 @@ static int static_field(mdff_ctx* h, bool fp32) {
 #define ESF(R, Q, D, MU)                                                                              \
   k_es_field<R, Q, D><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, MU, h->L.nbr, \
                                              h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, \
-                                             h->p.alphaES, cutsq, 1, 0, E)
+                                             h->p.alphaES, cutsq, 1, 0, E, h->p.thole_type)
   if (fp32 && dd) {
     k_to_float4<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_dipia, n, h->d_mu32);
     LAUNCH_CHECK();
@@ -817,7 +817,7 @@ static int static_field(mdff_ctx* h, bool fp32) {
   if (fp32 && !dd && h->lpolar && h->d_ddr) {
     // damped charge field + the pair cache of the FP32 solver iterations
     int pr = prof_begin(h, KC_ESFIELD, 0);
-    k_static_cache<<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, qq ? 1 : 0, E, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn);
+    k_static_cache<<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, qq ? 1 : 0, E, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->p.thole_type);
     LAUNCH_CHECK();
     prof_end(h, pr);
     h->dd_cache_ok = true;
@@ -1150,10 +1150,18 @@ static int run_engforce(mdff_ctx* h, int itime) {
     CK(cudaMemsetAsync(h->d_E, 0, sizeof(double4) * n, h->st));
     double cutsq = h->p.cutlongrange * h->p.cutlongrange;
     int prf = prof_begin(h, KC_ESFORCE, 0);
-    if (fp32)
-      k_es_force<float><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_mu_tot, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, h->task_qq, h->task_qd, h->task_dd, 1, h->coul_unit, h->d_E, h->d_force, h->d_part);
-    else
-      k_es_force<double><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_mu_tot, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, h->task_qq, h->task_qd, h->task_dd, 1, h->coul_unit, h->d_E, h->d_force, h->d_part);
+#define ESFORCE(R, TH)                                                                            \
+  k_es_force<R, TH><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_mu_tot, h->L.nbr,      \
+                                            h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, \
+                                            h->p.alphaES, cutsq, h->task_qq, h->task_qd,            \
+                                            h->task_dd, 1, h->coul_unit, h->d_E, h->d_force,        \
+                                            h->d_part)
+    const bool thole = h->p.thole_type != MDFF_THOLE_NONE;
+    if (fp32 && thole) ESFORCE(float, true);
+    else if (fp32) ESFORCE(float, false);
+    else if (thole) ESFORCE(double, true);
+    else ESFORCE(double, false);
+#undef ESFORCE
     LAUNCH_CHECK();
     prof_end(h, prf);
     if ((s = reduce_into(h, nbw, kESPart, h->d_scal + S_DIR))) return s;

@@ -28,9 +28,51 @@ struct NBPair {        // per ordered type pair (ti,tj), after symmetrisation
 struct ESPair {        // per ordered role pair (ta = type of "ia", tb = type of "ja")
   int ldamp;           // ldip_damping(ta,ta,tb) .or. ldip_damping(tb,ta,tb)
   int ka, kb;          // TT orders for the field on a / on b
-  int pad;
+  int thole;           // MDFF_THOLE_* when both types are polarisable, else 0
   double ba, ca, bb, cb;  // TT b, c for the field on a: (ta,ta,tb); on b: (tb,ta,tb)
+  double th_a, th_A;   // thole_param(ta,tb), (alpha_xx(ta) alpha_xx(tb))^(1/6)
 };
+
+// Thole functions on the dipole-dipole tensor (ewald_dir.f90:305-430): the
+// radial functions F1, F2 of T2 = 3 r r F2 / d^5 - F1 / d^3 for the field and
+// energy of a pair of polarisable ions (the force keeps the plain tensor)
+template <typename R>
+__device__ __forceinline__ void thole_radial(const ESPair& P, R d, R& F1, R& F2) {
+  switch (P.thole) {
+    case 1: {  // linear: no Ewald screening inside s = a A (:316-347)
+      R sth = (R)(P.th_a * P.th_A);
+      if (d < sth) {
+        R v = d / sth;
+        R v3 = v * v * v, v4 = v3 * v;
+        F2 = v4;
+        F1 = R(4) * v3 - R(3) * v4;
+      }
+    } break;
+    case 2: {  // expon1 (:353-373)
+      R x = d / (R)P.th_A;
+      R u = (R)P.th_a * (x * x * x);
+      R e = rexp<R>(-u);
+      F2 = F2 * (R(1) - (R(1) + u) * e);
+      F1 = F1 * (R(1) - e);
+    } break;
+    case 3: {  // expon2 (:378-399): u = a d A as written there
+      R ar = (R)P.th_a * d * (R)P.th_A;
+      R ar2 = ar * ar / R(2);
+      R ar3 = ar2 * ar / R(3);
+      R e = rexp<R>(-ar);
+      F2 = F2 * (R(1) - (R(1) + ar + ar2 + ar3) * e);
+      F1 = F1 * (R(1) - (R(1) + ar + ar2) * e);
+    } break;
+    case 4: {  // gauss (:404-422), NR error function
+      R ra = d / (R)P.th_a;
+      R e = (R)1.1283791670955125739 * ra * rexp<R>(-ra * ra);
+      R erfra = R(1) - nr_erfc<R>(ra);
+      F2 = F2 * (erfra - e * (R(1) + (R(2) / R(3)) * ra));
+      F1 = F1 * (erfra - e);
+    } break;
+    default: break;
+  }
+}
 
 // --------------------------------------------------------------------------
 // short range.  Partials per block: [u_bmh, vir_bmh, u_lj, vir_lj,
@@ -293,7 +335,7 @@ template <typename R, bool QQ, bool DD>
 __device__ __forceinline__ void es_field_pair(const ESPair* stab, int ntype, int i, int j, int ti,
                                               int tj, R rx, R ry, R rz, R r2, R alpha, int damp,
                                               double qj, bool dd, R mx, R my, R mz, R& ex, R& ey,
-                                              R& ez) {
+                                              R& ez, int thole = 0) {
   Radial<R> g;
   radial<R, false>(r2, alpha, g);
   if (QQ && qj != 0.0) {
@@ -317,7 +359,13 @@ __device__ __forceinline__ void es_field_pair(const ESPair* stab, int ntype, int
     ez += c * rz;
   }
   if (DD && dd) {
-    R B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5;
+    R F1 = g.F1, F2 = g.F2;
+    if (thole) {
+      bool i_is_a = half_mask(i, j);
+      const ESPair& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
+      if (P.thole) thole_radial<R>(P, g.d, F1, F2);
+    }
+    R B1 = F1 * g.dm3, B2 = R(3) * F2 * g.dm5;
     R rm = rx * mx + ry * my + rz * mz;
     ex += B2 * rx * rm - B1 * mx;
     ey += B2 * ry * rm - B1 * my;
@@ -345,7 +393,7 @@ static __global__ void __launch_bounds__(256) k_es_field(
     const int* __restrict__ ipolar, const typename vec4t<R>::T* __restrict__ mu,
     const int* __restrict__ nbr, const int* __restrict__ nnb, int cap, int natm,
     const CellC* __restrict__ cell, const ESPair* __restrict__ tab, int ntype, double alpha,
-    double cutsq, int damp, int dd_mask, double4* __restrict__ E) {
+    double cutsq, int damp, int dd_mask, double4* __restrict__ E, int thole = 0) {
   typedef typename vec4t<R>::T M4;
   __shared__ ESPair stab[MDFF_NT * MDFF_NT];
   __shared__ double cA[9];
@@ -379,10 +427,10 @@ static __global__ void __launch_bounds__(256) k_es_field(
       }
       double qj = QQ ? q[j] : 0.0;
       if (!dd && (!QQ || qj == 0.0)) continue;
-      int tj = (QQ && damp) ? itype[j] : 0;
+      int tj = ((QQ && damp) || (DD && thole)) ? itype[j] : 0;
       es_field_pair<R, QQ, DD>(stab, ntype, i, j, ti, tj, rx, ry, rz, r2, (R)alpha, damp, qj, dd,
                                DD ? (R)muj.x : R(0), DD ? (R)muj.y : R(0), DD ? (R)muj.z : R(0),
-                               ex, ey, ez);
+                               ex, ey, ez, thole);
     }
   }
   double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
@@ -406,7 +454,7 @@ static __global__ void __launch_bounds__(256) k_static_cache(
     const int* __restrict__ ipolar, const int* __restrict__ nbr, const int* __restrict__ nnb,
     int cap, int natm, const CellC* __restrict__ cell, const ESPair* __restrict__ tab, int ntype,
     double alpha, double cutsq, int has_q, double4* __restrict__ E, float4* __restrict__ cr,
-    float* __restrict__ cb1, int* __restrict__ cj, int* __restrict__ cn) {
+    float* __restrict__ cb1, int* __restrict__ cj, int* __restrict__ cn, int thole = 0) {
   __shared__ ESPair stab[MDFF_NT * MDFF_NT];
   __shared__ double cA[9];
   for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
@@ -460,8 +508,15 @@ static __global__ void __launch_bounds__(256) k_static_cache(
           }
           if (pp) {
             keep = true;
-            B1 = g.F1 * g.dm3;
-            B2 = 3.f * g.F2 * g.dm5;
+            float F1 = g.F1, F2 = g.F2;
+            if (thole) {
+              int tj = itype[j];
+              bool i_is_a = half_mask(i, j);
+              const ESPair& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
+              if (P.thole) thole_radial<float>(P, g.d, F1, F2);
+            }
+            B1 = F1 * g.dm3;
+            B2 = 3.f * F2 * g.dm5;
           }
         }
       }
@@ -524,7 +579,9 @@ constexpr int kESPart = 7;
 // qd, dd with damping, ewald_dir.f90:528-644): a = "ia", b = "ja", r = r_a - r_b.
 // Out: pair energy u, f_ij (the reference's f_i -= f_ij, f_j += f_ij,
 // ewald_dir.f90:714-721), fields Ea on a and Eb on b.
-template <typename R>
+// THOLE: Thole functions on the dd field and energy (P.thole); off, the code
+// is the same as without them.
+template <typename R, bool THOLE = false>
 __device__ __forceinline__ void es_force_pair(const ESPair& P, int damp_ind, R d2, R alpha,
                                               const R (&r)[3], R qa, R qb, const R (&ma)[3],
                                               const R (&mb)[3], bool dip_a, bool dip_b,
@@ -563,11 +620,19 @@ __device__ __forceinline__ void es_force_pair(const ESPair& P, int damp_ind, R d
     }
   }
   if (task_dd && dip_a && dip_b) {
-    u += -(B2 * rma * rmb - B1 * mab);
+    // energy and field with T2_thole (ewald_dir.f90:557-572), force with T3
+    R B1t = B1, B2t = B2;
+    if (THOLE && P.thole) {
+      R F1t = g.F1, F2t = g.F2;
+      thole_radial<R>(P, g.d, F1t, F2t);
+      B1t = F1t * g.dm3;
+      B2t = R(3) * F2t * g.dm5;
+    }
+    u += -(B2t * rma * rmb - B1t * mab);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      Ea[c] += B2 * r[c] * rmb - B1 * mb[c];
-      Eb[c] += B2 * r[c] * rma - B1 * ma[c];
+      Ea[c] += B2t * r[c] * rmb - B1t * mb[c];
+      Eb[c] += B2t * r[c] * rma - B1t * ma[c];
       fij[c] -= -B3 * rma * rmb * r[c] + B2 * (mab * r[c] + ma[c] * rmb + mb[c] * rma);
     }
   }
@@ -588,7 +653,7 @@ __device__ __forceinline__ void es_force_pair(const ESPair& P, int damp_ind, R d
   }
 }
 
-template <typename R>
+template <typename R, bool THOLE = false>
 static __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_es_force(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
     const double4* __restrict__ mu, const int* __restrict__ nbr, const int* __restrict__ nnb,
@@ -634,7 +699,7 @@ static __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_es_force
       bool dip_a = (ma4.x != 0.0 || ma4.y != 0.0 || ma4.z != 0.0);
       bool dip_b = (mb4.x != 0.0 || mb4.y != 0.0 || mb4.z != 0.0);
       R u, fij[3], Ea[3], Eb[3];
-      es_force_pair<R>(stab[ta * ntype + tb], damp_ind, (R)r2d, (R)alpha, r, qa, qb, ma, mb, dip_a,
+      es_force_pair<R, THOLE>(stab[ta * ntype + tb], damp_ind, (R)r2d, (R)alpha, r, qa, qb, ma, mb, dip_a,
                        dip_b, task_qq, task_qd, task_dd, u, fij, Ea, Eb);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {

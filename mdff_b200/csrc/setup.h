@@ -129,6 +129,18 @@ inline int setup_system(const mdff_params* pin, const double* cellA, Setup& S, c
     *err = "sum(natmi) != natm";
     return MDFF_ERR_BAD_ARGS;
   }
+  if (p.thole_type < MDFF_THOLE_NONE || p.thole_type > MDFF_THOLE_GAUSS) {
+    *err = "thole_type must be one of MDFF_THOLE_* (coulomb.f90:72)";
+    return MDFF_ERR_BAD_ARGS;
+  }
+  if (p.thole_type != MDFF_THOLE_NONE)
+    for (int it = 0; it < p.ntype; ++it)
+      for (int jt = 0; jt < p.ntype; ++jt)
+        if (p.ldip_polar[it] && p.ldip_polar[jt] &&
+            !(p.thole_param[it][jt] > 0.0 && p.poldip[it][0][0] > 0.0 && p.poldip[jt][0][0] > 0.0)) {
+          *err = "Thole functions need thole_param > 0 and alpha_xx > 0 for polarisable types";
+          return MDFF_ERR_BAD_ARGS;
+        }
   if (p.extrapolate_order < 0 || p.extrapolate_order > 4) {
     *err = "extrapolate_order must be 0..4 (moment_from_pola.f90:524-527)";
     return MDFF_ERR_BAD_ARGS;
@@ -249,7 +261,10 @@ inline int setup_system(const mdff_params* pin, const double* cellA, Setup& S, c
       E.kb = p.pol_damp_k[jt][it][jt];
       E.bb = p.pol_damp_b[jt][it][jt];
       E.cb = p.pol_damp_c[jt][it][jt];
-      E.pad = 0;
+      // Thole functions of a pair of polarisable types (ewald_dir.f90:308-311)
+      E.thole = (p.thole_type != MDFF_THOLE_NONE && p.ldip_polar[it] && p.ldip_polar[jt]) ? p.thole_type : 0;
+      E.th_a = p.thole_param[it][jt];
+      E.th_A = std::pow(p.poldip[it][0][0] * p.poldip[jt][0][0], 1.0 / 6.0);
     }
   return MDFF_OK;
 }

@@ -365,10 +365,18 @@ def _table(v, ndim, ntype):
     raise ValueError("multi-index table given as a plain list")
 
 
+_THOLE = {"linear": _abi.THOLE_LINEAR, "expon1": _abi.THOLE_EXPON1,
+          "expon2": _abi.THOLE_EXPON2, "gauss": _abi.THOLE_GAUSS}
+_THOLE_FIXED = {"expon1": 0.572, "expon2": 1.9088, "gauss": 0.957}
+
+
 def params_from_namelists(nl, natmi, **extra):
     """mdff_params for the ions per type natmi from parsed namelists, with the
     reference's defaults for everything not given.  Unsupported switches of
-    the path (Morse, direct Coulomb, quadrupoles, Thole) raise ValueError."""
+    the path (Morse, direct Coulomb, quadrupoles) raise ValueError.  Thole
+    functions (coulombtag: thole_functions, thole_function_type, thole_param)
+    follow coulomb_check_tag (coulomb.f90:228-234): expon1 / expon2 / gauss
+    replace every thole_param by 0.572 / 1.9088 / 0.957."""
     ntype = len(natmi)
     c = nl.get("controltag", {})
     fd = nl.get("fieldtag", {})
@@ -379,9 +387,19 @@ def params_from_namelists(nl, natmi, **extra):
         raise ValueError("lmorse: Morse is never dispatched by engforce")
     if str(c.get("longrange", "ewald")).lower() != "ewald":
         raise ValueError("longrange must be 'ewald'")
-    if cl.get("thole_functions", False):
-        raise ValueError("thole_functions are not built")
     kw = {}
+    if cl.get("thole_functions", False):
+        ttype = str(cl.get("thole_function_type", "linear")).lower()
+        if ttype not in _THOLE:
+            raise ValueError(f"thole_function_type {ttype!r} (coulomb.f90:72)")
+        kw["thole_type"] = _THOLE[ttype]
+        tp = np.full((_abi.NT, _abi.NT), 1.662)
+        if "thole_param" in cl:
+            for (i, j), v in _table(cl["thole_param"], 2, ntype).items():
+                tp[i, j] = float(v)
+        if ttype in _THOLE_FIXED:
+            tp[:] = _THOLE_FIXED[ttype]
+        kw["thole_param"] = tp
     for k in ("lcoulomb", "lbmhft", "lbmhftd", "lnmlj", "lsurf", "lreduced"):
         if k in c:
             kw[k] = int(bool(c[k]))
@@ -513,6 +531,13 @@ def write_control(path, p, names, masses=None, calc="md", extra_md=None):
     L.append(f"  epsw = {_f(p.epsw)}")
     L.append(f"  alphaES = {_f(p.alphaES)}")
     L.append(f"  kES = {p.kES[0]} {p.kES[1]} {p.kES[2]}")
+    if p.thole_type != _abi.THOLE_NONE:
+        tname = {v: k for k, v in _THOLE.items()}[p.thole_type]
+        L.append("  thole_functions = .true.")
+        L.append(f"  thole_function_type = '{tname}'")
+        for i in range(nt):
+            for j in range(nt):
+                L.append(f"  thole_param({i + 1},{j + 1}) = {_f(p.thole_param[i][j])}")
     L.append("&end")
     L.append("&pimtag")
     L.append(f"  symmetric_pot = {'.true.' if p.symmetric_pot_pim else '.false.'}")

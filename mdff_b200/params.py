@@ -11,7 +11,8 @@ reference's ``*_default_tag`` routines followed by a namelist read would:
 Keyword names are the namelist names.  Per-type tables are given as dicts
 keyed by 0-based type tuples, e.g. ``Abmhftd={(0, 1): 1312.9}``, or as
 numpy arrays.  New ``&gputag`` keywords: precision, solver, cg_tol,
-cg_max_iter, fail_on_nonconvergence, device, wall24.
+cg_max_iter, fail_on_nonconvergence, device, wall24.  Thole functions:
+thole_type (MDFF_THOLE_*) and thole_param (per ordered type pair).
 """
 import numpy as np
 
@@ -26,7 +27,7 @@ _DEFAULTS = dict(
     # &non_bondedtag
     trunc=_abi.TRUNC_NONE, symmetric_pot_nb=1,
     # &coulombtag
-    alphaES=1.0, kES=(10, 10, 10), lautoES=0, epsw=1e-6,
+    alphaES=1.0, kES=(10, 10, 10), lautoES=0, epsw=1e-6, thole_type=_abi.THOLE_NONE,
     # &pimtag
     conv_tol_ind=1e-6, min_scf_pol_iter=3, max_scf_pol_iter=100,
     extrapolate_order=0, symmetric_pot_pim=1,
@@ -36,7 +37,7 @@ _DEFAULTS = dict(
 )
 
 _TABLE2 = ("epslj", "sigmalj", "plj", "qlj", "Abmhftd", "Bbmhftd", "Cbmhftd",
-           "Dbmhftd", "BDbmhftd", "wall24")
+           "Dbmhftd", "BDbmhftd", "wall24", "thole_param")
 _TABLE3 = ("ldip_damping", "pol_damp_b", "pol_damp_c", "pol_damp_k")
 
 
@@ -65,6 +66,8 @@ def make_params(natmi, **kw):
     # LJ defaults qlj = 12, plj = 6 (non_bonded.f90:180-181)
     kw.setdefault("qlj", np.full((NT, NT), 12.0))
     kw.setdefault("plj", np.full((NT, NT), 6.0))
+    # thole_param = 1.662 (coulomb.f90:175)
+    kw.setdefault("thole_param", np.full((NT, NT), 1.662))
     unknown = set(kw) - set(_DEFAULTS) - set(_TABLE2) - set(_TABLE3) - {
         "qch", "dip", "ldip_polar", "poldip", "poldip_iso"}
     if unknown:

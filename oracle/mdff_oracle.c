@@ -736,6 +736,50 @@ static void or_nmlj(or_ctx* c, const double* sx, const double* sy, const double*
 }
 
 /* ---------------------------------------------------------------------- */
+/* Thole functions on the dd tensor of a pair of polarisable ions
+ * (ewald_dir.f90:305-430): F1, F2 (Ewald radial functions) -> the damped
+ * F1, F2 of T2_thole = 3 r r F2 / d^5 - F1 / d^3.  A = (alpha_i alpha_j)^(1/6)
+ * with alpha = poldipia(1,1) (:164, :194); a = thole_param(ita, jta).        */
+static void thole_f(int type, double a, double alpha_i, double alpha_j, double d, double* F1,
+                    double* F2) {
+  const double onesixth = 1.0 / 6.0, twothird = onesixth * 4.0;
+  const double twopiroot = 2.0 / sqrt(PI);
+  if (type == MDFF_THOLE_LINEAR) {
+    /* linear (:316-347): no Ewald screening inside s = a A */
+    double s = a * pow(alpha_i * alpha_j, onesixth);
+    if (d < s) {
+      double v = d / s;
+      double v3 = v * v * v, v4 = v3 * v;
+      *F2 = v4;
+      *F1 = 4.0 * v3 - 3.0 * v4;
+    }
+  } else if (type == MDFF_THOLE_EXPON1) {
+    /* expon1 (:353-373) */
+    double A = pow(alpha_i * alpha_j, onesixth);
+    double u = a * pow(d / A, 3.0);
+    double e = exp(-u);
+    *F2 = *F2 * (1.0 - (1.0 + u) * e);
+    *F1 = *F1 * (1.0 - e);
+  } else if (type == MDFF_THOLE_EXPON2) {
+    /* expon2 (:378-399), u = a d A as written there */
+    double A = pow(alpha_i * alpha_j, onesixth);
+    double ar = a * d * A;
+    double ar2 = ar * ar / 2.0;
+    double ar3 = ar2 * ar / 3.0;
+    double e = exp(-ar);
+    *F2 = *F2 * (1.0 - (1.0 + ar + ar2 + ar3) * e);
+    *F1 = *F1 * (1.0 - (1.0 + ar + ar2) * e);
+  } else if (type == MDFF_THOLE_GAUSS) {
+    /* gauss (:404-422) with the NR error function (functions.f90:44-50) */
+    double ra = d / a;
+    double At = twopiroot * ra;
+    double e = At * exp(-ra * ra);
+    double erfra = 1.0 - or_errfc(ra);
+    *F2 = *F2 * (erfra - e * (1.0 + twothird * ra));
+    *F1 = *F1 * (erfra - e);
+  }
+}
+
 /* multipole_ES_dir (ewald_dir.f90:40-798), tasks qq / qd / dd              */
 typedef struct {
   double u;
@@ -877,15 +921,30 @@ static void es_dir(or_ctx* c, const double* sx, const double* sy, const double* 
           if (do_forces)
             for (int a = 0; a < 3; ++a) fij[a] = fij[a] + qij * T1[a];
         }
-        /* dd (ewald_dir.f90:557-593); T2_thole = T2 (no Thole functions) */
+        /* dd (ewald_dir.f90:557-593): energy and field with T2_thole (= T2
+         * without Thole functions or unless both ions are polarisable), forces
+         * with T3 */
         if (dipole_dipole && (dip_i && dip_j)) {
+          double T2t[3][3];
+          memcpy(T2t, T2, sizeof(T2t));
+          if (p->thole_type != MDFF_THOLE_NONE && p->ldip_polar[ita] && p->ldip_polar[jta]) {
+            double F1t = F1, F2t = F2;
+            thole_f(p->thole_type, p->thole_param[ita][jta], p->poldip[ita][0][0],
+                    p->poldip[jta][0][0], d, &F1t, &F2t);
+            double F2t_dm5 = 3.0 * F2t * dm5, F1t_dm3 = F1t * dm3;
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) {
+                T2t[a][b] = r[a] * r[b] * F2t_dm5;
+                if (a == b) T2t[a][a] = T2t[a][a] - F1t_dm3;
+              }
+          }
           for (int j = 0; j < 3; ++j)
-            for (int k = 0; k < 3; ++k) u_dir = u_dir - mui[j] * T2[j][k] * muj[k];
+            for (int k = 0; k < 3; ++k) u_dir = u_dir - mui[j] * T2t[j][k] * muj[k];
           if (do_efield)
             for (int k = 0; k < 3; ++k)
               for (int a = 0; a < 3; ++a) {
-                ef[3 * ia + a] = ef[3 * ia + a] + T2[a][k] * muj[k];
-                ef[3 * ja + a] = ef[3 * ja + a] + T2[a][k] * mui[k];
+                ef[3 * ia + a] = ef[3 * ia + a] + T2t[a][k] * muj[k];
+                ef[3 * ja + a] = ef[3 * ja + a] + T2t[a][k] * mui[k];
               }
           if (do_efg)
             for (int k = 0; k < 3; ++k)

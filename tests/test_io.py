@@ -152,3 +152,27 @@ def test_dipff_efgall_round_trip(tmp_path):
     np.testing.assert_allclose(e["efg"], efg, rtol=1e-15)
     assert d["types"] == ["Na", "Na", "Cl", "Cl", "Cl"] and e["natmi"] == [2, 3]
     np.testing.assert_allclose(d["cell"], cell)
+
+
+def test_thole_keywords(tmp_path):
+    # coulomb_check_tag (coulomb.f90:228-234): linear keeps thole_param,
+    # expon1 / expon2 / gauss replace it by fixed values
+    nl = {"coulombtag": {"thole_functions": True, "thole_function_type": "linear",
+                         "thole_param": {(1, 2): 2.1, (2, 1): 2.1}}}
+    p = mdffio.params_from_namelists(nl, [2, 2])
+    assert p.thole_type == _abi.THOLE_LINEAR
+    assert p.thole_param[0][1] == 2.1 and p.thole_param[0][0] == 1.662
+    for t, v, code in (("expon1", 0.572, _abi.THOLE_EXPON1), ("expon2", 1.9088, _abi.THOLE_EXPON2),
+                       ("gauss", 0.957, _abi.THOLE_GAUSS)):
+        q = mdffio.params_from_namelists({"coulombtag": {"thole_functions": True,
+                                                         "thole_function_type": t}}, [2, 2])
+        assert q.thole_type == code and q.thole_param[1][0] == v
+    assert mdffio.params_from_namelists({}, [2, 2]).thole_type == _abi.THOLE_NONE
+    f = tmp_path / "control.F"
+    mdffio.write_control(f, p, ["A", "B"])
+    r = mdffio.params_from_namelists(mdffio.read_control(f), [2, 2])
+    assert r.thole_type == p.thole_type
+    assert np.array_equal(np.ctypeslib.as_array(r.thole_param), np.ctypeslib.as_array(p.thole_param))
+    with pytest.raises(ValueError):
+        mdffio.params_from_namelists({"coulombtag": {"thole_functions": True,
+                                                     "thole_function_type": "cubic"}}, [2, 2])

@@ -64,6 +64,15 @@ enum { MDFF_SOLVER_SCF = 0, MDFF_SOLVER_CG = 1 };
 /* thole_function_type (coulomb.f90:72) */
 enum { MDFF_THOLE_NONE = 0, MDFF_THOLE_LINEAR = 1, MDFF_THOLE_EXPON1 = 2, MDFF_THOLE_EXPON2 = 3,
        MDFF_THOLE_GAUSS = 4 };
+/* algo_moment_from_pola (pim.f90:89-91; dispatch moment_from_pola.f90:116-127).
+   KO_V3 and KO_V4_2 are rejected with MDFF_ERR_UNSUPPORTED: the reference's
+   kO_v3 never forms a new dipole increment (dmu_ind stays at its zero
+   initial value, moment_from_pola.f90:1716,1835) and kO_v4_2 reads
+   mu_h(:,:,0) at its first iteration (:2186). */
+enum { MDFF_ALGO_SCF = 0, MDFF_ALGO_KO_V1 = 1, MDFF_ALGO_KO_V2 = 2, MDFF_ALGO_KO_V3 = 3,
+       MDFF_ALGO_KO_V4_1 = 4, MDFF_ALGO_KO_V4_2 = 5 };
+/* algo_ext_dipole (pim.f90:85-87): predictor of the kO algorithms */
+enum { MDFF_EXT_ASPC = 0, MDFF_EXT_POLY = 1 };
 
 typedef struct mdff_params {
   int natm;                               /* config%natm                        */
@@ -132,6 +141,15 @@ typedef struct mdff_params {
      for expon1 / expon2 / gauss.  A = (alpha_xx(ta) alpha_xx(tb))^(1/6).     */
   int thole_type;                         /* MDFF_THOLE_*; NONE = off          */
   double thole_param[MDFF_NTYPEMAX][MDFF_NTYPEMAX];
+
+  /* &pimtag dipole algorithm of the SCF solver (pim.f90:72, 85-91, 127-131).
+     MDFF_ALGO_SCF is moment_from_pola_scf (always the ASPC predictor); the
+     kO algorithms need solver = MDFF_SOLVER_SCF and alpha_xx, alpha_yy,
+     alpha_zz > 0 on polarisable types; KO_V4_1 keeps at most 100 iterates
+     (max_scf_pol_iter <= 100, as the reference's history arrays). */
+  int algo_moment_from_pola;              /* MDFF_ALGO_*                        */
+  int algo_ext_dipole;                    /* MDFF_EXT_*: kO_v1 / kO_v2 predictor */
+  double omegakO;                         /* kO relaxation weight (0.7)         */
 } mdff_params;
 
 /* Results of one engforce call; pointer members are caller-owned host arrays

@@ -32,6 +32,8 @@ TRUNC_NONE, TRUNC_LINEAR, TRUNC_QUADRATIC = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 SOLVER_SCF, SOLVER_CG = 0, 1
 THOLE_NONE, THOLE_LINEAR, THOLE_EXPON1, THOLE_EXPON2, THOLE_GAUSS = 0, 1, 2, 3, 4
+ALGO_SCF, ALGO_KO_V1, ALGO_KO_V2, ALGO_KO_V3, ALGO_KO_V4_1, ALGO_KO_V4_2 = 0, 1, 2, 3, 4, 5
+EXT_ASPC, EXT_POLY = 0, 1
 
 _d = ctypes.c_double
 _i = ctypes.c_int
@@ -62,6 +64,7 @@ class MdffParams(ctypes.Structure):
         ("fail_on_nonconvergence", _i), ("device", _i),
         ("wall24", (_d * NT) * NT),
         ("thole_type", _i), ("thole_param", (_d * NT) * NT),
+        ("algo_moment_from_pola", _i), ("algo_ext_dipole", _i), ("omegakO", _d),
     ]
 
 

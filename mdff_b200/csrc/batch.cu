@@ -351,6 +351,10 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
       h->err = "Thole functions are not built into the batched engine (use mdff_gpu_create)";
       return MDFF_ERR_UNSUPPORTED;
     }
+    if (p.algo_moment_from_pola != MDFF_ALGO_SCF) {
+      h->err = "the kO dipole algorithms are not built into the batched engine (use mdff_gpu_create)";
+      return MDFF_ERR_UNSUPPORTED;
+    }
     h->pset_of.push_back(ps);
     long n = 0;
     for (int t = 0; t < MDFF_NTYPEMAX; ++t) {

@@ -21,6 +21,7 @@
 #include "recip_tc.cuh"
 #include "nlist.cuh"
 #include "pim.cuh"
+#include "ko.cuh"
 #include "realspace.cuh"
 #include "recip.cuh"
 #include "setup.h"
@@ -33,6 +34,7 @@ constexpr int NT = MDFF_NTYPEMAX;
 constexpr int kRhoThreads = 128;
 constexpr int kRhoChunk = 3072;    // ions per structure-factor block (4 chunks at 12k ions: fuller waves)
 constexpr int kFieldThreads = 128;
+constexpr int kKoHist = 100;       // F_h, mu_h depth of scf_kO_v4 (moment_from_pola.f90:2050)
 
 // scalar slots (device doubles, copied to the host at the end of a call)
 enum {
@@ -44,6 +46,7 @@ enum {
   S_RMS = 39,    // SCF rmsd^2 sum
   S_CG = 40,     // 40 rz, 41 rmsd^2 (init), 42 pq, 43 rzn, 44 rmsd^2 (update),
                  // 45 inner tolerance, 46 iterations, 47 iteration cap, 48 rmsd
+  S_KO = 49,     // 2: kO algorithms (inner residual, find_min dot products)
   S_MOM2 = 52,   // 8: moments of field passes
   S_DISP = 60,
   S_NSCAL = 64
@@ -125,6 +128,13 @@ struct mdff_ctx {
   int *d_ddj = nullptr, *d_ddn = nullptr;
   bool dd_cache_ok = false;
   double* d_efg = nullptr;       // [natm][9] electric field gradient (mdff_gpu_efg)
+  // kO dipole algorithms (ko.cuh): residual f_ind, increment, find_min
+  // point / previous residual (in place), previous dipoles, inner field;
+  // kO_v4_1 iterates F_h, mu_h [kKoHist][natm] and their weights
+  double4 *d_ko_f = nullptr, *d_ko_dmu = nullptr, *d_ko_g = nullptr, *d_ko_muprev = nullptr;
+  double4 *d_ko_fdir = nullptr, *d_Fh = nullptr, *d_muh = nullptr;
+  double* d_ko_x = nullptr;
+  double* h_ko = nullptr;        // pinned [kKoHist + 2]
   bool have_state = false;       // an engforce has run: positions, list, dipoles valid
   // outputs / reductions
   double* d_force = nullptr;     // [3][natm]
@@ -929,6 +939,329 @@ static int solve_scf(mdff_ctx* h, int itime, bool fp32) {
   return MDFF_OK;
 }
 
+// ---------------------------------------------------------------------------
+// kO dipole algorithms of the SCF solver (moment_from_pola.f90:822-942,
+// 1042-1639, 1987-2529); kernels in ko.cuh
+
+static int read_scals(mdff_ctx* h, int slot, int nv, double* v) {
+  CK(cudaMemcpyAsync(h->h_scal + slot, h->d_scal + slot, sizeof(double) * nv, cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  for (int k = 0; k < nv; ++k) v[k] = h->h_scal[slot + k];
+  return MDFF_OK;
+}
+
+// polint (moment_from_pola.f90:2365-2412) at x = 1 on the abscissae
+// xa(t) = 1 - t, t = 1..n, is linear in the ordinates: w[k] is its value for
+// the k-th unit ordinate vector.  The recurrence is the reference's, whose hp
+// is taken at xa(i+1) where Neville's scheme has xa(i+m) (from three points
+// on the result is not the interpolating polynomial).
+static void polint_weights(int n, double w[MDFF_ASPC_DEPTH]) {
+  int xa[MDFF_ASPC_DEPTH];
+  for (int t = 1; t <= n; ++t) xa[t - 1] = 1 - t;
+  int ns = 1;
+  double dif = std::fabs((double)(1 - xa[0]));
+  for (int i = 1; i <= n; ++i) {
+    double dift = std::fabs((double)(1 - xa[i - 1]));
+    if (dift < dif) {
+      ns = i;
+      dif = dift;
+    }
+  }
+  // c[i][k], d[i][k]: the tableaux of unit ordinate k
+  double c[MDFF_ASPC_DEPTH][MDFF_ASPC_DEPTH], d[MDFF_ASPC_DEPTH][MDFF_ASPC_DEPTH];
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < n; ++k) c[i][k] = d[i][k] = (i == k) ? 1.0 : 0.0;
+  for (int k = 0; k < n; ++k) w[k] = (k == ns - 1) ? 1.0 : 0.0;
+  ns = ns - 1;
+  for (int m = 1; m <= n - 1; ++m) {
+    for (int i = 1; i <= n - m; ++i) {
+      double ho = (double)(xa[i - 1] - 1), hp = (double)(xa[i] - 1);
+      for (int k = 0; k < n; ++k) {
+        double den = (c[i][k] - d[i - 1][k]) / (ho - hp);
+        d[i - 1][k] = hp * den;
+        c[i - 1][k] = ho * den;
+      }
+    }
+    if (2 * ns < n - m) {
+      for (int k = 0; k < n; ++k) w[k] += c[ns][k];
+    } else {
+      for (int k = 0; k < n; ++k) w[k] += d[ns - 1][k];
+      ns = ns - 1;
+    }
+  }
+}
+
+// extrapolate_dipole_poly (moment_from_pola.f90:2276-2363): order 0 repeats
+// the last dipoles; order 1 extrapolates linearly from the second call on;
+// higher orders use polint over order + 1 stored dipoles (itime + 1 while
+// itime <= order), then shift the history.  The reference's last shift step
+// reads dipia_ind_t(0); slot 1 is overwritten by the converged dipoles
+// before any read, so the shift stops at slot 2.
+static int poly_predict(mdff_ctx* h, int itime) {
+  int eo = h->p.extrapolate_order, npts = 0, nshift = 0;
+  double w[MDFF_ASPC_DEPTH] = {0, 0, 0, 0, 0};
+  if (eo == 0) {
+    npts = 1;
+    w[0] = 1.0;
+  } else if (eo == 1) {
+    nshift = 1;
+    if (itime > eo) {
+      npts = 2;
+      w[0] = 2.0;
+      w[1] = -1.0;
+    } else {
+      npts = 1;
+      w[0] = 1.0;
+    }
+  } else {
+    nshift = eo;
+    if (itime > eo) {
+      npts = eo + 1;
+      polint_weights(npts, w);
+    } else if (itime == 1) {
+      npts = 1;
+      w[0] = 1.0;
+    } else if (itime == 2) {
+      npts = 2;
+      w[0] = 2.0;
+      w[1] = -1.0;
+    } else if (itime > 2) {
+      npts = itime + 1;
+      polint_weights(npts, w);
+    }
+  }
+  k_poly_predict<<<cdiv(h->natm, 256), 256, 0, h->st>>>(h->d_hist, h->natm, npts, w[0], w[1], w[2], w[3],
+                                                       w[4], nshift, h->d_mu_ind);
+  LAUNCH_CHECK();
+  return MDFF_OK;
+}
+
+// induced_moment_inner (moment_from_pola.f90:822-942): the dipole increment
+// dmu relaxed in the direct-space dipole field at alphaES = 0.001 (undamped,
+// near neighbours only), weight omegakO, at most 10 passes or until its
+// residual is a tenth of the residual of f_ext.
+static int ko_inner(mdff_ctx* h, const double4* f_ext, double4* dmu) {
+  int n = h->natm, nb = cdiv(n, 256), nbw = cdiv((long)n * 32, 256), s;
+  PolDev P = poldev(h);
+  const double om = h->p.omegakO;
+  k_ko_start<<<nb, 256, 0, h->st>>>(f_ext, P, n, om, dmu, h->d_part);
+  LAUNCH_CHECK();
+  if ((s = reduce_into(h, nb, 1, h->d_scal + S_KO))) return s;
+  double r2;
+  if ((s = read_scal(h, S_KO, &r2))) return s;
+  const double rmsd_ref = std::sqrt(r2 / (double)h->npol);
+  const double a = 0.001;  // moment_from_pola.f90:893
+  const double selfa2 = 2.0 * (a / std::sqrt(kPi)) * (a * a) / 3.0;
+  const double fpi_3V = 2.0 * (kTwoPi / h->omega / 3.0);
+  const double cutsq = h->p.cutlongrange * h->p.cutlongrange;
+  double rmsd_inner = HUGE_VAL;
+  for (int it = 1; it <= 10 && rmsd_inner > 0.1 * rmsd_ref; ++it) {
+    CK(cudaMemsetAsync(h->d_ko_fdir, 0, sizeof(double4) * n, h->st));
+    if (h->p.lsurf && (s = moments(h, dmu, 0, h->d_scal + S_MOM2))) return s;
+    int pr = prof_begin(h, KC_ESFIELD, 0);
+    k_es_field<double, false, true><<<nbw, 256, 0, h->st>>>(
+        h->d_s, h->d_q, h->d_itype, h->d_ipolar, dmu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab,
+        h->ntype, a, cutsq, 0, 0, h->d_ko_fdir, h->p.thole_type);
+    LAUNCH_CHECK();
+    prof_end(h, pr);
+    k_ko_relax<<<nb, 256, 0, h->st>>>(f_ext, h->d_ko_fdir, P, n, om, 2.0 * selfa2, h->p.lsurf, fpi_3V,
+                                      h->d_scal + S_MOM2, dmu, h->d_part);
+    LAUNCH_CHECK();
+    if ((s = reduce_into(h, nb, 1, h->d_scal + S_KO))) return s;
+    if ((s = read_scal(h, S_KO, &r2))) return s;
+    rmsd_inner = std::sqrt(r2 / (double)h->npol);
+  }
+  return MDFF_OK;
+}
+
+// u_pol of the current dipoles into S_UPOL (moment_from_pola.f90:387-395)
+static int upol_pass(mdff_ctx* h) {
+  int nb = cdiv(h->natm, 256);
+  k_upol_part<<<nb, 256, 0, h->st>>>(h->d_mu_ind, poldev(h), h->natm, h->d_part);
+  LAUNCH_CHECK();
+  return reduce_into(h, nb, 1, h->d_scal + S_UPOL);
+}
+
+static int aspc_correct(mdff_ctx* h, int itime) {
+  int ord;
+  double B[5], w;
+  aspc_coef(itime, h->p.extrapolate_order, &ord, B, &w);
+  k_aspc_correct<<<cdiv(h->natm, 256), 256, 0, h->st>>>(h->d_Efield, poldev(h), h->natm, w, h->d_mu_ind);
+  LAUNCH_CHECK();
+  return MDFF_OK;
+}
+
+// moment_from_pola_scf_kO_v1 (moment_from_pola.f90:1042-1320) and, with
+// find_min along the last step, moment_from_pola_scf_kO_v2 (:1335-1639)
+static int solve_ko_v12(mdff_ctx* h, int itime, bool fp32, bool v2) {
+  int n = h->natm, nb = cdiv(n, 256), s;
+  PolDev P = poldev(h);
+  CK(cudaMemcpyAsync(h->d_Efield, h->d_Estat, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemcpyAsync(h->d_ko_f, h->d_Estat, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->st));
+  CK(cudaMemsetAsync(h->d_ko_g, 0, sizeof(double4) * n, h->st));
+  CK(cudaMemsetAsync(h->d_ko_muprev, 0, sizeof(double4) * n, h->st));
+  const bool ismd = h->p.calc == MDFF_CALC_MD, isopt = h->p.calc == MDFF_CALC_OPT;
+  const bool aspc_on = h->p.algo_ext_dipole == MDFF_EXT_ASPC;
+  int iscf = 0;
+  double rmsd = HUGE_VAL;
+  while (((iscf < h->p.max_scf_pol_iter) && (rmsd > h->p.conv_tol_ind)) ||
+         (iscf < h->p.min_scf_pol_iter)) {
+    iscf++;
+    if (iscf != 1 || (!ismd && !isopt)) {
+      // kO_v2 relaxes along the line-minimised residual from its third pass
+      const double4* fx = (v2 && iscf > 2) ? h->d_ko_g : h->d_ko_f;
+      if ((s = ko_inner(h, fx, h->d_ko_dmu))) return s;
+      k_add4<<<nb, 256, 0, h->st>>>(h->d_mu_ind, h->d_ko_dmu, n, h->d_mu_ind);
+      LAUNCH_CHECK();
+    } else {
+      s = aspc_on ? aspc_predict(h, itime) : poly_predict(h, itime);
+      if (s) return s;
+    }
+    if ((s = upol_pass(h))) return s;
+    if ((s = field_of_mu(h, h->d_mu_ind, 0, fp32, h->d_Eind))) return s;
+    k_add4<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Eind, n, h->d_Efield);
+    LAUNCH_CHECK();
+    if (iscf == 1 && ismd && aspc_on && (s = aspc_correct(h, itime))) return s;
+    k_ko_residual<<<nb, 256, 0, h->st>>>(h->d_Efield, h->d_mu_ind, P, n, h->d_ko_f, h->d_part);
+    LAUNCH_CHECK();
+    if (!v2) {
+      if ((s = reduce_into(h, nb, 1, h->d_scal + S_RMS))) return s;
+      double r2;
+      if ((s = read_scal(h, S_RMS, &r2))) return s;
+      rmsd = std::sqrt(r2 / (double)h->npol);
+      continue;
+    }
+    if (iscf != 1) {
+      // find_min (moment_from_pola.f90:2415-2455); its 1e-10 guard is a
+      // single-precision literal
+      k_findmin_dots<<<nb, 256, 0, h->st>>>(h->d_ko_g, h->d_ko_f, P, n, h->d_part);
+      LAUNCH_CHECK();
+      if ((s = reduce_into(h, nb, 2, h->d_scal + S_KO))) return s;
+      double dots[2];
+      if ((s = read_scals(h, S_KO, 2, dots))) return s;
+      double alpha = -dots[0] / dots[1];
+      if (std::fabs(dots[1]) < (double)1e-10f) alpha = 1.0;
+      k_findmin_apply<<<nb, 256, 0, h->st>>>(h->d_ko_g, h->d_ko_f, alpha, h->d_ko_muprev, P, n, h->d_mu_ind,
+                                             h->d_part);
+      LAUNCH_CHECK();
+      if ((s = reduce_into(h, nb, 1, h->d_scal + S_RMS))) return s;
+      double r2;
+      if ((s = read_scal(h, S_RMS, &r2))) return s;
+      rmsd = std::sqrt(r2 / (double)h->npol);
+    }
+    CK(cudaMemcpyAsync(h->d_ko_muprev, h->d_mu_ind, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->st));
+  }
+  h->stats.n_pol_iter = iscf;
+  h->stats.rmsd = rmsd;
+  h->stats.converged = rmsd <= h->p.conv_tol_ind;
+  CK(cudaMemcpyAsync(h->d_hist, h->d_mu_ind, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->st));
+  return MDFF_OK;
+}
+
+// A x = b for the kO_v4_1 weights with DGESV's semantics
+// (moment_from_pola.f90:2500): LU with partial pivoting (first largest
+// |pivot|); an exactly zero pivot leaves b as given (INFO > 0, no solve).
+static void lu_solve(int n, std::vector<double>& A, double* b) {
+  std::vector<int> piv(n);
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    for (int i = k + 1; i < n; ++i)
+      if (std::fabs(A[(size_t)i * n + k]) > std::fabs(A[(size_t)p * n + k])) p = i;
+    piv[k] = p;
+    if (A[(size_t)p * n + k] == 0.0) return;
+    if (p != k)
+      for (int j = 0; j < n; ++j) std::swap(A[(size_t)k * n + j], A[(size_t)p * n + j]);
+    for (int i = k + 1; i < n; ++i) {
+      double l = A[(size_t)i * n + k] / A[(size_t)k * n + k];
+      A[(size_t)i * n + k] = l;
+      for (int j = k + 1; j < n; ++j) A[(size_t)i * n + j] -= l * A[(size_t)k * n + j];
+    }
+  }
+  for (int k = 0; k < n; ++k) std::swap(b[k], b[piv[k]]);
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < i; ++j) b[i] -= A[(size_t)i * n + j] * b[j];
+  for (int i = n - 1; i >= 0; --i) {
+    for (int j = i + 1; j < n; ++j) b[i] -= A[(size_t)i * n + j] * b[j];
+    b[i] /= A[(size_t)i * n + i];
+  }
+}
+
+// moment_from_pola_scf_kO_v4 with scf_kO_v4_1 (moment_from_pola.f90:1987-2273)
+// and find_min_ex (:2457-2529).  The Gram matrix of the residuals F_h is
+// grown by one row per iteration (earlier iterates do not change).
+static int solve_ko_v4(mdff_ctx* h, int itime, bool fp32) {
+  int n = h->natm, nb = cdiv(n, 256), s;
+  PolDev P = poldev(h);
+  CK(cudaMemcpyAsync(h->d_Efield, h->d_Estat, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->st));
+  const bool ismd = h->p.calc == MDFF_CALC_MD, isopt = h->p.calc == MDFF_CALC_OPT;
+  const bool aspc_on = h->p.algo_ext_dipole == MDFF_EXT_ASPC;
+  std::vector<double> G((size_t)kKoHist * kKoHist), Aw;
+  double b[kKoHist];
+  int iscf = 0;
+  double rmsd = HUGE_VAL;
+  while (((iscf < h->p.max_scf_pol_iter) && (rmsd > h->p.conv_tol_ind)) ||
+         (iscf < h->p.min_scf_pol_iter)) {
+    iscf++;
+    if (iscf > kKoHist) {
+      h->err = "scf_kO_v4_1 ran past its 100 stored iterates";
+      return MDFF_ERR_BAD_ARGS;
+    }
+    bool induce = iscf != 1 || (!ismd && !isopt);
+    if (!induce) {
+      if (aspc_on && (s = aspc_predict(h, itime))) return s;
+      k_count_nonzero<<<nb, 256, 0, h->st>>>(h->d_mu_ind, n, h->d_part);
+      LAUNCH_CHECK();
+      if ((s = reduce_into(h, nb, 1, h->d_scal + S_KO))) return s;
+      double nz;
+      if ((s = read_scal(h, S_KO, &nz))) return s;
+      induce = nz == 0.0;
+    }
+    if (induce) {
+      k_induce<<<nb, 256, 0, h->st>>>(h->d_Efield, P, n, h->d_mu_ind);
+      LAUNCH_CHECK();
+    }
+    if ((s = upol_pass(h))) return s;
+    if ((s = field_of_mu(h, h->d_mu_ind, 0, fp32, h->d_Eind))) return s;
+    k_add4<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Eind, n, h->d_Efield);
+    LAUNCH_CHECK();
+    const int m = iscf - 1;
+    k_diis_store<<<nb, 256, 0, h->st>>>(h->d_mu_ind, h->d_Eind, P, n, h->d_Fh + (size_t)m * n,
+                                        h->d_muh + (size_t)m * n);
+    LAUNCH_CHECK();
+    k_diis_dots<<<dim3(nb, m + 2), 256, 0, h->st>>>(h->d_Fh, m, n, h->d_ipolar, h->d_Estat, h->d_part);
+    LAUNCH_CHECK();
+    if ((s = reduce_into(h, nb, m + 2, h->d_ko_x))) return s;
+    CK(cudaMemcpyAsync(h->h_ko, h->d_ko_x, sizeof(double) * (m + 2), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int j = 0; j <= m; ++j) G[(size_t)m * kKoHist + j] = G[(size_t)j * kKoHist + m] = h->h_ko[j];
+    b[m] = h->h_ko[m + 1];
+    if (iscf > 1) {
+      const int k = m + 1;
+      Aw.assign((size_t)k * k, 0.0);
+      for (int i = 0; i < k; ++i)
+        for (int j = 0; j < k; ++j) Aw[(size_t)i * k + j] = G[(size_t)i * kKoHist + j];
+      for (int i = 0; i < k; ++i) h->h_ko[i] = b[i];
+      lu_solve(k, Aw, h->h_ko);
+      CK(cudaMemcpyAsync(h->d_ko_x, h->h_ko, sizeof(double) * k, cudaMemcpyHostToDevice, h->st));
+    }
+    k_diis_combine<<<nb, 256, 0, h->st>>>(h->d_Fh, h->d_muh, h->d_ko_x, m + 1, iscf == 1 ? 1 : 0, n, h->d_Estat,
+                                          P, h->d_mu_ind, h->d_Efield);
+    LAUNCH_CHECK();
+    if (iscf == 1 && ismd && aspc_on && (s = aspc_correct(h, itime))) return s;
+    k_rmsd_part<<<nb, 256, 0, h->st>>>(h->d_mu_ind, h->d_Efield, P, n, h->d_part);
+    LAUNCH_CHECK();
+    if ((s = reduce_into(h, nb, 1, h->d_scal + S_RMS))) return s;
+    double r2;
+    if ((s = read_scal(h, S_RMS, &r2))) return s;
+    rmsd = std::sqrt(r2 / (double)h->npol);
+  }
+  h->stats.n_pol_iter = iscf;
+  h->stats.rmsd = rmsd;
+  h->stats.converged = rmsd <= h->p.conv_tol_ind;
+  CK(cudaMemcpyAsync(h->d_hist, h->d_mu_ind, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->st));
+  return MDFF_OK;
+}
+
 // the step scalars after an inner CG iteration: rz <- rz_new, count, rmsd of
 // the recurrence residual, and (inside the graph) the while-loop condition
 __global__ void k_cg_inner_check(double* __restrict__ sc, int npol, int in_graph,
@@ -1139,8 +1472,13 @@ static int run_engforce(mdff_ctx* h, int itime) {
     h->stats.n_pol_iter = 0;
     if (h->lpolar) {
       if ((s = static_field(h, fp32))) return s;
+      const int algo = h->p.algo_moment_from_pola;
       if (h->p.solver == MDFF_SOLVER_CG)
         s = solve_cg(h, itime, fp32);
+      else if (algo == MDFF_ALGO_KO_V1 || algo == MDFF_ALGO_KO_V2)
+        s = solve_ko_v12(h, itime, fp32, algo == MDFF_ALGO_KO_V2);
+      else if (algo == MDFF_ALGO_KO_V4_1)
+        s = solve_ko_v4(h, itime, fp32);
       else
         s = solve_scf(h, itime, fp32);
       if (s) return s;
@@ -1383,9 +1721,24 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_qv, n);
   DALLOC(h->d_Tp, n);
   DALLOC(h->d_mu32, n);
+  if (p.algo_moment_from_pola != MDFF_ALGO_SCF) {
+    DALLOC(h->d_ko_f, n);
+    DALLOC(h->d_ko_dmu, n);
+    DALLOC(h->d_ko_g, n);
+    DALLOC(h->d_ko_muprev, n);
+    DALLOC(h->d_ko_fdir, n);
+    DALLOC(h->d_ko_x, kKoHist + 2);
+    CK(cudaMallocHost((void**)&h->h_ko, sizeof(double) * (kKoHist + 2)));
+    if (p.algo_moment_from_pola == MDFF_ALGO_KO_V4_1) {
+      DALLOC(h->d_Fh, (size_t)kKoHist * n);
+      DALLOC(h->d_muh, (size_t)kKoHist * n);
+    }
+  }
   DALLOC(h->d_force, 3 * (size_t)n);
   DALLOC(h->d_pack, 3 * (size_t)n);
   h->part_cap = (size_t)std::max(cdiv((long)n * 32, 256), cdiv(n, 256)) * 16 + 64;
+  // kO_v4_1 Gram row: kKoHist + 2 dot products per block
+  h->part_cap = std::max(h->part_cap, (size_t)cdiv(n, 256) * (kKoHist + 2));
   DALLOC(h->d_part, h->part_cap);
   DALLOC(h->d_scal, S_NSCAL);
   DALLOC(h->d_cata, 2);  // [0] catastrophe, [1] a tensor-core wait gave up
@@ -1749,7 +2102,8 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_G, h->d_H, h->d_Estat, h->d_Eind, h->d_Efield, h->d_mu_ind, h->d_mu_tot,
                   h->d_hist, h->d_E, h->d_r, h->d_z, h->d_pv, h->d_qv, h->d_Tp, h->d_mu32, h->d_force,
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
-                  h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb};
+                  h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
+                  h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);
@@ -1757,6 +2111,7 @@ void mdff_gpu_destroy(mdff_handle h) {
   if (h->h_scal) cudaFreeHost(h->h_scal);
   if (h->h_flags) cudaFreeHost(h->h_flags);
   if (h->h_cata) cudaFreeHost(h->h_cata);
+  if (h->h_ko) cudaFreeHost(h->h_ko);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->st) cudaStreamDestroy(h->st);

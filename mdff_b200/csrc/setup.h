@@ -115,7 +115,7 @@ struct Setup {
 };
 
 // Everything of the reference's set-up that needs no device.  Returns
-// MDFF_OK, or MDFF_ERR_BAD_ARGS with *err set.
+// MDFF_OK, or MDFF_ERR_BAD_ARGS / MDFF_ERR_UNSUPPORTED with *err set.
 inline int setup_system(const mdff_params* pin, const double* cellA, Setup& S, const char** err) {
   S.p = *pin;
   mdff_params& p = S.p;
@@ -144,6 +144,34 @@ inline int setup_system(const mdff_params* pin, const double* cellA, Setup& S, c
   if (p.extrapolate_order < 0 || p.extrapolate_order > 4) {
     *err = "extrapolate_order must be 0..4 (moment_from_pola.f90:524-527)";
     return MDFF_ERR_BAD_ARGS;
+  }
+  if (p.algo_moment_from_pola < MDFF_ALGO_SCF || p.algo_moment_from_pola > MDFF_ALGO_KO_V4_2 ||
+      (p.algo_ext_dipole != MDFF_EXT_ASPC && p.algo_ext_dipole != MDFF_EXT_POLY)) {
+    *err = "algo_moment_from_pola / algo_ext_dipole out of range (pim.f90:85-91)";
+    return MDFF_ERR_BAD_ARGS;
+  }
+  if (p.algo_moment_from_pola == MDFF_ALGO_KO_V3 || p.algo_moment_from_pola == MDFF_ALGO_KO_V4_2) {
+    *err = "scf_kO_v3 / scf_kO_v4_2 are not built: the reference's kO_v3 never forms a dipole "
+           "increment and kO_v4_2 reads mu_h(:,:,0) (moment_from_pola.f90:1835,2186)";
+    return MDFF_ERR_UNSUPPORTED;
+  }
+  if (p.algo_moment_from_pola != MDFF_ALGO_SCF) {
+    if (p.solver != MDFF_SOLVER_SCF) {
+      *err = "the kO dipole algorithms run with solver = MDFF_SOLVER_SCF";
+      return MDFF_ERR_BAD_ARGS;
+    }
+    // f_ind = E - mu / alpha_aa on every polarisable component
+    // (moment_from_pola.f90:1247, 1548, 2172)
+    for (int it = 0; it < p.ntype; ++it)
+      if (p.ldip_polar[it] && !(p.poldip[it][0][0] > 0.0 && p.poldip[it][1][1] > 0.0 && p.poldip[it][2][2] > 0.0)) {
+        *err = "the kO dipole algorithms need alpha_xx, alpha_yy, alpha_zz > 0 on polarisable types";
+        return MDFF_ERR_BAD_ARGS;
+      }
+    // F_h(3, natm, 100), mu_h(3, natm, 100) (moment_from_pola.f90:2050)
+    if (p.algo_moment_from_pola == MDFF_ALGO_KO_V4_1 && p.max_scf_pol_iter > 100) {
+      *err = "scf_kO_v4_1 keeps at most 100 iterates: max_scf_pol_iter <= 100";
+      return MDFF_ERR_BAD_ARGS;
+    }
   }
   int ntype = p.ntype, n = p.natm;
   if (p.symmetric_pot_nb) {

@@ -368,6 +368,14 @@ def _table(v, ndim, ntype):
 _THOLE = {"linear": _abi.THOLE_LINEAR, "expon1": _abi.THOLE_EXPON1,
           "expon2": _abi.THOLE_EXPON2, "gauss": _abi.THOLE_GAUSS}
 _THOLE_FIXED = {"expon1": 0.572, "expon2": 1.9088, "gauss": 0.957}
+# algo_moment_from_pola_allowed / algo_ext_dipole_allowed (pim.f90:85-91)
+_ALGO = {"scf": _abi.ALGO_SCF, "scf_ko_v1": _abi.ALGO_KO_V1, "scf_ko_v2": _abi.ALGO_KO_V2,
+         "scf_ko_v3": _abi.ALGO_KO_V3, "scf_ko_v4_1": _abi.ALGO_KO_V4_1,
+         "scf_ko_v4_2": _abi.ALGO_KO_V4_2}
+_ALGO_NAME = {_abi.ALGO_SCF: "scf", _abi.ALGO_KO_V1: "scf_kO_v1", _abi.ALGO_KO_V2: "scf_kO_v2",
+              _abi.ALGO_KO_V3: "scf_kO_v3", _abi.ALGO_KO_V4_1: "scf_kO_v4_1",
+              _abi.ALGO_KO_V4_2: "scf_kO_v4_2"}
+_EXT = {"aspc": _abi.EXT_ASPC, "poly": _abi.EXT_POLY}
 
 
 def params_from_namelists(nl, natmi, **extra):
@@ -449,6 +457,18 @@ def params_from_namelists(nl, natmi, **extra):
     for k in ("min_scf_pol_iter", "max_scf_pol_iter", "extrapolate_order"):
         if k in pm:
             kw[k] = int(pm[k])
+    if "algo_moment_from_pola" in pm:
+        a = str(pm["algo_moment_from_pola"]).lower()
+        if a not in _ALGO:
+            raise ValueError(f"algo_moment_from_pola {a!r} (pim.f90:89-91)")
+        kw["algo_moment_from_pola"] = _ALGO[a]
+    if "algo_ext_dipole" in pm:
+        a = str(pm["algo_ext_dipole"]).lower()
+        if a not in _EXT:
+            raise ValueError(f"algo_ext_dipole {a!r} (pim.f90:85-87)")
+        kw["algo_ext_dipole"] = _EXT[a]
+    if "omegako" in pm:
+        kw["omegakO"] = float(pm["omegako"])
     if "ldip_polar" in pm:
         t = _table(pm["ldip_polar"], 1, ntype)
         kw["ldip_polar"] = [int(bool(t.get((i,), False))) for i in range(ntype)]
@@ -545,8 +565,9 @@ def write_control(path, p, names, masses=None, calc="md", extra_md=None):
     L.append(f"  min_scf_pol_iter = {p.min_scf_pol_iter}")
     L.append(f"  max_scf_pol_iter = {p.max_scf_pol_iter}")
     L.append(f"  extrapolate_order = {p.extrapolate_order}")
-    L.append("  algo_moment_from_pola = 'scf'")
-    L.append("  algo_ext_dipole = 'aspc'")
+    L.append(f"  algo_moment_from_pola = '{_ALGO_NAME[p.algo_moment_from_pola]}'")
+    L.append(f"  algo_ext_dipole = '{'poly' if p.algo_ext_dipole == _abi.EXT_POLY else 'aspc'}'")
+    L.append(f"  omegakO = {_f(p.omegakO)}")
     for it in range(nt):
         if p.ldip_polar[it]:
             L.append(f"  ldip_polar({it + 1}) = .true.")

@@ -12,7 +12,9 @@ Keyword names are the namelist names.  Per-type tables are given as dicts
 keyed by 0-based type tuples, e.g. ``Abmhftd={(0, 1): 1312.9}``, or as
 numpy arrays.  New ``&gputag`` keywords: precision, solver, cg_tol,
 cg_max_iter, fail_on_nonconvergence, device, wall24.  Thole functions:
-thole_type (MDFF_THOLE_*) and thole_param (per ordered type pair).
+thole_type (MDFF_THOLE_*) and thole_param (per ordered type pair).  Dipole
+algorithms: algo_moment_from_pola (MDFF_ALGO_*), algo_ext_dipole (MDFF_EXT_*)
+and omegakO.
 """
 import numpy as np
 
@@ -30,7 +32,8 @@ _DEFAULTS = dict(
     alphaES=1.0, kES=(10, 10, 10), lautoES=0, epsw=1e-6, thole_type=_abi.THOLE_NONE,
     # &pimtag
     conv_tol_ind=1e-6, min_scf_pol_iter=3, max_scf_pol_iter=100,
-    extrapolate_order=0, symmetric_pot_pim=1,
+    extrapolate_order=0, symmetric_pot_pim=1, algo_moment_from_pola=_abi.ALGO_SCF,
+    algo_ext_dipole=_abi.EXT_ASPC, omegakO=0.7,
     # &gputag
     precision=_abi.PREC_FP64, solver=_abi.SOLVER_SCF, cg_tol=0.0, cg_max_iter=200,
     fail_on_nonconvergence=0, device=0,

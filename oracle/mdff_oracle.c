@@ -13,8 +13,9 @@
  *  - Forces start from zero on every call (the reference keeps stale fx when
  *    no short-range potential is switched on, engforce_driver.f90:116-135).
  *  - The electric field returned is always the do_efield=.true. field.
- *  - Quadrupole tasks (task_coul(4:6)) and Thole functions are not built
- *    (theta is zeroed by engforce; thole_functions defaults to .false.).
+ *  - Quadrupole tasks (task_coul(4:6)) are not built (theta is zeroed by
+ *    engforce).  Of the kO dipole algorithms, scf_kO_v3 and scf_kO_v4_2 are
+ *    rejected (MDFF_ERR_UNSUPPORTED).
  *  - One optional extension: a W/r^24 wall added to BMH pairs (params.wall24,
  *    zero = reference behaviour).
  */
@@ -29,6 +30,7 @@
 
 #define NT MDFF_NTYPEMAX
 #define TT_MAX 8
+#define KO_HIST 100 /* F_h, mu_h depth of scf_kO_v4 (moment_from_pola.f90:2050) */
 
 /* constants.f90:65-94 */
 static const double PI = 3.14159265358979323846264338327950;
@@ -1155,8 +1157,9 @@ typedef struct {
 static void multipole_ES(or_ctx* c, const double* rx, const double* ry, const double* rz,
                          const double* sx, const double* sy, const double* sz, const csr_t* L,
                          const double* q, const double* mu, const int* task, int damp_ind,
-                         int do_efield, int do_efg, int do_forces, int do_stress, double u_pol,
-                         double* ef, double* efg, double* f /* [natm][3], += */, es_out* o) {
+                         int do_efield, int do_efg, int do_forces, int do_stress, int do_rec,
+                         double u_pol, double* ef, double* efg, double* f /* [natm][3], += */,
+                         es_out* o) {
   int natm = c->natm;
   double alphaES = c->p.alphaES;
   double piroot = sqrt(PI);
@@ -1188,7 +1191,7 @@ static void multipole_ES(or_ctx* c, const double* rx, const double* ry, const do
   rec.f = calloc((size_t)natm * 3, sizeof(double));
   rec.efg = calloc((size_t)natm * 9, sizeof(double));
   es_dir(c, sx, sy, sz, L, q, mu, task, damp_ind, do_efield, do_efg, do_forces, do_stress, &dir);
-  es_rec(c, rx, ry, rz, q, mu, task, do_efield, do_efg, do_forces, do_stress, &rec);
+  if (do_rec) es_rec(c, rx, ry, rz, q, mu, task, do_efield, do_efg, do_forces, do_stress, &rec);
 
   double u_surf = (qtot[0] * qtot[0] + qtot[1] * qtot[1] + qtot[2] * qtot[2]) +
                   2.0 * (qtot[0] * mutot[0] + qtot[1] * mutot[1] + qtot[2] * mutot[2]) +
@@ -1296,10 +1299,461 @@ static void aspc(or_ctx* c, double* mu_ind, const double* Efield, int key, int i
   }
 }
 
+/* One configuration seen by the induced-dipole solvers. */
+typedef struct {
+  or_ctx* c;
+  const double *rx, *ry, *rz, *sx, *sy, *sz;
+  const csr_t* L;
+  const double* qzero;  /* charges set to zero (moment_from_pola.f90:345-349) */
+  double* fsink;        /* [natm][3] force sink of the field passes */
+  const double* Estat;  /* damped static field of the charges (+ static dipoles) */
+  int itime;
+} pim_env;
+
+static double upol_of(or_ctx* c, const double* mu) {
+  double u = 0.0;
+  for (int ia = 0; ia < c->natm; ++ia)
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b)
+        u = u + mu[3 * ia + a] * c->invpoldipia[9 * ia + 3 * a + b] * mu[3 * ia + b];
+  return u * 0.5;
+}
+
+/* Efield_ind of mu: multipole_ES with charges zeroed, the dd task, undamped,
+   direct + reciprocal (moment_from_pola.f90:401-404).  do_rec = 0 with
+   alphaES = 0.001 is the kO inner pass (:893-898). */
+static void field_ind(pim_env* e, const double* mu, int do_rec, double u_pol, double* E) {
+  int task_ind[6] = {0, 0, 1, 0, 0, 0};
+  es_out o;
+  memset(e->fsink, 0, sizeof(double) * 3 * e->c->natm);
+  multipole_ES(e->c, e->rx, e->ry, e->rz, e->sx, e->sy, e->sz, e->L, e->qzero, mu, task_ind, 0, 1, 0, 0,
+               0, do_rec, u_pol, E, NULL, e->fsink, &o);
+}
+
+/* polint (moment_from_pola.f90:2365-2412) at x = 1.  The reference's
+   recurrence takes hp from xa(i+1) where Neville's scheme has xa(i+m), so
+   from three points on it is not the interpolating polynomial; it is
+   restated as written. */
+static double polint1(const int* xa, const double* ya, int n) {
+  double c[10], d[10];
+  int ns = 1;
+  double dif = fabs((double)(1 - xa[0]));
+  for (int i = 1; i <= n; ++i) {
+    double dift = fabs((double)(1 - xa[i - 1]));
+    if (dift < dif) {
+      ns = i;
+      dif = dift;
+    }
+    c[i - 1] = ya[i - 1];
+    d[i - 1] = ya[i - 1];
+  }
+  double y = ya[ns - 1], dy;
+  ns = ns - 1;
+  for (int m = 1; m <= n - 1; ++m) {
+    for (int i = 1; i <= n - m; ++i) {
+      double ho = (double)(xa[i - 1] - 1);
+      double hp = (double)(xa[i] - 1);
+      double w = c[i] - d[i - 1];
+      double den = ho - hp;
+      den = w / den;
+      d[i - 1] = hp * den;
+      c[i - 1] = ho * den;
+    }
+    if (2 * ns < n - m) {
+      dy = c[ns];
+    } else {
+      dy = d[ns - 1];
+      ns = ns - 1;
+    }
+    y = y + dy;
+  }
+  return y;
+}
+
+double or_polint(const int* xa, const double* ya, int n) { return polint1(xa, ya, n); }
+
+/* extrapolate_dipole_poly (moment_from_pola.f90:2276-2363) */
+static void poly_predict(or_ctx* c, double* mu_ind, int itime) {
+  int natm = c->natm, eo = c->p.extrapolate_order;
+  size_t n3 = (size_t)natm * 3;
+  double* h = c->hist; /* h[k * n3 + i] = dipia_ind_t(k+1, ...) */
+  int npts = 0;        /* points of a polint call */
+  if (eo == 0) {
+    memcpy(mu_ind, h, sizeof(double) * n3);
+    return;
+  }
+  if (eo == 1) {
+    if (itime > eo)
+      for (size_t i = 0; i < n3; ++i) mu_ind[i] = 2.0 * h[i] - h[n3 + i];
+    else
+      memcpy(mu_ind, h, sizeof(double) * n3);
+    memcpy(h + n3, h, sizeof(double) * n3);
+    return;
+  }
+  if (itime > eo) {
+    npts = eo + 1;
+  } else {
+    if (itime == 1) memcpy(mu_ind, h, sizeof(double) * n3);
+    if (itime == 2)
+      for (size_t i = 0; i < n3; ++i) mu_ind[i] = 2.0 * h[i] - h[n3 + i];
+    if (itime > 2) npts = itime + 1;
+  }
+  if (npts > 0) {
+    int xa[MDFF_ASPC_DEPTH];
+    double ya[MDFF_ASPC_DEPTH];
+    for (int t = 1; t <= npts; ++t) xa[t - 1] = 1 - t;
+    for (size_t i = 0; i < n3; ++i) {
+      for (int t = 0; t < npts; ++t) ya[t] = h[t * n3 + i];
+      mu_ind[i] = polint1(xa, ya, npts);
+    }
+  }
+  /* dipia_ind_t(ie) = dipia_ind_t(ie-1) for ie = order+1..2; the reference's
+     last step (ie = 1) reads index 0, and slot 1 is overwritten by the
+     converged dipoles before any read */
+  for (int k = eo; k >= 1; --k) memcpy(h + k * n3, h + (k - 1) * n3, sizeof(double) * n3);
+}
+
+/* predictor of the kO algorithms (moment_from_pola.f90:1183-1184) */
+static void ko_predict(or_ctx* c, double* mu_ind, const double* Efield, int itime) {
+  if (c->p.algo_ext_dipole == MDFF_EXT_POLY)
+    poly_predict(c, mu_ind, itime);
+  else
+    aspc(c, mu_ind, Efield, 1, itime);
+}
+
+/* induced_moment_inner (moment_from_pola.f90:822-942): relaxation of the
+   dipole increment in the field of its near neighbours (direct space only,
+   alphaES = 0.001, undamped), weight omegakO, at most 10 passes or until the
+   residual falls below a tenth of the residual of f_ext. */
+static void induced_moment_inner(pim_env* e, const double* f_ext, double* mu) {
+  or_ctx* c = e->c;
+  size_t n3 = (size_t)c->natm * 3;
+  double om = c->p.omegakO;
+  double* zero = calloc(n3, sizeof(double));
+  double* mu_prev = malloc(sizeof(double) * n3);
+  double* f_tot = malloc(sizeof(double) * n3);
+  double* f = malloc(sizeof(double) * n3);
+  double rmsd_ref = get_rmsd_mu(c, f_ext, zero);
+  memcpy(f_tot, f_ext, sizeof(double) * n3);
+  induced_moment(c, f_tot, mu);
+  for (size_t i = 0; i < n3; ++i) mu[i] = om * mu[i];
+  double rmsd_inner = HUGE_VAL;
+  int it = 1;
+  double alpha_save = c->p.alphaES;
+  while (it <= 10 && rmsd_inner > 0.1 * rmsd_ref) {
+    memcpy(mu_prev, mu, sizeof(double) * n3);
+    c->p.alphaES = 0.001;
+    field_ind(e, mu, 0, 0.0, f);
+    c->p.alphaES = alpha_save;
+    for (size_t i = 0; i < n3; ++i) f_tot[i] = f_ext[i] + f[i];
+    rmsd_inner = get_rmsd_mu(c, f_tot, mu);
+    induced_moment(c, f_tot, mu);
+    for (size_t i = 0; i < n3; ++i) mu[i] = (1.0 - om) * mu_prev[i] + om * mu[i];
+    it++;
+  }
+  free(zero);
+  free(mu_prev);
+  free(f_tot);
+  free(f);
+}
+
+/* f = E - mu / alpha_aa on polarisable components (moment_from_pola.f90:1242-1249) */
+static void ko_residual(or_ctx* c, const double* E, const double* mu, double* f) {
+  for (int ia = 0; ia < c->natm; ++ia) {
+    if (!c->ipolar[ia]) continue;
+    for (int a = 0; a < 3; ++a)
+      f[3 * ia + a] = E[3 * ia + a] - mu[3 * ia + a] / c->poldipia[9 * ia + 4 * a];
+  }
+}
+
+#define SCF_CONTINUE(iscf, rmsd)                                                   \
+  (((iscf) < c->p.max_scf_pol_iter && (rmsd) > c->p.conv_tol_ind) ||             \
+   ((iscf) < c->p.min_scf_pol_iter))
+
+/* moment_from_pola_scf (moment_from_pola.f90:240-485) */
+static void scf_plain(pim_env* e, double* mu, double* u_pol, int* n_scf, double* rmsd_out) {
+  or_ctx* c = e->c;
+  size_t n3 = (size_t)c->natm * 3;
+  double* Efield = malloc(sizeof(double) * n3);
+  double* Eind = malloc(sizeof(double) * n3);
+  memcpy(Efield, e->Estat, sizeof(double) * n3);
+  int ismd = (c->p.calc == MDFF_CALC_MD), isopt = (c->p.calc == MDFF_CALC_OPT);
+  int iscf = 0;
+  double rmsd = HUGE_VAL;
+  while (SCF_CONTINUE(iscf, rmsd)) {
+    iscf++;
+    if (iscf != 1 || (!ismd && !isopt))
+      induced_moment(c, Efield, mu);
+    else
+      aspc(c, mu, Efield, 1, e->itime);
+    *u_pol = upol_of(c, mu);
+    field_ind(e, mu, 1, *u_pol, Eind);
+    for (size_t i = 0; i < n3; ++i) Efield[i] = e->Estat[i] + Eind[i];
+    if (iscf == 1 && ismd) aspc(c, mu, Efield, 2, e->itime);
+    rmsd = get_rmsd_mu(c, Efield, mu);
+  }
+  *n_scf = iscf;
+  *rmsd_out = rmsd;
+  free(Efield);
+  free(Eind);
+}
+
+/* moment_from_pola_scf_kO_v1 (moment_from_pola.f90:1042-1320) */
+static void scf_ko_v1(pim_env* e, double* mu, double* u_pol, int* n_scf, double* rmsd_out) {
+  or_ctx* c = e->c;
+  size_t n3 = (size_t)c->natm * 3;
+  double* Efield = malloc(sizeof(double) * n3);
+  double* Eind = malloc(sizeof(double) * n3);
+  double* f_ind = malloc(sizeof(double) * n3);
+  double* dmu = calloc(n3, sizeof(double));
+  memcpy(Efield, e->Estat, sizeof(double) * n3);
+  memcpy(f_ind, Efield, sizeof(double) * n3);
+  int ismd = (c->p.calc == MDFF_CALC_MD), isopt = (c->p.calc == MDFF_CALC_OPT);
+  int aspc_on = c->p.algo_ext_dipole == MDFF_EXT_ASPC;
+  int iscf = 0;
+  double rmsd = HUGE_VAL;
+  while (SCF_CONTINUE(iscf, rmsd)) {
+    iscf++;
+    if (iscf != 1 || (!ismd && !isopt)) {
+      induced_moment_inner(e, f_ind, dmu);
+      for (size_t i = 0; i < n3; ++i) mu[i] = mu[i] + dmu[i];
+    } else {
+      ko_predict(c, mu, Efield, e->itime);
+    }
+    *u_pol = upol_of(c, mu);
+    field_ind(e, mu, 1, *u_pol, Eind);
+    for (size_t i = 0; i < n3; ++i) Efield[i] = e->Estat[i] + Eind[i];
+    if (iscf == 1 && ismd && aspc_on) aspc(c, mu, Efield, 2, e->itime);
+    rmsd = get_rmsd_mu(c, Efield, mu);
+    ko_residual(c, Efield, mu, f_ind);
+  }
+  *n_scf = iscf;
+  *rmsd_out = rmsd;
+  free(Efield);
+  free(Eind);
+  free(f_ind);
+  free(dmu);
+}
+
+/* find_min (moment_from_pola.f90:2415-2455): the point of least |g| on the
+   line g0 + a (g1 - g0); the step a times d1.  The 1e-10 guard is a
+   single-precision literal in the reference. */
+static void find_min(or_ctx* c, const double* g0, const double* g1, const double* d1, double* gmin,
+                     double* dmin) {
+  size_t n3 = (size_t)c->natm * 3;
+  double g0sq = 0.0, g0g1mg0 = 0.0;
+  for (int ia = 0; ia < c->natm; ++ia) {
+    if (!c->ipolar[ia]) continue;
+    for (int k = 0; k < 3; ++k) {
+      double g = g0[3 * ia + k], dg = g1[3 * ia + k] - g;
+      g0sq = g0sq + g * g;
+      g0g1mg0 = g0g1mg0 + g * dg;
+    }
+  }
+  double a = -g0sq / g0g1mg0;
+  if (fabs(g0g1mg0) < (double)1e-10f) a = 1.0;
+  for (size_t i = 0; i < n3; ++i) {
+    gmin[i] = g0[i] + a * (g1[i] - g0[i]);
+    dmin[i] = a * d1[i];
+  }
+}
+
+/* moment_from_pola_scf_kO_v2 (moment_from_pola.f90:1335-1639) */
+static void scf_ko_v2(pim_env* e, double* mu, double* u_pol, int* n_scf, double* rmsd_out) {
+  or_ctx* c = e->c;
+  size_t n3 = (size_t)c->natm * 3;
+  double* Efield = malloc(sizeof(double) * n3);
+  double* Eind = malloc(sizeof(double) * n3);
+  double* f_ind = malloc(sizeof(double) * n3);
+  double* f_prev = calloc(n3, sizeof(double));
+  double* gmin = calloc(n3, sizeof(double));
+  double* mu_prev = calloc(n3, sizeof(double));
+  double* dmin = calloc(n3, sizeof(double));
+  double* d1 = malloc(sizeof(double) * n3);
+  double* zero = calloc(n3, sizeof(double));
+  double* dmu = calloc(n3, sizeof(double));
+  memcpy(Efield, e->Estat, sizeof(double) * n3);
+  memcpy(f_ind, Efield, sizeof(double) * n3);
+  int ismd = (c->p.calc == MDFF_CALC_MD), isopt = (c->p.calc == MDFF_CALC_OPT);
+  int aspc_on = c->p.algo_ext_dipole == MDFF_EXT_ASPC;
+  int iscf = 0;
+  double rmsd = HUGE_VAL;
+  while (SCF_CONTINUE(iscf, rmsd)) {
+    iscf++;
+    if (iscf != 1 || (!ismd && !isopt)) {
+      induced_moment_inner(e, iscf <= 2 ? f_ind : gmin, dmu);
+      for (size_t i = 0; i < n3; ++i) mu[i] = mu[i] + dmu[i];
+    } else {
+      ko_predict(c, mu, Efield, e->itime);
+    }
+    *u_pol = upol_of(c, mu);
+    field_ind(e, mu, 1, *u_pol, Eind);
+    for (size_t i = 0; i < n3; ++i) Efield[i] = e->Estat[i] + Eind[i];
+    if (iscf == 1 && ismd && aspc_on) aspc(c, mu, Efield, 2, e->itime);
+    ko_residual(c, Efield, mu, f_ind);
+    if (iscf != 1) {
+      for (size_t i = 0; i < n3; ++i) d1[i] = mu[i] - mu_prev[i];
+      find_min(c, f_prev, f_ind, d1, gmin, dmin);
+      for (size_t i = 0; i < n3; ++i) mu[i] = mu_prev[i] + dmin[i];
+      rmsd = get_rmsd_mu(c, gmin, zero);
+    }
+    memcpy(mu_prev, mu, sizeof(double) * n3);
+    memcpy(f_prev, gmin, sizeof(double) * n3);
+  }
+  *n_scf = iscf;
+  *rmsd_out = rmsd;
+  free(Efield);
+  free(Eind);
+  free(f_ind);
+  free(f_prev);
+  free(gmin);
+  free(mu_prev);
+  free(dmin);
+  free(d1);
+  free(zero);
+  free(dmu);
+}
+
+/* DGESV semantics for A x = b, n <= KO_HIST: LU with partial pivoting (first
+   largest |pivot|); an exactly zero pivot leaves b as given (info > 0, no
+   solve). */
+static void dgesv_small(int n, double* A /* [n][n] row-major */, double* b) {
+  int piv[KO_HIST];
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    double amax = fabs(A[k * n + k]);
+    for (int i = k + 1; i < n; ++i)
+      if (fabs(A[i * n + k]) > amax) {
+        amax = fabs(A[i * n + k]);
+        p = i;
+      }
+    piv[k] = p;
+    if (A[p * n + k] == 0.0) return;
+    if (p != k)
+      for (int j = 0; j < n; ++j) {
+        double t = A[k * n + j];
+        A[k * n + j] = A[p * n + j];
+        A[p * n + j] = t;
+      }
+    for (int i = k + 1; i < n; ++i) {
+      double l = A[i * n + k] / A[k * n + k];
+      A[i * n + k] = l;
+      for (int j = k + 1; j < n; ++j) A[i * n + j] -= l * A[k * n + j];
+    }
+  }
+  for (int k = 0; k < n; ++k)
+    if (piv[k] != k) {
+      double t = b[k];
+      b[k] = b[piv[k]];
+      b[piv[k]] = t;
+    }
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < i; ++j) b[i] -= A[i * n + j] * b[j];
+  for (int i = n - 1; i >= 0; --i) {
+    for (int j = i + 1; j < n; ++j) b[i] -= A[i * n + j] * b[j];
+    b[i] /= A[i * n + i];
+  }
+}
+
+/* DDOTF (moment_from_pola.f90:2531-2552): dot product over polarisable ions */
+static double ddotf(or_ctx* c, const double* v1, const double* v2) {
+  double s = 0.0;
+  for (int ia = 0; ia < c->natm; ++ia) {
+    if (!c->ipolar[ia]) continue;
+    for (int k = 0; k < 3; ++k) s = s + v1[3 * ia + k] * v2[3 * ia + k];
+  }
+  return s;
+}
+
+/* moment_from_pola_scf_kO_v4 with scf_kO_v4_1 (moment_from_pola.f90:1987-2273)
+   and find_min_ex (:2457-2529): the dipoles are the combination of all
+   earlier iterates whose residuals F = mu / alpha - E_ind best match E_stat
+   (normal equations). */
+static void scf_ko_v4_1(pim_env* e, double* mu, double* u_pol, int* n_scf, double* rmsd_out) {
+  or_ctx* c = e->c;
+  int natm = c->natm;
+  size_t n3 = (size_t)natm * 3;
+  double* Efield = malloc(sizeof(double) * n3);
+  double* Eind = malloc(sizeof(double) * n3);
+  double* F = calloc(n3, sizeof(double));
+  double* Fh = calloc(n3 * KO_HIST, sizeof(double));
+  double* muh = calloc(n3 * KO_HIST, sizeof(double));
+  double* A = malloc(sizeof(double) * KO_HIST * KO_HIST);
+  double b[KO_HIST];
+  memcpy(Efield, e->Estat, sizeof(double) * n3);
+  int ismd = (c->p.calc == MDFF_CALC_MD), isopt = (c->p.calc == MDFF_CALC_OPT);
+  int aspc_on = c->p.algo_ext_dipole == MDFF_EXT_ASPC;
+  int iscf = 0;
+  double rmsd = HUGE_VAL;
+  while (SCF_CONTINUE(iscf, rmsd)) {
+    iscf++;
+    if (iscf != 1 || (!ismd && !isopt)) {
+      induced_moment(c, Efield, mu);
+    } else {
+      if (aspc_on) aspc(c, mu, Efield, 1, e->itime);
+      int allzero = 1;
+      for (size_t i = 0; i < n3; ++i)
+        if (mu[i] != 0.0) allzero = 0;
+      if (allzero) induced_moment(c, Efield, mu);
+    }
+    *u_pol = upol_of(c, mu);
+    field_ind(e, mu, 1, *u_pol, Eind);
+    for (size_t i = 0; i < n3; ++i) Efield[i] = e->Estat[i] + Eind[i];
+    for (int ia = 0; ia < natm; ++ia) {
+      if (!c->ipolar[ia]) continue;
+      for (int a = 0; a < 3; ++a)
+        F[3 * ia + a] = mu[3 * ia + a] / c->poldipia[9 * ia + 4 * a] - Eind[3 * ia + a];
+    }
+    /* find_min_ex */
+    memcpy(Fh + (size_t)(iscf - 1) * n3, F, sizeof(double) * n3);
+    memcpy(muh + (size_t)(iscf - 1) * n3, mu, sizeof(double) * n3);
+    if (iscf > 1) {
+      int m = iscf;
+      for (int j = 0; j < m; ++j)
+        for (int i = j; i < m; ++i) {
+          A[i * m + j] = ddotf(c, Fh + (size_t)i * n3, Fh + (size_t)j * n3);
+          A[j * m + i] = A[i * m + j];
+        }
+      for (int i = 0; i < m; ++i) b[i] = ddotf(c, e->Estat, Fh + (size_t)i * n3);
+      dgesv_small(m, A, b);
+      for (size_t k = 0; k < n3; ++k) {
+        double t = 0.0, u = 0.0;
+        for (int i = 0; i < m; ++i) {
+          t = t + b[i] * Fh[(size_t)i * n3 + k];
+          u = u + b[i] * muh[(size_t)i * n3 + k];
+        }
+        mu[k] = u;
+        F[k] = -e->Estat[k] + t;
+      }
+    }
+    for (int ia = 0; ia < natm; ++ia) {
+      if (!c->ipolar[ia]) continue;
+      for (int a = 0; a < 3; ++a)
+        Efield[3 * ia + a] = -F[3 * ia + a] + mu[3 * ia + a] / c->poldipia[9 * ia + 4 * a];
+    }
+    if (iscf == 1 && ismd && aspc_on) aspc(c, mu, Efield, 2, e->itime);
+    rmsd = get_rmsd_mu(c, Efield, mu);
+  }
+  *n_scf = iscf;
+  *rmsd_out = rmsd;
+  free(Efield);
+  free(Eind);
+  free(F);
+  free(Fh);
+  free(muh);
+  free(A);
+}
+
 int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz, int itime,
                 mdff_result* out, or_extra* ex) {
   int natm = c->natm;
   if (c->p.extrapolate_order < 0 || c->p.extrapolate_order > 4) return MDFF_ERR_BAD_ARGS;
+  {
+    int al = c->p.algo_moment_from_pola;
+    if (al < MDFF_ALGO_SCF || al > MDFF_ALGO_KO_V4_2) return MDFF_ERR_BAD_ARGS;
+    if (al == MDFF_ALGO_KO_V3 || al == MDFF_ALGO_KO_V4_2) return MDFF_ERR_UNSUPPORTED;
+    if (al == MDFF_ALGO_KO_V4_1 && c->p.max_scf_pol_iter > KO_HIST) return MDFF_ERR_BAD_ARGS;
+  }
   double* sx = malloc(sizeof(double) * natm);
   double* sy = malloc(sizeof(double) * natm);
   double* sz = malloc(sizeof(double) * natm);
@@ -1350,8 +1804,6 @@ int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
        (:240-485) */
     if (c->lpolar_any) {
       double* Estat = calloc(n3, sizeof(double));
-      double* Eind = calloc(n3, sizeof(double));
-      double* Efield = calloc(n3, sizeof(double));
       double* qzero = calloc(natm, sizeof(double));
       int ldip = 0;
       for (int it = 0; it < MDFF_NTYPEMAX; ++it)
@@ -1362,41 +1814,23 @@ int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
         for (int i = 0; i < 6; ++i) task_static[i] = 1;
       es_out o;
       multipole_ES(c, rx, ry, rz, sx, sy, sz, &Lc, c->qia, c->dipia, task_static, 1, 1, 0, 0, 0,
-                   0.0, Estat, NULL, zero_f, &o);
-      memcpy(Efield, Estat, sizeof(double) * n3);
+                   1, 0.0, Estat, NULL, zero_f, &o);
+      pim_env env = {c, rx, ry, rz, sx, sy, sz, &Lc, qzero, zero_f, Estat, itime};
       int iscf = 0;
       double rmsd = HUGE_VAL;
-      int task_ind[6] = {0, 0, 1, 0, 0, 0};
-      int ismd = (c->p.calc == MDFF_CALC_MD), isopt = (c->p.calc == MDFF_CALC_OPT);
-      while (((iscf < c->p.max_scf_pol_iter) && (rmsd > c->p.conv_tol_ind)) ||
-             (iscf < c->p.min_scf_pol_iter)) {
-        iscf++;
-        if (iscf != 1 || (!ismd && !isopt))
-          induced_moment(c, Efield, dipia_ind);
-        else
-          aspc(c, dipia_ind, Efield, 1, itime);
-        u_pol = 0.0;
-        for (int ia = 0; ia < natm; ++ia)
-          for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b)
-              u_pol = u_pol + dipia_ind[3 * ia + a] * c->invpoldipia[9 * ia + 3 * a + b] *
-                                  dipia_ind[3 * ia + b];
-        u_pol = u_pol * 0.5;
-        memset(zero_f, 0, sizeof(double) * n3);
-        multipole_ES(c, rx, ry, rz, sx, sy, sz, &Lc, qzero, dipia_ind, task_ind, 0, 1, 0, 0, 0,
-                     u_pol, Eind, NULL, zero_f, &o);
-        for (size_t i = 0; i < n3; ++i) Efield[i] = Estat[i] + Eind[i];
-        if (iscf == 1 && ismd) aspc(c, dipia_ind, Efield, 2, itime);
-        rmsd = get_rmsd_mu(c, Efield, dipia_ind);
+      switch (c->p.algo_moment_from_pola) {
+        case MDFF_ALGO_KO_V1: scf_ko_v1(&env, dipia_ind, &u_pol, &iscf, &rmsd); break;
+        case MDFF_ALGO_KO_V2: scf_ko_v2(&env, dipia_ind, &u_pol, &iscf, &rmsd); break;
+        case MDFF_ALGO_KO_V4_1: scf_ko_v4_1(&env, dipia_ind, &u_pol, &iscf, &rmsd); break;
+        default: scf_plain(&env, dipia_ind, &u_pol, &iscf, &rmsd); break;
       }
+      /* store induced dipole at t (moment_from_pola.f90:465) */
       memcpy(c->hist, dipia_ind, sizeof(double) * n3);
       if (ex) {
         ex->n_scf = iscf;
         ex->rmsd = rmsd;
       }
       free(Estat);
-      free(Eind);
-      free(Efield);
       free(qzero);
     }
     for (size_t i = 0; i < n3; ++i) mu[i] = c->dipia[i] + dipia_ind[i];
@@ -1407,7 +1841,7 @@ int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
     if (status == MDFF_OK) {
       es_out o;
       int do_efg = ex ? ex->do_efg : 0;
-      multipole_ES(c, rx, ry, rz, sx, sy, sz, &Lc, c->qia, mu, c->task, 1, 1, do_efg, 1, 1, u_pol,
+      multipole_ES(c, rx, ry, rz, sx, sy, sz, &Lc, c->qia, mu, c->task, 1, 1, do_efg, 1, 1, 1, u_pol,
                    ef, (ex && ex->efg) ? ex->efg : NULL, f, &o);
       out->u_coul = o.u_coul;
       out->u_pol = u_pol;

@@ -60,6 +60,8 @@ int or_get_kmesh(or_ctx* c, double* kx, double* ky, double* kz, double* kk,
 /* NR erfc (functions.f90:28-40) and TT damping (tt_damp.f90:68-97) */
 double or_errfc(double x);
 void or_tt_damp(double b, double c, double r, int order, double* f, double* fd);
+/* polint (moment_from_pola.f90:2365-2412) at x = 1 through (xa_i, ya_i), n <= 10 */
+double or_polint(const int* xa, const double* ya, int n);
 
 #ifdef __cplusplus
 }

@@ -59,6 +59,8 @@ def lib():
         L.or_get_setup.argtypes = [P, ctypes.POINTER(SetupInfo)]
         L.or_get_kmesh.argtypes = [P, DP, DP, DP, DP, DP, DP]
         L.or_errfc.restype = ctypes.c_double
+        L.or_polint.restype = ctypes.c_double
+        L.or_polint.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.c_int]
         L.or_errfc.argtypes = [ctypes.c_double]
         L.or_tt_damp.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                  DP, DP]
@@ -72,6 +74,15 @@ def set_threads(n):
 
 def errfc(x):
     return lib().or_errfc(float(x))
+
+
+def polint(xa, ya):
+    """polint of the reference at x = 1 through the points (xa, ya)."""
+    xa = np.ascontiguousarray(xa, dtype=np.int32)
+    ya = np.ascontiguousarray(ya, dtype=np.float64)
+    assert xa.size == ya.size <= 10
+    return lib().or_polint(xa.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                           ya.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), int(xa.size))
 
 
 def tt_damp(b, c, r, order):

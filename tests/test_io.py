@@ -176,3 +176,21 @@ def test_thole_keywords(tmp_path):
     with pytest.raises(ValueError):
         mdffio.params_from_namelists({"coulombtag": {"thole_functions": True,
                                                      "thole_function_type": "cubic"}}, [2, 2])
+
+
+def test_dipole_algorithm_keywords(tmp_path):
+    # pimtag algo_moment_from_pola / algo_ext_dipole / omegakO (pim.f90:85-131)
+    p = mdffio.params_from_namelists({}, [2, 2])
+    assert (p.algo_moment_from_pola, p.algo_ext_dipole, p.omegakO) == (_abi.ALGO_SCF, _abi.EXT_ASPC, 0.7)
+    nl = {"pimtag": {"algo_moment_from_pola": "scf_kO_v2", "algo_ext_dipole": "poly", "omegako": 0.55}}
+    p = mdffio.params_from_namelists(nl, [2, 2])
+    assert (p.algo_moment_from_pola, p.algo_ext_dipole, p.omegakO) == (_abi.ALGO_KO_V2, _abi.EXT_POLY, 0.55)
+    f = tmp_path / "control.F"
+    mdffio.write_control(f, p, ["A", "B"])
+    text = f.read_text()
+    assert "algo_moment_from_pola = 'scf_kO_v2'" in text and "algo_ext_dipole = 'poly'" in text
+    r = mdffio.params_from_namelists(mdffio.read_control(f), [2, 2])
+    assert (r.algo_moment_from_pola, r.algo_ext_dipole, r.omegakO) == (_abi.ALGO_KO_V2, _abi.EXT_POLY, 0.55)
+    for bad in ({"algo_moment_from_pola": "scf_kO_v9"}, {"algo_ext_dipole": "cubic"}):
+        with pytest.raises(ValueError):
+            mdffio.params_from_namelists({"pimtag": bad}, [2, 2])

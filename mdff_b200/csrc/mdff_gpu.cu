@@ -60,6 +60,14 @@ struct mdff_ctx {
   mdff_params p;
   int natm = 0, ntype = 0, device = 0;
   cudaStream_t st = nullptr;
+  // side streams: st_sr runs the short-range pass beside the whole Coulomb
+  // chain; st_rs runs the real-space half of a field or force pass beside
+  // its reciprocal half.  Each is joined into st before the first kernel that
+  // writes the same outputs.  Used when overlap is on (MDFF_OVERLAP unset or
+  // not 0) and per-class profiling is off.
+  cudaStream_t st_sr = nullptr, st_rs = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join_sr = nullptr, ev_join_rs = nullptr;
+  bool overlap = true, call_overlap = false, sr_open = false, rs_open = false;
   std::string err;
   // cell / units / tasks
   double A[9], B[9], omega = 0, W[3], ANORM[3];
@@ -139,6 +147,7 @@ struct mdff_ctx {
   // outputs / reductions
   double* d_force = nullptr;     // [3][natm]
   double* d_part = nullptr;
+  double* d_part2 = nullptr;     // partial sums of the side-stream passes
   size_t part_cap = 0;
   double* d_scal = nullptr;
   double* h_scal = nullptr;      // pinned
@@ -519,6 +528,49 @@ static int reduce_into(mdff_ctx* h, int nblk, int nv, double* out) {
   return MDFF_OK;
 }
 
+// ---- side streams ---------------------------------------------------------
+// side stream s waits for everything issued on st so far
+static int fork_to(mdff_ctx* h, cudaStream_t s) {
+  CK(cudaEventRecord(h->ev_fork, h->st));
+  CK(cudaStreamWaitEvent(s, h->ev_fork, 0));
+  return MDFF_OK;
+}
+// stream of the short-range pass (st when overlap is off for this call)
+static int sr_fork(mdff_ctx* h, cudaStream_t* s) {
+  *s = h->st;
+  if (!h->call_overlap) return MDFF_OK;
+  int e = fork_to(h, h->st_sr);
+  if (e) return e;
+  h->sr_open = true;
+  *s = h->st_sr;
+  return MDFF_OK;
+}
+static int sr_join(mdff_ctx* h) {
+  if (!h->sr_open) return MDFF_OK;
+  h->sr_open = false;
+  CK(cudaEventRecord(h->ev_join_sr, h->st_sr));
+  CK(cudaStreamWaitEvent(h->st, h->ev_join_sr, 0));
+  return MDFF_OK;
+}
+// stream of the real-space half of a pass; rec_pass_t joins it before its
+// final sum into the same field / forces
+static int rs_fork(mdff_ctx* h, cudaStream_t* s) {
+  *s = h->st;
+  if (!h->call_overlap) return MDFF_OK;
+  int e = fork_to(h, h->st_rs);
+  if (e) return e;
+  h->rs_open = true;
+  *s = h->st_rs;
+  return MDFF_OK;
+}
+static int rs_join(mdff_ctx* h) {
+  if (!h->rs_open) return MDFF_OK;
+  h->rs_open = false;
+  CK(cudaEventRecord(h->ev_join_rs, h->st_rs));
+  CK(cudaStreamWaitEvent(h->st, h->ev_join_rs, 0));
+  return MDFF_OK;
+}
+
 // moments [qtot(3), mutot(3), qsq, musq] of (q?, mu) into out (device)
 static int moments(mdff_ctx* h, const double4* mu, int has_q, double* out) {
   int n = h->natm, nb = cdiv(n, 256);
@@ -633,6 +685,8 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
                       SelfField sf, int* defer_nch, bool weights_ready) {
   int n = h->natm;
   if (h->nk == 0) {
+    int e = rs_join(h);
+    if (e) return e;
     if (sf.on) {
       k_self_surf_field<<<cdiv(n, 256), 256, 0, h->st>>>(sf.mu, n, sf.selfa2, sf.lsurf, sf.fpi_3V, sf.mom, E);
       LAUNCH_CHECK();
@@ -721,6 +775,9 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   LAUNCH_CHECK();
   prof_end(h, pr);
   double fpi_V = 2.0 * tpi_V;
+  // the real-space half of this pass (side stream) adds into the same E / forces
+  int e = rs_join(h);
+  if (e) return e;
   if (defer_nch) {
     // the caller's kernel sums the field partials (k_dd_cached_rec)
     *defer_nch = nch;
@@ -789,8 +846,17 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   // final kernel adds the self / surface field
   int nch = 0;
   SelfField sf = self_field(h, mu, h->d_scal + S_MOM2);
-  s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, sf, fp32 ? h->d_mu32 : nullptr,
-               fused ? &nch : nullptr, fp32 && weights_ready);
+  if (!fp32) {
+    // FP64: the real-space dipole field beside the reciprocal pass
+    cudaStream_t rs;
+    if ((s = rs_fork(h, &rs))) return s;
+    int pr = prof_begin(h, KC_ESFIELD, 0);
+    k_es_field<double, false, true><<<nb, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E, h->p.thole_type);
+    LAUNCH_CHECK();
+    prof_end(h, pr);
+    return rec_pass(h, false, mu, 0, 1, 0, E, nullptr, sf);
+  }
+  s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, sf, h->d_mu32, fused ? &nch : nullptr, weights_ready);
   if (s) return s;
   int pr = prof_begin(h, KC_ESFIELD, 0);
   if (fused)
@@ -798,10 +864,8 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
                                            h->d_G, nch, h->d_cell, 2.0 * (2.0 * (kTwoPi / h->omega)), sf, E);
   else if (fp32 && dd_mask == 1 && h->dd_cache_ok)
     k_dd_cached<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n, E);
-  else if (fp32)
-    k_es_field<float, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu32, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E, h->p.thole_type);
   else
-    k_es_field<double, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E, h->p.thole_type);
+    k_es_field<float, false, true><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu32, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E, h->p.thole_type);
   LAUNCH_CHECK();
   prof_end(h, pr);
   return MDFF_OK;
@@ -816,7 +880,7 @@ static int static_field(mdff_ctx* h, bool fp32) {
   int nb = cdiv((long)n * 32, 256);
   bool qq = h->task_qq != 0, dd = h->ldip_static != 0;
 #define ESF(R, Q, D, MU)                                                                              \
-  k_es_field<R, Q, D><<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, MU, h->L.nbr, \
+  k_es_field<R, Q, D><<<nb, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, MU, h->L.nbr, \
                                              h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, \
                                              h->p.alphaES, cutsq, 1, 0, E, h->p.thole_type)
   if (fp32 && dd) {
@@ -824,10 +888,14 @@ static int static_field(mdff_ctx* h, bool fp32) {
     LAUNCH_CHECK();
   }
   h->dd_cache_ok = false;
+  // the real-space half beside the reciprocal pass (joined before its final sum)
+  cudaStream_t rs;
+  int s;
+  if ((s = rs_fork(h, &rs))) return s;
   if (fp32 && !dd && h->lpolar && h->d_ddr) {
     // damped charge field + the pair cache of the FP32 solver iterations
     int pr = prof_begin(h, KC_ESFIELD, 0);
-    k_static_cache<<<nb, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, qq ? 1 : 0, E, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->p.thole_type);
+    k_static_cache<<<nb, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, qq ? 1 : 0, E, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->p.thole_type);
     LAUNCH_CHECK();
     prof_end(h, pr);
     h->dd_cache_ok = true;
@@ -846,7 +914,6 @@ static int static_field(mdff_ctx* h, bool fp32) {
     prof_end(h, pr);
   }
 #undef ESF
-  int s;
   if (h->p.lsurf) {
     s = moments(h, h->d_dipia, 1, h->d_scal + S_MOM2);
     if (s) return s;
@@ -1321,14 +1388,16 @@ static int build_cg_graph(mdff_ctx* h, bool fp32) {
   cudaGraphNode_t node;
   CK(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  bool prof = h->prof;
+  bool prof = h->prof, ovl = h->call_overlap;
   h->prof = false;
+  h->call_overlap = false;
   int launches0 = h->launches;
   CK(cudaStreamBeginCaptureToGraph(h->st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   int s = cg_iteration(h, fp32, 1, hc);
   cudaGraph_t captured;
   cudaError_t e = cudaStreamEndCapture(h->st, &captured);
   h->prof = prof;
+  h->call_overlap = ovl;
   h->cg_body_launches = h->launches - launches0;
   h->launches = launches0;
   if (s) return s;
@@ -1440,6 +1509,9 @@ static int run_engforce(mdff_ctx* h, int itime) {
   int n = h->natm, s;
   bool fp32 = h->p.precision == MDFF_PREC_MIXED;
   h->launches = 0;
+  // side work of an earlier call that ended early is joined first
+  if ((s = sr_join(h)) || (s = rs_join(h))) return s;
+  h->call_overlap = h->overlap && !h->prof;
   k_kardir<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_pos, n, h->d_cell, h->d_s);
   LAUNCH_CHECK();
   if ((s = list_update(h))) return s;
@@ -1448,21 +1520,25 @@ static int run_engforce(mdff_ctx* h, int itime) {
   int nbw = cdiv((long)n * 32, 256);
   if (h->lsr) {
     int do_bmh = (h->p.lbmhft || h->p.lbmhftd) ? 1 : 0;
+    // beside the Coulomb chain; joined before the force pass
+    cudaStream_t ss;
+    if ((s = sr_fork(h, &ss))) return s;
     int pr = prof_begin(h, KC_SR, 0);
     // short range stays FP64 in the mixed mode too: BKS-type pair forces of
     // tens of eV/A cancel to net forces of a few eV/A, and FP32 rounding of the
     // pair terms alone gives ~1e-5 relative force error
 #define SRK(MODE)                                                                              \
-  k_shortrange<double, MODE><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_itype, h->L.nbr, h->L.nnb,     \
-                                                     h->L.cap, n, h->d_cell, h->d_nbtab, h->ntype, \
-                                                     h->p.lbmhftd, h->p.trunc, h->d_force, h->d_part)
+  k_shortrange<double, MODE><<<nbw, 256, 0, ss>>>(h->d_s, h->d_itype, h->L.nbr, h->L.nnb,        \
+                                                  h->L.cap, n, h->d_cell, h->d_nbtab, h->ntype,    \
+                                                  h->p.lbmhftd, h->p.trunc, h->d_force, h->d_part2)
     if (do_bmh && h->p.lnmlj) SRK(3);
     else if (do_bmh) SRK(1);
     else SRK(2);
 #undef SRK
     LAUNCH_CHECK();
     prof_end(h, pr);
-    if ((s = reduce_into(h, nbw, kSRPart, h->d_scal + S_SR))) return s;
+    k_reduce_partials<<<kSRPart, 256, 0, ss>>>(h->d_part2, nbw, kSRPart, h->d_scal + S_SR);
+    LAUNCH_CHECK();
   }
   // per-call flags: [0] catastrophe, [1] a tensor-core wait gave up
   CK(cudaMemsetAsync(h->d_cata, 0, 2 * sizeof(int), h->st));
@@ -1487,13 +1563,18 @@ static int run_engforce(mdff_ctx* h, int itime) {
     LAUNCH_CHECK();
     CK(cudaMemsetAsync(h->d_E, 0, sizeof(double4) * n, h->st));
     double cutsq = h->p.cutlongrange * h->p.cutlongrange;
+    // the short-range forces are written first; the real-space force pass
+    // runs beside the reciprocal one, which joins it before its final sum
+    if ((s = sr_join(h))) return s;
+    cudaStream_t rs;
+    if ((s = rs_fork(h, &rs))) return s;
     int prf = prof_begin(h, KC_ESFORCE, 0);
 #define ESFORCE(R, TH)                                                                            \
-  k_es_force<R, TH><<<nbw, 256, 0, h->st>>>(h->d_s, h->d_q, h->d_itype, h->d_mu_tot, h->L.nbr,      \
+  k_es_force<R, TH><<<nbw, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_mu_tot, h->L.nbr,      \
                                             h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, \
                                             h->p.alphaES, cutsq, h->task_qq, h->task_qd,            \
                                             h->task_dd, 1, h->coul_unit, h->d_E, h->d_force,        \
-                                            h->d_part)
+                                            h->d_part2)
     const bool thole = h->p.thole_type != MDFF_THOLE_NONE;
     if (fp32 && thole) ESFORCE(float, true);
     else if (fp32) ESFORCE(float, false);
@@ -1502,13 +1583,15 @@ static int run_engforce(mdff_ctx* h, int itime) {
 #undef ESFORCE
     LAUNCH_CHECK();
     prof_end(h, prf);
-    if ((s = reduce_into(h, nbw, kESPart, h->d_scal + S_DIR))) return s;
+    k_reduce_partials<<<kESPart, 256, 0, rs>>>(h->d_part2, nbw, kESPart, h->d_scal + S_DIR);
+    LAUNCH_CHECK();
     int has_mu = (h->task_qd || h->task_dd) ? 1 : 0;
     if ((s = moments(h, h->d_mu_tot, 1, h->d_scal + S_MOM))) return s;
     if ((s = rec_pass(h, fp32, h->d_mu_tot, h->task_qq ? 1 : 0, has_mu, 1, h->d_E, h->d_scal + S_REC,
                       self_field(h, h->d_mu_tot, h->d_scal + S_MOM))))
       return s;
   }
+  if ((s = sr_join(h)) || (s = rs_join(h))) return s;
   CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(h->h_flags, h->L.flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(h->h_cata, h->d_cata, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->st));
@@ -1650,7 +1733,20 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   h->device = p.device;
   CK(cudaSetDevice(h->device));
   CK(cudaDeviceGetAttribute(&h->nsm, cudaDevAttrMultiProcessorCount, h->device));
-  CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  // the main chain and the real-space halves at the highest priority; the
+  // short-range pass fills the SMs they leave idle
+  int prio_lo = 0, prio_hi = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+  CK(cudaStreamCreateWithPriority(&h->st, cudaStreamNonBlocking, prio_hi));
+  CK(cudaStreamCreateWithPriority(&h->st_rs, cudaStreamNonBlocking, prio_hi));
+  CK(cudaStreamCreateWithPriority(&h->st_sr, cudaStreamNonBlocking, prio_lo));
+  CK(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->ev_join_sr, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h->ev_join_rs, cudaEventDisableTiming));
+  {
+    const char* ov = std::getenv("MDFF_OVERLAP");
+    h->overlap = !(ov && ov[0] == '0');
+  }
   CK(cudaEventCreate(&h->ev0));
   CK(cudaEventCreate(&h->ev1));
   h->npol = S.npol;
@@ -1740,6 +1836,7 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   // kO_v4_1 Gram row: kKoHist + 2 dot products per block
   h->part_cap = std::max(h->part_cap, (size_t)cdiv(n, 256) * (kKoHist + 2));
   DALLOC(h->d_part, h->part_cap);
+  DALLOC(h->d_part2, h->part_cap);
   DALLOC(h->d_scal, S_NSCAL);
   DALLOC(h->d_cata, 2);  // [0] catastrophe, [1] a tensor-core wait gave up
   DALLOC(h->d_ekin_part, cdiv(n, 256));
@@ -2103,7 +2200,7 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_hist, h->d_E, h->d_r, h->d_z, h->d_pv, h->d_qv, h->d_Tp, h->d_mu32, h->d_force,
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
-                  h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x};
+                  h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);
@@ -2112,6 +2209,11 @@ void mdff_gpu_destroy(mdff_handle h) {
   if (h->h_flags) cudaFreeHost(h->h_flags);
   if (h->h_cata) cudaFreeHost(h->h_cata);
   if (h->h_ko) cudaFreeHost(h->h_ko);
+  if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+  if (h->ev_join_sr) cudaEventDestroy(h->ev_join_sr);
+  if (h->ev_join_rs) cudaEventDestroy(h->ev_join_rs);
+  if (h->st_sr) cudaStreamDestroy(h->st_sr);
+  if (h->st_rs) cudaStreamDestroy(h->st_rs);
   if (h->ev0) cudaEventDestroy(h->ev0);
   if (h->ev1) cudaEventDestroy(h->ev1);
   if (h->st) cudaStreamDestroy(h->st);

@@ -8,7 +8,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libmdff_gpu.so")
 SOURCES = ["mdff_gpu.cu", "mdff_noalloc.cu", "batch.cu"]
-HEADERS = ["common.cuh", "nlist.cuh", "realspace.cuh", "recip.cuh", "recip_tc.cuh", "pim.cuh", "batch.cuh", "adjoint.cuh",
+HEADERS = ["common.cuh", "nlist.cuh", "realspace.cuh", "recip.cuh", "recip_tc.cuh", "pim.cuh", "ko.cuh", "batch.cuh", "adjoint.cuh",
            "setup.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -209,8 +209,19 @@ __device__ bool grid_sum_last(const double (&v)[NV], double* part, unsigned* cnt
   if (ticket != gridDim.x - 1) return false;
   __threadfence();
   for (int k = 0; k < NV; ++k) {
+    // four loads in flight per step, added in block order
     double acc = 0.0;
-    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) acc += __ldcg(&part[(size_t)b * NV + k]);
+    unsigned b = threadIdx.x;
+    const unsigned st = blockDim.x, nb = gridDim.x;
+    for (; b + 3 * st < nb; b += 4 * st) {
+      double x0 = __ldcg(&part[(size_t)b * NV + k]), x1 = __ldcg(&part[(size_t)(b + st) * NV + k]);
+      double x2 = __ldcg(&part[(size_t)(b + 2 * st) * NV + k]), x3 = __ldcg(&part[(size_t)(b + 3 * st) * NV + k]);
+      acc += x0;
+      acc += x1;
+      acc += x2;
+      acc += x3;
+    }
+    for (; b < nb; b += st) acc += __ldcg(&part[(size_t)b * NV + k]);
     sh[threadIdx.x] = acc;
     __syncthreads();
     for (int w = blockDim.x >> 1; w > 0; w >>= 1) {

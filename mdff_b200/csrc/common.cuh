@@ -147,18 +147,6 @@ __device__ __forceinline__ void tt_damp(R b, R c, R r, int order, R& f, R& fd) {
 }
 
 // ---------------------------------------------------------------------------
-// per-ion polarisability tables of the induced-dipole solvers
-struct PolDev {
-  const double* pol;     // [natm][9] poldipia (row-major a,b)
-  const double* invpol;  // [natm][9]
-  const int* ipolar;     // [natm]
-};
-
-__device__ __forceinline__ double4 matvec3(const double* m, double4 v) {
-  return make_double4(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
-                      m[6] * v.x + m[7] * v.y + m[8] * v.z, 0.0);
-}
-
 // warp / block reductions (fixed order -> deterministic)
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -187,52 +175,6 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* smem) {
     }
   }
   __syncthreads();
-}
-
-// Grid sum without a second launch.  Every block stores its NV partials (v,
-// valid in thread 0) in part[block][NV]; the last block to arrive (atomic
-// ticket on *cnt) sums them exactly as k_reduce_partials does (per-thread
-// strided sums over the blocks, then a tree over 256 threads), writes
-// out[0..NV-1], resets *cnt and returns true in all its threads.  Needs
-// blockDim.x == 256 and the same grid size on every use of part / cnt.
-template <int NV>
-__device__ bool grid_sum_last(const double (&v)[NV], double* part, unsigned* cnt, double* out) {
-  __shared__ unsigned ticket;
-  __shared__ double sh[256];
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) part[(size_t)blockIdx.x * NV + k] = v[k];
-    __threadfence();
-    ticket = atomicAdd(cnt, 1u);
-  }
-  __syncthreads();
-  if (ticket != gridDim.x - 1) return false;
-  __threadfence();
-  for (int k = 0; k < NV; ++k) {
-    // four loads in flight per step, added in block order
-    double acc = 0.0;
-    unsigned b = threadIdx.x;
-    const unsigned st = blockDim.x, nb = gridDim.x;
-    for (; b + 3 * st < nb; b += 4 * st) {
-      double x0 = __ldcg(&part[(size_t)b * NV + k]), x1 = __ldcg(&part[(size_t)(b + st) * NV + k]);
-      double x2 = __ldcg(&part[(size_t)(b + 2 * st) * NV + k]), x3 = __ldcg(&part[(size_t)(b + 3 * st) * NV + k]);
-      acc += x0;
-      acc += x1;
-      acc += x2;
-      acc += x3;
-    }
-    for (; b < nb; b += st) acc += __ldcg(&part[(size_t)b * NV + k]);
-    sh[threadIdx.x] = acc;
-    __syncthreads();
-    for (int w = blockDim.x >> 1; w > 0; w >>= 1) {
-      if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) out[k] = sh[0];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) *cnt = 0u;
-  return true;
 }
 
 }  // namespace mdff

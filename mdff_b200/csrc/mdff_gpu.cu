@@ -45,8 +45,7 @@ enum {
   S_UPOL = 38,   // u_pol
   S_RMS = 39,    // SCF rmsd^2 sum
   S_CG = 40,     // 40 rz, 41 rmsd^2 (init), 42 pq, 43 rzn, 44 rmsd^2 (update),
-                 // 45 inner tolerance, 46 iterations, 47 iteration cap, 48 rmsd,
-                 // 51 beta
+                 // 45 inner tolerance, 46 iterations, 47 iteration cap, 48 rmsd
   S_KO = 49,     // 2: kO algorithms (inner residual, find_min dot products)
   S_MOM2 = 52,   // 8: moments of field passes
   S_DISP = 60,
@@ -154,7 +153,6 @@ struct mdff_ctx {
   double* h_scal = nullptr;      // pinned
   int* d_cata = nullptr;
   int* h_cata = nullptr;
-  unsigned* d_cnt = nullptr;     // tickets of grid_sum_last: [0] CG operator, [1] CG update
   double* d_pack = nullptr;      // [natm][3] staging for mu/ef output
   double* d_ekin_part = nullptr;
   // stats
@@ -830,9 +828,8 @@ static int build_tables(mdff_ctx* h) {
 // induced pass / the CG operator.  E = T mu.
 // weights_ready: d_w32 / d_mu32 already hold the FP32 operands of mu (written
 // by the CG direction kernels)
-// ce: the CG epilogue of the fused FP32 operator (q = A p and p.q), or null
 static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, double4* E,
-                       bool weights_ready = false, const CgOpEpi* ce = nullptr) {
+                       bool weights_ready = false) {
   int n = h->natm;
   // FP32 CG operator with the pair cache: one kernel writes E (reciprocal +
   // self + cached real-space dipole field)
@@ -862,14 +859,9 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, sf, h->d_mu32, fused ? &nch : nullptr, weights_ready);
   if (s) return s;
   int pr = prof_begin(h, KC_ESFIELD, 0);
-  if (fused && ce)
-    k_dd_cached_rec<true><<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap,
-                                                 n, h->d_G, nch, h->d_cell, 2.0 * (2.0 * (kTwoPi / h->omega)),
-                                                 sf, E, *ce);
-  else if (fused)
-    k_dd_cached_rec<false><<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap,
-                                                  n, h->d_G, nch, h->d_cell, 2.0 * (2.0 * (kTwoPi / h->omega)),
-                                                  sf, E, CgOpEpi{});
+  if (fused)
+    k_dd_cached_rec<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n,
+                                           h->d_G, nch, h->d_cell, 2.0 * (2.0 * (kTwoPi / h->omega)), sf, E);
   else if (fp32 && dd_mask == 1 && h->dd_cache_ok)
     k_dd_cached<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n, E);
   else
@@ -1337,6 +1329,19 @@ static int solve_ko_v4(mdff_ctx* h, int itime, bool fp32) {
   return MDFF_OK;
 }
 
+// the step scalars after an inner CG iteration: rz <- rz_new, count, rmsd of
+// the recurrence residual, and (inside the graph) the while-loop condition
+__global__ void k_cg_inner_check(double* __restrict__ sc, int npol, int in_graph,
+                                 cudaGraphConditionalHandle hc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  sc[0] = sc[3];
+  double it = sc[6] + 1.0;
+  sc[6] = it;
+  double rm = sqrt(sc[4] / (double)npol);
+  sc[8] = rm;
+  if (in_graph) cudaGraphSetConditional(hc, (rm > sc[5] && it < sc[7]) ? 1u : 0u);
+}
+
 __global__ void k_setd2(double* __restrict__ a, double va, double* __restrict__ b, double vb) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     *a = va;
@@ -1344,27 +1349,22 @@ __global__ void k_setd2(double* __restrict__ a, double va, double* __restrict__ 
   }
 }
 
-// one inner CG iteration: p -> T p -> q = A p; x, r, z updated; p <- z + beta p.
-// Three launches after the reciprocal pass with the FP32 pair cache: the
-// operator kernel also forms q and p.q, the update kernel's last block sums
-// r.z and closes the iteration (grid_sum_last).
+// one inner CG iteration: p -> T p -> q = A p; x, r, z updated; p <- z + beta p
 static int cg_iteration(mdff_ctx* h, bool fp32, int in_graph, cudaGraphConditionalHandle hc) {
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
   double* sc = h->d_scal + S_CG;
-  const bool fused = fp32 && h->dd_cache_ok && h->nk > 0;  // as in field_of_mu (dd_mask 1)
-  CgOpEpi ce{h->d_pv, P, h->d_qv, h->d_part, h->d_cnt, sc + 2};
-  if ((s = field_of_mu(h, h->d_pv, 1, fp32, h->d_Tp, fp32, fused ? &ce : nullptr))) return s;
-  if (!fused) {
-    k_cg_Ap<<<nb, 256, 0, h->st>>>(h->d_pv, h->d_Tp, P, n, h->d_qv, h->d_part);
-    LAUNCH_CHECK();
-    if ((s = reduce_into(h, nb, 1, sc + 2))) return s;
-  }
-  k_cg_update<<<nb, 256, 0, h->st>>>(sc, P, n, h->d_pv, h->d_qv, h->d_mu_ind, h->d_r, h->d_z, h->d_part,
-                                     h->d_cnt + 1, h->npol, in_graph, hc);
+  if ((s = field_of_mu(h, h->d_pv, 1, fp32, h->d_Tp, fp32))) return s;
+  k_cg_Ap<<<nb, 256, 0, h->st>>>(h->d_pv, h->d_Tp, P, n, h->d_qv, h->d_part);
   LAUNCH_CHECK();
-  k_cg_dir<<<nb, 256, 0, h->st>>>(sc + 11, n, h->d_z, h->d_pv, h->d_cell, fp32 ? h->d_w32 : nullptr,
-                                  h->d_mu32);
+  if ((s = reduce_into(h, nb, 1, sc + 2))) return s;
+  k_cg_update<<<nb, 256, 0, h->st>>>(sc + 0, sc + 2, P, n, h->d_pv, h->d_qv, h->d_mu_ind, h->d_r, h->d_z, h->d_part);
+  LAUNCH_CHECK();
+  if ((s = reduce_into(h, nb, 2, sc + 3))) return s;
+  k_cg_dir<<<nb, 256, 0, h->st>>>(sc + 0, sc + 3, n, h->d_z, h->d_pv, h->d_cell,
+                                  fp32 ? h->d_w32 : nullptr, h->d_mu32);
+  LAUNCH_CHECK();
+  k_cg_inner_check<<<1, 32, 0, h->st>>>(sc, h->npol, in_graph, hc);
   LAUNCH_CHECK();
   return MDFF_OK;
 }
@@ -1839,8 +1839,6 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_part2, h->part_cap);
   DALLOC(h->d_scal, S_NSCAL);
   DALLOC(h->d_cata, 2);  // [0] catastrophe, [1] a tensor-core wait gave up
-  DALLOC(h->d_cnt, 2);
-  CK(cudaMemsetAsync(h->d_cnt, 0, 2 * sizeof(unsigned), h->st));
   DALLOC(h->d_ekin_part, cdiv(n, 256));
   CK(cudaMallocHost((void**)&h->h_scal, sizeof(double) * S_NSCAL));
   CK(cudaMallocHost((void**)&h->h_cata, 2 * sizeof(int)));
@@ -2202,8 +2200,7 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_hist, h->d_E, h->d_r, h->d_z, h->d_pv, h->d_qv, h->d_Tp, h->d_mu32, h->d_force,
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
-                  h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
-                  h->d_cnt};
+                  h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);

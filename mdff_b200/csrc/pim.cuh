@@ -15,6 +15,16 @@
 
 namespace mdff {
 
+struct PolDev {
+  const double* pol;     // [natm][9] poldipia (row-major a,b)
+  const double* invpol;  // [natm][9]
+  const int* ipolar;     // [natm]
+};
+
+__device__ __forceinline__ double4 matvec3(const double* m, double4 v) {
+  return make_double4(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[3] * v.x + m[4] * v.y + m[5] * v.z,
+                      m[6] * v.x + m[7] * v.y + m[8] * v.z, 0.0);
+}
 
 // mu_i = alpha_i E_i on polarisable ions, 0 elsewhere (induced_moment)
 __global__ void k_induce(const double4* __restrict__ E, PolDev P, int natm, double4* __restrict__ mu) {
@@ -213,20 +223,16 @@ __global__ void k_cg_Ap(const double4* __restrict__ p, const double4* __restrict
   if (threadIdx.x == 0) part[blockIdx.x] = v[0];
 }
 
-// al = rz / pq ; x += al p ; r -= al q ; z = alpha_pol r ; r.z (new) and
-// rmsd^2 summed over the grid by its last block, which then closes the
-// iteration: beta = rz_new / rz (sc[11]), rz <- rz_new, iteration count,
-// rmsd of the recurrence residual and (inside the graph) the while-loop
-// condition.  sc = the CG scalars: 0 rz, 2 pq, 3 rz_new, 4 rmsd^2,
-// 5 inner tolerance, 6 iterations, 7 iteration cap, 8 rmsd, 11 beta.
-__global__ void k_cg_update(double* __restrict__ sc, PolDev P, int natm, const double4* __restrict__ p,
+// al = rz / pq ; x += al p ; r -= al q ; z = alpha_pol r ;
+// partial r.z (new) and rmsd^2
+__global__ void k_cg_update(const double* __restrict__ rz_p, const double* __restrict__ pq_p,
+                            PolDev P, int natm, const double4* __restrict__ p,
                             const double4* __restrict__ qv, double4* __restrict__ x,
                             double4* __restrict__ r, double4* __restrict__ z,
-                            double* __restrict__ part, unsigned* __restrict__ cnt, int npol,
-                            int in_graph, cudaGraphConditionalHandle hc) {
+                            double* __restrict__ part) {
   __shared__ double red[2 * 32];
   double v[2] = {0.0, 0.0};
-  double rz = sc[0], pq = sc[2];
+  double rz = *rz_p, pq = *pq_p;
   double al = (pq != 0.0) ? rz / pq : 0.0;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < natm && P.ipolar[i]) {
@@ -248,23 +254,19 @@ __global__ void k_cg_update(double* __restrict__ sc, PolDev P, int natm, const d
       if (a[4 * c] != 0.0) v[1] += rr[c] * rr[c];
   }
   block_sum<2>(v, red);
-  if (grid_sum_last<2>(v, part, cnt, sc + 3) && threadIdx.x == 0) {
-    double rzn = sc[3];
-    sc[11] = (rz != 0.0) ? rzn / rz : 0.0;
-    sc[0] = rzn;
-    double it = sc[6] + 1.0;
-    sc[6] = it;
-    double rm = sqrt(sc[4] / (double)npol);
-    sc[8] = rm;
-    if (in_graph) cudaGraphSetConditional(hc, (rm > sc[5] && it < sc[7]) ? 1u : 0u);
+  if (threadIdx.x == 0) {
+    part[(size_t)blockIdx.x * 2] = v[0];
+    part[(size_t)blockIdx.x * 2 + 1] = v[1];
   }
 }
 
-// p = z + beta p (beta from k_cg_update)
-__global__ void k_cg_dir(const double* __restrict__ be_p, int natm, const double4* __restrict__ z,
-                         double4* __restrict__ p, const CellC* __restrict__ cell,
-                         float4* __restrict__ w32, float4* __restrict__ mu32) {
-  double be = *be_p;
+// p = z + beta p with beta = rz_new / rz
+__global__ void k_cg_dir(const double* __restrict__ rz_p, const double* __restrict__ rzn_p,
+                         int natm, const double4* __restrict__ z, double4* __restrict__ p,
+                         const CellC* __restrict__ cell, float4* __restrict__ w32,
+                         float4* __restrict__ mu32) {
+  double rz = *rz_p, rzn = *rzn_p;
+  double be = (rz != 0.0) ? rzn / rz : 0.0;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < natm) {
     double4 pi = p[i], zi = z[i];

@@ -796,19 +796,8 @@ static __global__ void k_reduce_partials(const double* __restrict__ part, int nb
                                          double* __restrict__ out) {
   __shared__ double sh[256];
   const int v = blockIdx.x;
-  // four loads in flight per step, added in block order
   double acc = 0.0;
-  int b = threadIdx.x;
-  const int st = blockDim.x;
-  for (; b + 3 * st < nblk; b += 4 * st) {
-    double x0 = part[(size_t)b * nv + v], x1 = part[(size_t)(b + st) * nv + v];
-    double x2 = part[(size_t)(b + 2 * st) * nv + v], x3 = part[(size_t)(b + 3 * st) * nv + v];
-    acc += x0;
-    acc += x1;
-    acc += x2;
-    acc += x3;
-  }
-  for (; b < nblk; b += st) acc += part[(size_t)b * nv + v];
+  for (int b = threadIdx.x; b < nblk; b += blockDim.x) acc += part[(size_t)b * nv + v];
   sh[threadIdx.x] = acc;
   __syncthreads();
   for (int w = blockDim.x >> 1; w > 0; w >>= 1) {

@@ -483,45 +483,31 @@ static __global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const 
   }
 }
 
-// CG epilogue of the fused operator: q = alpha^-1 p - T p on polarisable
-// ions (0 elsewhere) and p.q summed over the grid (k_cg_Ap + its reduction)
-struct CgOpEpi {
-  const double4* p;
-  PolDev P;
-  double4* q;
-  double* part;
-  unsigned* cnt;
-  double* out;
-};
-
 // The CG operator's last step, fused: E_i = (reciprocal field from the chunk
 // partials G + self / surface field) + real-space dipole field from the FP32
 // pair cache of k_static_cache, written (not added).  The same operations, in
 // the same order, as k_rec_field_sum (no forces) into a zeroed E followed by
 // k_dd_cached, so the results are identical; one launch and no memset instead.
-// With CG, the epilogue of CgOpEpi follows.
-template <bool CG>
 static __global__ void __launch_bounds__(256) k_dd_cached_rec(
     const float4* __restrict__ mu, const float4* __restrict__ cr, const float* __restrict__ cb1,
     const int* __restrict__ cj, const int* __restrict__ cn, int cap, int natm,
     const double4* __restrict__ Gpart, int nchunk, const CellC* __restrict__ cell, double scale,
-    SelfField sf, double4* __restrict__ E, CgOpEpi ce) {
+    SelfField sf, double4* __restrict__ E) {
   int lane = threadIdx.x & 31;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const bool act = i < natm;
-  if (!CG && !act) return;  // (the CG epilogue needs every thread at its barriers)
+  if (i >= natm) return;
   // lanes 0-3: strided chunk sums of the reciprocal partials, as the four
   // threads of an ion in k_rec_field_sum (loads issued before the pair loop)
   double g[3] = {0.0, 0.0, 0.0};
-  if (act && lane < 4)
+  if (lane < 4)
     for (int c = lane; c < nchunk; c += 4) {
       double4 v = Gpart[(size_t)c * natm + i];
       g[0] += v.x;
       g[1] += v.y;
       g[2] += v.z;
     }
-  double4 mi = (act && lane == 0 && sf.on && sf.mu) ? sf.mu[i] : make_double4(0, 0, 0, 0);
-  int n = act ? cn[i] : 0;
+  double4 mi = (lane == 0 && sf.on && sf.mu) ? sf.mu[i] : make_double4(0, 0, 0, 0);
+  int n = cn[i];
   size_t base = (size_t)i * cap;
   float ex = 0.f, ey = 0.f, ez = 0.f;
   for (int k = lane; k < n; k += 32) {
@@ -539,41 +525,24 @@ static __global__ void __launch_bounds__(256) k_dd_cached_rec(
     g[a] += __shfl_xor_sync(FULL_MASK, g[a], 1);
     g[a] += __shfl_xor_sync(FULL_MASK, g[a], 2);
   }
-  double pq[1] = {0.0};
-  if (act && lane == 0) {
-    const double* B = cell->B;
-    double e[3];
-    for (int a = 0; a < 3; ++a)
-      e[a] = -kTwoPi * (B[3 * a + 0] * g[0] + B[3 * a + 1] * g[1] + B[3 * a + 2] * g[2]) * scale;
-    double s3[3] = {0.0, 0.0, 0.0};
-    if (sf.on) {
-      if (sf.lsurf) {
-        s3[0] = -(sf.mom[0] + sf.mom[3]) * sf.fpi_3V;
-        s3[1] = -(sf.mom[1] + sf.mom[4]) * sf.fpi_3V;
-        s3[2] = -(sf.mom[2] + sf.mom[5]) * sf.fpi_3V;
-      }
-      s3[0] += 2.0 * sf.selfa2 * mi.x;
-      s3[1] += 2.0 * sf.selfa2 * mi.y;
-      s3[2] += 2.0 * sf.selfa2 * mi.z;
+  if (lane != 0) return;
+  const double* B = cell->B;
+  double e[3];
+  for (int a = 0; a < 3; ++a)
+    e[a] = -kTwoPi * (B[3 * a + 0] * g[0] + B[3 * a + 1] * g[1] + B[3 * a + 2] * g[2]) * scale;
+  double s3[3] = {0.0, 0.0, 0.0};
+  if (sf.on) {
+    if (sf.lsurf) {
+      s3[0] = -(sf.mom[0] + sf.mom[3]) * sf.fpi_3V;
+      s3[1] = -(sf.mom[1] + sf.mom[4]) * sf.fpi_3V;
+      s3[2] = -(sf.mom[2] + sf.mom[5]) * sf.fpi_3V;
     }
-    double4 Ei = make_double4((0.0 + e[0] + s3[0]) + dx, (0.0 + e[1] + s3[1]) + dy,
-                              (0.0 + e[2] + s3[2]) + dz, 0.0);
-    E[i] = Ei;
-    if (CG) {
-      double4 pi = ce.p[i], qi = make_double4(0, 0, 0, 0);
-      if (ce.P.ipolar[i]) {
-        double4 ap = matvec3(ce.P.invpol + 9 * (size_t)i, pi);
-        qi = make_double4(ap.x - Ei.x, ap.y - Ei.y, ap.z - Ei.z, 0);
-      }
-      ce.q[i] = qi;
-      pq[0] = pi.x * qi.x + pi.y * qi.y + pi.z * qi.z;
-    }
+    s3[0] += 2.0 * sf.selfa2 * mi.x;
+    s3[1] += 2.0 * sf.selfa2 * mi.y;
+    s3[2] += 2.0 * sf.selfa2 * mi.z;
   }
-  if constexpr (CG) {
-    __shared__ double red[32];
-    block_sum<1>(pq, red);
-    grid_sum_last<1>(pq, ce.part, ce.cnt, ce.out);
-  }
+  E[i] = make_double4((0.0 + e[0] + s3[0]) + dx, (0.0 + e[1] + s3[1]) + dy,
+                      (0.0 + e[2] + s3[2]) + dz, 0.0);
 }
 
 

@@ -150,6 +150,19 @@ typedef struct mdff_params {
   int algo_moment_from_pola;              /* MDFF_ALGO_*                        */
   int algo_ext_dipole;                    /* MDFF_EXT_*: kO_v1 / kO_v2 predictor */
   double omegakO;                         /* kO relaxation weight (0.7)         */
+
+  /* &pimtag Wannier centres (pim.f90:93-96, 134-136; moment_from_pola.f90:
+     136-147, 632-807).  Ions of a type with lwfc < 0 are Wannier centres;
+     when some type has lwfc > 0, every other ion gets the dipole
+     -2 sum (r_wfc - r_ion) over the centres with |r|^2 < rcut_wfc (the
+     reference compares the squared distance with rcut_wfc itself), added
+     to its total dipole after the induced-dipole solve when ldip_wfc; an
+     ion of a type with lwfc > 0 must find exactly lwfc centres
+     (MDFF_ERR_BAD_ARGS otherwise).  Centre types come after all other
+     types, as the reference's list bookkeeping needs. */
+  int lwfc[MDFF_NTYPEMAX];
+  int ldip_wfc;                           /* default 1                          */
+  double rcut_wfc;                        /* default 0.5                        */
 } mdff_params;
 
 /* Results of one engforce call; pointer members are caller-owned host arrays

@@ -65,6 +65,7 @@ class MdffParams(ctypes.Structure):
         ("wall24", (_d * NT) * NT),
         ("thole_type", _i), ("thole_param", (_d * NT) * NT),
         ("algo_moment_from_pola", _i), ("algo_ext_dipole", _i), ("omegakO", _d),
+        ("lwfc", _i * NT), ("ldip_wfc", _i), ("rcut_wfc", _d),
     ]
 
 

@@ -355,6 +355,11 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
       h->err = "the kO dipole algorithms are not built into the batched engine (use mdff_gpu_create)";
       return MDFF_ERR_UNSUPPORTED;
     }
+    for (int t = 0; t < MDFF_NTYPEMAX; ++t)
+      if (p.lwfc[t] != 0) {
+        h->err = "Wannier centres are not built into the batched engine (use mdff_gpu_create)";
+        return MDFF_ERR_UNSUPPORTED;
+      }
     h->pset_of.push_back(ps);
     long n = 0;
     for (int t = 0; t < MDFF_NTYPEMAX; ++t) {

@@ -151,8 +151,12 @@ struct mdff_ctx {
   size_t part_cap = 0;
   double* d_scal = nullptr;
   double* h_scal = nullptr;      // pinned
-  int* d_cata = nullptr;
+  int* d_cata = nullptr;         // [0] catastrophe, [1] tensor-core wait gave up, [2] Wannier count
   int* h_cata = nullptr;
+  // Wannier centres: per-type lwfc, the centres' dipoles of the last call
+  bool lwannier = false;
+  int* d_lwfc = nullptr;
+  double4* d_mu_wfc = nullptr;
   double* d_pack = nullptr;      // [natm][3] staging for mu/ef output
   double* d_ekin_part = nullptr;
   // stats
@@ -1540,8 +1544,8 @@ static int run_engforce(mdff_ctx* h, int itime) {
     k_reduce_partials<<<kSRPart, 256, 0, ss>>>(h->d_part2, nbw, kSRPart, h->d_scal + S_SR);
     LAUNCH_CHECK();
   }
-  // per-call flags: [0] catastrophe, [1] a tensor-core wait gave up
-  CK(cudaMemsetAsync(h->d_cata, 0, 2 * sizeof(int), h->st));
+  // per-call flags: [0] catastrophe, [1] a tensor-core wait gave up, [2] Wannier count
+  CK(cudaMemsetAsync(h->d_cata, 0, 3 * sizeof(int), h->st));
   if (h->p.lcoulomb) {
     if ((s = build_tables(h))) return s;
     CK(cudaMemsetAsync(h->d_mu_ind, 0, sizeof(double4) * n, h->st));
@@ -1559,7 +1563,15 @@ static int run_engforce(mdff_ctx* h, int itime) {
         s = solve_scf(h, itime, fp32);
       if (s) return s;
     }
-    k_mu_total<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_dipia, h->d_mu_ind, n, h->d_mu_tot, h->d_cata);
+    // dipoles of the Wannier centres (moment_from_pola.f90:136-147)
+    if (h->lwannier) {
+      k_wfc_dipoles<<<nbw, 256, 0, h->st>>>(h->d_s, h->d_itype, h->d_lwfc, h->L.nbr, h->L.nnb, h->L.cap, n,
+                                            h->d_cell, h->p.rcut_wfc, h->d_mu_wfc, h->d_cata + 2);
+      LAUNCH_CHECK();
+    }
+    k_mu_total<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_dipia, h->d_mu_ind,
+                                                (h->lwannier && h->p.ldip_wfc) ? h->d_mu_wfc : nullptr, n,
+                                                h->d_mu_tot, h->d_cata);
     LAUNCH_CHECK();
     CK(cudaMemsetAsync(h->d_E, 0, sizeof(double4) * n, h->st));
     double cutsq = h->p.cutlongrange * h->p.cutlongrange;
@@ -1594,7 +1606,7 @@ static int run_engforce(mdff_ctx* h, int itime) {
   if ((s = sr_join(h)) || (s = rs_join(h))) return s;
   CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(h->h_flags, h->L.flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, h->st));
-  CK(cudaMemcpyAsync(h->h_cata, h->d_cata, 2 * sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaMemcpyAsync(h->h_cata, h->d_cata, 3 * sizeof(int), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   prof_collect(h);
   h->stats.list_rebuilds = h->h_flags[3];
@@ -1604,6 +1616,10 @@ static int run_engforce(mdff_ctx* h, int itime) {
     h->err = h->h_cata[1] == 2 ? "tensor-core reciprocal kernel launched with too little shared memory"
                                : "a tensor-core reciprocal-kernel wait gave up";
     return MDFF_ERR_TIMEOUT;
+  }
+  if (h->h_cata[2]) {
+    h->err = "a Wannier centre is missing for an ion of a type with lwfc > 0 (moment_from_pola.f90:731-737)";
+    return MDFF_ERR_BAD_ARGS;
   }
   if (h->h_cata[0]) return MDFF_ERR_CATASTROPHE;
   if (h->lpolar && !h->stats.converged && h->p.fail_on_nonconvergence) return MDFF_ERR_NOT_CONVERGED;
@@ -1838,10 +1854,21 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_part, h->part_cap);
   DALLOC(h->d_part2, h->part_cap);
   DALLOC(h->d_scal, S_NSCAL);
-  DALLOC(h->d_cata, 2);  // [0] catastrophe, [1] a tensor-core wait gave up
+  DALLOC(h->d_cata, 3);  // [0] catastrophe, [1] a tensor-core wait gave up, [2] Wannier count
+  for (int it = 0; it < p.ntype; ++it)
+    if (p.lwfc[it] > 0) h->lwannier = true;
+  if (h->lwannier) {
+    DALLOC(h->d_lwfc, NT);
+    DALLOC(h->d_mu_wfc, n);
+    CK(cudaMemcpyAsync(h->d_lwfc, p.lwfc, sizeof(int) * NT, cudaMemcpyHostToDevice, h->st));
+    if (p.rcut_wfc >= h->L.rskinsq) {
+      h->err = "rcut_wfc (a squared distance) must be below the squared list cutoff";
+      return MDFF_ERR_BAD_ARGS;
+    }
+  }
   DALLOC(h->d_ekin_part, cdiv(n, 256));
   CK(cudaMallocHost((void**)&h->h_scal, sizeof(double) * S_NSCAL));
-  CK(cudaMallocHost((void**)&h->h_cata, 2 * sizeof(int)));
+  CK(cudaMallocHost((void**)&h->h_cata, 3 * sizeof(int)));
   CK(cudaStreamSynchronize(h->st));
   return MDFF_OK;
 }
@@ -2200,7 +2227,8 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_hist, h->d_E, h->d_r, h->d_z, h->d_pv, h->d_qv, h->d_Tp, h->d_mu32, h->d_force,
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
-                  h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2};
+                  h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
+                  h->d_lwfc, h->d_mu_wfc};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);

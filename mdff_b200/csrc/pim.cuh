@@ -280,14 +280,72 @@ __global__ void k_copy1(double* __restrict__ dst, const double* __restrict__ src
   if (threadIdx.x == 0 && blockIdx.x == 0) *dst = *src;
 }
 
-// mu_tot = dipia + mu_ind ; catastrophe flag if any component > 10
-// (moment_from_pola.f90:176-178: positive components only)
+// moment_from_WFc (moment_from_pola.f90:632-807), warp per ion over its
+// (full, ascending) neighbour row: every ion of a type with lwfc >= 0 sums
+// r_j - r_i (minimum image, the reference's two-rounding arithmetic) over
+// the Wannier centres j (lwfc < 0) with |r_ij|^2 < rcut_wfc, in ascending j as
+// the reference does; mu_wfc = -2 sum.  An ion of a type with lwfc > 0 that
+// finds a different number of centres sets *bad (the reference STOPs).
+__global__ void k_wfc_dipoles(const double4* __restrict__ s, const int* __restrict__ itype,
+                              const int* __restrict__ lwfc, const int* __restrict__ nbr,
+                              const int* __restrict__ nnb, int cap, int natm,
+                              const CellC* __restrict__ cell, double rcut_wfc,
+                              double4* __restrict__ mu_wfc, int* __restrict__ bad) {
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= natm) return;
+  const int lw = lwfc[itype[i]];
+  if (lw < 0) {
+    if (lane == 0) mu_wfc[i] = make_double4(0, 0, 0, 0);
+    return;
+  }
+  const double4 si = s[i];
+  const int n = nnb[i];
+  double ax = 0.0, ay = 0.0, az = 0.0;
+  int cnt = 0;
+  for (int k0 = 0; k0 < n; k0 += 32) {
+    int k = k0 + lane;
+    bool hit = false;
+    double rx = 0.0, ry = 0.0, rz = 0.0;
+    if (k < n) {
+      int j = nbr[(size_t)i * cap + k];
+      if (lwfc[itype[j]] < 0) {
+        double4 sj = s[j];
+        double r2 = min_image_exact(cell->A, xsub(sj.x, si.x), xsub(sj.y, si.y), xsub(sj.z, si.z), rx, ry, rz);
+        hit = r2 < rcut_wfc;
+      }
+    }
+    unsigned m = __ballot_sync(FULL_MASK, hit);
+    while (m) {  // in ascending neighbour order
+      int l = __ffs(m) - 1;
+      m &= m - 1;
+      double x = __shfl_sync(FULL_MASK, rx, l), y = __shfl_sync(FULL_MASK, ry, l),
+             z = __shfl_sync(FULL_MASK, rz, l);
+      ax = ax + x;
+      ay = ay + y;
+      az = az + z;
+      cnt++;
+    }
+  }
+  if (lane == 0) {
+    mu_wfc[i] = make_double4(-2.0 * ax, -2.0 * ay, -2.0 * az, 0.0);
+    if (lw > 0 && cnt != lw) atomicExch(bad, 1);
+  }
+}
+
+// mu_tot = (dipia + mu_ind) [+ mu_wfc] ; catastrophe flag if any component > 10
+// (moment_from_pola.f90:136-147, 176-178: positive components only)
 __global__ void k_mu_total(const double4* __restrict__ dip, const double4* __restrict__ mu_ind,
-                           int natm, double4* __restrict__ mu_tot, int* __restrict__ flag) {
+                           const double4* __restrict__ mu_wfc, int natm, double4* __restrict__ mu_tot,
+                           int* __restrict__ flag) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   double4 a = dip[i], b = mu_ind[i];
   double4 m = make_double4(a.x + b.x, a.y + b.y, a.z + b.z, 0.0);
+  if (mu_wfc) {
+    double4 w = mu_wfc[i];
+    m = make_double4(m.x + w.x, m.y + w.y, m.z + w.z, 0.0);
+  }
   mu_tot[i] = m;
   if (m.x > 10.0 || m.y > 10.0 || m.z > 10.0) atomicExch(flag, 1);
 }

@@ -173,6 +173,13 @@ inline int setup_system(const mdff_params* pin, const double* cellA, Setup& S, c
       return MDFF_ERR_BAD_ARGS;
     }
   }
+  // Wannier-centre types after all other types: the reference's list of
+  // centres per ion (moment_from_pola.f90:718-722) assumes it
+  for (int it = 1; it < p.ntype; ++it)
+    if (p.lwfc[it - 1] < 0 && p.lwfc[it] >= 0) {
+      *err = "Wannier-centre types (lwfc < 0) must come after all other types";
+      return MDFF_ERR_BAD_ARGS;
+    }
   int ntype = p.ntype, n = p.natm;
   if (p.symmetric_pot_nb) {
     sym2(p.epslj, ntype); sym2(p.sigmalj, ntype); sym2(p.plj, ntype); sym2(p.qlj, ntype);

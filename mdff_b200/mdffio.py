@@ -177,9 +177,10 @@ def write_dipff(path, system, cell, names, natmi, mu):
             f.write(f"{i + 1:8d}  {names[typ[i]]:3s}" + "".join(fortran_e(v) for v in mu[i]) + "\n")
 
 
-def write_efgall(path, system, cell, names, natmi, efg):
+def write_efgall(path, system, cell, names, natmi, efg, lwfc=None):
     """EFGALL, formatted variant (iefgall_format /= 0, field.f90:392-448):
-    vxx vyy vzz vxy vxz vyz per ion; efg is (natm, 3, 3) or (natm, 9)."""
+    vxx vyy vzz vxy vxz vyz per ion; efg is (natm, 3, 3) or (natm, 9).  Ions
+    of Wannier-centre types (lwfc < 0 per type) are left out (field.f90:422)."""
     A = np.asarray(cell, dtype=np.float64)
     v = np.asarray(efg, dtype=np.float64).reshape(-1, 3, 3)
     typ = np.repeat(np.arange(len(names)), natmi)
@@ -188,6 +189,8 @@ def write_efgall(path, system, cell, names, natmi, efg):
         f.write("      ia type                   vxx                     vyy                     vzz"
                 "                     vxy                     vxz                     vyz\n")
         for i in range(v.shape[0]):
+            if lwfc is not None and lwfc[typ[i]] < 0:
+                continue
             e = v[i]
             vals = (e[0, 0], e[1, 1], e[2, 2], e[0, 1], e[0, 2], e[1, 2])
             f.write(f"{i + 1:8d}  {names[typ[i]]:3s}" + "".join(fortran_e(x) for x in vals) + "\n")
@@ -469,6 +472,13 @@ def params_from_namelists(nl, natmi, **extra):
         kw["algo_ext_dipole"] = _EXT[a]
     if "omegako" in pm:
         kw["omegakO"] = float(pm["omegako"])
+    if "lwfc" in pm:  # Wannier centres (pim.f90:93-96)
+        t = _table(pm["lwfc"], 1, ntype)
+        kw["lwfc"] = [int(t.get((i,), 0)) for i in range(ntype)]
+    if "ldip_wfc" in pm:
+        kw["ldip_wfc"] = int(bool(pm["ldip_wfc"]))
+    if "rcut_wfc" in pm:
+        kw["rcut_wfc"] = float(pm["rcut_wfc"])
     if "ldip_polar" in pm:
         t = _table(pm["ldip_polar"], 1, ntype)
         kw["ldip_polar"] = [int(bool(t.get((i,), False))) for i in range(ntype)]
@@ -568,6 +578,11 @@ def write_control(path, p, names, masses=None, calc="md", extra_md=None):
     L.append(f"  algo_moment_from_pola = '{_ALGO_NAME[p.algo_moment_from_pola]}'")
     L.append(f"  algo_ext_dipole = '{'poly' if p.algo_ext_dipole == _abi.EXT_POLY else 'aspc'}'")
     L.append(f"  omegakO = {_f(p.omegakO)}")
+    if any(p.lwfc[it] != 0 for it in range(nt)):
+        L.append(f"  ldip_wfc = {'.true.' if p.ldip_wfc else '.false.'}")
+        L.append(f"  rcut_wfc = {_f(p.rcut_wfc)}")
+        for it in range(nt):
+            L.append(f"  lwfc({it + 1}) = {p.lwfc[it]}")
     for it in range(nt):
         if p.ldip_polar[it]:
             L.append(f"  ldip_polar({it + 1}) = .true.")

@@ -14,7 +14,7 @@ numpy arrays.  New ``&gputag`` keywords: precision, solver, cg_tol,
 cg_max_iter, fail_on_nonconvergence, device, wall24.  Thole functions:
 thole_type (MDFF_THOLE_*) and thole_param (per ordered type pair).  Dipole
 algorithms: algo_moment_from_pola (MDFF_ALGO_*), algo_ext_dipole (MDFF_EXT_*)
-and omegakO.
+and omegakO.  Wannier centres: lwfc (per type), ldip_wfc, rcut_wfc.
 """
 import numpy as np
 
@@ -33,7 +33,7 @@ _DEFAULTS = dict(
     # &pimtag
     conv_tol_ind=1e-6, min_scf_pol_iter=3, max_scf_pol_iter=100,
     extrapolate_order=0, symmetric_pot_pim=1, algo_moment_from_pola=_abi.ALGO_SCF,
-    algo_ext_dipole=_abi.EXT_ASPC, omegakO=0.7,
+    algo_ext_dipole=_abi.EXT_ASPC, omegakO=0.7, ldip_wfc=1, rcut_wfc=0.5,
     # &gputag
     precision=_abi.PREC_FP64, solver=_abi.SOLVER_SCF, cg_tol=0.0, cg_max_iter=200,
     fail_on_nonconvergence=0, device=0,
@@ -72,7 +72,7 @@ def make_params(natmi, **kw):
     # thole_param = 1.662 (coulomb.f90:175)
     kw.setdefault("thole_param", np.full((NT, NT), 1.662))
     unknown = set(kw) - set(_DEFAULTS) - set(_TABLE2) - set(_TABLE3) - {
-        "qch", "dip", "ldip_polar", "poldip", "poldip_iso"}
+        "qch", "dip", "ldip_polar", "poldip", "poldip_iso", "lwfc"}
     if unknown:
         raise KeyError(f"unknown keywords: {sorted(unknown)}")
     for k, v in _DEFAULTS.items():
@@ -90,6 +90,7 @@ def make_params(natmi, **kw):
         dt = np.int32 if name in ("ldip_damping", "pol_damp_k") else np.float64
         _fill(getattr(p, name), kw.get(name), (NT, NT, NT), dt)
     _fill(p.ldip_polar, kw.get("ldip_polar"), (NT,), np.int32)
+    _fill(p.lwfc, kw.get("lwfc"), (NT,), np.int32)
     pol = np.zeros((NT, 3, 3))
     if kw.get("poldip") is not None:
         src = kw["poldip"]

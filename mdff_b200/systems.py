@@ -312,6 +312,33 @@ def random_ionic(n_per_type=(20, 20), L=14.0, seed=7, q=(1.5, -1.5), pol=(0.0, 1
     return System("random_ionic", p, cell, pos, mass, vel, dict(L=L, seed=seed))
 
 
+def wannier_box(n_pairs=16, L=9.0, seed=31, nwfc=4, d_wfc=0.35, pol_cation=0.5, **extra):
+    """Seeded box with Wannier centres (pim.f90:93-96): n_pairs cations M (+2,
+    polarisable, lwfc 0) and anions O (+6, lwfc = nwfc), each O carrying nwfc
+    centres W (-2, lwfc -1) at d_wfc A along tetrahedral directions jittered
+    by 0.05 A; types in the order M, O, W (centres last)."""
+    rng = np.random.default_rng(seed)
+    base = rsi(rng, [n_pairs, n_pairs], L, [[2.4, 2.2], [2.2, 2.6]])
+    tet = np.array([[1, 1, 1], [1, -1, -1], [-1, 1, -1], [-1, -1, 1]], dtype=np.float64) / np.sqrt(3.0)
+    w = []
+    for o in base[n_pairs:]:
+        for k in range(nwfc):
+            v = tet[k % 4] * d_wfc + rng.uniform(-0.05, 0.05, 3)
+            w.append(o + v)
+    pos = np.concatenate([base, np.array(w)]) % L
+    cell = np.eye(3) * L
+    rc = 0.45 * L
+    kw = dict(lcoulomb=1, cutlongrange=rc, skindiff=0.5, qch=[2.0, 6.0, -2.0], alphaES=0.6,
+              kES=(8, 8, 8), ldip_polar=[1, 0, 0], poldip_iso={0: pol_cation},
+              lwfc=[0, nwfc, -1], conv_tol_ind=1e-11, max_scf_pol_iter=300)
+    kw.update(extra)
+    p = make_params([n_pairs, n_pairs, n_pairs * nwfc], **kw)
+    n = pos.shape[0]
+    mass = np.full(n, 20.0)
+    vel = np.zeros((n, 3))
+    return System("wannier_box", p, cell, pos, mass, vel, dict(L=L, seed=seed))
+
+
 # --------------------------------------------------------------------------
 # batched workloads: many small independent boxes
 

@@ -1744,6 +1744,42 @@ static void scf_ko_v4_1(pim_env* e, double* mu, double* u_pol, int* n_scf, doubl
   free(A);
 }
 
+/* moment_from_WFc (moment_from_pola.f90:632-807): for every ion of a type
+   with lwfc >= 0, mu = -2 sum (r_j - r_i) over the Wannier centres j (types
+   with lwfc < 0) with |r_ij|^2 < rcut_wfc (the squared distance against
+   rcut_wfc itself, :710), minimum image through direct coordinates; an ion
+   of a type with lwfc > 0 must find lwfc centres (:731-737). */
+static int moment_from_wfc(or_ctx* c, const double* sx, const double* sy, const double* sz, double* mu) {
+  int natm = c->natm;
+  const double(*A)[3] = c->A;
+  for (int ia = 0; ia < natm; ++ia) {
+    int it = c->itype[ia];
+    if (c->p.lwfc[it] < 0) continue;
+    int cnt = 0;
+    double m[3] = {0.0, 0.0, 0.0};
+    for (int ja = 0; ja < natm; ++ja) {
+      if (c->p.lwfc[c->itype[ja]] >= 0) continue;
+      double ssx = sx[ja] - sx[ia], ssy = sy[ja] - sy[ia], ssz = sz[ja] - sz[ia];
+      ssx = ssx - fnint(ssx);
+      ssy = ssy - fnint(ssy);
+      ssz = ssz - fnint(ssz);
+      double rxij = ssx * A[0][0] + ssy * A[0][1] + ssz * A[0][2];
+      double ryij = ssx * A[1][0] + ssy * A[1][1] + ssz * A[1][2];
+      double rzij = ssx * A[2][0] + ssy * A[2][1] + ssz * A[2][2];
+      double rijsq = rxij * rxij + ryij * ryij + rzij * rzij;
+      if (rijsq < c->p.rcut_wfc) {
+        cnt++;
+        m[0] = m[0] + rxij;
+        m[1] = m[1] + ryij;
+        m[2] = m[2] + rzij;
+      }
+    }
+    if (c->p.lwfc[it] > 0 && cnt != c->p.lwfc[it]) return MDFF_ERR_BAD_ARGS;
+    for (int a = 0; a < 3; ++a) mu[3 * ia + a] = -2.0 * m[a];
+  }
+  return MDFF_OK;
+}
+
 int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz, int itime,
                 mdff_result* out, or_extra* ex) {
   int natm = c->natm;
@@ -1834,6 +1870,19 @@ int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
       free(qzero);
     }
     for (size_t i = 0; i < n3; ++i) mu[i] = c->dipia[i] + dipia_ind[i];
+    /* Wannier centres (moment_from_pola.f90:130-147, moment_from_WFc :632-807) */
+    if (status == MDFF_OK) {
+      int lwannier = 0;
+      for (int it = 0; it < c->p.ntype; ++it)
+        if (c->p.lwfc[it] > 0) lwannier = 1;
+      if (lwannier) {
+        double* mw = calloc(n3, sizeof(double));
+        status = moment_from_wfc(c, sx, sy, sz, mw);
+        if (status == MDFF_OK && c->p.ldip_wfc)
+          for (size_t i = 0; i < n3; ++i) mu[i] = mu[i] + mw[i];
+        free(mw);
+      }
+    }
     /* polarisation catastrophe (moment_from_pola.f90:176-216) */
     for (int ia = 0; ia < natm && status == MDFF_OK; ++ia)
       for (int a = 0; a < 3; ++a)

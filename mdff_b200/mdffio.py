@@ -177,6 +177,19 @@ def write_dipff(path, system, cell, names, natmi, mu):
             f.write(f"{i + 1:8d}  {names[typ[i]]:3s}" + "".join(fortran_e(v) for v in mu[i]) + "\n")
 
 
+def write_dipwfc(path, names, natmi, mu, lwfc):
+    """DIPWFC (lwrite_dip_wfc, moment_from_pola.f90:775-782): per ion of a type
+    with lwfc >= 0, the type label (a3) and its Wannier-centre dipole in
+    3e16.8; mu is the centres' dipoles (natm, 3)."""
+    mu = np.asarray(mu, dtype=np.float64).reshape(-1, 3)
+    typ = np.repeat(np.arange(len(names)), natmi)
+    with open(path, "w") as f:
+        for i in range(mu.shape[0]):
+            if lwfc[typ[i]] < 0:
+                continue
+            f.write(f"{names[typ[i]]:3.3s}" + "".join(fortran_e(v, 16, 8) for v in mu[i]) + "\n")
+
+
 def write_efgall(path, system, cell, names, natmi, efg, lwfc=None):
     """EFGALL, formatted variant (iefgall_format /= 0, field.f90:392-448):
     vxx vyy vzz vxy vxz vyz per ion; efg is (natm, 3, 3) or (natm, 9).  Ions

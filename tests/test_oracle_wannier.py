@@ -48,3 +48,13 @@ def test_wannier_keywords(tmp_path):
     assert list(r.lwfc[:3]) == [0, 4, -1] and r.ldip_wfc == 0 and r.rcut_wfc == 0.4
     d = mdffio.params_from_namelists({}, [2, 2])
     assert list(d.lwfc[:2]) == [0, 0] and d.ldip_wfc == 1 and d.rcut_wfc == 0.5
+
+
+def test_dipwfc_layout(tmp_path):
+    f = tmp_path / "DIPWFC"
+    mdffio.write_dipwfc(f, ["M", "O", "W"], [1, 1, 2], [[0, 0, 0], [0.25, -1.5e-3, 0.0], [0, 0, 0], [0, 0, 0]],
+                        [0, 4, -1])
+    lines = f.read_text().splitlines()
+    # '(a,3e16.8)': a3 label then three E16.8 fields; centres (lwfc < 0) left out
+    assert lines == ["M    0.00000000E+00  0.00000000E+00  0.00000000E+00",
+                     "O    0.25000000E+00 -0.15000000E-02  0.00000000E+00"]

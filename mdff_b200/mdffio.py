@@ -177,6 +177,47 @@ def write_dipff(path, system, cell, names, natmi, mu):
             f.write(f"{i + 1:8d}  {names[typ[i]]:3s}" + "".join(fortran_e(v) for v in mu[i]) + "\n")
 
 
+PRESS_UNIT = 0.00624150964712042   # GPa -> eV / A^3 (constants.f90:88)
+BOLTZ_UNIT = 8.61734229648141e-05   # eV / K (constants.f90:89)
+_OSZ_HEADER = ("     step      Time/Temp   Etot/Pressure    Ekin/Pvir_nb  Utot/Pvir_coul"
+               "      U_nb/Omega     U_coul/Htot")
+
+
+def thermo_nve(res, natm, omega, e_kin, temp, lreducedN=False):
+    """calc_thermo (thermo.f90:122-211) for an NVE run with no Morse, harmonic
+    or tail terms: the quantities write_thermo prints, from one engforce
+    result (u_lj, u_bmhft, u_coul, vir_lj, vir_bmhft, pvirial_coul), the cell
+    volume and the caller's kinetic energy (eV) and temperature (K).  With
+    lreducedN energies and virial pressures are per ion."""
+    nr = float(natm) if lreducedN else 1.0
+    u_lj_r, u_bmhft_r, u_coul_r = res["u_lj"] / nr, res["u_bmhft"] / nr, res["u_coul"] / nr
+    e_kin_r = e_kin / nr
+    u_tot = (u_lj_r + u_coul_r) + u_bmhft_r
+    e_tot = u_tot + e_kin_r
+    pv_lj_r = (res["vir_lj"] / omega) / nr
+    pv_bmhft_r = (res["vir_bmhft"] / omega) / nr
+    pv_coul_r = res["pvirial_coul"] / nr
+    pv_tot_r = (pv_lj_r + pv_coul_r) + pv_bmhft_r
+    pressure_tot_r = (pv_tot_r + float(natm) * temp * BOLTZ_UNIT / omega) / PRESS_UNIT
+    return dict(e_tot=e_tot, e_kin_r=e_kin_r, u_tot=u_tot, u_vdw_r=u_lj_r + u_bmhft_r, u_coul_r=u_coul_r,
+                temp_r=temp, pressure_tot_r=pressure_tot_r, pvirial_vdw_r=pv_lj_r + pv_bmhft_r,
+                pvirial_coul_r=pv_coul_r, pvirial_tot_r=pv_tot_r, omega=omega, h_tot=e_tot)
+
+
+def write_osziff(f, step, time_ps, th, oszcall):
+    """One write_thermo(..., 'osz') record (thermo.f90:370-385) into the open
+    file f: every tenth call a 110-dash separator, the column header and a
+    separator, then two lines I9,2X,6E16.8.  Returns the next oszcall."""
+    if oszcall % 10 == 0:
+        f.write("-" * 110 + "\n" + _OSZ_HEADER + "\n" + "-" * 110 + "\n")
+    row1 = (time_ps, th["e_tot"], th["e_kin_r"], th["u_tot"], th["u_vdw_r"], th["u_coul_r"])
+    row2 = (th["temp_r"], th["pressure_tot_r"], th["pvirial_vdw_r"], th["pvirial_coul_r"], th["omega"],
+            th["h_tot"])
+    for row in (row1, row2):
+        f.write(f"{int(step):9d}  " + "".join(fortran_e(v, 16, 8) for v in row) + "\n")
+    return oszcall + 1
+
+
 def write_dipwfc(path, names, natmi, mu, lwfc):
     """DIPWFC (lwrite_dip_wfc, moment_from_pola.f90:775-782): per ion of a type
     with lwfc >= 0, the type label (a3) and its Wannier-centre dipole in

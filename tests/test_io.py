@@ -194,3 +194,26 @@ def test_dipole_algorithm_keywords(tmp_path):
     for bad in ({"algo_moment_from_pola": "scf_kO_v9"}, {"algo_ext_dipole": "cubic"}):
         with pytest.raises(ValueError):
             mdffio.params_from_namelists({"pimtag": bad}, [2, 2])
+
+
+def test_osziff_record(tmp_path):
+    # calc_thermo (thermo.f90:122-211) for NVE and write_thermo 'osz' (:370-385)
+    res = dict(u_lj=0.0, u_bmhft=-120.5, u_coul=-3000.25, vir_lj=0.0, vir_bmhft=42.0, pvirial_coul=-0.125)
+    th = mdffio.thermo_nve(res, natm=100, omega=1000.0, e_kin=12.5, temp=300.0)
+    assert th["u_tot"] == (0.0 + -3000.25) + -120.5 and th["e_tot"] == th["u_tot"] + 12.5
+    assert th["h_tot"] == th["e_tot"]
+    pv = (0.0 + -0.125) + 42.0 / 1000.0
+    assert th["pressure_tot_r"] == (pv + 100.0 * 300.0 * mdffio.BOLTZ_UNIT / 1000.0) / mdffio.PRESS_UNIT
+    thr = mdffio.thermo_nve(res, natm=100, omega=1000.0, e_kin=12.5, temp=300.0, lreducedN=True)
+    assert thr["u_coul_r"] == -3000.25 / 100.0
+    f = tmp_path / "OSZIFF"
+    with open(f, "w") as fh:
+        k = 0
+        for step in (1, 2):
+            k = mdffio.write_osziff(fh, step, 0.001 * step, th, k)
+    lines = f.read_text().splitlines()
+    assert k == 2 and len(lines) == 3 + 4
+    assert lines[0] == "-" * 110 and lines[2] == "-" * 110 and lines[1].startswith("     step      Time/Temp")
+    assert lines[3] == ("        1    0.10000000E-02 -0.31082500E+04  0.12500000E+02 -0.31207500E+04"
+                        " -0.12050000E+03 -0.30002500E+04")
+    assert lines[4].startswith("        1    0.30000000E+03") and lines[4].endswith(" 0.10000000E+04 -0.31082500E+04")

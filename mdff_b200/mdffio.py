@@ -563,6 +563,22 @@ def params_from_namelists(nl, natmi, **extra):
 # mdff_params -> control file
 
 
+def load_deck(posff_path, control_path, include_dir=None, **extra):
+    """A reference run's inputs as the engine takes them: the control file's
+    namelists (with its posff_data, controltag) and the POSFF it names.
+    Returns dict(params, cell, pos (natm, 3), names, natmi, system[, vel,
+    force]); extra keywords override the control file's (e.g. precision)."""
+    nl = read_control(control_path, include_dir=include_dir)
+    posff_data = str(nl.get("controltag", {}).get("posff_data", "rnn")).lower()
+    d = read_posff(posff_path, posff_data=posff_data)
+    p = params_from_namelists(nl, d["natmi"], **extra)
+    out = dict(params=p, cell=d["cell"], pos=d["pos"], names=d["names"], natmi=d["natmi"], system=d["system"])
+    for k in ("vel", "force"):
+        if k in d:
+            out[k] = d[k]
+    return out
+
+
 def _f(x):
     return f"{float(x):.16e}".replace("e", "d")
 

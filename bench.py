@@ -96,47 +96,110 @@ def engine_params(s, precision, solver):
     return p
 
 
+def _physical_gpu(local_rank):
+    """The device index / UUID nvidia-smi and NVML know for this rank's GPU."""
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").strip()
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids):
+            return ids[local_rank]
+    return str(local_rank)
+
+
 class Clocks:
-    """nvidia-smi sampler running during the timed region."""
+    """SM clocks and clock-event reasons during the timed region: nvidia-smi
+    every 200 ms and, beside it, NVML read in-process every 5 ms (the timed
+    region of the default run is ~50 ms).  Reading only; nothing is set."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, gpu_index):
+        gpu = _physical_gpu(gpu_index)
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
-            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.Q}",
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu}", f"--query-gpu={self.Q}",
                                        "--format=csv,noheader,nounits", "-lms", "200"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        self.nv, self.nv_max, self.t = [], None, None
+        try:
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            h = (nv.nvmlDeviceGetHandleByUUID(gpu) if not gpu.isdigit()
+                 else nv.nvmlDeviceGetHandleByIndex(int(gpu)))
+            self.nv_max = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._nvml, self._halt = nv, threading.Event()
+
+            def loop():
+                while not self._halt.is_set():
+                    try:
+                        self.nv.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                        int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                    except Exception:
+                        return
+                    self._halt.wait(0.005)
+
+            self.t = threading.Thread(target=loop, daemon=True)
+            self.t.start()
+        except Exception:
+            self.t = None
+
+    def _stop_nvml(self):
+        if self.t is None:
+            return []
+        self._halt.set()
+        self.t.join(timeout=2.0)
+        try:
+            self._nvml.nvmlShutdown()
+        except Exception:
+            pass
+        nv, out = self._nvml, []
+        bits = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+                ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+                ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+                ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
+        for mhz, mask in list(self.nv):
+            out.append((mhz, {nm for nm, c in bits if mask & int(getattr(nv, c, 0))}))
+        return out
 
     def stop(self):
-        if self.p is None:
-            return None
-        self.p.terminate()
+        nvml = self._stop_nvml()
+        rows = []
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except Exception:
+                self.p.kill()
+            self.f.flush()
+            rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
         try:
-            self.p.wait(timeout=5)
-        except Exception:
-            self.p.kill()
-        self.f.flush()
-        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
-        os.unlink(self.f.name)
-        sm, mx, reasons = [], None, set()
+            os.unlink(self.f.name)
+        except OSError:
+            pass
+        sm, mx, reasons = [], self.nv_max, set()
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        n_smi = 0
         for r in rows:
             try:
                 sm.append(float(r[1]))
                 mx = float(r[2])
+                n_smi += 1
                 for nm, v in zip(names, r[5:9]):
                     if "Active" in v and "Not" not in v:
                         reasons.add(nm)
             except (ValueError, IndexError):
                 continue
+        for mhz, rs in nvml:
+            sm.append(mhz)
+            reasons |= rs
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "samples_nvidia_smi": n_smi, "samples_nvml": len(nvml)}
 
 
 def fire_relax(eng, pos, mass, iters, fmax_stop=0.5):

@@ -2217,6 +2217,9 @@ void mdff_gpu_destroy(mdff_handle h) {
     cudaEventDestroy(r.b);
   }
   cudaSetDevice(h->device);
+  // side-stream work of a call that returned early may still run
+  if (h->st_sr) cudaStreamSynchronize(h->st_sr);
+  if (h->st_rs) cudaStreamSynchronize(h->st_rs);
   if (h->st) cudaStreamSynchronize(h->st);
   void* ptrs[] = {h->d_cell, h->d_pos, h->d_s, h->d_itype, h->d_ipolar, h->d_q, h->d_qzero,
                   h->d_dipia, h->d_pol, h->d_invpol, h->d_nbtab, h->d_estab, h->L.nbr, h->L.nnb,

@@ -234,3 +234,23 @@ def test_load_deck_round_trip(tmp_path, oracle):
     f2 = np.stack([o2["fx"], o2["fy"], o2["fz"]], 1)
     assert np.abs(f1 - f2).max() <= 1e-9 * np.abs(f1).max()
     assert abs(o1["u_coul"] - o2["u_coul"]) <= 1e-9 * abs(o1["u_coul"])
+
+
+def test_load_deck_wannier_ko(tmp_path, oracle):
+    # Wannier centres and a kO dipole algorithm survive the deck round trip
+    from mdff_b200 import systems
+    s = systems.wannier_box(calc=_abi.CALC_OTHER, algo_moment_from_pola=_abi.ALGO_KO_V2,
+                            algo_ext_dipole=_abi.EXT_POLY, omegakO=0.6, conv_tol_ind=1e-10)
+    names = ["M", "O", "W"]
+    natmi = [s.params.natmi[t] for t in range(3)]
+    mdffio.write_control(tmp_path / "control.F", s.params, names, calc="efg")  # calc other than md / opt
+    mdffio.write_posff(tmp_path / "POSFF", "wfc", s.cell, names, natmi, s.pos)
+    d = mdffio.load_deck(tmp_path / "POSFF", tmp_path / "control.F")
+    p = d["params"]
+    assert (p.algo_moment_from_pola, p.algo_ext_dipole, p.omegakO) == (_abi.ALGO_KO_V2, _abi.EXT_POLY, 0.6)
+    assert list(p.lwfc[:3]) == [0, 4, -1]
+    o1 = oracle.Oracle(s.params, s.cell).engforce(*s.soa())
+    o2 = oracle.Oracle(p, d["cell"]).engforce(*(np.ascontiguousarray(d["pos"][:, a]) for a in range(3)))
+    assert o1["n_scf"] == o2["n_scf"]
+    assert np.abs(o1["mu"] - o2["mu"]).max() <= 1e-9 * np.abs(o1["mu"]).max()
+    assert abs(o1["u_coul"] - o2["u_coul"]) <= 1e-9 * abs(o1["u_coul"])

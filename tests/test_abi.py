@@ -44,3 +44,22 @@ def test_strerror_and_bad_args(lib):
     h = ctypes.c_void_p()
     # a NULL parameter block is rejected before any device work
     assert lib.mdff_gpu_create(None, None, ctypes.byref(h)) == _abi.MDFF_ERR_BAD_ARGS
+
+
+def test_c_consumer_sees_the_library_layouts(lib, tmp_path):
+    """A gcc-compiled C program (tests/c_abi/abi_layout.c) linked against the
+    library: C and the library agree on every ABI struct's size."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        pytest.skip("no C compiler")
+    here = os.path.dirname(os.path.abspath(__file__))
+    libdir = os.path.dirname(os.path.abspath(_abi.LIB_PATH))
+    exe = str(tmp_path / "abi_layout")
+    subprocess.run([gcc, "-std=c11", "-Wall", "-Werror", "-I", os.path.join(here, "..", "include"),
+                    os.path.join(here, "c_abi", "abi_layout.c"), "-L", libdir, "-lmdff_gpu",
+                    f"-Wl,-rpath,{libdir}", "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "layouts agree" in r.stdout

@@ -63,3 +63,40 @@ def test_c_consumer_sees_the_library_layouts(lib, tmp_path):
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "layouts agree" in r.stdout
+
+
+def _fortran_layout(block):
+    """(name, offset, size) of each field of a Fortran bind(c) derived type,
+    laid out by the C interoperability rules (natural alignment)."""
+    kinds = {"integer(c_int)": 4, "real(c_double)": 8, "type(c_ptr)": 8}
+    NT = _abi.NT
+    out, off = [], 0
+    for ln in block:
+        ln = ln.split("!")[0].strip()
+        if "::" not in ln:
+            continue
+        decl, names = (x.strip() for x in ln.split("::", 1))
+        w = kinds[decl.replace(" ", "").lower()]
+        for m in re.finditer(r"(\w+)\s*(\(([^)]*)\))?", names):
+            n = 1
+            if m.group(3):
+                for d in m.group(3).split(","):
+                    n *= NT if d.strip() == "NT" else int(d)
+            off = (off + w - 1) // w * w
+            out.append((m.group(1).lower(), off, w * n))
+            off += w * n
+    return out, (off + 7) // 8 * 8
+
+
+@pytest.mark.parametrize("tname,ctype", [("mdff_params", _abi.MdffParams), ("mdff_result", _abi.MdffResult)])
+def test_fortran_shim_type_matches_header(tname, ctype):
+    """The bind(c) derived types of the Fortran shim documented in
+    INTEGRATION.md have the header's fields, in order, at the header's
+    offsets, and the header's size."""
+    txt = open(os.path.join(os.path.dirname(HDR), "..", "INTEGRATION.md")).read().splitlines()
+    i0 = next(i for i, l in enumerate(txt) if re.match(rf"\s*TYPE, bind\(c\) :: {tname}\s*$", l))
+    i1 = next(i for i in range(i0, len(txt)) if txt[i].strip() == "END TYPE")
+    fields, size = _fortran_layout(txt[i0 + 1:i1])
+    ref = [(n.lower(), getattr(ctype, n).offset, getattr(ctype, n).size) for n, _ in ctype._fields_]
+    assert fields == ref
+    assert size == ctypes.sizeof(ctype)

@@ -49,20 +49,39 @@ def test_strerror_and_bad_args(lib):
 def test_c_consumer_sees_the_library_layouts(lib, tmp_path):
     """A gcc-compiled C program (tests/c_abi/abi_layout.c) linked against the
     library: C and the library agree on every ABI struct's size."""
-    import shutil
     import subprocess
-    gcc = shutil.which("gcc")
-    if gcc is None:
+    from .c_abi.build_host import compile_c
+    exe = compile_c("abi_layout", tmp_path)
+    if exe is None:
         pytest.skip("no C compiler")
-    here = os.path.dirname(os.path.abspath(__file__))
-    libdir = os.path.dirname(os.path.abspath(_abi.LIB_PATH))
-    exe = str(tmp_path / "abi_layout")
-    subprocess.run([gcc, "-std=c11", "-Wall", "-Werror", "-I", os.path.join(here, "..", "include"),
-                    os.path.join(here, "c_abi", "abi_layout.c"), "-L", libdir, "-lmdff_gpu",
-                    f"-Wl,-rpath,{libdir}", "-o", exe], check=True)
     r = subprocess.run([exe], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "layouts agree" in r.stdout
+
+
+def test_c_host_program_reaches_the_engine(lib, tmp_path):
+    """The C host driver (tests/c_abi/engforce_host.c) reads its inputs and
+    calls mdff_gpu_create; without a device that returns MDFF_ERR_NO_DEVICE
+    (the GPU run is in tests/test_gpu_c_host.py)."""
+    import subprocess
+    import numpy as np
+    from mdff_b200 import systems
+    from .c_abi.build_host import compile_c
+    exe = compile_c("engforce_host", tmp_path)
+    if exe is None:
+        pytest.skip("no C compiler")
+    s = systems.random_ionic((6, 6), L=9.0, seed=3, calc=_abi.CALC_OTHER)
+    (tmp_path / "p.bin").write_bytes(bytes(s.params))
+    np.ascontiguousarray(s.cell, dtype=np.float64).tofile(str(tmp_path / "c.bin"))
+    np.ascontiguousarray(np.concatenate(s.soa())).tofile(str(tmp_path / "x.bin"))
+    r = subprocess.run([exe, str(tmp_path / "p.bin"), str(tmp_path / "c.bin"), str(tmp_path / "x.bin"),
+                        str(tmp_path / "o.bin"), "1"], capture_output=True, text=True)
+    assert r.returncode in (0, _abi.MDFF_ERR_NO_DEVICE), r.stderr
+    # a truncated parameter file is refused before the library is called
+    (tmp_path / "q.bin").write_bytes(bytes(s.params)[:-8])
+    r = subprocess.run([exe, str(tmp_path / "q.bin"), str(tmp_path / "c.bin"), str(tmp_path / "x.bin"),
+                        str(tmp_path / "o.bin"), "1"], capture_output=True, text=True)
+    assert r.returncode == 102
 
 
 def _fortran_layout(block):

@@ -218,6 +218,32 @@ def write_osziff(f, step, time_ps, th, oszcall):
     return oszcall + 1
 
 
+def read_osziff(path):
+    """OSZIFF records (write_thermo 'osz', thermo.f90:370-385) as a dict of
+    arrays keyed like thermo_nve's output plus step and time; separator and
+    header lines are skipped."""
+    keys1 = ("time", "e_tot", "e_kin_r", "u_tot", "u_vdw_r", "u_coul_r")
+    keys2 = ("temp_r", "pressure_tot_r", "pvirial_vdw_r", "pvirial_coul_r", "omega", "h_tot")
+    rows = []
+    for ln in open(path).read().splitlines():
+        t = ln.split()
+        if len(t) != 7 or not t[0].isdigit():
+            continue
+        rows.append((int(t[0]), [float(x.replace("D", "E")) for x in t[1:]]))
+    if len(rows) % 2:
+        raise ValueError("OSZIFF: records come in pairs of lines")
+    out = {k: [] for k in ("step",) + keys1 + keys2}
+    for (s1, v1), (s2, v2) in zip(rows[0::2], rows[1::2]):
+        if s1 != s2:
+            raise ValueError("OSZIFF: the two lines of a record carry different steps")
+        out["step"].append(s1)
+        for k, v in zip(keys1, v1):
+            out[k].append(v)
+        for k, v in zip(keys2, v2):
+            out[k].append(v)
+    return {k: np.array(v) for k, v in out.items()}
+
+
 def write_dipwfc(path, names, natmi, mu, lwfc):
     """DIPWFC (lwrite_dip_wfc, moment_from_pola.f90:775-782): per ion of a type
     with lwfc >= 0, the type label (a3) and its Wannier-centre dipole in

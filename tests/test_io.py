@@ -217,6 +217,9 @@ def test_osziff_record(tmp_path):
     assert lines[3] == ("        1    0.10000000E-02 -0.31082500E+04  0.12500000E+02 -0.31207500E+04"
                         " -0.12050000E+03 -0.30002500E+04")
     assert lines[4].startswith("        1    0.30000000E+03") and lines[4].endswith(" 0.10000000E+04 -0.31082500E+04")
+    back = mdffio.read_osziff(f)
+    assert list(back["step"]) == [1, 2] and np.allclose(back["time"], [0.001, 0.002])
+    assert np.allclose(back["e_tot"], th["e_tot"], rtol=1e-8) and np.allclose(back["omega"], 1000.0)
 
 
 def test_load_deck_round_trip(tmp_path, oracle):

@@ -257,3 +257,71 @@ def test_load_deck_wannier_ko(tmp_path, oracle):
     assert o1["n_scf"] == o2["n_scf"]
     assert np.abs(o1["mu"] - o2["mu"]).max() <= 1e-9 * np.abs(o1["mu"]).max()
     assert abs(o1["u_coul"] - o2["u_coul"]) <= 1e-9 * abs(o1["u_coul"])
+
+
+def _random_params(rng):
+    from mdff_b200.params import make_params
+    nt = int(rng.integers(1, 5))
+    natmi = [int(rng.integers(1, 6)) for _ in range(nt)]
+
+    def tab2():
+        return {(i, j): float(rng.uniform(0.5, 3.0)) for i in range(nt) for j in range(nt)}
+
+    def tab3(lo, hi, integer=False):
+        return {(i, j, k): (int(rng.integers(lo, hi)) if integer else float(rng.uniform(lo, hi)))
+                for i in range(nt) for j in range(nt) for k in range(nt)}
+
+    kw = dict(lcoulomb=int(rng.integers(0, 2)), lbmhft=int(rng.integers(0, 2)), lbmhftd=int(rng.integers(0, 2)),
+              lnmlj=int(rng.integers(0, 2)), lsurf=int(rng.integers(0, 2)),
+              cutshortrange=float(rng.uniform(4, 8)), cutlongrange=float(rng.uniform(4, 8)),
+              skindiff=float(rng.uniform(0.1, 1.0)), qch=[float(rng.uniform(-2, 2)) for _ in range(nt)],
+              epslj=tab2(), sigmalj=tab2(), plj=tab2(), qlj=tab2(), Abmhftd=tab2(), Bbmhftd=tab2(),
+              Cbmhftd=tab2(), Dbmhftd=tab2(), BDbmhftd=tab2(), trunc=int(rng.integers(0, 3)),
+              alphaES=float(rng.uniform(0.2, 0.8)), kES=tuple(int(x) for x in rng.integers(3, 12, 3)),
+              lautoES=int(rng.integers(0, 2)), epsw=float(10 ** rng.uniform(-8, -4)),
+              ldip_polar=[int(rng.integers(0, 2)) for _ in range(nt)],
+              poldip_iso={i: float(rng.uniform(0.5, 2)) for i in range(nt)},
+              ldip_damping=tab3(0, 2, True), pol_damp_b=tab3(1, 5), pol_damp_c=tab3(0.5, 2),
+              pol_damp_k=tab3(1, 5, True), conv_tol_ind=float(10 ** rng.uniform(-12, -5)),
+              min_scf_pol_iter=int(rng.integers(1, 5)), max_scf_pol_iter=int(rng.integers(10, 100)),
+              extrapolate_order=int(rng.integers(0, 5)), symmetric_pot_nb=0, symmetric_pot_pim=0,
+              algo_moment_from_pola=int(rng.choice([0, 1, 2, 4])), algo_ext_dipole=int(rng.integers(0, 2)),
+              omegakO=float(rng.uniform(0.3, 0.9)), thole_type=int(rng.integers(0, 2)), thole_param=tab2(),
+              lwfc=[0] * (nt - 1) + [int(rng.choice([0, 4]))] if nt == 1 else
+              [0] * (nt - 2) + [int(rng.choice([0, 4])), int(rng.choice([0, -1]))],
+              ldip_wfc=int(rng.integers(0, 2)), rcut_wfc=float(rng.uniform(0.2, 0.8)))
+    return make_params(natmi, **kw), natmi
+
+
+def test_control_file_round_trip_random(tmp_path):
+    """write_control -> read_control -> params_from_namelists reproduces every
+    field the reference reads, over seeded random parameter sets (asymmetric
+    tables with symmetric_pot off).  Not compared: entries the reference never
+    reads (damping b, c, k where ldip_damping is off; thole_param with Thole
+    off or outside the types; the Wannier cut-off and switch without centres)
+    and wall24, an engine extension a reference deck cannot carry."""
+    rng = np.random.default_rng(2029)
+    for trial in range(25):
+        p, natmi = _random_params(rng)
+        nt = len(natmi)
+        f = tmp_path / f"control{trial}.F"
+        mdffio.write_control(f, p, [f"T{i}" for i in range(nt)], calc="efg")
+        q = mdffio.params_from_namelists(mdffio.read_control(f), natmi)
+        damp = np.ctypeslib.as_array(p.ldip_damping) != 0
+        for name, _ in p._fields_:
+            if name in ("calc", "wall24"):
+                continue
+            a, b = getattr(p, name), getattr(q, name)
+            if hasattr(a, "_length_"):
+                a, b = np.ctypeslib.as_array(a), np.ctypeslib.as_array(b)
+                if name in ("pol_damp_b", "pol_damp_c", "pol_damp_k"):
+                    a, b = a[damp], b[damp]
+                if name == "thole_param":
+                    if p.thole_type == _abi.THOLE_NONE:
+                        continue
+                    a, b = a[:nt, :nt], b[:nt, :nt]
+                assert np.array_equal(a, b), (trial, name)
+            else:
+                if name in ("ldip_wfc", "rcut_wfc") and not any(p.lwfc[t] for t in range(nt)):
+                    continue
+                assert a == b, (trial, name, a, b)

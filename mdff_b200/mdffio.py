@@ -467,7 +467,10 @@ def params_from_namelists(nl, natmi, **extra):
     the path (Morse, direct Coulomb, quadrupoles) raise ValueError.  Thole
     functions (coulombtag: thole_functions, thole_function_type, thole_param)
     follow coulomb_check_tag (coulomb.f90:228-234): expon1 / expon2 / gauss
-    replace every thole_param by 0.572 / 1.9088 / 0.957."""
+    replace every thole_param by 0.572 / 1.9088 / 0.957.  pimtag's
+    algo_moment_from_pola, algo_ext_dipole, omegakO (pim.f90:85-131) and the
+    Wannier-centre keywords lwfc, ldip_wfc, rcut_wfc (:93-136) map onto their
+    fields; extra keywords (e.g. the engine's precision, solver) override."""
     ntype = len(natmi)
     c = nl.get("controltag", {})
     fd = nl.get("fieldtag", {})

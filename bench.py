@@ -33,6 +33,8 @@ sys.path.insert(0, ROOT)
 from mdff_b200 import replicas  # noqa: E402
 
 DT_FS = 1.0
+# the headline metric, printed identically by both arms
+METRIC = "PIM+Ewald steps/s @12k ions: mixed vs FP64 GPU (F err\u22641e-5), vs CPU host"
 
 
 def parse():
@@ -51,6 +53,8 @@ def parse():
     ap.add_argument("--drift-steps", type=int, default=5000, help="NVE steps for the energy drift")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-evaluation measurement")
     ap.add_argument("--no-fit", action="store_true", help="skip the fitting-gradient measurement")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the MgO 8,000 and NaCl 1,728 records")
     return ap.parse_args()
 
 
@@ -409,6 +413,8 @@ def run_ours(args, rank, world, local_rank):
     extra["stats"] = eng.stats()
     extra["_cpu_point"] = (soa, hist, itime)
     eng.close()
+    if not args.no_cpu:
+        extra["_at_point"] = gpu_at_point(s, hist, itime, soa, local_rank)
     return res, extra
 
 
@@ -448,21 +454,28 @@ def run_e2e_loop(extra, eng, s, soa, vel, itime, ne, l2buf, dt):
     invm_h = 1.0 / s.mass
     r0 = eng.engforce(rx, ry, rz, itime=itime, want_ef=False)
     f = np.stack([r0["fx"], r0["fy"], r0["fz"]])
-    e_ms = []
+    e_ms, wall = [], []
     for k in range(ne):
+        flush_l2(l2buf)
+        torch.cuda.synchronize()
+        # wall clock of one whole step as a host caller runs it: kick + drift on
+        # the host, the ABI call (positions in, forces and dipoles out), kick
+        t0 = time.perf_counter()
         v_h += 0.5 * dt * f * invm_h
         rx += dt * v_h[0]
         ry += dt * v_h[1]
         rz += dt * v_h[2]
-        flush_l2(l2buf)
-        torch.cuda.synchronize()
         itime += 1
         r = eng.engforce(rx, ry, rz, itime=itime, want_ef=False)
-        e_ms.append(eng.stats()["ms_last"])
         f = np.stack([r["fx"], r["fy"], r["fz"]])
         v_h += 0.5 * dt * f * invm_h
-    extra["e2e"] = {"value": 1e3 / float(np.mean(e_ms)), "unit": "steps/s",
-                    "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 3 * n * 8 * 2 + 8 * 7 + 8 * 27}
+        wall.append(time.perf_counter() - t0)
+        e_ms.append(eng.stats()["ms_last"])
+    extra["e2e"] = {"value": ne / float(np.sum(wall)), "unit": "steps/s",
+                    "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 3 * n * 8 * 2 + 8 * 7 + 8 * 27,
+                    "timing": "host wall clock (perf_counter) per step: host integrator + "
+                              "mdff_gpu_engforce with host arrays",
+                    "device_span_value": 1e3 / float(np.mean(e_ms))}
 
 
 
@@ -470,10 +483,20 @@ def dist_barrier(world):
     replicas.barrier(world)
 
 
+def host_cores(threads):
+    """Threads the CPU leg used and what the host offers."""
+    try:
+        aff = len(os.sched_getaffinity(0))
+    except AttributeError:
+        aff = None
+    return {"cores": threads, "host_cpus": os.cpu_count(), "host_cpus_usable": aff}
+
+
 def cpu_baseline_sample(s, hist, itime, pos_soa):
     """Oracle (C restatement of the reference engforce, OpenMP over all host
     threads): one warm-start engforce (SCF, ASPC history from the GPU run) of
-    the same workload = one MD step of the reference algorithm."""
+    the same workload = one MD step of the reference algorithm.  Its result is
+    also the FP64 reference the GPU engines' errors are stated against."""
     from oracle import oracle as O
     from mdff_b200.params import params_copy
     o = O.Oracle(params_copy(s.params), s.cell)
@@ -481,7 +504,38 @@ def cpu_baseline_sample(s, hist, itime, pos_soa):
     t = time.perf_counter()
     r = o.engforce(*pos_soa, itime=itime)
     dt_s = time.perf_counter() - t
-    return dt_s, r["n_scf"], O.lib().or_get_threads()
+    return dt_s, r["n_scf"], O.lib().or_get_threads(), r
+
+
+def gpu_at_point(s, hist, itime, soa, local_rank):
+    """One engforce of the FP64 engine (the reference's SCF) and of the mixed
+    engine (CG) at a trajectory point, both with the run's ASPC history: the
+    results compared with the oracle's at the same point."""
+    from mdff_b200.engine import ForceEngine
+    out = {}
+    for tag, prec, solver in (("fp64_scf", "fp64", "scf"), ("mixed", "mixed", "cg")):
+        p = engine_params(s, prec, solver)
+        p.device = local_rank
+        with ForceEngine(p, s.cell) as e:
+            e.set_aspc_history(hist)
+            r = e.engforce(*soa, itime=itime)
+            r["n_iter"] = e.stats()["n_pol_iter"]
+        out[tag] = r
+    return out
+
+
+def errors_vs_oracle(g, o):
+    """Relative errors of a GPU result g against the oracle's o: RMS and max
+    over the forces, RMS over the dipoles, total energy."""
+    fg = np.stack([g["fx"], g["fy"], g["fz"]], 1)
+    fo = np.stack([o["fx"], o["fy"], o["fz"]], 1)
+    ug = g["u_coul"] + g["u_bmhft"] + g["u_lj"]
+    uo = o["u_coul"] + o["u_bmhft"] + o["u_lj"]
+    mo = float((o["mu"] ** 2).sum())
+    return {"force_rms_rel": float(np.sqrt(((fg - fo) ** 2).sum() / (fo ** 2).sum())),
+            "force_max_rel": float(np.abs(fg - fo).max() / np.abs(fo).max()),
+            "dipole_rms_rel": float(np.sqrt(((g["mu"] - o["mu"]) ** 2).sum() / mo)) if mo > 0 else 0.0,
+            "energy_rel": float(abs(ug - uo) / abs(uo))}
 
 
 KCLS = ("list_build", "short_range", "real_space_field", "real_space_force",
@@ -558,17 +612,97 @@ def run_reference(args, rank, world):
     tot = sum(times)
     val = args.steps / tot
     cores = O.lib().or_get_threads()
-    line = {"metric": "PIM+Ewald MD steps/s @12k ions", "impl": "reference", "value": val,
+    line = {"metric": METRIC, "impl": "reference", "value": val,
             "unit": "steps/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
             "config": dict(wl, solver="scf (reference algorithm)", precision="fp64"),
-            "cpu_baseline": {"value": val, "unit": "steps/s", "cores": cores, "kind": "port",
-                             "sample": f"{args.steps} MD steps (velocity Verlet, warm ASPC) of the "
-                                       f"{wl['natm']}-ion workload, C restatement of engforce, "
-                                       f"OpenMP {cores} threads"},
+            "cpu_baseline": dict({"value": val, "unit": "steps/s", "kind": "port",
+                                  "sample": f"{args.steps} MD steps (velocity Verlet, warm ASPC) of the "
+                                            f"{wl['natm']}-ion workload, C restatement of engforce, "
+                                            f"OpenMP {cores} threads"}, **host_cores(cores)),
             "e2e": {"value": val, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_config_record(name, local_rank, l2buf, steps=20, warmup=5, fp64_steps=10, cpu=True):
+    """One of the other single-box workloads (MgO 8,000 ions, NaCl 1,728 ions)
+    from its seeded lattice start: velocity-Verlet MD steps/s of the mixed
+    engine and of the FP64 engine (the reference's SCF; FP64 + CG too when
+    the ions are polarisable), device-timed with L2 flushed before each step;
+    at the last configuration, one engforce of each engine and, with cpu, one
+    warm-start oracle engforce (the CPU figure of this workload) against which
+    their errors are stated."""
+    import torch
+    from mdff_b200 import systems
+    from mdff_b200.engine import ForceEngine
+    dev = torch.device("cuda", local_rank)
+    s, wl = make_system(name)
+    pim = bool(s.params.ldip_polar[1])
+    dt = DT_FS * 1e-3 * systems.TIME_UNIT
+    pos = torch.tensor(np.ascontiguousarray(s.pos.T), dtype=torch.float64, device=dev).contiguous()
+    vel = torch.tensor(np.ascontiguousarray(s.vel.T), dtype=torch.float64, device=dev).contiguous()
+    invm = torch.tensor(1.0 / s.mass, dtype=torch.float64, device=dev)
+    out = {"config": dict(wl, start=f"seeded rock-salt lattice + jitter, Maxwell velocities "
+                                     f"(seed {s.info['seed']})")}
+    if "epsw" in s.info:
+        out["config"]["epsw"] = s.info["epsw"]
+    p = engine_params(s, "mixed", "cg")
+    p.device = local_rank
+    eng = ForceEngine(p, s.cell)
+    itime = 0
+    for _ in range(warmup):
+        eng.md_nve(pos.data_ptr(), vel.data_ptr(), invm.data_ptr(), dt, 1, itime, energies=False)
+        itime += 1
+    ms, its = [], []
+    for _ in range(steps):
+        flush_l2(l2buf)
+        torch.cuda.synchronize()
+        eng.md_nve(pos.data_ptr(), vel.data_ptr(), invm.data_ptr(), dt, 1, itime, energies=False)
+        itime += 1
+        st = eng.stats()
+        ms.append(st["ms_last"])
+        its.append(st["n_pol_iter"])
+    out["mixed"] = {"steps_per_s": 1e3 / float(np.mean(ms)), "ms_per_step": float(np.mean(ms)),
+                    "cg_iters_mean": float(np.mean(its)), "nk": st["nk"], "kES": st["kES"]}
+    pos_h = pos.cpu().numpy()
+    soa = tuple(np.ascontiguousarray(pos_h[a]) for a in range(3))
+    hist = eng.aspc_history()
+    eng.close()
+    runs = [("fp64_scf", "fp64", "scf")] + ([("fp64_cg", "fp64", "cg")] if pim else [])
+    for tag, prec, solver in runs:
+        pe = engine_params(s, prec, solver)
+        pe.device = local_rank
+        with ForceEngine(pe, s.cell) as e2:
+            e2.set_aspc_history(hist)
+            p2, v2, it = pos.clone(), vel.clone(), itime
+            ms, its = [], []
+            for k in range(fp64_steps + 2):
+                flush_l2(l2buf)
+                torch.cuda.synchronize()
+                e2.md_nve(p2.data_ptr(), v2.data_ptr(), invm.data_ptr(), dt, 1, it, energies=False)
+                it += 1
+                if k >= 2:
+                    st = e2.stats()
+                    ms.append(st["ms_last"])
+                    its.append(st["n_pol_iter"])
+        out[tag] = {"steps_per_s": 1e3 / float(np.mean(ms)), "ms_per_step": float(np.mean(ms)),
+                    "iters_mean": float(np.mean(its))}
+    for tag in [r[0] for r in runs]:
+        out["speedup_mixed_vs_" + tag] = out["mixed"]["steps_per_s"] / out[tag]["steps_per_s"]
+    if cpu:
+        at = gpu_at_point(s, hist, itime, soa, local_rank)
+        dt_s, nscf, cores, ro = cpu_baseline_sample(s, hist, itime, soa)
+        out["cpu_baseline"] = dict({"value": 1.0 / dt_s, "unit": "steps/s", "kind": "port",
+                                    "sample": f"one warm-start engforce (= one MD step, {nscf} SCF "
+                                              f"iterations) at the last configuration"},
+                                   **host_cores(cores))
+        out["vs_oracle"] = {
+            "fp64_scf": dict(errors_vs_oracle(at["fp64_scf"], ro), scf_iters=at["fp64_scf"]["n_iter"],
+                             oracle_scf_iters=nscf),
+            "mixed": dict(errors_vs_oracle(at["mixed"], ro), cg_iters=at["mixed"]["n_iter"])}
+    torch.cuda.synchronize()
+    return out
 
 
 def run_batch_bench(local_rank, cpu=True):
@@ -710,7 +844,7 @@ def main():
     if rank == 0:
         wl = res["wl"]
         line = {
-            "metric": "PIM+Ewald MD steps/s @12k ions (mixed FP32/FP64 engine)",
+            "metric": METRIC,
             "value": res["value"], "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
@@ -723,7 +857,7 @@ def main():
             "gpu_launches": int(res["launches"]),
             "clocks": res["clocks"],
         }
-        line.update({k: v for k, v in extra.items() if k not in ("stats", "_cpu_point")})
+        line.update({k: v for k, v in extra.items() if not k.startswith("_") and k != "stats"})
         if "fp64_scf_steps_per_s" in extra:
             line["speedup_vs_fp64_scf"] = res["value"] / world / extra["fp64_scf_steps_per_s"]
             line["speedup_vs_fp64_cg"] = res["value"] / world / extra["fp64_cg_steps_per_s"]
@@ -731,12 +865,27 @@ def main():
         if world == 1 and not args.no_cpu:
             s, _ = make_system(args.workload)
             soa, hist, itime = extra["_cpu_point"]
-            dt_s, nscf, cores = cpu_baseline_sample(s, hist, itime, soa)
-            line["cpu_baseline"] = {
-                "value": 1.0 / dt_s, "unit": "steps/s", "cores": cores, "kind": "port",
+            dt_s, nscf, cores, ro = cpu_baseline_sample(s, hist, itime, soa)
+            line["cpu_baseline"] = dict({
+                "value": 1.0 / dt_s, "unit": "steps/s", "kind": "port",
                 "sample": f"one warm-start engforce (= one MD step, SCF to 1e-8, {nscf} iterations) "
                           f"of the {wl['natm']}-ion workload at the GPU run's last configuration; "
-                          f"C restatement of the reference engforce, OpenMP {cores} threads"}
+                          f"C restatement of the reference engforce, OpenMP {cores} threads"},
+                **host_cores(cores))
+            at = extra["_at_point"]
+            line["vs_oracle"] = {
+                "point": "the GPU run's last configuration, ASPC history of the run, calc md; "
+                         "oracle = C restatement of engforce (FP64, SCF to 1e-8)",
+                "oracle_scf_iters": nscf,
+                "fp64_scf": dict(errors_vs_oracle(at["fp64_scf"], ro), scf_iters=at["fp64_scf"]["n_iter"]),
+                "mixed": dict(errors_vs_oracle(at["mixed"], ro), cg_iters=at["mixed"]["n_iter"])}
+            line["force_err_rms_rel_vs_oracle"] = line["vs_oracle"]["mixed"]["force_rms_rel"]
+        if world == 1 and not args.no_configs and args.workload == "sio2":
+            import torch
+            l2buf = torch.zeros(256 * 2 ** 20 // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+            line["configs"] = {n: run_config_record(n, local_rank, l2buf, cpu=not args.no_cpu)
+                               for n in ("mgo", "nacl")}
+            del l2buf
         if world == 1 and not args.no_batch:
             line["batch"] = run_batch_bench(local_rank, cpu=not args.no_cpu)
         if world == 1 and not args.no_fit:

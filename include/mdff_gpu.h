@@ -259,11 +259,15 @@ int mdff_gpu_verlet_half_list(mdff_handle h, int which, const double* rx,
    fail or fragment that pool), or a utility that needs only the list and
    should not create an engine.  Host inputs / outputs as for
    mdff_gpu_verlet_half_list; params supplies natm, the cutoffs, skindiff,
-   lcoulomb (half-cell clamp of cutlongrange) and device.  Limits:
-   natm <= 32768 and list entries <= 4194304 (else MDFF_ERR_BAD_ARGS /
-   MDFF_ERR_LIST_OVERFLOW with a message on stderr).  The first call on a
-   device looks up the array's address.  Calls share the array: two calls
-   overlapping on the same GPU race. */
+   lcoulomb (half-cell clamp of cutlongrange) and device.  Limits of the
+   static array: natm <= 32768, list entries <= 4194304 and at most 4096
+   entries in one row; beyond any of them the call returns MDFF_ERR_BAD_ARGS
+   with a message on stderr (*n_out holds the entry count when the entry
+   limit was the one exceeded).  MDFF_ERR_LIST_OVERFLOW means only that
+   capacity is below *n_out: grow list and call again.  The first call on a
+   device looks up the array's address.  Every call shares the one array and
+   clears what it needs: two calls overlapping on the same GPU (from two
+   host threads) race on it. */
 int mdff_gpu_verlet_half_list_noalloc(const mdff_params* p, const double cell_A[9], int which,
                                       const double* rx, const double* ry, const double* rz,
                                       int* point, int* list, int capacity, int* n_out);
@@ -293,6 +297,17 @@ int mdff_gpu_efg(mdff_handle h, double* efg);
 #define MDFF_NKCLASS 7
 int mdff_gpu_profile(mdff_handle h, int enable);
 int mdff_gpu_kernel_times(mdff_handle h, double* ms, long long* launches, double* work);
+
+/* Test hook for the timeout path; no counterpart in the reference.  polls =
+   how many times the tensor-core structure factor of the mixed engine's CG
+   operator polls, before it gives up, the mbarrier that frees an operand
+   stage (each poll may suspend the thread for up to 1 us); polls < 0 restores
+   the default of 2^22.  With polls = 0 every such wait gives up at once: the
+   kernel stops issuing matrix products, waits with the default bound for the
+   products already issued, frees its tensor memory and returns, and the
+   engforce call returns MDFF_ERR_TIMEOUT.  The setting stays on the handle
+   until changed; the handle remains usable. */
+int mdff_gpu_set_tc_wait_limit(mdff_handle h, int polls);
 
 /* Measured FMA throughput of a device (TFLOP/s, FMA = 2 flops) for fp64 = 1
    (double) or 0 (float): a saturating register-resident FMA loop over every

@@ -129,6 +129,7 @@ SIGNATURES = {
                                                 _IP, _IP, _i, _IP]),
     "mdff_gpu_md_nve": (_i, [_P, _P, _P, _P, _d, _i, _i, _DP]),
     "mdff_gpu_profile": (_i, [_P, _i]),
+    "mdff_gpu_set_tc_wait_limit": (_i, [_P, _i]),
     "mdff_gpu_kernel_times": (_i, [_P, _DP, ctypes.POINTER(ctypes.c_longlong), _DP]),
     "mdff_gpu_peak_flops": (_i, [_i, _i, _DP]),
     "mdff_gpu_efg": (_i, [_P, _DP]),

@@ -151,7 +151,8 @@ struct mdff_ctx {
   size_t part_cap = 0;
   double* d_scal = nullptr;
   double* h_scal = nullptr;      // pinned
-  int* d_cata = nullptr;         // [0] catastrophe, [1] tensor-core wait gave up, [2] Wannier count
+  int* d_cata = nullptr;         // [0] catastrophe, [1] tensor-core wait gave up, [2] Wannier count,
+                                 // [3] operand-wait polls of k_rec_rho_tc (-1 = default; kept across calls)
   int* h_cata = nullptr;
   // Wannier centres: per-type lwfc, the centres' dipoles of the last call
   bool lwannier = false;
@@ -630,15 +631,16 @@ template <int NB>
 static void launch_rho_tc_n(mdff_ctx* h, const RecMesh& M, int n, int has_q, int has_mu) {
   size_t smem = rho_tc_smem_n(NB, M.kmax[0], M.kmax[1], M.kmax[2]);
   int* err = h->d_cata + 1;
+  const int* wcfg = h->d_cata + 3;
   if (has_mu) {
     dim3 g((unsigned)cdiv(M.nrows, 32), (unsigned)h->n_tc_chunks);
     if (has_q)
-      k_rec_rho_tc<true, true, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err);
+      k_rec_rho_tc<true, true, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err, wcfg);
     else
-      k_rec_rho_tc<false, true, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err);
+      k_rec_rho_tc<false, true, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err, wcfg);
   } else {
     dim3 g((unsigned)cdiv(M.nrows, 64), (unsigned)h->n_tc_chunks);
-    k_rec_rho_tc<true, false, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err);
+    k_rec_rho_tc<true, false, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err, wcfg);
   }
 }
 
@@ -1854,7 +1856,9 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_part, h->part_cap);
   DALLOC(h->d_part2, h->part_cap);
   DALLOC(h->d_scal, S_NSCAL);
-  DALLOC(h->d_cata, 3);  // [0] catastrophe, [1] a tensor-core wait gave up, [2] Wannier count
+  DALLOC(h->d_cata, 4);  // [0] catastrophe, [1] a tensor-core wait gave up, [2] Wannier count
+  k_seti<<<1, 32, 0, h->st>>>(h->d_cata + 3, -1);  // [3] default operand-wait limit
+  LAUNCH_CHECK();
   for (int it = 0; it < p.ntype; ++it)
     if (p.lwfc[it] > 0) h->lwannier = true;
   if (h->lwannier) {
@@ -2163,6 +2167,15 @@ int mdff_gpu_profile(mdff_handle h, int enable) {
     h->kl[c] = 0;
     h->kwork[c] = 0;
   }
+  return MDFF_OK;
+}
+
+int mdff_gpu_set_tc_wait_limit(mdff_handle h, int polls) {
+  if (!h) return MDFF_ERR_BAD_ARGS;
+  CK(cudaSetDevice(h->device));
+  k_seti<<<1, 32, 0, h->st>>>(h->d_cata + 3, polls < 0 ? -1 : polls);
+  LAUNCH_CHECK();
+  CK(cudaStreamSynchronize(h->st));
   return MDFF_OK;
 }
 

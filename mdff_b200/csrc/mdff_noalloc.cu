@@ -14,7 +14,9 @@
 //
 // Limits: natm <= kNAMaxAtoms (32768), list entries <= kNAMaxEntries
 // (4,194,304), row length <= kNAMaxRow (4096); larger inputs are rejected
-// with a message on stderr.  All calls share the one array, and each call
+// with MDFF_ERR_BAD_ARGS and a message on stderr (MDFF_ERR_LIST_OVERFLOW is
+// kept for a caller capacity below the list size, as the existing entry
+// point returns it).  All calls share the one array, and each call
 // clears what must start at zero; two calls that overlap on the same GPU
 // (from two host threads) race on it.  The first call on a device looks up
 // the array's device address (cudaGetSymbolAddress, with that device
@@ -366,11 +368,14 @@ extern "C" int mdff_gpu_verlet_half_list_noalloc(const mdff_params* p, const dou
   NA_CK(cudaMemcpy(&total, d_rowoff + n, sizeof(int), cudaMemcpyDeviceToHost));
   NA_CK(cudaMemcpy(&maxrow, d_flags, sizeof(int), cudaMemcpyDeviceToHost));
   *n_out = total;
+  // a list larger than the static array is a hard limit of this entry point,
+  // not a short caller capacity: a different status, so that a caller that
+  // grows its buffer on MDFF_ERR_LIST_OVERFLOW does not retry for ever
   if (total > kNAMaxEntries) {
     fprintf(stderr,
             "mdff_gpu_verlet_half_list_noalloc: %d list entries exceed the static scratch limit "
             "of %d\n", total, kNAMaxEntries);
-    return MDFF_ERR_LIST_OVERFLOW;
+    return MDFF_ERR_BAD_ARGS;
   }
   if (maxrow > kNAMaxRow) return na_fail("a row longer than 4096 entries exceeds the sort buffer");
   int P = 1;

@@ -173,7 +173,7 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int by
 template <bool HAS_Q, bool HAS_MU, int N>
 static __global__ void __launch_bounds__(kRhoTcThreads) k_rec_rho_tc(
     const float2* __restrict__ tab, const float4* __restrict__ w, int natm, int chunk, RecMesh M,
-    double2* __restrict__ part, int* __restrict__ err) {
+    double2* __restrict__ part, int* __restrict__ err, const int* __restrict__ wait_cfg) {
   constexpr int NT = kRhoTcThreads;
   constexpr int RPT = HAS_MU ? 32 : 64;         // mesh rows per tile
   constexpr int KB = tc::KB;
@@ -264,6 +264,9 @@ static __global__ void __launch_bounds__(kRhoTcThreads) k_rec_rho_tc(
   };
 
   const int nkb = (a1 - a0 + KB - 1) / KB;
+  // polls of the wait for a free operand stage: tc::kWaitLimit unless the
+  // host set a limit (a test hook; the drain wait below keeps kWaitLimit)
+  const long opwait = *wait_cfg >= 0 ? (long)*wait_cfg : tc::kWaitLimit;
   if (nkb > 0) stage_tables(0);
   int issued = 0;  // K blocks committed by thread 0
   for (int kb = 0; kb < nkb; ++kb) {
@@ -279,7 +282,7 @@ static __global__ void __launch_bounds__(kRhoTcThreads) k_rec_rho_tc(
     // one thread waits for the tensor core to release stage st; the barrier
     // holds the others
     if (kb >= 2 && tid == 0 &&
-        !tc::mbar_wait(tc::smem_u32(&mbar[st]), ((kb - 2) >> 1) & 1, tc::kWaitLimit))
+        !tc::mbar_wait(tc::smem_u32(&mbar[st]), ((kb - 2) >> 1) & 1, opwait))
       abort_flag = 1;
     __syncthreads();
     if (abort_flag) break;

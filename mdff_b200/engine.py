@@ -112,6 +112,11 @@ class ForceEngine:
         self._check(self._lib.mdff_gpu_efg(self._h, dptr(e)), "efg")
         return e
 
+    def set_tc_wait_limit(self, polls):
+        """Test hook of the timeout path (mdff_gpu_set_tc_wait_limit): polls of
+        the tensor-core structure factor's operand-stage wait; < 0 = default."""
+        self._check(self._lib.mdff_gpu_set_tc_wait_limit(self._h, int(polls)), "set_tc_wait_limit")
+
     def stats(self):
         s = _abi.MdffStats()
         self._check(self._lib.mdff_gpu_get_stats(self._h, ctypes.byref(s)), "stats")

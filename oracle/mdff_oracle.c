@@ -60,6 +60,9 @@ struct or_ctx {
   double *kx, *ky, *kz, *kk, *Ak, *kcoe;
   /* ASPC history dipia_ind_t(5,3,natm) -> [5][natm][3] */
   double* hist;
+  /* direct coordinates at the last list build, config%xs/ys/zs
+     (config.f90:66); written only by or_vnlistcheck */
+  double *xs, *ys, *zs;
   int lpolar_any;
 };
 
@@ -417,6 +420,11 @@ or_ctx* or_create(const mdff_params* pin, const double cell_A[9], int* status) {
   c->poldipia = calloc(9 * (size_t)natm, sizeof(double));
   c->invpoldipia = calloc(9 * (size_t)natm, sizeof(double));
   c->hist = calloc((size_t)MDFF_ASPC_DEPTH * 3 * natm, sizeof(double));
+  /* config.f90:268 allocates xs/ys/zs and nothing sets them before the
+     first vnlistcheck; they start at zero here */
+  c->xs = calloc((size_t)natm, sizeof(double));
+  c->ys = calloc((size_t)natm, sizeof(double));
+  c->zs = calloc((size_t)natm, sizeof(double));
   int ia = 0;
   for (int it = 0; it < ntype; ++it) {
     double inv[9];
@@ -473,6 +481,9 @@ void or_destroy(or_ctx* c) {
   free(c->poldipia);
   free(c->invpoldipia);
   free(c->hist);
+  free(c->xs);
+  free(c->ys);
+  free(c->zs);
   free(c->kx);
   free(c->ky);
   free(c->kz);
@@ -561,6 +572,45 @@ int or_vnlist(or_ctx* c, const double* rx, const double* ry, const double* rz, i
   free(sy);
   free(sz);
   return status;
+}
+
+/* vnlistcheck (tools.f90:444-537): the largest and second largest
+   minimum-image displacement since the last build, with the reference's
+   running top-2 update (:494-501); a rebuild when their sum is .gt. skindiff
+   (:513), after which the direct coordinates become the new xs/ys/zs
+   (:518-524).  The rebuilt lists themselves are or_vnlist's.  Positions are
+   not modified (the reference converts rx in place with kardir/dirkar). */
+int or_vnlistcheck(or_ctx* c, const double* rx, const double* ry, const double* rz, double* disp,
+                   int* rebuilt) {
+  int natm = c->natm;
+  double* sx = malloc(sizeof(double) * natm);
+  double* sy = malloc(sizeof(double) * natm);
+  double* sz = malloc(sizeof(double) * natm);
+  or_kardir(c, rx, ry, rz, sx, sy, sz);
+  double drneimax = 0.0, drneimax2 = 0.0;
+  for (int ia = 0; ia < natm; ++ia) {
+    double x, y, z;
+    double drnei = sqrt(min_image(c, sx[ia] - c->xs[ia], sy[ia] - c->ys[ia], sz[ia] - c->zs[ia],
+                                  &x, &y, &z));
+    if (drnei > drneimax) {
+      drneimax2 = drneimax;
+      drneimax = drnei;
+    } else if (drnei > drneimax2) {
+      drneimax2 = drnei;
+    }
+  }
+  if (disp) *disp = drneimax + drneimax2;
+  int r = (drneimax + drneimax2 > c->p.skindiff) ? 1 : 0;
+  if (r) {
+    memcpy(c->xs, sx, sizeof(double) * natm);
+    memcpy(c->ys, sy, sizeof(double) * natm);
+    memcpy(c->zs, sz, sizeof(double) * natm);
+  }
+  if (rebuilt) *rebuilt = r;
+  free(sx);
+  free(sy);
+  free(sz);
+  return MDFF_OK;
 }
 
 /* CSR half list, 0-based, for internal use */

@@ -43,6 +43,13 @@ int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
 int or_vnlist(or_ctx* c, const double* rx, const double* ry, const double* rz,
               int which, int* point, int* list, int capacity, int* n_out);
 
+/* vnlistcheck (tools.f90:444-537): *disp = largest + second largest
+   displacement since the last rebuild (stored direct coordinates start at
+   zero, so the first call rebuilds); *rebuilt = 1 when the sum is above
+   skindiff, and the positions become the new reference. */
+int or_vnlistcheck(or_ctx* c, const double* rx, const double* ry, const double* rz, double* disp,
+                   int* rebuilt);
+
 int or_get_aspc(or_ctx* c, double* buf);
 int or_set_aspc(or_ctx* c, const double* buf);
 

@@ -54,6 +54,8 @@ def lib():
                                   ctypes.POINTER(Extra)]
         L.or_vnlist.restype = ctypes.c_int
         L.or_vnlist.argtypes = [P, DP, DP, DP, ctypes.c_int, IP, IP, ctypes.c_int, IP]
+        L.or_vnlistcheck.restype = ctypes.c_int
+        L.or_vnlistcheck.argtypes = [P, DP, DP, DP, DP, IP]
         L.or_get_aspc.argtypes = [P, DP]
         L.or_set_aspc.argtypes = [P, DP]
         L.or_get_setup.argtypes = [P, ctypes.POINTER(SetupInfo)]
@@ -165,6 +167,17 @@ class Oracle:
         st = lib().or_vnlist(self._h, _abi.dptr(rx), _abi.dptr(ry), _abi.dptr(rz), int(which),
                              _abi.iptr(point), _abi.iptr(lst), int(cap), ctypes.byref(nout))
         return st, point, lst[: min(nout.value, cap)].copy(), nout.value
+
+    def vnlistcheck(self, rx, ry, rz):
+        """vnlistcheck (tools.f90:444-537) against the direct coordinates of
+        the last rebuild (zero before the first): returns (rebuilt, disp)
+        with disp = largest + second largest displacement."""
+        rx, ry, rz = (np.ascontiguousarray(a, dtype=np.float64) for a in (rx, ry, rz))
+        d = ctypes.c_double(0.0)
+        r = ctypes.c_int(0)
+        lib().or_vnlistcheck(self._h, _abi.dptr(rx), _abi.dptr(ry), _abi.dptr(rz), ctypes.byref(d),
+                             ctypes.byref(r))
+        return bool(r.value), d.value
 
     def get_aspc(self):
         b = np.zeros((_abi.ASPC_DEPTH, self.natm, 3))

@@ -5,9 +5,9 @@ file assembled the way examples/ex09/config/gen_tests does it (placeholders
 from test.config, '!INCLUDE <file>' expanded) and read with mdff_b200.mdffio.
 
 The fixture stores, per test, the parsed mdff_params as raw bytes, plus the
-POSFF's cell, names, ions per type and wrapped positions.  Run once where the
-reference is mounted:
-    python tests/golden/make_ex09_decks.py /root/reference
+POSFF's cell, names, ions per type and wrapped positions.  Run once with the
+path of a checkout of the reference (argument, or MDFF_REFERENCE):
+    python tests/golden/make_ex09_decks.py <reference checkout>
 """
 import ctypes
 import os
@@ -87,4 +87,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("MDFF_REFERENCE", "")
+    if not ref:
+        sys.exit("usage: make_ex09_decks.py <reference checkout> (or set MDFF_REFERENCE)")
+    main(ref)

@@ -71,3 +71,43 @@ def small_systems():
     out.append(systems.mgo(ncell=2, calc=P._abi.CALC_OTHER, conv_tol_ind=1e-12))
     out.append(systems.sio2(nsio2=120, seed=8, calc=P._abi.CALC_OTHER, conv_tol_ind=1e-12))
     return out
+
+
+def sio2_prepared():
+    """The 12,000-ion SiO2-like glass at its prepared state
+    (tests/golden/sio2_state.npz, written by make_bench_states.py)."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "sio2_state.npz"))
+    s = systems.sio2(place=False)
+    assert int(z["natm"]) == s.natm and np.allclose(z["cell"], s.cell)
+    s.pos = np.array(z["pos"])
+    s.vel = np.array(z["vel"])
+    return s
+
+
+def config_systems(**extra):
+    """The three single-box workloads at their full sizes: SiO2-like glass
+    12,000 ions (PIM + TT, kmax 12), MgO 8,000 ions (PIM + TT, kmax from
+    ewald_param at epsw 1e-7), molten NaCl 1,728 ions (BMH + Ewald)."""
+    kw = dict(calc=P._abi.CALC_OTHER)
+    kw.update(extra)
+    s = sio2_prepared()
+    for k, v in kw.items():
+        setattr(s.params, k, v)
+    return {"sio2_12000": s, "mgo_8000": systems.mgo(**kw), "nacl_1728": systems.nacl(**kw)}
+
+
+def cells_per_axis(s, which):
+    """Cells per axis of the device list build for system s: the face widths
+    over the build cutoff (the larger of the two lists' cut + skin)."""
+    A = np.asarray(s.cell, dtype=np.float64)
+    B = np.linalg.inv(A).T * np.linalg.det(A)
+    om = abs(np.linalg.det(A))
+    W = om / np.linalg.norm(B, axis=0)
+    p = s.params
+    rc = p.cutlongrange
+    if p.lcoulomb:
+        rc = min(rc, 0.5 * W.min())
+    rs = max(rc if p.lcoulomb else 0.0, p.cutshortrange if (p.lbmhft or p.lbmhftd or p.lnmlj) else 0.0)
+    rs += p.skindiff
+    return [int(np.floor(w / (rs * (1 + 1e-9) + 1e-9))) for w in W]

@@ -109,10 +109,10 @@ def _fortran_layout(block):
 
 @pytest.mark.parametrize("tname,ctype", [("mdff_params", _abi.MdffParams), ("mdff_result", _abi.MdffResult)])
 def test_fortran_shim_type_matches_header(tname, ctype):
-    """The bind(c) derived types of the Fortran shim documented in
-    INTEGRATION.md have the header's fields, in order, at the header's
-    offsets, and the header's size."""
-    txt = open(os.path.join(os.path.dirname(HDR), "..", "INTEGRATION.md")).read().splitlines()
+    """The bind(c) derived types of the Fortran shim include/engforce_gpu.f90
+    have the header's fields, in order, at the header's offsets, and the
+    header's size."""
+    txt = open(os.path.join(os.path.dirname(HDR), "engforce_gpu.f90")).read().splitlines()
     i0 = next(i for i, l in enumerate(txt) if re.match(rf"\s*TYPE, bind\(c\) :: {tname}\s*$", l))
     i1 = next(i for i in range(i0, len(txt)) if txt[i].strip() == "END TYPE")
     fields, size = _fortran_layout(txt[i0 + 1:i1])

@@ -60,3 +60,33 @@ def test_bad_parameters_rejected():
     with pytest.raises(MdffError) as e:
         ForceEngine(params_copy(s.params), s.cell)
     assert e.value.status == _abi.MDFF_ERR_BAD_ARGS
+
+
+def test_tensor_core_wait_timeout_is_reported_and_recovers(oracle):
+    """A bounded device wait that runs out: with the operand-stage wait of the
+    tensor-core structure factor (the mixed engine's CG operator) limited to
+    zero polls, every CTA with more than two K blocks gives up at its first
+    such wait, drains the products it issued and frees its tensor memory; the
+    call returns MDFF_ERR_TIMEOUT.  With the default limit restored the same
+    handle computes the forces again, equal to a fresh handle's and within the
+    mixed engine's bar of the oracle."""
+    s = systems.sio2(nsio2=1000, seed=64, calc=_abi.CALC_OTHER)   # 3000 ions: 4 K blocks per chunk
+    p = params_copy(s.params)
+    p.precision = _abi.PREC_MIXED
+    p.solver = _abi.SOLVER_CG
+    p.cg_tol = 1e-8
+    with ForceEngine(p, s.cell) as eng:
+        eng.set_tc_wait_limit(0)
+        with pytest.raises(MdffError) as e:
+            eng.engforce(*s.soa())
+        assert e.value.status == _abi.MDFF_ERR_TIMEOUT
+        eng.set_tc_wait_limit(-1)
+        g = eng.engforce(*s.soa())
+    with ForceEngine(params_copy(p), s.cell) as eng2:
+        g2 = eng2.engforce(*s.soa())
+    for k in ("fx", "fy", "fz", "mu"):
+        assert np.array_equal(g[k], g2[k]), k
+    o = oracle.Oracle(params_copy(s.params), s.cell).engforce(*s.soa())
+    f = np.stack([g["fx"], g["fy"], g["fz"]], 1)
+    fo = np.stack([o["fx"], o["fy"], o["fz"]], 1)
+    assert np.sqrt(((f - fo) ** 2).sum() / (fo ** 2).sum()) <= 1e-5

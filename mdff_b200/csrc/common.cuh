@@ -112,6 +112,14 @@ __device__ __forceinline__ double rsqrt_<double>(double x) { return sqrt(x); }
 template <>
 __device__ __forceinline__ float rsqrt_<float>(float x) { return sqrtf(x); }
 
+// 1/sqrt(x)
+template <typename R>
+__device__ __forceinline__ R rinv_sqrt(R x);
+template <>
+__device__ __forceinline__ double rinv_sqrt<double>(double x) { return rsqrt(x); }
+template <>
+__device__ __forceinline__ float rinv_sqrt<float>(float x) { return rsqrtf(x); }
+
 // Tang-Toennies damping (tt_damp.f90:68-97):
 //   f  = 1 - c e^{-br} sum_{k=0}^{n} (br)^k / k!
 //   fd = c b e^{-br} (br)^n / n!
@@ -144,6 +152,48 @@ __device__ __forceinline__ void tt_damp(R b, R c, R r, int order, R& f, R& fd) {
   for (int k = 1; k <= MDFF_TT_MAX; ++k)
     if (k == order) eo = e[k];
   fd = eo * pw * expbdr * b;
+}
+
+// 1/k! built as the reference's E_TT table, E(k) = E(k-1) / k (tt_damp.f90:50-53)
+template <typename R, int k>
+__host__ __device__ constexpr R inv_fact() {
+  if constexpr (k == 0)
+    return R(1);
+  else
+    return inv_fact<R, k - 1>() / R(k);
+}
+
+// Horner sum of tt_damp.f90:80-84 for a compile-time order: acc = E(K), then
+// acc = acc*br + E(k) for k = K-1 .. 1, then acc*br + E(0)
+template <typename R, int K, int k>
+__device__ __forceinline__ R tt_horner(R acc, R br) {
+  if constexpr (k < 1) {
+    return acc * br + R(1);
+  } else {
+    constexpr R ek = inv_fact<R, k>();
+    return tt_horner<R, K, k - 1>(acc * br + ek, br);
+  }
+}
+
+// Tang-Toennies damping with a compile-time order K in 1..8 (the same
+// operations as tt_damp for that order, without the runtime-order selects);
+// K = 0 falls back to tt_damp with the runtime order.
+template <typename R, int K>
+__device__ __forceinline__ void tt_damp_k(R b, R c, R r, int order, R& f, R& fd) {
+  if constexpr (K == 0) {
+    tt_damp<R>(b, c, r, order, f, fd);
+  } else {
+    static_assert(K >= 1 && K <= MDFF_TT_MAX, "TT order");
+    R br = b * r;
+    R expbdr = rexp<R>(-br) * c;
+    constexpr R eK = inv_fact<R, K>();
+    R ff = tt_horner<R, K, K - 1>(eK, br);
+    R pw = br;
+#pragma unroll
+    for (int k = 2; k <= K; ++k) pw = pw * br;
+    f = R(1) - ff * expbdr;
+    fd = eK * pw * expbdr * b;
+  }
 }
 
 // ---------------------------------------------------------------------------

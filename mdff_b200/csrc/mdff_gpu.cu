@@ -130,6 +130,10 @@ struct mdff_ctx {
   double4 *d_mu_tot = nullptr, *d_hist = nullptr, *d_E = nullptr;
   double4 *d_r = nullptr, *d_z = nullptr, *d_pv = nullptr, *d_qv = nullptr, *d_Tp = nullptr;
   float4* d_mu32 = nullptr;      // FP32 copy of the dipoles of an FP32 pass
+  float4* d_qm32 = nullptr;      // (mu_tot, q) in FP32 for the mixed final pass
+  // Tang-Toennies order shared by every damped ion pair (both field roles), the
+  // compile-time order of the damped real-space kernels; 0 = orders differ
+  int tt_k = 0;
   // FP32 dipole-field pair cache of the mixed mode (k_static_cache), ELL [natm][cap]
   float4* d_ddr = nullptr;
   float* d_ddb1 = nullptr;
@@ -885,10 +889,16 @@ static int static_field(mdff_ctx* h, bool fp32) {
   double cutsq = h->p.cutlongrange * h->p.cutlongrange;
   int nb = cdiv((long)n * 32, 256);
   bool qq = h->task_qq != 0, dd = h->ldip_static != 0;
-#define ESF(R, Q, D, MU)                                                                              \
-  k_es_field<R, Q, D><<<nb, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, MU, h->L.nbr, \
+#define ESFK(R, Q, D, MU, K)                                                                        \
+  k_es_field<R, Q, D, K><<<nb, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, MU, h->L.nbr, \
                                              h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, \
                                              h->p.alphaES, cutsq, 1, 0, E, h->p.thole_type)
+  // the damped charge field with the compile-time Tang-Toennies order when it applies
+#define ESF(R, Q, D, MU)                    \
+  do {                                      \
+    if (h->tt_k == 4) ESFK(R, Q, D, MU, 4); \
+    else ESFK(R, Q, D, MU, 0);              \
+  } while (0)
   if (fp32 && dd) {
     k_to_float4<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_dipia, n, h->d_mu32);
     LAUNCH_CHECK();
@@ -901,7 +911,14 @@ static int static_field(mdff_ctx* h, bool fp32) {
   if (fp32 && !dd && h->lpolar && h->d_ddr) {
     // damped charge field + the pair cache of the FP32 solver iterations
     int pr = prof_begin(h, KC_ESFIELD, 0);
-    k_static_cache<<<nb, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, qq ? 1 : 0, E, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->p.thole_type);
+#define STC(K)                                                                                      \
+  k_static_cache<K><<<nb, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->L.nbr, h->L.nnb, \
+                                        h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES,   \
+                                        cutsq, qq ? 1 : 0, E, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, \
+                                        h->p.thole_type)
+    if (h->tt_k == 4) STC(4);
+    else STC(0);
+#undef STC
     LAUNCH_CHECK();
     prof_end(h, pr);
     h->dd_cache_ok = true;
@@ -910,16 +927,17 @@ static int static_field(mdff_ctx* h, bool fp32) {
     if (fp32) {
       if (qq && dd) ESF(float, true, true, h->d_mu32);
       else if (qq) ESF(float, true, false, h->d_mu32);
-      else ESF(float, false, true, h->d_mu32);
+      else ESFK(float, false, true, h->d_mu32, 0);
     } else {
       if (qq && dd) ESF(double, true, true, h->d_dipia);
       else if (qq) ESF(double, true, false, h->d_dipia);
-      else ESF(double, false, true, h->d_dipia);
+      else ESFK(double, false, true, h->d_dipia, 0);
     }
     LAUNCH_CHECK();
     prof_end(h, pr);
   }
 #undef ESF
+#undef ESFK
   if (h->p.lsurf) {
     s = moments(h, h->d_dipia, 1, h->d_scal + S_MOM2);
     if (s) return s;
@@ -1573,7 +1591,7 @@ static int run_engforce(mdff_ctx* h, int itime) {
     }
     k_mu_total<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_dipia, h->d_mu_ind,
                                                 (h->lwannier && h->p.ldip_wfc) ? h->d_mu_wfc : nullptr, n,
-                                                h->d_mu_tot, h->d_cata);
+                                                h->d_mu_tot, h->d_cata, h->d_q, fp32 ? h->d_qm32 : nullptr);
     LAUNCH_CHECK();
     CK(cudaMemsetAsync(h->d_E, 0, sizeof(double4) * n, h->st));
     double cutsq = h->p.cutlongrange * h->p.cutlongrange;
@@ -1583,17 +1601,19 @@ static int run_engforce(mdff_ctx* h, int itime) {
     cudaStream_t rs;
     if ((s = rs_fork(h, &rs))) return s;
     int prf = prof_begin(h, KC_ESFORCE, 0);
-#define ESFORCE(R, TH)                                                                            \
-  k_es_force<R, TH><<<nbw, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_mu_tot, h->L.nbr,      \
-                                            h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, \
-                                            h->p.alphaES, cutsq, h->task_qq, h->task_qd,            \
-                                            h->task_dd, 1, h->coul_unit, h->d_E, h->d_force,        \
-                                            h->d_part2)
+#define ESFORCE(R, K, TH)                                                                        \
+  k_es_force<R, K, TH><<<nbw, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_mu_tot, h->d_qm32,  \
+                                            h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell,          \
+                                            h->d_estab, h->ntype, h->p.alphaES, cutsq,           \
+                                            h->task_qq, h->task_qd, h->task_dd, 1, h->coul_unit, \
+                                            h->d_E, h->d_force, h->d_part2)
     const bool thole = h->p.thole_type != MDFF_THOLE_NONE;
-    if (fp32 && thole) ESFORCE(float, true);
-    else if (fp32) ESFORCE(float, false);
-    else if (thole) ESFORCE(double, true);
-    else ESFORCE(double, false);
+    if (fp32 && thole) ESFORCE(float, 0, true);
+    else if (fp32 && h->tt_k == 4) ESFORCE(float, 4, false);
+    else if (fp32) ESFORCE(float, 0, false);
+    else if (thole) ESFORCE(double, 0, true);
+    else if (h->tt_k == 4) ESFORCE(double, 4, false);
+    else ESFORCE(double, 0, false);
 #undef ESFORCE
     LAUNCH_CHECK();
     prof_end(h, prf);
@@ -1790,6 +1810,18 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_estab, es.size());
   CK(cudaMemcpyAsync(h->d_nbtab, nb.data(), sizeof(NBPair) * nb.size(), cudaMemcpyHostToDevice, h->st));
   CK(cudaMemcpyAsync(h->d_estab, es.data(), sizeof(ESPair) * es.size(), cudaMemcpyHostToDevice, h->st));
+  {
+    int k = -1;
+    bool same = true;
+    for (const ESPair& e : es) {
+      if (!e.ldamp) continue;
+      for (int o : {e.ka, e.kb}) {
+        if (k < 0) k = o;
+        same = same && o == k;
+      }
+    }
+    h->tt_k = (same && k == 4) ? 4 : 0;  // the instantiated order (examples use 4)
+  }
   // list
   double cut = 0.0;
   if (h->lsr) cut = std::max(cut, p.cutshortrange);
@@ -1835,6 +1867,7 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_qv, n);
   DALLOC(h->d_Tp, n);
   DALLOC(h->d_mu32, n);
+  if (p.precision == MDFF_PREC_MIXED && p.lcoulomb) DALLOC(h->d_qm32, n);
   if (p.algo_moment_from_pola != MDFF_ALGO_SCF) {
     DALLOC(h->d_ko_f, n);
     DALLOC(h->d_ko_dmu, n);
@@ -2244,7 +2277,7 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
                   h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
-                  h->d_lwfc, h->d_mu_wfc};
+                  h->d_lwfc, h->d_mu_wfc, h->d_qm32};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);

@@ -335,9 +335,11 @@ __global__ void k_wfc_dipoles(const double4* __restrict__ s, const int* __restri
 
 // mu_tot = (dipia + mu_ind) [+ mu_wfc] ; catastrophe flag if any component > 10
 // (moment_from_pola.f90:136-147, 176-178: positive components only)
+// qm32 (optional): (mu_x, mu_y, mu_z, q) in FP32 for the mixed final pass
 __global__ void k_mu_total(const double4* __restrict__ dip, const double4* __restrict__ mu_ind,
                            const double4* __restrict__ mu_wfc, int natm, double4* __restrict__ mu_tot,
-                           int* __restrict__ flag) {
+                           int* __restrict__ flag, const double* __restrict__ q = nullptr,
+                           float4* __restrict__ qm32 = nullptr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   double4 a = dip[i], b = mu_ind[i];
@@ -347,6 +349,7 @@ __global__ void k_mu_total(const double4* __restrict__ dip, const double4* __res
     m = make_double4(m.x + w.x, m.y + w.y, m.z + w.z, 0.0);
   }
   mu_tot[i] = m;
+  if (qm32) qm32[i] = make_float4((float)m.x, (float)m.y, (float)m.z, (float)q[i]);
   if (m.x > 10.0 || m.y > 10.0 || m.z > 10.0) atomicExch(flag, 1);
 }
 

@@ -12,7 +12,8 @@
 // Warp per atom i; lanes stride i's row.  Each pair is visited from both
 // sides; the reference's role of the pair (which ion is "ia") is recovered
 // from the parity mask, so asymmetric damping tables behave as in the
-// reference.  Per-atom sums are formed in registers with no atomics; pair
+// reference.  Where every damped pair uses one Tang-Toennies order the
+// kernels are instantiated for it (compile-time Horner, tt_damp_k).  Per-atom sums are formed in registers with no atomics; pair
 // energies/stresses are halved and reduced per block in a fixed order.
 #pragma once
 #include "common.cuh"
@@ -84,8 +85,12 @@ constexpr int kSRPart = 16;
 // The reference skips pairs with A = 0 (:1153); the optional wall acts on its own.
 template <typename R>
 __device__ __forceinline__ void sr_pair_bmh(const NBPair& P, int lbmhftd, R rijsq, R& u, R& wij) {
-  R ir2 = R(1) / rijsq;
-  R d = rsqrt_<R>(rijsq);
+  // 1/d from one reciprocal square root; d, 1/r^2 and the divisions by d of
+  // non_bonded.f90:1180-1200 become products (a few ulp from the reference's
+  // square root and quotients)
+  R dinv = rinv_sqrt<R>(rijsq);
+  R d = rijsq * dinv;
+  R ir2 = dinv * dinv;
   R wnum = R(0);
   u = R(0);
   if (P.A != 0.0) {
@@ -96,12 +101,12 @@ __device__ __forceinline__ void sr_pair_bmh(const NBPair& P, int lbmhftd, R rijs
     ir8 = ir8 * (R)P.D;
     R f6 = R(1), f8 = R(1), fd6 = R(0), fd8 = R(0);
     if (lbmhftd) {
-      tt_damp<R>((R)P.BD, R(1), d, 6, f6, fd6);
-      tt_damp<R>((R)P.BD, R(1), d, 8, f8, fd8);
+      tt_damp_k<R, 6>((R)P.BD, R(1), d, 6, f6, fd6);
+      tt_damp_k<R, 8>((R)P.BD, R(1), d, 8, f8, fd8);
     }
     R ir6d = ir6 * f6, ir8d = ir8 * f8;
-    R ir7 = R(6) * ir6d / d;
-    R ir9 = R(8) * ir8d / d;
+    R ir7 = R(6) * ir6d * dinv;
+    R ir9 = R(8) * ir8d * dinv;
     u = erh - ir6d - ir8d;
     wnum = (R)P.B * erh - ir7 - ir9 + ir6 * fd6 + ir8 * fd8;
   }
@@ -109,9 +114,9 @@ __device__ __forceinline__ void sr_pair_bmh(const NBPair& P, int lbmhftd, R rijs
     R ir8r = (ir2 * ir2) * (ir2 * ir2);
     R uw = (R)P.wall * (ir8r * ir8r * ir8r);
     u += uw;
-    wnum += R(24) * uw / d;
+    wnum += R(24) * uw * dinv;
   }
-  wij = wnum / d;
+  wij = wnum * dinv;
 }
 
 // one n-m LJ pair (engforce_nmlj_pbc, non_bonded.f90:740-790): energy with the
@@ -228,24 +233,28 @@ struct Radial {
   R d, dm1, dm3, dm5, dm7, F0, F1, F2, F3;
 };
 
+// (FP64: the reference's divisions by d, d^2, sqrt(pi), 3 and 15 are products
+// with reciprocals, ~1 ulp from its quotients)
 template <typename R, bool NEED_F3>
 __device__ __forceinline__ void radial(R d2, R alpha, Radial<R>& o) {
-  const R piroot = (R)1.7724538509055160273;
-  R d = rsqrt_<R>(d2);
+  const R rpiroot = (R)0.56418958354775628695;  // 1/sqrt(pi)
+  R rinv = rinv_sqrt<R>(d2);
+  R dm2 = rinv * rinv;
+  R d = d2 * rinv;
   o.d = d;
-  o.dm1 = R(1) / d;
-  o.dm3 = o.dm1 / d2;
-  o.dm5 = o.dm3 / d2;
-  o.dm7 = o.dm5 / d2;
+  o.dm1 = rinv;
+  o.dm3 = rinv * dm2;
+  o.dm5 = o.dm3 * dm2;
+  o.dm7 = o.dm5 * dm2;
   R a2 = alpha * alpha, a3 = a2 * alpha;
-  R expon = rexp<R>(-a2 * d2) / piroot;
+  R expon = rexp<R>(-a2 * d2) * rpiroot;
   o.F0 = nr_erfc<R>(alpha * d);
   o.F1 = o.F0 + R(2) * alpha * d * expon;
   R d3 = d2 * d;
-  o.F2 = o.F1 + R(4) * a3 * d3 * expon / R(3);
+  o.F2 = o.F1 + (R(4) / R(3)) * a3 * d3 * expon;
   if (NEED_F3) {
     R a5 = a3 * a2, d5 = d3 * d2;
-    o.F3 = o.F2 + R(8) * a5 * d5 * expon / R(15);
+    o.F3 = o.F2 + (R(8) / R(15)) * a5 * d5 * expon;
   } else {
     o.F3 = R(0);
   }
@@ -282,10 +291,31 @@ __device__ __forceinline__ void radial<float, false>(float d2, float alpha, Radi
 }
 template <>
 __device__ __forceinline__ void radial<float, true>(float d2, float alpha, Radial<float>& o) {
-  radial<float, false>(d2, alpha, o);
+  float rinv = rsqrtf(d2);
+  float dm2 = rinv * rinv;
+  o.d = d2 * rinv;
+  o.dm1 = rinv;
+  o.dm3 = rinv * dm2;
+  o.dm5 = o.dm3 * dm2;
+  o.dm7 = o.dm5 * dm2;
   float a2 = alpha * alpha;
-  float ade = alpha * o.d * expf(-a2 * d2) * 0.56418958354775628695f;
-  o.F3 = o.F2 + (8.0f / 15.0f) * a2 * a2 * d2 * d2 * ade;
+  float expon = expf(-a2 * d2) * 0.56418958354775628695f;  // 1/sqrt(pi)
+  float z = alpha * o.d;
+  float t = __frcp_rn(1.0f + 0.5f * z);
+  float p = -.82215223f + t * .17087277f;
+  p = 1.48851587f + t * p;
+  p = -1.13520398f + t * p;
+  p = .27886807f + t * p;
+  p = -.18628806f + t * p;
+  p = .09678418f + t * p;
+  p = .37409196f + t * p;
+  p = 1.00002368f + t * p;
+  o.F0 = t * expf(-z * z - 1.26551223f + t * p);
+  float ade = z * expon;
+  float a2d2 = a2 * d2;
+  o.F1 = o.F0 + 2.0f * ade;
+  o.F2 = o.F1 + (4.0f / 3.0f) * a2d2 * ade;
+  o.F3 = o.F2 + (8.0f / 15.0f) * a2d2 * a2d2 * ade;
 }
 
 // --------------------------------------------------------------------------
@@ -306,8 +336,8 @@ struct vec4t<float> {
 };
 
 // minimum-image vector of the pair (i, j) and its square.  FP64: the
-// reference's exact arithmetic.  FP32: the direct-coordinate difference in
-// FP64 (positions of a 50 A box need it), the image shift and A.s in FP32.
+// reference's exact arithmetic.  FP32: the direct-coordinate difference and
+// its image shift in FP64 (positions of a 50 A box need it), A.s in FP32.
 template <typename R>
 __device__ __forceinline__ R pair_vec(const double* A, double4 si, double4 sj, R& rx, R& ry, R& rz);
 template <>
@@ -318,10 +348,10 @@ __device__ __forceinline__ double pair_vec<double>(const double* A, double4 si, 
 template <>
 __device__ __forceinline__ float pair_vec<float>(const double* A, double4 si, double4 sj,
                                                  float& rx, float& ry, float& rz) {
-  float dx = (float)(si.x - sj.x), dy = (float)(si.y - sj.y), dz = (float)(si.z - sj.z);
-  dx -= rintf(dx);
-  dy -= rintf(dy);
-  dz -= rintf(dz);
+  // the image shift in FP64 too, so that a pair across the boundary keeps
+  // FP32's relative precision in its (small) direct-coordinate difference
+  double ddx = si.x - sj.x, ddy = si.y - sj.y, ddz = si.z - sj.z;
+  float dx = (float)(ddx - rint(ddx)), dy = (float)(ddy - rint(ddy)), dz = (float)(ddz - rint(ddz));
   rx = dx * (float)A[0] + dy * (float)A[1] + dz * (float)A[2];
   ry = dx * (float)A[3] + dy * (float)A[4] + dz * (float)A[5];
   rz = dx * (float)A[6] + dy * (float)A[7] + dz * (float)A[8];
@@ -331,7 +361,7 @@ __device__ __forceinline__ float pair_vec<float>(const double* A, double4 si, do
 // field at i from j of the field-only passes (k_es_field): the charge field
 // q_j r dm3 (F1 - F1d) with the pair's damping roles, and the dipole field
 // T2 . mu_j (ewald_dir.f90:533-541, 566-571); added into (ex, ey, ez).
-template <typename R, bool QQ, bool DD>
+template <typename R, bool QQ, bool DD, int K = 0>
 __device__ __forceinline__ void es_field_pair(const ESPair* stab, int ntype, int i, int j, int ti,
                                               int tj, R rx, R ry, R rz, R r2, R alpha, int damp,
                                               double qj, bool dd, R mx, R my, R mz, R& ex, R& ey,
@@ -347,9 +377,9 @@ __device__ __forceinline__ void es_field_pair(const ESPair* stab, int ntype, int
       if (P.ldamp) {
         R fdm, fdd;
         if (i_is_a)
-          tt_damp<R>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
+          tt_damp_k<R, K>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
         else
-          tt_damp<R>((R)P.bb, (R)P.cb, g.d, P.kb, fdm, fdd);
+          tt_damp_k<R, K>((R)P.bb, (R)P.cb, g.d, P.kb, fdm, fdd);
         F1d = R(1) - fdm;
       }
     }
@@ -386,8 +416,9 @@ static __global__ void k_to_float4(const double4* __restrict__ in, int n, float4
 //   DD : E_i += T2(r_ij) . mu_j                  (dd block, ewald_dir.f90:566-571)
 // dd_mask: 0 -> the reference's condition any(mu_i /= 0) .and. any(mu_j /= 0)
 //          1 -> both ions polarisable (the linear operator of the CG solve)
-// mu is double4 for FP64 and float4 for FP32 (k_to_float4).
-template <typename R, bool QQ, bool DD>
+// mu is double4 for FP64 and float4 for FP32 (k_to_float4).  K: compile-time
+// Tang-Toennies order of the damped charge field (0 = per pair).
+template <typename R, bool QQ, bool DD, int K = 0>
 static __global__ void __launch_bounds__(256) k_es_field(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
     const int* __restrict__ ipolar, const typename vec4t<R>::T* __restrict__ mu,
@@ -428,7 +459,7 @@ static __global__ void __launch_bounds__(256) k_es_field(
       double qj = QQ ? q[j] : 0.0;
       if (!dd && (!QQ || qj == 0.0)) continue;
       int tj = ((QQ && damp) || (DD && thole)) ? itype[j] : 0;
-      es_field_pair<R, QQ, DD>(stab, ntype, i, j, ti, tj, rx, ry, rz, r2, (R)alpha, damp, qj, dd,
+      es_field_pair<R, QQ, DD, K>(stab, ntype, i, j, ti, tj, rx, ry, rz, r2, (R)alpha, damp, qj, dd,
                                DD ? (R)muj.x : R(0), DD ? (R)muj.y : R(0), DD ? (R)muj.z : R(0),
                                ex, ey, ez, thole);
     }
@@ -448,7 +479,9 @@ static __global__ void __launch_bounds__(256) k_es_field(
 //   cr[i][m] = (rx, ry, rz, B2), cb1[i][m] = B1, cj[i][m] = j,  cn[i] = count
 // (compacted with a warp ballot, row order kept).  The FP32 iterations of the
 // dipole solve then read these instead of recomputing erfc / exp per pair
-// (positions are fixed within a call).
+// (positions are fixed within a call).  K: compile-time Tang-Toennies order
+// (0 = per pair).
+template <int K>
 static __global__ void __launch_bounds__(256) k_static_cache(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
     const int* __restrict__ ipolar, const int* __restrict__ nbr, const int* __restrict__ nnb,
@@ -496,9 +529,9 @@ static __global__ void __launch_bounds__(256) k_static_cache(
             if (P.ldamp) {
               float fdm, fdd;
               if (i_is_a)
-                tt_damp<float>((float)P.ba, (float)P.ca, g.d, P.ka, fdm, fdd);
+                tt_damp_k<float, K>((float)P.ba, (float)P.ca, g.d, P.ka, fdm, fdd);
               else
-                tt_damp<float>((float)P.bb, (float)P.cb, g.d, P.kb, fdm, fdd);
+                tt_damp_k<float, K>((float)P.bb, (float)P.cb, g.d, P.kb, fdm, fdd);
               F1d = 1.f - fdm;
             }
             float c = (float)qj * g.dm3 * (g.F1 - F1d);
@@ -538,6 +571,42 @@ static __global__ void __launch_bounds__(256) k_static_cache(
   }
 }
 
+// this lane's part of the cached dipole field of row i: entries lane, lane +
+// 32, ... in that order.  Four entries per lane are in flight at once (their
+// cache words first, then the four dipole gathers), so the row costs a
+// quarter of the dependent load round trips of a one-entry loop.
+__device__ __forceinline__ void dd_cached_row(const float4* __restrict__ mu,
+                                              const float4* __restrict__ cr,
+                                              const float* __restrict__ cb1,
+                                              const int* __restrict__ cj, size_t base, int n,
+                                              int lane, float& ex, float& ey, float& ez) {
+  constexpr int U = 4;
+  for (int k0 = lane; k0 < n; k0 += 32 * U) {
+    float4 r[U];
+    float b1[U];
+    int j[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int k = k0 + 32 * u;
+      const bool ok = k < n;
+      j[u] = ok ? cj[base + k] : 0;
+      r[u] = ok ? cr[base + k] : make_float4(0.f, 0.f, 0.f, 0.f);
+      b1[u] = ok ? cb1[base + k] : 0.f;
+    }
+    float4 m[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) m[u] = (k0 + 32 * u < n) ? mu[j[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (k0 + 32 * u >= n) break;
+      float rm = r[u].x * m[u].x + r[u].y * m[u].y + r[u].z * m[u].z;
+      ex += r[u].w * r[u].x * rm - b1[u] * m[u].x;
+      ey += r[u].w * r[u].y * rm - b1[u] * m[u].y;
+      ez += r[u].w * r[u].z * rm - b1[u] * m[u].z;
+    }
+  }
+}
+
 // FP32 dipole field of mu (float4) from the pair cache of k_static_cache:
 // E_i += sum_m T2(r_im) mu_j over the polarisable partners (k_es_field<float,
 // false, true> with dd_mask = 1, without the per-pair radial functions)
@@ -552,15 +621,7 @@ static __global__ void __launch_bounds__(256) k_dd_cached(
   if (n == 0) return;
   size_t base = (size_t)i * cap;
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  for (int k = lane; k < n; k += 32) {
-    float4 r = cr[base + k];
-    float B1 = cb1[base + k];
-    float4 m = mu[cj[base + k]];
-    float rm = r.x * m.x + r.y * m.y + r.z * m.z;
-    ex += r.w * r.x * rm - B1 * m.x;
-    ey += r.w * r.y * rm - B1 * m.y;
-    ez += r.w * r.z * rm - B1 * m.z;
-  }
+  dd_cached_row(mu, cr, cb1, cj, base, n, lane, ex, ey, ez);
   double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
   if (lane == 0) {
     double4 o = E[i];
@@ -653,17 +714,120 @@ __device__ __forceinline__ void es_force_pair(const ESPair& P, int damp_ind, R d
   }
 }
 
-template <typename R, bool THOLE = false>
+// one pair of the final real-space pass seen from ion i, r = r_i - r_j: the
+// qq, qd and dd blocks of multipole_ES_dir (ewald_dir.f90:528-644) written in
+// i's frame.  The reference's formulas are role-symmetric once the damping of
+// the field on i (Di) and on j (Dj) are picked from its (ta,ta,tb) /
+// (tb,ta,tb) tables by i's role (ewald_dir.f90:218-222):
+//   f_i = q_i q_j B1 r + dd: -B3 (r.m_i)(r.m_j) r + B2 [(m_i.m_j) r + m_i (r.m_j) + m_j (r.m_i)]
+//         + qd: q_i (T2 - T2d_j) m_j - q_j (T2 - T2d_i) m_i
+//   E_i = q_j (B1 - B1d_i) r + dd: T2 m_j
+//   u   = q_i q_j B0 + dd: -(m_i.T2.m_j) + qd: q_i (B1 - B1d_j)(r.m_j) - q_j (B1 - B1d_i)(r.m_i)
+// (f_i = the reference's -f_ij when i is "ia", +f_ij when i is "ja").  Only
+// i's field is formed.  K: compile-time Tang-Toennies order (0 = per pair).
+template <typename R, int K, bool THOLE>
+__device__ __forceinline__ void es_force_ipair(const ESPair& P, bool i_is_a, bool ldamp, R d2,
+                                               R alpha, const R (&r)[3], R qi, R qj,
+                                               const R (&mi)[3], const R (&mj)[3], bool dip_i,
+                                               bool dip_j, int task_qq, int task_qd, int task_dd,
+                                               R& u, R (&fi)[3], R (&Ei)[3]) {
+  Radial<R> g;
+  radial<R, true>(d2, alpha, g);
+  const R B0 = g.dm1 * g.F0, B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5;
+  R C1i = B1, C2i = B2, C1j = B1, C2j = B2;  // B - B_damped for the field on i / on j
+  if (ldamp) {
+    R fdm, fdd;
+    tt_damp_k<R, K>((R)(i_is_a ? P.ba : P.bb), (R)(i_is_a ? P.ca : P.cb), g.d, i_is_a ? P.ka : P.kb,
+                    fdm, fdd);
+    R F1d = R(1) - fdm;
+    C1i = B1 - F1d * g.dm3;
+    C2i = B2 - R(3) * (F1d + (g.d / R(3)) * fdd) * g.dm5;
+    tt_damp_k<R, K>((R)(i_is_a ? P.bb : P.ba), (R)(i_is_a ? P.cb : P.ca), g.d, i_is_a ? P.kb : P.ka,
+                    fdm, fdd);
+    F1d = R(1) - fdm;
+    C1j = B1 - F1d * g.dm3;
+    C2j = B2 - R(3) * (F1d + (g.d / R(3)) * fdd) * g.dm5;
+  }
+  const R rmi = r[0] * mi[0] + r[1] * mi[1] + r[2] * mi[2];
+  const R rmj = r[0] * mj[0] + r[1] * mj[1] + r[2] * mj[2];
+  u = R(0);
+  R fr = R(0);  // coefficient of r in f_i
+  R fmi = R(0), fmj = R(0);  // coefficients of m_i and m_j in f_i
+  R er = R(0), emj = R(0);   // E_i = er r + emj m_j
+  if (task_qq) {
+    u += qi * qj * B0;
+    fr += qi * qj * B1;
+    er += qj * C1i;
+  }
+  if (task_dd && dip_i && dip_j) {
+    R B1t = B1, B2t = B2;
+    if (THOLE && P.thole) {
+      R F1t = g.F1, F2t = g.F2;
+      thole_radial<R>(P, g.d, F1t, F2t);
+      B1t = F1t * g.dm3;
+      B2t = R(3) * F2t * g.dm5;
+    }
+    const R B3 = R(15) * g.F3 * g.dm7;
+    const R mij = mi[0] * mj[0] + mi[1] * mj[1] + mi[2] * mj[2];
+    u -= B2t * rmi * rmj - B1t * mij;
+    er += B2t * rmj;
+    emj -= B1t;
+    fr += B2 * mij - B3 * rmi * rmj;
+    fmi += B2 * rmj;
+    fmj += B2 * rmi;
+  }
+  if (task_qd && (dip_i || dip_j)) {
+    u += qi * C1j * rmj - qj * C1i * rmi;
+    fr += qi * C2j * rmj - qj * C2i * rmi;
+    fmj -= qi * C1j;
+    fmi += qj * C1i;
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    fi[c] = fr * r[c] + fmi * mi[c] + fmj * mj[c];
+    Ei[c] = er * r[c] + emj * mj[c];
+  }
+}
+
+// per-ion charge and dipole of the final pass: FP64 from q[] and the double4
+// dipoles, FP32 from one float4 (mu_x, mu_y, mu_z, q) written by k_mu_total
+template <typename R>
+__device__ __forceinline__ void load_qm(const double* q, const double4* mu, const float4* qm32,
+                                        int j, R& qj, R (&mj)[3]);
+template <>
+__device__ __forceinline__ void load_qm<double>(const double* q, const double4* mu, const float4*,
+                                                int j, double& qj, double (&mj)[3]) {
+  double4 m = mu[j];
+  qj = q[j];
+  mj[0] = m.x;
+  mj[1] = m.y;
+  mj[2] = m.z;
+}
+template <>
+__device__ __forceinline__ void load_qm<float>(const double*, const double4*, const float4* qm32,
+                                               int j, float& qj, float (&mj)[3]) {
+  float4 m = qm32[j];
+  qj = m.w;
+  mj[0] = m.x;
+  mj[1] = m.y;
+  mj[2] = m.z;
+}
+
+// final real-space pass, warp per ion over the full list; each visit of a
+// pair adds i's force and field and half the pair's energy and stress.
+template <typename R, int K, bool THOLE>
 static __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_es_force(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
-    const double4* __restrict__ mu, const int* __restrict__ nbr, const int* __restrict__ nnb,
-    int cap, int natm, const CellC* __restrict__ cell, const ESPair* __restrict__ tab, int ntype,
-    double alpha, double cutsq, int task_qq, int task_qd, int task_dd, int damp_ind,
-    double fscale, double4* __restrict__ E, double* __restrict__ force /* SoA [3][natm], += */,
-    double* __restrict__ part) {
+    const double4* __restrict__ mu, const float4* __restrict__ qm32, const int* __restrict__ nbr,
+    const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
+    const ESPair* __restrict__ tab, int ntype, double alpha, double cutsq, int task_qq,
+    int task_qd, int task_dd, int damp_ind, double fscale, double4* __restrict__ E,
+    double* __restrict__ force /* SoA [3][natm], += */, double* __restrict__ part) {
   __shared__ ESPair stab[MDFF_NT * MDFF_NT];
+  __shared__ double cA[9];
   __shared__ double red[kESPart * 8];
   for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
+  if (threadIdx.x < 9) cA[threadIdx.x] = cell->A[threadIdx.x];
   __syncthreads();
   int lane = threadIdx.x & 31;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -671,48 +835,41 @@ static __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_es_force
 #pragma unroll
   for (int k = 0; k < kESPart; ++k) acc[k] = 0.0;
   if (i < natm) {
-    double4 si = s[i];
-    int ti = itype[i];
-    double qi = q[i];
-    double4 mui = mu[i];
-    int n = nnb[i];
+    const double4 si = s[i];
+    const int ti = itype[i];
+    R qi, mi[3];
+    load_qm<R>(q, mu, qm32, i, qi, mi);
+    const bool dip_i = mi[0] != R(0) || mi[1] != R(0) || mi[2] != R(0);
+    const int n = nnb[i];
     const int* row = nbr + (size_t)i * cap;
+    const R rc2 = (R)cutsq, ra = (R)alpha;
     double e[3] = {0, 0, 0}, f[3] = {0, 0, 0};
     for (int k = lane; k < n; k += 32) {
-      int j = row[k];
-      double4 sj = s[j];
-      double rxd, ryd, rzd;
-      double r2d = min_image_exact(cell->A, xsub(si.x, sj.x), xsub(si.y, sj.y), xsub(si.z, sj.z),
-                                   rxd, ryd, rzd);
-      if (r2d > cutsq) continue;
-      int tj = itype[j];
-      double qj = q[j];
-      double4 muj = mu[j];
-      bool i_is_a = half_mask(i, j);
-      // canonical pair: a = "ia", b = "ja", r = r_a - r_b
-      R sg = i_is_a ? R(1) : R(-1);
-      R r[3] = {sg * (R)rxd, sg * (R)ryd, sg * (R)rzd};
-      int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
-      R qa = (R)(i_is_a ? qi : qj), qb = (R)(i_is_a ? qj : qi);
-      double4 ma4 = i_is_a ? mui : muj, mb4 = i_is_a ? muj : mui;
-      R ma[3] = {(R)ma4.x, (R)ma4.y, (R)ma4.z}, mb[3] = {(R)mb4.x, (R)mb4.y, (R)mb4.z};
-      bool dip_a = (ma4.x != 0.0 || ma4.y != 0.0 || ma4.z != 0.0);
-      bool dip_b = (mb4.x != 0.0 || mb4.y != 0.0 || mb4.z != 0.0);
-      R u, fij[3], Ea[3], Eb[3];
-      es_force_pair<R, THOLE>(stab[ta * ntype + tb], damp_ind, (R)r2d, (R)alpha, r, qa, qb, ma, mb, dip_a,
-                       dip_b, task_qq, task_qd, task_dd, u, fij, Ea, Eb);
+      const int j = row[k];
+      R r[3];
+      const R r2 = pair_vec<R>(cA, si, s[j], r[0], r[1], r[2]);
+      if (r2 > rc2) continue;  // ewald_dir.f90:202 ( d2 .gt. cutsq ) cycle
+      R qj, mj[3];
+      load_qm<R>(q, mu, qm32, j, qj, mj);
+      const bool dip_j = mj[0] != R(0) || mj[1] != R(0) || mj[2] != R(0);
+      const int tj = itype[j];
+      const bool i_is_a = half_mask(i, j);
+      const ESPair& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
+      R u, fi[3], Ei[3];
+      es_force_ipair<R, K, THOLE>(P, i_is_a, damp_ind && P.ldamp, r2, ra, r, qi, qj, mi, mj, dip_i,
+                                  dip_j, task_qq, task_qd, task_dd, u, fi, Ei);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        f[c] += (double)(i_is_a ? -fij[c] : fij[c]);
-        e[c] += (double)(i_is_a ? Ea[c] : Eb[c]);
+        f[c] += (double)fi[c];
+        e[c] += (double)Ei[c];
       }
       acc[0] += 0.5 * (double)u;
-      acc[1] += -(double)(r[0] * fij[0]);
-      acc[2] += -(double)(r[1] * fij[1]);
-      acc[3] += -(double)(r[2] * fij[2]);
-      acc[4] += -0.5 * (double)(r[0] * fij[1] + r[1] * fij[0]);
-      acc[5] += -0.5 * (double)(r[0] * fij[2] + r[2] * fij[0]);
-      acc[6] += -0.5 * (double)(r[1] * fij[2] + r[2] * fij[1]);
+      acc[1] += (double)(r[0] * fi[0]);
+      acc[2] += (double)(r[1] * fi[1]);
+      acc[3] += (double)(r[2] * fi[2]);
+      acc[4] += 0.5 * (double)(r[0] * fi[1] + r[1] * fi[0]);
+      acc[5] += 0.5 * (double)(r[0] * fi[2] + r[2] * fi[0]);
+      acc[6] += 0.5 * (double)(r[1] * fi[2] + r[2] * fi[1]);
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) {

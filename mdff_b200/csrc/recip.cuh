@@ -17,6 +17,7 @@
 //   k_rec_field_sum : chunk sum, E = -2 pi B G, F = q E + 2 pi B H, scaled
 #pragma once
 #include "common.cuh"
+#include "realspace.cuh"
 
 namespace mdff {
 
@@ -510,15 +511,7 @@ static __global__ void __launch_bounds__(256) k_dd_cached_rec(
   int n = cn[i];
   size_t base = (size_t)i * cap;
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  for (int k = lane; k < n; k += 32) {
-    float4 r = cr[base + k];
-    float B1 = cb1[base + k];
-    float4 m = mu[cj[base + k]];
-    float rm = r.x * m.x + r.y * m.y + r.z * m.z;
-    ex += r.w * r.x * rm - B1 * m.x;
-    ey += r.w * r.y * rm - B1 * m.y;
-    ez += r.w * r.z * rm - B1 * m.z;
-  }
+  dd_cached_row(mu, cr, cb1, cj, base, n, lane, ex, ey, ez);
   double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {

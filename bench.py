@@ -334,7 +334,7 @@ def run_ours(args, rank, world, local_rank):
     value, total_s = replicas.throughput(world, args.steps, sum(step_ms) / 1e3)
     res = dict(value=value, ms_per_step=1e3 * total_s / args.steps, launches=launches,
                cg_iters_mean=float(np.mean(iters)), clocks=clocks, wl=wl,
-               kms=kms, kl=kl, kw=kw)
+               kms=kms, kl=kl, kw=kw, prof_steps=min(args.steps, 30))
     if rank != 0:
         return res, None
     # ---- extras on rank 0 ---------------------------------------------------
@@ -579,6 +579,10 @@ def roofline_block(res, extra):
     achieved = ops_per_launch / (avg_ms * 1e-3) / 1e12
     peak = extra["peak_fp32_tflops"]
     share = {KCLS[i]: round(float(kms[i] / kms.sum()), 4) for i in range(len(KCLS)) if kms[i] > 0}
+    # kernel time per step of each class in the profiling pass (one stream,
+    # events around every launch), against the overlapped step's ms_per_step
+    per_step = {KCLS[i]: round(float(kms[i] / res["prof_steps"]), 4)
+                for i in range(len(KCLS)) if kms[i] > 0}
     tr = TRAFFIC.get(KCLS[c])
     return {"kernel": KCLS[c], "bound": "fp32_fma", "achieved": round(achieved, 3),
             "peak": round(peak, 3), "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
@@ -590,7 +594,7 @@ def roofline_block(res, extra):
             "note": "achieved counts algorithmic ops of the class (all its launches); the FP32 CG-operator "
                     "launches of the reciprocal classes run on the tcgen05 tensor cores (split TF32), so "
                     "frac compares with the CUDA-core FP32 ceiling",
-            "time_share": share}
+            "time_share": share, "class_ms_per_step": per_step}
 
 
 def run_reference(args, rank, world):

@@ -9,7 +9,7 @@
 // = alpha^-1 - T symmetric, so
 //     dJ/dtheta = dJ/dtheta|_mu - lambda . dR/dtheta,   H lambda = dJ/dmu,
 // one adjoint solve with the forward's own PCG operator.  Every term
-// differentiates the expressions the forward evaluates (es_force_pair, the
+// differentiates the expressions the forward evaluates (es_force_ipair, the
 // short-range pair, the reciprocal sums), not an idealised energy, so the
 // gradient is that of the computed forces to the solver tolerance.
 //

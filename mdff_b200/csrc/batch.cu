@@ -347,10 +347,6 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
       return MDFF_ERR_BAD_ARGS;
     }
     mdff_params p = psets[ps];
-    if (p.thole_type != MDFF_THOLE_NONE) {
-      h->err = "Thole functions are not built into the batched engine (use mdff_gpu_create)";
-      return MDFF_ERR_UNSUPPORTED;
-    }
     if (p.algo_moment_from_pola != MDFF_ALGO_SCF) {
       h->err = "the kO dipole algorithms are not built into the batched engine (use mdff_gpu_create)";
       return MDFF_ERR_UNSUPPORTED;
@@ -404,6 +400,7 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
     if (S.task_qd) fl |= BF_QD;
     if (S.task_dd) fl |= BF_DD;
     if (P.lsurf) fl |= BF_SURF;
+    if (P.thole_type != MDFF_THOLE_NONE) fl |= BF_THOLE;
     if (S.ldip_static) fl |= BF_DIPST;
     B.flags = fl;
     B.trunc = P.trunc;
@@ -733,11 +730,16 @@ int mdff_gpu_batch_fit_define(mdff_batch_handle h, int nparam, const int* kind, 
     if (h) h->err = "0 <= nparam <= 16 and kind/t1/t2 arrays required";
     return MDFF_ERR_BAD_ARGS;
   }
-  for (int c = 0; c < h->nconf; ++c)
+  for (int c = 0; c < h->nconf; ++c) {
     if (h->pconf[c].lsurf) {
       h->err = "the fit gradient does not cover the surface term (lsurf)";
       return MDFF_ERR_BAD_ARGS;
     }
+    if (h->pconf[c].thole_type != MDFF_THOLE_NONE) {
+      h->err = "the fit gradient does not cover Thole functions";
+      return MDFF_ERR_UNSUPPORTED;
+    }
+  }
   int ntmin = MDFF_NTYPEMAX;
   for (const auto& p : h->base) ntmin = std::min(ntmin, p.ntype);
   h->nparam = nparam;

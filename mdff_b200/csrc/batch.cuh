@@ -56,7 +56,7 @@ enum {
 
 enum {
   BF_COUL = 1, BF_SR = 2, BF_BMH = 4, BF_BMHFTD = 8, BF_LJ = 16, BF_POLAR = 32,
-  BF_QQ = 64, BF_QD = 128, BF_DD = 256, BF_SURF = 512, BF_DIPST = 1024
+  BF_QQ = 64, BF_QD = 128, BF_DD = 256, BF_SURF = 512, BF_DIPST = 1024, BF_THOLE = 2048
 };
 
 struct BConf {
@@ -476,7 +476,7 @@ __device__ void bfield(const BatchArgs& a, const BCtx& X, const BShared& S, int 
         double qj = QQ ? sj.w : 0.0;
         if (!dd && (!QQ || qj == 0.0)) continue;
         es_field_pair<R, QQ, DD>(S.es, c.ntype, i, j, ti, S.t[j], rx, ry, rz, r2, (R)c.alpha, damp,
-                                 qj, dd, mx, my, mz, ex, ey, ez);
+                                 qj, dd, mx, my, mz, ex, ey, ez, (c.flags & BF_THOLE) ? 1 : 0);
       }
     }
     double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
@@ -582,29 +582,28 @@ __device__ void bforce(const BatchArgs& a, const BCtx& X, const BShared& S, doub
       double qj = sj.w;
       double4 muj = S.v[j];
       bool i_is_a = half_mask(i, j);
-      R sg = i_is_a ? R(1) : R(-1);
-      R r[3] = {sg * (R)rxd, sg * (R)ryd, sg * (R)rzd};
-      int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
-      R qa = (R)(i_is_a ? qi : qj), qb = (R)(i_is_a ? qj : qi);
-      double4 ma4 = i_is_a ? mui : muj, mb4 = i_is_a ? muj : mui;
-      R ma[3] = {(R)ma4.x, (R)ma4.y, (R)ma4.z}, mb[3] = {(R)mb4.x, (R)mb4.y, (R)mb4.z};
-      bool dip_a = (ma4.x != 0.0 || ma4.y != 0.0 || ma4.z != 0.0);
-      bool dip_b = (mb4.x != 0.0 || mb4.y != 0.0 || mb4.z != 0.0);
-      R u, fij[3], Ea[3], Eb[3];
-      es_force_pair<R>(S.es[ta * c.ntype + tb], 1, (R)r2d, (R)c.alpha, r, qa, qb, ma, mb, dip_a,
-                       dip_b, task_qq, task_qd, task_dd, u, fij, Ea, Eb);
+      const ESPair& P = S.es[(i_is_a ? ti : tj) * c.ntype + (i_is_a ? tj : ti)];
+      R r[3] = {(R)rxd, (R)ryd, (R)rzd};
+      R mi[3] = {(R)mui.x, (R)mui.y, (R)mui.z}, mj[3] = {(R)muj.x, (R)muj.y, (R)muj.z};
+      bool dip_i = (mui.x != 0.0 || mui.y != 0.0 || mui.z != 0.0);
+      bool dip_j = (muj.x != 0.0 || muj.y != 0.0 || muj.z != 0.0);
+      R u, fi[3], Ei[3];
+      // the single engine's pair (i's frame; Thole on the dd field and energy
+      // where the pair's table entry has it)
+      es_force_ipair<R, 0, true>(P, i_is_a, P.ldamp != 0, (R)r2d, (R)c.alpha, r, (R)qi, (R)qj, mi,
+                                 mj, dip_i, dip_j, task_qq, task_qd, task_dd, u, fi, Ei);
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        f[d] += (double)(i_is_a ? -fij[d] : fij[d]);
-        e[d] += (double)(i_is_a ? Ea[d] : Eb[d]);
+        f[d] += (double)fi[d];
+        e[d] += (double)Ei[d];
       }
       acc[0] += 0.5 * (double)u;
-      acc[1] += -(double)(r[0] * fij[0]);
-      acc[2] += -(double)(r[1] * fij[1]);
-      acc[3] += -(double)(r[2] * fij[2]);
-      acc[4] += -0.5 * (double)(r[0] * fij[1] + r[1] * fij[0]);
-      acc[5] += -0.5 * (double)(r[0] * fij[2] + r[2] * fij[0]);
-      acc[6] += -0.5 * (double)(r[1] * fij[2] + r[2] * fij[1]);
+      acc[1] += (double)(r[0] * fi[0]);
+      acc[2] += (double)(r[1] * fi[1]);
+      acc[3] += (double)(r[2] * fi[2]);
+      acc[4] += 0.5 * (double)(r[0] * fi[1] + r[1] * fi[0]);
+      acc[5] += 0.5 * (double)(r[0] * fi[2] + r[2] * fi[0]);
+      acc[6] += 0.5 * (double)(r[1] * fi[2] + r[2] * fi[1]);
     }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {

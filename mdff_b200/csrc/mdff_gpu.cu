@@ -131,6 +131,7 @@ struct mdff_ctx {
   double4 *d_r = nullptr, *d_z = nullptr, *d_pv = nullptr, *d_qv = nullptr, *d_Tp = nullptr;
   float4* d_mu32 = nullptr;      // FP32 copy of the dipoles of an FP32 pass
   float4* d_qm32 = nullptr;      // (mu_tot, q) in FP32 for the mixed final pass
+  double4* d_Edd = nullptr;      // cached real-space dipole field of a CG operator (side stream)
   // Tang-Toennies order shared by every damped ion pair (both field roles), the
   // compile-time order of the damped real-space kernels; 0 = orders differ
   int tt_k = 0;
@@ -475,6 +476,7 @@ static int alloc_list(mdff_ctx* h, int cap) {
     DALLOC(h->d_ddb1, (size_t)h->natm * cap);
     DALLOC(h->d_ddj, (size_t)h->natm * cap);
     if (!h->d_ddn) DALLOC(h->d_ddn, h->natm);
+    if (!h->d_Edd) DALLOC(h->d_Edd, h->natm);
   }
   h->stats.list_capacity = cap * h->natm;
   return MDFF_OK;
@@ -866,12 +868,24 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
     prof_end(h, pr);
     return rec_pass(h, false, mu, 0, 1, 0, E, nullptr, sf);
   }
+  // the CG operator with its FP32 operands ready (inside the CG graph too):
+  // the cached real-space dipole field on the side stream beside the
+  // reciprocal pass, whose rs_join joins it before the final kernel adds it
+  const bool dd_side = fused && weights_ready && h->overlap && !h->prof && h->d_Edd;
+  if (dd_side) {
+    if ((s = fork_to(h, h->st_rs))) return s;
+    h->rs_open = true;
+    k_dd_cached_part<<<nb, 256, 0, h->st_rs>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn,
+                                                h->L.cap, n, h->d_Edd);
+    LAUNCH_CHECK();
+  }
   s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, sf, h->d_mu32, fused ? &nch : nullptr, weights_ready);
   if (s) return s;
   int pr = prof_begin(h, KC_ESFIELD, 0);
   if (fused)
     k_dd_cached_rec<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n,
-                                           h->d_G, nch, h->d_cell, 2.0 * (2.0 * (kTwoPi / h->omega)), sf, E);
+                                           h->d_G, nch, h->d_cell, 2.0 * (2.0 * (kTwoPi / h->omega)), sf, E,
+                                           dd_side ? h->d_Edd : nullptr);
   else if (fp32 && dd_mask == 1 && h->dd_cache_ok)
     k_dd_cached<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n, E);
   else
@@ -1811,13 +1825,18 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   CK(cudaMemcpyAsync(h->d_nbtab, nb.data(), sizeof(NBPair) * nb.size(), cudaMemcpyHostToDevice, h->st));
   CK(cudaMemcpyAsync(h->d_estab, es.data(), sizeof(ESPair) * es.size(), cudaMemcpyHostToDevice, h->st));
   {
+    // a role with c = 0 damps nothing at any order (f = 1, fd = 0 exactly),
+    // so only the roles with c != 0 have to share the order
     int k = -1;
     bool same = true;
     for (const ESPair& e : es) {
       if (!e.ldamp) continue;
-      for (int o : {e.ka, e.kb}) {
-        if (k < 0) k = o;
-        same = same && o == k;
+      const int ord[2] = {e.ka, e.kb};
+      const double c[2] = {e.ca, e.cb};
+      for (int r = 0; r < 2; ++r) {
+        if (c[r] == 0.0) continue;
+        if (k < 0) k = ord[r];
+        same = same && ord[r] == k;
       }
     }
     h->tt_k = (same && k == 4) ? 4 : 0;  // the instantiated order (examples use 4)
@@ -2277,7 +2296,7 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
                   h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
-                  h->d_lwfc, h->d_mu_wfc, h->d_qm32};
+                  h->d_lwfc, h->d_mu_wfc, h->d_qm32, h->d_Edd};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);

@@ -374,7 +374,7 @@ __device__ __forceinline__ void es_field_pair(const ESPair* stab, int ntype, int
       bool i_is_a = half_mask(i, j);
       int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
       const ESPair& P = stab[ta * ntype + tb];
-      if (P.ldamp) {
+      if (P.ldamp && (i_is_a ? P.ca : P.cb) != 0.0) {  // c = 0 damps nothing
         R fdm, fdd;
         if (i_is_a)
           tt_damp_k<R, K>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
@@ -526,7 +526,7 @@ static __global__ void __launch_bounds__(256) k_static_cache(
             bool i_is_a = half_mask(i, j);
             int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
             const ESPair& P = stab[ta * ntype + tb];
-            if (P.ldamp) {
+            if (P.ldamp && (i_is_a ? P.ca : P.cb) != 0.0) {  // c = 0 damps nothing
               float fdm, fdd;
               if (i_is_a)
                 tt_damp_k<float, K>((float)P.ba, (float)P.ca, g.d, P.ka, fdm, fdd);
@@ -607,6 +607,23 @@ __device__ __forceinline__ void dd_cached_row(const float4* __restrict__ mu,
   }
 }
 
+// the cached dipole field of every row as a warp-summed double4 (0 for rows
+// without partners), for the CG operator to add in its final kernel: it runs
+// on a side stream beside the reciprocal pass of the same operator
+static __global__ void __launch_bounds__(256) k_dd_cached_part(
+    const float4* __restrict__ mu, const float4* __restrict__ cr, const float* __restrict__ cb1,
+    const int* __restrict__ cj, const int* __restrict__ cn, int cap, int natm,
+    double4* __restrict__ Edd) {
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= natm) return;
+  int n = cn[i];
+  float ex = 0.f, ey = 0.f, ez = 0.f;
+  dd_cached_row(mu, cr, cb1, cj, (size_t)i * cap, n, lane, ex, ey, ez);
+  double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
+  if (lane == 0) Edd[i] = make_double4(dx, dy, dz, 0.0);
+}
+
 // FP32 dipole field of mu (float4) from the pair cache of k_static_cache:
 // E_i += sum_m T2(r_im) mu_j over the polarisable partners (k_es_field<float,
 // false, true> with dd_mask = 1, without the per-pair radial functions)
@@ -636,84 +653,6 @@ static __global__ void __launch_bounds__(256) k_dd_cached(
 // (tau is the reference's  - sum (r_j f_k + r_k f_j)  before *0.5/omega).
 constexpr int kESPart = 7;
 
-// one canonical pair of the final real-space pass (multipole_ES_dir tasks qq,
-// qd, dd with damping, ewald_dir.f90:528-644): a = "ia", b = "ja", r = r_a - r_b.
-// Out: pair energy u, f_ij (the reference's f_i -= f_ij, f_j += f_ij,
-// ewald_dir.f90:714-721), fields Ea on a and Eb on b.
-// THOLE: Thole functions on the dd field and energy (P.thole); off, the code
-// is the same as without them.
-template <typename R, bool THOLE = false>
-__device__ __forceinline__ void es_force_pair(const ESPair& P, int damp_ind, R d2, R alpha,
-                                              const R (&r)[3], R qa, R qb, const R (&ma)[3],
-                                              const R (&mb)[3], bool dip_a, bool dip_b,
-                                              int task_qq, int task_qd, int task_dd, R& u,
-                                              R (&fij)[3], R (&Ea)[3], R (&Eb)[3]) {
-  Radial<R> g;
-  radial<R, true>(d2, alpha, g);
-  bool ldamp = damp_ind && P.ldamp;
-  R F1d = R(0), F2d = R(0), F1d2 = R(0), F2d2 = R(0);
-  if (ldamp) {
-    R fdm, fdd, fdm2, fdd2;
-    tt_damp<R>((R)P.ba, (R)P.ca, g.d, P.ka, fdm, fdd);
-    tt_damp<R>((R)P.bb, (R)P.cb, g.d, P.kb, fdm2, fdd2);
-    F1d = R(1) - fdm;
-    F2d = F1d + (g.d / R(3)) * fdd;
-    F1d2 = R(1) - fdm2;
-    F2d2 = F1d2 + (g.d / R(3)) * fdd2;
-  }
-  R B0 = g.dm1 * g.F0, B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5, B3 = R(15) * g.F3 * g.dm7;
-  R B1d = F1d * g.dm3, B2d = R(3) * F2d * g.dm5, B1d2 = F1d2 * g.dm3, B2d2 = R(3) * F2d2 * g.dm5;
-  R rma = r[0] * ma[0] + r[1] * ma[1] + r[2] * ma[2];
-  R rmb = r[0] * mb[0] + r[1] * mb[1] + r[2] * mb[2];
-  R mab = ma[0] * mb[0] + ma[1] * mb[1] + ma[2] * mb[2];
-  u = R(0);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) fij[c] = Ea[c] = Eb[c] = R(0);
-  if (task_qq) {
-    u += qa * qb * B0;
-    R ca = qb * (B1 - (ldamp ? B1d : R(0)));
-    R cb = -qa * (B1 - (ldamp ? B1d2 : R(0)));
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      Ea[c] += ca * r[c];
-      Eb[c] += cb * r[c];
-      fij[c] += -qa * qb * B1 * r[c];
-    }
-  }
-  if (task_dd && dip_a && dip_b) {
-    // energy and field with T2_thole (ewald_dir.f90:557-572), force with T3
-    R B1t = B1, B2t = B2;
-    if (THOLE && P.thole) {
-      R F1t = g.F1, F2t = g.F2;
-      thole_radial<R>(P, g.d, F1t, F2t);
-      B1t = F1t * g.dm3;
-      B2t = R(3) * F2t * g.dm5;
-    }
-    u += -(B2t * rma * rmb - B1t * mab);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      Ea[c] += B2t * r[c] * rmb - B1t * mb[c];
-      Eb[c] += B2t * r[c] * rma - B1t * ma[c];
-      fij[c] -= -B3 * rma * rmb * r[c] + B2 * (mab * r[c] + ma[c] * rmb + mb[c] * rma);
-    }
-  }
-  if (task_qd && (dip_a || dip_b)) {
-    u += qa * B1 * rmb - qb * B1 * rma;
-    if (ldamp) u += -qa * B1d2 * rmb + qb * B1d * rma;
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      R T2mb = B2 * r[c] * rmb - B1 * mb[c];
-      R T2ma = B2 * r[c] * rma - B1 * ma[c];
-      fij[c] += -qa * T2mb + qb * T2ma;
-      if (ldamp) {
-        R T2dma = B2d * r[c] * rma - B1d * ma[c];
-        R T2d2mb = B2d2 * r[c] * rmb - B1d2 * mb[c];
-        fij[c] += -qb * T2dma + qa * T2d2mb;
-      }
-    }
-  }
-}
-
 // one pair of the final real-space pass seen from ion i, r = r_i - r_j: the
 // qq, qd and dd blocks of multipole_ES_dir (ewald_dir.f90:528-644) written in
 // i's frame.  The reference's formulas are role-symmetric once the damping of
@@ -736,17 +675,22 @@ __device__ __forceinline__ void es_force_ipair(const ESPair& P, bool i_is_a, boo
   const R B0 = g.dm1 * g.F0, B1 = g.F1 * g.dm3, B2 = R(3) * g.F2 * g.dm5;
   R C1i = B1, C2i = B2, C1j = B1, C2j = B2;  // B - B_damped for the field on i / on j
   if (ldamp) {
+    // a role with c = 0 damps nothing (f = 1, fd = 0 at any order): skipped
+    // (the field on a non-polarisable ion, warp-uniform for its rows)
+    const R ci = (R)(i_is_a ? P.ca : P.cb), cj = (R)(i_is_a ? P.cb : P.ca);
     R fdm, fdd;
-    tt_damp_k<R, K>((R)(i_is_a ? P.ba : P.bb), (R)(i_is_a ? P.ca : P.cb), g.d, i_is_a ? P.ka : P.kb,
-                    fdm, fdd);
-    R F1d = R(1) - fdm;
-    C1i = B1 - F1d * g.dm3;
-    C2i = B2 - R(3) * (F1d + (g.d / R(3)) * fdd) * g.dm5;
-    tt_damp_k<R, K>((R)(i_is_a ? P.bb : P.ba), (R)(i_is_a ? P.cb : P.ca), g.d, i_is_a ? P.kb : P.ka,
-                    fdm, fdd);
-    F1d = R(1) - fdm;
-    C1j = B1 - F1d * g.dm3;
-    C2j = B2 - R(3) * (F1d + (g.d / R(3)) * fdd) * g.dm5;
+    if (ci != R(0)) {
+      tt_damp_k<R, K>((R)(i_is_a ? P.ba : P.bb), ci, g.d, i_is_a ? P.ka : P.kb, fdm, fdd);
+      const R F1d = R(1) - fdm;
+      C1i = B1 - F1d * g.dm3;
+      C2i = B2 - R(3) * (F1d + (g.d / R(3)) * fdd) * g.dm5;
+    }
+    if (cj != R(0)) {
+      tt_damp_k<R, K>((R)(i_is_a ? P.bb : P.ba), cj, g.d, i_is_a ? P.kb : P.ka, fdm, fdd);
+      const R F1d = R(1) - fdm;
+      C1j = B1 - F1d * g.dm3;
+      C2j = B2 - R(3) * (F1d + (g.d / R(3)) * fdd) * g.dm5;
+    }
   }
   const R rmi = r[0] * mi[0] + r[1] * mi[1] + r[2] * mi[2];
   const R rmj = r[0] * mj[0] + r[1] * mj[1] + r[2] * mj[2];

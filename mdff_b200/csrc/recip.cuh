@@ -493,7 +493,7 @@ static __global__ void __launch_bounds__(256) k_dd_cached_rec(
     const float4* __restrict__ mu, const float4* __restrict__ cr, const float* __restrict__ cb1,
     const int* __restrict__ cj, const int* __restrict__ cn, int cap, int natm,
     const double4* __restrict__ Gpart, int nchunk, const CellC* __restrict__ cell, double scale,
-    SelfField sf, double4* __restrict__ E) {
+    SelfField sf, double4* __restrict__ E, const double4* __restrict__ Edd) {
   int lane = threadIdx.x & 31;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= natm) return;
@@ -508,11 +508,20 @@ static __global__ void __launch_bounds__(256) k_dd_cached_rec(
       g[2] += v.z;
     }
   double4 mi = (lane == 0 && sf.on && sf.mu) ? sf.mu[i] : make_double4(0, 0, 0, 0);
-  int n = cn[i];
-  size_t base = (size_t)i * cap;
-  float ex = 0.f, ey = 0.f, ez = 0.f;
-  dd_cached_row(mu, cr, cb1, cj, base, n, lane, ex, ey, ez);
-  double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
+  // the cached dipole field: already summed by k_dd_cached_part (Edd), else here
+  double dx, dy, dz;
+  if (Edd) {
+    double4 v = Edd[i];
+    dx = v.x;
+    dy = v.y;
+    dz = v.z;
+  } else {
+    float ex = 0.f, ey = 0.f, ez = 0.f;
+    dd_cached_row(mu, cr, cb1, cj, (size_t)i * cap, cn[i], lane, ex, ey, ez);
+    dx = warp_sum((double)ex);
+    dy = warp_sum((double)ey);
+    dz = warp_sum((double)ez);
+  }
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     g[a] += __shfl_xor_sync(FULL_MASK, g[a], 1);

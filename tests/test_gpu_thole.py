@@ -1,8 +1,8 @@
 """Thole functions on the dipole-dipole field and energy (ewald_dir.f90:305-430):
 the four variants (linear, expon1, expon2, gauss) of the FP64 engine against
 the CPU oracle (the reference's SCF to a tight tolerance) to 1e-9, the mixed
-engine (CG) to the 1e-5 force bar, and Thole visibly active.  The batched
-engine rejects Thole parameters."""
+engine (CG) to the 1e-5 force bar, and Thole visibly active; the batched
+engine with Thole against the same oracle (its fit gradient rejects Thole)."""
 import numpy as np
 import pytest
 
@@ -56,8 +56,42 @@ def test_thole_mixed_cg(oracle, case):
     assert rms_rel(g["mu"], o["mu"]) <= 1e-5
 
 
-def test_batch_rejects_thole():
+def test_batch_thole_matches_oracle(oracle):
+    """The batched engine with the four Thole functions in one batch (one
+    parameter set each), FP64: every box equals the oracle to 1e-9; mixed:
+    within the 1e-5 force bar."""
+    systs = [_system(*c) for c in CASES]
+    for prec, tol in ((_abi.PREC_FP64, None), (_abi.PREC_MIXED, 1e-5)):
+        psets, configs = [], []
+        for k, s in enumerate(systs):
+            p = params_copy(s.params)
+            p.precision = prec
+            p.solver = _abi.SOLVER_CG
+            p.cg_tol = 1e-12
+            p.cg_max_iter = 2000
+            psets.append(p)
+            configs.append((k, [p.natmi[0], p.natmi[1]], s.cell))
+        P = np.concatenate([s.pos for s in systs])
+        with BatchEngine(psets, configs) as eng:
+            out = eng.engforce(P[:, 0], P[:, 1], P[:, 2])
+            offs = eng.offsets
+        for k, s in enumerate(systs):
+            o = oracle.Oracle(s.params, s.cell).engforce(*s.soa())
+            a, b = offs[k], offs[k + 1]
+            g = {key: out[key][a:b] for key in ("fx", "fy", "fz", "mu", "ef")}
+            g.update(out["conf"][k])
+            if tol is None:
+                compare(g, o, 1e-9)
+            else:
+                assert rms_rel(forces(g), forces(o)) <= tol
+
+
+def test_batch_fit_rejects_thole():
+    """The fit gradient does not cover Thole functions."""
     s = _system(*CASES[0])
     p = params_copy(s.params)
-    with pytest.raises(MdffError):
-        BatchEngine([p], [(0, [p.natmi[0], p.natmi[1]], s.cell)])
+    p.solver = _abi.SOLVER_CG
+    with BatchEngine([p], [(0, [p.natmi[0], p.natmi[1]], s.cell)]) as eng:
+        with pytest.raises(MdffError) as e:
+            eng.fit_define([(_abi.FIT_A, 0, 1)])
+        assert e.value.status == _abi.MDFF_ERR_UNSUPPORTED

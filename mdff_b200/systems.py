@@ -15,6 +15,10 @@ from . import _abi
 from .params import make_params
 
 TIME_UNIT = 98.2269514139276      # ps -> internal time (constants.f90:90)
+# ASPC order of the polarisable MD workloads: the order the reference's own
+# MD decks use (examples/ex12/config/mdff/control_md.F:53,
+# examples/ex14/config/control_md_full_run_pim.F:46)
+ASPC_ORDER_MD = 4
 BOLTZ_UNIT = 8.61734229648141e-05  # eV/K (constants.f90:89)
 RHO_UNIT = 1.660538782             # g/cm3 -> amu/A^3 (constants.f90:93)
 J_TO_EV = 1.0 / 1.602176487e-19    # constants.f90:76 evtoj
@@ -195,7 +199,7 @@ def mgo(ncell=10, seed=4321, density=3.58, jitter=0.2, temp=2000.0, rcut=10.0,
               ldip_polar=[0, 1], poldip_iso={1: 1.6},
               ldip_damping={(1, 0, 1): 1}, pol_damp_b={(1, 0, 1): 3.0},
               pol_damp_c={(1, 0, 1): 1.0}, pol_damp_k={(1, 0, 1): 4},
-              conv_tol_ind=1e-8, extrapolate_order=2)
+              conv_tol_ind=1e-8, extrapolate_order=ASPC_ORDER_MD)
     kw.update(extra)
     p = make_params([nf, nf], **kw)
     mass = np.concatenate([np.full(nf, 24.305), np.full(nf, 15.9994)])
@@ -273,7 +277,7 @@ def sio2(nsio2=4000, seed=2024, density=2.2, temp=300.0, rcut=10.0, alpha=0.3, k
               pol_damp_b={(1, 1, 1): 5.58406251008641721012, (1, 0, 1): 3.66418041600447487325},
               pol_damp_c={(1, 1, 1): 2.8904937083, (1, 0, 1): 1.4460000000},
               pol_damp_k={(1, 1, 1): 4, (1, 0, 1): 4},
-              conv_tol_ind=1e-8, extrapolate_order=2)
+              conv_tol_ind=1e-8, extrapolate_order=ASPC_ORDER_MD)
     kw.update(extra)
     p = make_params([nsio2, 2 * nsio2], **kw)
     mass = np.concatenate([np.full(nsio2, 28.0855), np.full(2 * nsio2, 15.9994)])

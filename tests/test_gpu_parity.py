@@ -61,16 +61,18 @@ def test_repeat_calls_are_deterministic():
     assert a["u_coul"] == b["u_coul"]
 
 
-def test_aspc_md_sequence_matches_oracle(oracle):
-    """calc='md' with ASPC order 2 over several moving steps: the predictor,
-    corrector and history rotation (moment_from_pola.f90:493-598)."""
-    s = systems.random_ionic((20, 20), L=12.5, seed=41, calc=_abi.CALC_MD, extrapolate_order=2,
-                             conv_tol_ind=1e-9)
+@pytest.mark.parametrize("order", [2, 4])
+def test_aspc_md_sequence_matches_oracle(oracle, order):
+    """calc='md' with ASPC orders 2 and 4 (the MD workloads' order) over
+    moving steps past the order ramp: the predictor, corrector and history
+    rotation (moment_from_pola.f90:493-598)."""
+    s = systems.random_ionic((20, 20), L=12.5, seed=41, calc=_abi.CALC_MD,
+                             extrapolate_order=order, conv_tol_ind=1e-9)
     orc = oracle.Oracle(s.params, s.cell)
     rng = np.random.default_rng(1)
     pos = s.pos.copy()
     with ForceEngine(params_copy(s.params), s.cell) as eng:
-        for itime in range(0, 5):
+        for itime in range(0, order + 4):
             soa = tuple(np.ascontiguousarray(pos[:, a]) for a in range(3))
             o = orc.engforce(*soa, itime=itime)
             g = eng.engforce(*soa, itime=itime)

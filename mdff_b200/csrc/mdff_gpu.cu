@@ -49,8 +49,14 @@ enum {
   S_KO = 49,     // 2: kO algorithms (inner residual, find_min dot products)
   S_MOM2 = 52,   // 8: moments of field passes
   S_DISP = 60,
-  S_NSCAL = 64
+  S_CGP = 64,    // CG plan of the graph: 64 rmsd of the FP64 residual, 65 stop,
+                 // 66 outer iterations, 67 recurrence trusted
+  S_NSCAL = 72
 };
+
+// FP32 CG: the recurrence residual drifts from the true one by about the FP32
+// matvec error, a few 1e-6 of the residual it started from (see solve_cg)
+constexpr double kCgGap = 3e-6;
 
 thread_local std::string g_err;
 
@@ -1380,6 +1386,28 @@ __global__ void k_cg_inner_check(double* __restrict__ sc, int npol, int in_graph
   if (in_graph) cudaGraphSetConditional(hc, (rm > sc[5] && it < sc[7]) ? 1u : 0u);
 }
 
+// head of the CG graph: the decision solve_cg's host loop takes after a FP64
+// residual (stop, or the inner tolerance and whether the recurrence is
+// trusted), taken on the device so that the graph follows the residual
+// without a host round trip; sets the WHILE condition of the inner loop
+__global__ void k_cg_plan(double* __restrict__ sc, double* __restrict__ plan, int npol, double tol,
+                          double maxit, int fp32, cudaGraphConditionalHandle hc) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double rmsd = sqrt(sc[1] / (double)npol);
+  const double outer = plan[2];
+  plan[0] = rmsd;
+  const bool stop = rmsd <= tol || sc[6] >= maxit || outer >= 8.0;
+  plan[1] = stop ? 1.0 : 0.0;
+  if (!stop) {
+    const bool trust = !fp32 || kCgGap * rmsd <= 0.5 * tol;
+    sc[5] = !fp32 ? tol : (trust ? 0.5 * tol : fmax(tol, 1e-4 * rmsd));
+    sc[7] = maxit;
+    plan[2] = outer + 1.0;
+    plan[3] = trust ? 1.0 : 0.0;
+  }
+  cudaGraphSetConditional(hc, stop ? 0u : 1u);
+}
+
 __global__ void k_setd2(double* __restrict__ a, double va, double* __restrict__ b, double vb) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     *a = va;
@@ -1418,13 +1446,29 @@ static int build_cg_graph(mdff_ctx* h, bool fp32) {
   h->cg_graph = g;
   cudaGraphConditionalHandle hc;
   CK(cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault));
+  // head: k_cg_plan decides from the FP64 residual and sets the condition
+  double* sc = h->d_scal + S_CG;
+  double* plan = h->d_scal + S_CGP;
+  int npol = h->npol;
+  double tol = h->p.cg_tol > 0 ? h->p.cg_tol : h->p.conv_tol_ind;
+  double maxit = (double)(h->p.cg_max_iter > 0 ? h->p.cg_max_iter : 200);
+  int f32 = fp32 ? 1 : 0;
+  void* kargs[] = {&sc, &plan, &npol, &tol, &maxit, &f32, &hc};
+  cudaKernelNodeParams kp = {};
+  kp.func = (void*)k_cg_plan;
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(32);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = kargs;
+  cudaGraphNode_t head;
+  CK(cudaGraphAddKernelNode(&head, g, nullptr, 0, &kp));
   cudaGraphNodeParams cp = {};
   cp.type = cudaGraphNodeTypeConditional;
   cp.conditional.handle = hc;
   cp.conditional.type = cudaGraphCondTypeWhile;
   cp.conditional.size = 1;
   cudaGraphNode_t node;
-  CK(cudaGraphAddNode(&node, g, nullptr, 0, &cp));
+  CK(cudaGraphAddNode(&node, g, &head, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   bool prof = h->prof, ovl = h->call_overlap;
   h->prof = false;
@@ -1451,8 +1495,10 @@ static int build_cg_graph(mdff_ctx* h, bool fp32) {
 
 // preconditioned CG on (alpha^-1 - T) mu = E_stat.  fp32: matvecs in FP32,
 // residual refreshed with an FP64 matvec (iterative refinement).  The inner
-// iterations run as one CUDA-graph launch (device-side while loop); the
-// host reads one rmsd per outer (FP64 residual) iteration.
+// iterations run as one CUDA-graph launch (device-side while loop, headed by
+// the device-side stop / tolerance decision); the host reads the outcome
+// once per outer (FP64 residual) iteration.  Without the graph (per-kernel
+// profiling) the host loop below takes the same decisions itself.
 static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
@@ -1474,7 +1520,40 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
   double rmsd = HUGE_VAL, rmsd0 = HUGE_VAL;
   int outer = 0, it = 0, nres = 0;
   bool need_residual = true;
-  while (true) {
+  // With the graph, each outer iteration is the FP64 residual followed at once
+  // by the graph, whose head (k_cg_plan) takes the decision below on the
+  // device; the host reads the outcome once per outer iteration.
+  double* plan = h->d_scal + S_CGP;
+  if (use_graph) {
+    k_setd2<<<1, 32, 0, h->st>>>(plan + 1, 0.0, plan + 2, 0.0);
+    LAUNCH_CHECK();
+  }
+  while (use_graph) {
+    if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp))) return s;
+    k_cg_init<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
+                                     h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32);
+    LAUNCH_CHECK();
+    if ((s = reduce_into(h, nb, 2, sc))) return s;
+    ++nres;
+    CK(cudaGraphLaunch(h->cg_exec, h->st));
+    CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * (S_CGP + 4 - S_CG), cudaMemcpyDeviceToHost,
+                       h->st));
+    CK(cudaStreamSynchronize(h->st));
+    const double* hp = h->h_scal + S_CGP;
+    rmsd = hp[0];
+    if (nres == 1) rmsd0 = rmsd;
+    it = (int)h->h_scal[S_CG + 6];
+    if (hp[1] != 0.0) break;  // converged (or a limit) at the FP64 residual
+    if (hp[3] != 0.0) {       // trusted recurrence: its residual is final
+      double rin = h->h_scal[S_CG + 8];
+      if (rin <= h->h_scal[S_CG + 5]) {
+        rmsd = rin;
+        break;
+      }
+      if (it >= maxit) break;
+    }
+  }
+  while (!use_graph) {
     if (need_residual) {
       // true residual (FP64 matvec)
       if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp))) return s;
@@ -1500,20 +1579,15 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
     // (on the 12k-ion SiO2 MD the true residual then ends at <= 0.26 tol),
     // else it reduces the residual by 1e-4 and a new FP64 residual restarts
     // it (iterative refinement).
-    constexpr double kGap = 3e-6;
-    bool trust = !fp32 || kGap * rmsd <= 0.5 * tol;
+    bool trust = !fp32 || kCgGap * rmsd <= 0.5 * tol;
     double tol_in = !fp32 ? tol : (trust ? 0.5 * tol : std::max(tol, 1e-4 * rmsd));
     k_setd2<<<1, 32, 0, h->st>>>(sc + 5, tol_in, sc + 7, (double)maxit);
     LAUNCH_CHECK();
-    if (use_graph) {
-      CK(cudaGraphLaunch(h->cg_exec, h->st));
-    } else {
-      while (true) {
-        if ((s = cg_iteration(h, fp32, 0, 0))) return s;
-        CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * 9, cudaMemcpyDeviceToHost, h->st));
-        CK(cudaStreamSynchronize(h->st));
-        if (!(h->h_scal[S_CG + 8] > tol_in && h->h_scal[S_CG + 6] < maxit)) break;
-      }
+    while (true) {
+      if ((s = cg_iteration(h, fp32, 0, 0))) return s;
+      CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * 9, cudaMemcpyDeviceToHost, h->st));
+      CK(cudaStreamSynchronize(h->st));
+      if (!(h->h_scal[S_CG + 8] > tol_in && h->h_scal[S_CG + 6] < maxit)) break;
     }
     need_residual = true;
     if (trust) {
@@ -1530,7 +1604,7 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
   }
   h->stats.rmsd_initial = rmsd0;
   h->stats.n_fp64_residuals = nres;
-  if (use_graph) h->launches += h->cg_body_launches * it;
+  if (use_graph) h->launches += h->cg_body_launches * it + nres;  // + one k_cg_plan per graph launch
   h->stats.n_pol_iter = it;
   h->stats.rmsd = rmsd;
   h->stats.converged = rmsd <= tol;

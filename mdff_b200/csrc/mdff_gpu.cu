@@ -138,6 +138,13 @@ struct mdff_ctx {
   float4* d_mu32 = nullptr;      // FP32 copy of the dipoles of an FP32 pass
   float4* d_qm32 = nullptr;      // (mu_tot, q) in FP32 for the mixed final pass
   double4* d_Edd = nullptr;      // cached real-space dipole field of a CG operator (side stream)
+  double* d_fsr = nullptr;       // short-range forces SoA [3][natm] (copied into d_force by ef_back)
+  double4* d_hist_save = nullptr;  // ASPC history at the start of a call ([5][natm])
+  // whole-step graph (run_engforce_graph)
+  cudaGraph_t step_graph = nullptr;
+  cudaGraphExec_t step_exec = nullptr;
+  int step_gen = -1;
+  int step_fp32 = -1, step_launches = 0;
   // Tang-Toennies order shared by every damped ion pair (both field roles), the
   // compile-time order of the damped real-space kernels; 0 = orders differ
   int tt_k = 0;
@@ -451,6 +458,7 @@ static int setup_list_cells(mdff_ctx* h) {
     h->L.nc[a] = nc[a];
   }
   int ncell = nc[0] * nc[1] * nc[2];
+  h->gen++;  // the list geometry is captured in the graphs
   if (ncell != h->ncell) {
     cudaFree(h->L.cell_count);
     cudaFree(h->L.cell_start);
@@ -1498,69 +1506,121 @@ static int build_cg_graph(mdff_ctx* h, bool fp32) {
 // iterations run as one CUDA-graph launch (device-side while loop, headed by
 // the device-side stop / tolerance decision); the host reads the outcome
 // once per outer (FP64 residual) iteration.  Without the graph (per-kernel
-// profiling) the host loop below takes the same decisions itself.
-static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
+// profiling) the host loop below takes the same decisions itself.  The pieces
+// (prologue, FP64 residual, the outcome of a graph launch, epilogue) are also
+// the parts of the whole-step graph (run_engforce_graph).
+
+static double cg_tol_of(const mdff_ctx* h) { return h->p.cg_tol > 0 ? h->p.cg_tol : h->p.conv_tol_ind; }
+static int cg_maxit_of(const mdff_ctx* h) { return h->p.cg_max_iter > 0 ? h->p.cg_max_iter : 200; }
+
+// first guess (ASPC predictor for calc md / opt, else alpha E_stat) and the
+// loop counters
+static int cg_prologue(mdff_ctx* h, int itime) {
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
-  bool ismd = h->p.calc == MDFF_CALC_MD, isopt = h->p.calc == MDFF_CALC_OPT;
-  if (ismd || isopt) {
+  if (h->p.calc == MDFF_CALC_MD || h->p.calc == MDFF_CALC_OPT) {
     if ((s = aspc_predict(h, itime))) return s;
   } else {
     k_induce<<<nb, 256, 0, h->st>>>(h->d_Estat, P, n, h->d_mu_ind);
     LAUNCH_CHECK();
   }
-  double tol = h->p.cg_tol > 0 ? h->p.cg_tol : h->p.conv_tol_ind;
-  int maxit = h->p.cg_max_iter > 0 ? h->p.cg_max_iter : 200;
+  double* sc = h->d_scal + S_CG;
+  double* plan = h->d_scal + S_CGP;
+  k_setd2<<<1, 32, 0, h->st>>>(sc + 6, 0.0, sc + 7, (double)cg_maxit_of(h));
+  LAUNCH_CHECK();
+  k_setd2<<<1, 32, 0, h->st>>>(plan + 1, 0.0, plan + 2, 0.0);
+  LAUNCH_CHECK();
+  return MDFF_OK;
+}
+
+// true residual of the current dipoles (FP64 matvec), the CG start vectors
+// and their norms (sc[0], sc[1])
+static int cg_residual(mdff_ctx* h, bool fp32) {
+  int n = h->natm, nb = cdiv(n, 256), s;
+  PolDev P = poldev(h);
+  if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp))) return s;
+  k_cg_init<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
+                                   h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32);
+  LAUNCH_CHECK();
+  return reduce_into(h, nb, 2, h->d_scal + S_CG);
+}
+
+// outcome of one launch of the CG graph from the host copies of the scalars:
+// true when the solve is finished; *rmsd, *it as the loop leaves them
+static bool cg_graph_outcome(const mdff_ctx* h, double* rmsd, int* it) {
+  const double* hs = h->h_scal;
+  const double* hp = hs + S_CGP;
+  *rmsd = hp[0];
+  *it = (int)hs[S_CG + 6];
+  if (hp[1] != 0.0) return true;  // converged (or a limit) at the FP64 residual
+  if (hp[3] != 0.0) {             // trusted recurrence: its residual is final
+    double rin = hs[S_CG + 8];
+    if (rin <= hs[S_CG + 5]) {
+      *rmsd = rin;
+      return true;
+    }
+    if (*it >= cg_maxit_of(h)) return true;
+  }
+  return false;
+}
+
+// u_pol of the converged dipoles, which become the newest ASPC history entry
+static int cg_epilogue(mdff_ctx* h) {
+  int n = h->natm, nb = cdiv(n, 256), s;
+  PolDev P = poldev(h);
+  k_upol_part<<<nb, 256, 0, h->st>>>(h->d_mu_ind, P, n, h->d_part);
+  LAUNCH_CHECK();
+  if ((s = reduce_into(h, nb, 1, h->d_scal + S_UPOL))) return s;
+  CK(cudaMemcpyAsync(h->d_hist, h->d_mu_ind, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->st));
+  return MDFF_OK;
+}
+
+static void cg_stats(mdff_ctx* h, double rmsd0, double rmsd, int it, int nres) {
+  h->stats.rmsd_initial = rmsd0;
+  h->stats.n_fp64_residuals = nres;
+  h->stats.n_pol_iter = it;
+  h->stats.rmsd = rmsd;
+  h->stats.converged = rmsd <= cg_tol_of(h);
+}
+
+// further outer iterations after a first graph launch that did not finish
+// the solve (the FP64 residual of the dipoles it left, then the CG graph)
+// (*first: the rmsd of the first FP64 residual of the solve, when it is this call's)
+static int cg_continue(mdff_ctx* h, bool fp32, double* rmsd, int* it, int* nres, double* first) {
+  int s;
+  while (true) {
+    if ((s = cg_residual(h, fp32))) return s;
+    ++*nres;
+    CK(cudaGraphLaunch(h->cg_exec, h->st));
+    CK(cudaMemcpyAsync(h->h_scal + S_CG, h->d_scal + S_CG, sizeof(double) * (S_CGP + 4 - S_CG),
+                       cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (*nres == 1 && first) *first = h->h_scal[S_CGP];
+    if (cg_graph_outcome(h, rmsd, it)) return MDFF_OK;
+  }
+}
+
+static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
+  int s;
+  double tol = cg_tol_of(h);
+  int maxit = cg_maxit_of(h);
   double* sc = h->d_scal + S_CG;
   bool use_graph = !h->prof;
   if (use_graph && (h->cg_exec == nullptr || h->cg_gen != h->gen || h->cg_fp32 != (fp32 ? 1 : 0)))
     if ((s = build_cg_graph(h, fp32))) return s;
-  k_setd2<<<1, 32, 0, h->st>>>(sc + 6, 0.0, sc + 7, (double)maxit);
-  LAUNCH_CHECK();
+  if ((s = cg_prologue(h, itime))) return s;
   double rmsd = HUGE_VAL, rmsd0 = HUGE_VAL;
   int outer = 0, it = 0, nres = 0;
-  bool need_residual = true;
-  // With the graph, each outer iteration is the FP64 residual followed at once
-  // by the graph, whose head (k_cg_plan) takes the decision below on the
-  // device; the host reads the outcome once per outer iteration.
-  double* plan = h->d_scal + S_CGP;
   if (use_graph) {
-    k_setd2<<<1, 32, 0, h->st>>>(plan + 1, 0.0, plan + 2, 0.0);
-    LAUNCH_CHECK();
+    if ((s = cg_continue(h, fp32, &rmsd, &it, &nres, &rmsd0))) return s;
+    h->launches += h->cg_body_launches * it + nres;  // + one k_cg_plan per graph launch
+    cg_stats(h, rmsd0, rmsd, it, nres);
+    return cg_epilogue(h);
   }
-  while (use_graph) {
-    if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp))) return s;
-    k_cg_init<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
-                                     h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32);
-    LAUNCH_CHECK();
-    if ((s = reduce_into(h, nb, 2, sc))) return s;
-    ++nres;
-    CK(cudaGraphLaunch(h->cg_exec, h->st));
-    CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * (S_CGP + 4 - S_CG), cudaMemcpyDeviceToHost,
-                       h->st));
-    CK(cudaStreamSynchronize(h->st));
-    const double* hp = h->h_scal + S_CGP;
-    rmsd = hp[0];
-    if (nres == 1) rmsd0 = rmsd;
-    it = (int)h->h_scal[S_CG + 6];
-    if (hp[1] != 0.0) break;  // converged (or a limit) at the FP64 residual
-    if (hp[3] != 0.0) {       // trusted recurrence: its residual is final
-      double rin = h->h_scal[S_CG + 8];
-      if (rin <= h->h_scal[S_CG + 5]) {
-        rmsd = rin;
-        break;
-      }
-      if (it >= maxit) break;
-    }
-  }
-  while (!use_graph) {
+  bool need_residual = true;
+  while (true) {
     if (need_residual) {
-      // true residual (FP64 matvec)
-      if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp))) return s;
-      k_cg_init<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
-                                       h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32);
-      LAUNCH_CHECK();
-      if ((s = reduce_into(h, nb, 2, sc))) return s;
+      if ((s = cg_residual(h, fp32))) return s;
       CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * 9, cudaMemcpyDeviceToHost, h->st));
       CK(cudaStreamSynchronize(h->st));
       ++nres;
@@ -1591,8 +1651,6 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
     }
     need_residual = true;
     if (trust) {
-      CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * 9, cudaMemcpyDeviceToHost, h->st));
-      CK(cudaStreamSynchronize(h->st));
       double rin = h->h_scal[S_CG + 8];
       it = (int)h->h_scal[S_CG + 6];
       if (rin <= tol_in) {
@@ -1602,32 +1660,23 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
       if (it >= maxit) break;
     }
   }
-  h->stats.rmsd_initial = rmsd0;
-  h->stats.n_fp64_residuals = nres;
-  if (use_graph) h->launches += h->cg_body_launches * it + nres;  // + one k_cg_plan per graph launch
-  h->stats.n_pol_iter = it;
-  h->stats.rmsd = rmsd;
-  h->stats.converged = rmsd <= tol;
-  k_upol_part<<<nb, 256, 0, h->st>>>(h->d_mu_ind, P, n, h->d_part);
-  LAUNCH_CHECK();
-  if ((s = reduce_into(h, nb, 1, h->d_scal + S_UPOL))) return s;
-  CK(cudaMemcpyAsync(h->d_hist, h->d_mu_ind, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->st));
-  return MDFF_OK;
+  cg_stats(h, rmsd0, rmsd, it, nres);
+  return cg_epilogue(h);
 }
 
-// one engforce on the positions in h->d_pos; results stay on the device,
-// scalars land in h->h_scal.
-static int run_engforce(mdff_ctx* h, int itime) {
+// One engforce on the positions in h->d_pos; results stay on the device,
+// scalars land in h->h_scal.  It is three parts: ef_front (list, short
+// range on its side stream, phase tables, static field), the dipole solve,
+// ef_back (the converged dipoles' force pass, the joins and the copies of the
+// scalars and flags to the host), and ef_status on the host after the sync.
+// ef_back can run again on the same front: the short-range pass writes its
+// own buffer, which ef_back copies into the forces before adding the rest.
+
+static int ef_front(mdff_ctx* h, bool fp32) {
   int n = h->natm, s;
-  bool fp32 = h->p.precision == MDFF_PREC_MIXED;
-  h->launches = 0;
-  // side work of an earlier call that ended early is joined first
-  if ((s = sr_join(h)) || (s = rs_join(h))) return s;
-  h->call_overlap = h->overlap && !h->prof;
   k_kardir<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_pos, n, h->d_cell, h->d_s);
   LAUNCH_CHECK();
   if ((s = list_update(h))) return s;
-  CK(cudaMemsetAsync(h->d_force, 0, sizeof(double) * 3 * n, h->st));
   CK(cudaMemsetAsync(h->d_scal, 0, sizeof(double) * S_NSCAL, h->st));
   int nbw = cdiv((long)n * 32, 256);
   if (h->lsr) {
@@ -1642,7 +1691,7 @@ static int run_engforce(mdff_ctx* h, int itime) {
 #define SRK(MODE)                                                                              \
   k_shortrange<double, MODE><<<nbw, 256, 0, ss>>>(h->d_s, h->d_itype, h->L.nbr, h->L.nnb,        \
                                                   h->L.cap, n, h->d_cell, h->d_nbtab, h->ntype,    \
-                                                  h->p.lbmhftd, h->p.trunc, h->d_force, h->d_part2)
+                                                  h->p.lbmhftd, h->p.trunc, h->d_fsr, h->d_part2)
     if (do_bmh && h->p.lnmlj) SRK(3);
     else if (do_bmh) SRK(1);
     else SRK(2);
@@ -1659,18 +1708,30 @@ static int run_engforce(mdff_ctx* h, int itime) {
     CK(cudaMemsetAsync(h->d_mu_ind, 0, sizeof(double4) * n, h->st));
     h->stats.n_pol_iter = 0;
     if (h->lpolar) {
+      // the ASPC history as the call found it (a redo after a list overflow
+      // restores it: the predictors shift it in place)
+      if (h->d_hist_save)
+        CK(cudaMemcpyAsync(h->d_hist_save, h->d_hist, sizeof(double4) * MDFF_ASPC_DEPTH * n,
+                           cudaMemcpyDeviceToDevice, h->st));
       if ((s = static_field(h, fp32))) return s;
-      const int algo = h->p.algo_moment_from_pola;
-      if (h->p.solver == MDFF_SOLVER_CG)
-        s = solve_cg(h, itime, fp32);
-      else if (algo == MDFF_ALGO_KO_V1 || algo == MDFF_ALGO_KO_V2)
-        s = solve_ko_v12(h, itime, fp32, algo == MDFF_ALGO_KO_V2);
-      else if (algo == MDFF_ALGO_KO_V4_1)
-        s = solve_ko_v4(h, itime, fp32);
-      else
-        s = solve_scf(h, itime, fp32);
-      if (s) return s;
     }
+  }
+  return MDFF_OK;
+}
+
+static int ef_solve(mdff_ctx* h, int itime, bool fp32) {
+  if (!h->p.lcoulomb || !h->lpolar) return MDFF_OK;
+  const int algo = h->p.algo_moment_from_pola;
+  if (h->p.solver == MDFF_SOLVER_CG) return solve_cg(h, itime, fp32);
+  if (algo == MDFF_ALGO_KO_V1 || algo == MDFF_ALGO_KO_V2) return solve_ko_v12(h, itime, fp32, algo == MDFF_ALGO_KO_V2);
+  if (algo == MDFF_ALGO_KO_V4_1) return solve_ko_v4(h, itime, fp32);
+  return solve_scf(h, itime, fp32);
+}
+
+static int ef_back(mdff_ctx* h, bool fp32) {
+  int n = h->natm, s;
+  int nbw = cdiv((long)n * 32, 256);
+  if (h->p.lcoulomb) {
     // dipoles of the Wannier centres (moment_from_pola.f90:136-147)
     if (h->lwannier) {
       k_wfc_dipoles<<<nbw, 256, 0, h->st>>>(h->d_s, h->d_itype, h->d_lwfc, h->L.nbr, h->L.nnb, h->L.cap, n,
@@ -1682,10 +1743,17 @@ static int run_engforce(mdff_ctx* h, int itime) {
                                                 h->d_mu_tot, h->d_cata, h->d_q, fp32 ? h->d_qm32 : nullptr);
     LAUNCH_CHECK();
     CK(cudaMemsetAsync(h->d_E, 0, sizeof(double4) * n, h->st));
+  }
+  // the forces start from the short-range pass's (zero without one)
+  if ((s = sr_join(h))) return s;
+  if (h->lsr)
+    CK(cudaMemcpyAsync(h->d_force, h->d_fsr, sizeof(double) * 3 * n, cudaMemcpyDeviceToDevice, h->st));
+  else
+    CK(cudaMemsetAsync(h->d_force, 0, sizeof(double) * 3 * n, h->st));
+  if (h->p.lcoulomb) {
     double cutsq = h->p.cutlongrange * h->p.cutlongrange;
-    // the short-range forces are written first; the real-space force pass
-    // runs beside the reciprocal one, which joins it before its final sum
-    if ((s = sr_join(h))) return s;
+    // the real-space force pass runs beside the reciprocal one, which joins
+    // it before its final sum
     cudaStream_t rs;
     if ((s = rs_fork(h, &rs))) return s;
     int prf = prof_begin(h, KC_ESFORCE, 0);
@@ -1713,14 +1781,17 @@ static int run_engforce(mdff_ctx* h, int itime) {
                       self_field(h, h->d_mu_tot, h->d_scal + S_MOM))))
       return s;
   }
-  if ((s = sr_join(h)) || (s = rs_join(h))) return s;
+  if ((s = rs_join(h))) return s;
   CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(h->h_flags, h->L.flags, sizeof(int) * 4, cudaMemcpyDeviceToHost, h->st));
   CK(cudaMemcpyAsync(h->h_cata, h->d_cata, 3 * sizeof(int), cudaMemcpyDeviceToHost, h->st));
-  CK(cudaStreamSynchronize(h->st));
-  prof_collect(h);
+  return MDFF_OK;
+}
+
+// status of a call from the host copies of its flags (after the sync)
+static int ef_status(mdff_ctx* h) {
   h->stats.list_rebuilds = h->h_flags[3];
-  h->stats.list_needed = h->h_flags[2] * n;
+  h->stats.list_needed = h->h_flags[2] * h->natm;
   if (h->h_flags[1]) return MDFF_ERR_LIST_OVERFLOW;
   if (h->h_cata[1]) {
     h->err = h->h_cata[1] == 2 ? "tensor-core reciprocal kernel launched with too little shared memory"
@@ -1736,10 +1807,196 @@ static int run_engforce(mdff_ctx* h, int itime) {
   return MDFF_OK;
 }
 
+static int run_engforce(mdff_ctx* h, int itime) {
+  bool fp32 = h->p.precision == MDFF_PREC_MIXED;
+  int s;
+  h->launches = 0;
+  // side work of an earlier call that ended early is joined first
+  if ((s = sr_join(h)) || (s = rs_join(h))) return s;
+  h->call_overlap = h->overlap && !h->prof;
+  if ((s = ef_front(h, fp32))) return s;
+  if ((s = ef_solve(h, itime, fp32))) return s;
+  if ((s = ef_back(h, fp32))) return s;
+  CK(cudaStreamSynchronize(h->st));
+  prof_collect(h);
+  return ef_status(h);
+}
+
+// ---------------------------------------------------------------------------
+// Whole-step graph.  In the steady state of an MD run with the CG solver (the
+// list built, the ASPC order ramp past, no per-kernel profiling) one
+// engforce is the same ~130 launches every step; they are replayed as one
+// CUDA graph: ef_front + the CG prologue and first FP64 residual (captured),
+// k_cg_plan, the CG inner WHILE node, the CG epilogue + ef_back (captured).
+// The host then reads the scalars once.  A solve that needs another outer
+// iteration (rare: the trusted-recurrence test failed) continues with the CG
+// graph and repeats ef_back; a list overflow redoes the call without the
+// graph after growing the list.
+
+static bool step_graph_usable(const mdff_ctx* h, int itime) {
+  if (h->prof || !h->have_list || h->lwannier) return false;
+  if (!h->lpolar || !h->p.lcoulomb) return true;
+  if (h->p.solver != MDFF_SOLVER_CG) return false;
+  if (h->p.calc == MDFF_CALC_MD || h->p.calc == MDFF_CALC_OPT)
+    return itime >= h->p.extrapolate_order + 1;  // constant ASPC coefficients
+  return true;
+}
+
+static int capture_begin(mdff_ctx* h) {
+  CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+  return MDFF_OK;
+}
+static int capture_end(mdff_ctx* h, int s, cudaGraph_t* g) {
+  cudaError_t e = cudaStreamEndCapture(h->st, g);
+  if (s) {
+    if (e == cudaSuccess && *g) cudaGraphDestroy(*g);
+    *g = nullptr;
+    return s;
+  }
+  if (e != cudaSuccess) {
+    h->err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+    return MDFF_ERR_CUDA;
+  }
+  return MDFF_OK;
+}
+
+static void step_graph_free(mdff_ctx* h) {
+  if (h->step_exec) cudaGraphExecDestroy(h->step_exec);
+  if (h->step_graph) cudaGraphDestroy(h->step_graph);
+  h->step_exec = nullptr;
+  h->step_graph = nullptr;
+}
+
+static int build_step_graph(mdff_ctx* h, int itime, bool fp32) {
+  step_graph_free(h);
+  const bool cg = h->p.lcoulomb && h->lpolar;
+  int s;
+  if (cg && (h->cg_exec == nullptr || h->cg_gen != h->gen || h->cg_fp32 != (fp32 ? 1 : 0)))
+    if ((s = build_cg_graph(h, fp32))) return s;
+  bool prof = h->prof;
+  h->prof = false;
+  h->call_overlap = h->overlap;
+  int launches0 = h->launches;
+  h->launches = 0;
+  // front: list, short range, tables, static field, CG prologue + FP64 residual
+  cudaGraph_t gA = nullptr, gB = nullptr;
+  if ((s = capture_begin(h))) return s;
+  s = ef_front(h, fp32);
+  if (!s && cg) s = cg_prologue(h, itime);
+  if (!s && cg) s = cg_residual(h, fp32);
+  // a capture ends joined: the short-range pass (~100 us) joins at the end of
+  // the front, which takes longer (static field + FP64 residual)
+  if (!s) s = sr_join(h);
+  if ((s = capture_end(h, s, &gA))) return s;
+  // back: CG epilogue, force pass, copies to the host
+  if ((s = capture_begin(h))) {
+    cudaGraphDestroy(gA);
+    return s;
+  }
+  s = cg ? cg_epilogue(h) : MDFF_OK;
+  if (!s) s = ef_back(h, fp32);
+  if ((s = capture_end(h, s, &gB))) {
+    cudaGraphDestroy(gA);
+    return s;
+  }
+  h->step_launches = h->launches;
+  h->launches = launches0;
+  h->prof = prof;
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  h->step_graph = g;
+  cudaGraphNode_t nA, nB, last;
+  CK(cudaGraphAddChildGraphNode(&nA, g, nullptr, 0, gA));
+  last = nA;
+  if (cg) {
+    // k_cg_plan + the inner WHILE node, as in the CG graph
+    cudaGraphConditionalHandle hc;
+    CK(cudaGraphConditionalHandleCreate(&hc, g, 1, cudaGraphCondAssignDefault));
+    double* sc = h->d_scal + S_CG;
+    double* plan = h->d_scal + S_CGP;
+    int npol = h->npol;
+    double tol = cg_tol_of(h);
+    double maxit = (double)cg_maxit_of(h);
+    int f32 = fp32 ? 1 : 0;
+    void* kargs[] = {&sc, &plan, &npol, &tol, &maxit, &f32, &hc};
+    cudaKernelNodeParams kp = {};
+    kp.func = (void*)k_cg_plan;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(32);
+    kp.kernelParams = kargs;
+    cudaGraphNode_t head;
+    CK(cudaGraphAddKernelNode(&head, g, &last, 1, &kp));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = hc;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    CK(cudaGraphAddNode(&wnode, g, &head, 1, &cp));
+    bool ovl = h->call_overlap;
+    h->call_overlap = false;
+    int l0 = h->launches;
+    CK(cudaStreamBeginCaptureToGraph(h->st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+    s = cg_iteration(h, fp32, 1, hc);
+    cudaGraph_t captured;
+    cudaError_t e = cudaStreamEndCapture(h->st, &captured);
+    h->call_overlap = ovl;
+    h->launches = l0;
+    if (s) return s;
+    if (e != cudaSuccess) {
+      h->err = std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e);
+      return MDFF_ERR_CUDA;
+    }
+    last = wnode;
+  }
+  CK(cudaGraphAddChildGraphNode(&nB, g, &last, 1, gB));
+  cudaGraphDestroy(gA);
+  cudaGraphDestroy(gB);
+  CK(cudaGraphInstantiate(&h->step_exec, g, 0));
+  h->step_gen = h->gen;
+  h->step_fp32 = fp32 ? 1 : 0;
+  return MDFF_OK;
+}
+
+// one engforce through the whole-step graph; *used = false when the call
+// is not in the graph's steady state (the caller runs run_engforce instead)
+static int run_engforce_graph(mdff_ctx* h, int itime, bool* used) {
+  *used = false;
+  if (!step_graph_usable(h, itime)) return MDFF_OK;
+  bool fp32 = h->p.precision == MDFF_PREC_MIXED;
+  int s;
+  if ((s = sr_join(h)) || (s = rs_join(h))) return s;
+  if (!h->step_exec || h->step_gen != h->gen || h->step_fp32 != (fp32 ? 1 : 0))
+    if ((s = build_step_graph(h, itime, fp32))) return s;
+  *used = true;
+  h->launches = 0;
+  CK(cudaGraphLaunch(h->step_exec, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  h->launches = h->step_launches;
+  if (h->p.lcoulomb && h->lpolar) {
+    double rmsd, rmsd0 = h->h_scal[S_CGP];
+    int it, nres = 1;
+    if (!cg_graph_outcome(h, &rmsd, &it)) {
+      // another outer iteration: from the dipoles the graph left, then the
+      // back part again on the converged dipoles
+      h->call_overlap = h->overlap;
+      if ((s = cg_continue(h, fp32, &rmsd, &it, &nres, nullptr))) return s;
+      if ((s = cg_epilogue(h)) || (s = ef_back(h, fp32))) return s;
+      CK(cudaStreamSynchronize(h->st));
+    }
+    h->launches += h->cg_body_launches * it + nres;
+    cg_stats(h, rmsd0, rmsd, it, nres);
+  }
+  return ef_status(h);
+}
+
 // overflow -> grow the rows and redo the call (the reference STOPs instead,
 // tools.f90:337-350)
 static int engforce_retry(mdff_ctx* h, int itime) {
-  int s = run_engforce(h, itime);
+  bool used = false;
+  int s = run_engforce_graph(h, itime, &used);
+  if (!used && !s) s = run_engforce(h, itime);
   h->launches_call += h->launches;
   for (int tries = 0; s == MDFF_ERR_LIST_OVERFLOW && tries < 3; ++tries) {
     int need = h->h_flags[2];
@@ -1748,6 +2005,10 @@ static int engforce_retry(mdff_ctx* h, int itime) {
     if (e) return e;
     k_seti<<<1, 32, 0, h->st>>>(&h->L.flags[1], 0);
     h->have_list = false;
+    // the predictors of the failed attempt shifted the ASPC history
+    if (h->d_hist_save)
+      CK(cudaMemcpyAsync(h->d_hist, h->d_hist_save, sizeof(double4) * MDFF_ASPC_DEPTH * h->natm,
+                         cudaMemcpyDeviceToDevice, h->st));
     s = run_engforce(h, itime);
     h->launches_call += h->launches;
   }
@@ -1953,6 +2214,7 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_mu_ind, n);
   DALLOC(h->d_mu_tot, n);
   DALLOC(h->d_hist, (size_t)MDFF_ASPC_DEPTH * n);
+  if (h->lpolar) DALLOC(h->d_hist_save, (size_t)MDFF_ASPC_DEPTH * n);
   DALLOC(h->d_E, n);
   DALLOC(h->d_r, n);
   DALLOC(h->d_z, n);
@@ -1975,6 +2237,7 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
     }
   }
   DALLOC(h->d_force, 3 * (size_t)n);
+  if (h->lsr) DALLOC(h->d_fsr, 3 * (size_t)n);
   DALLOC(h->d_pack, 3 * (size_t)n);
   h->part_cap = (size_t)std::max(cdiv((long)n * 32, 256), cdiv(n, 256)) * 16 + 64;
   // kO_v4_1 Gram row: kKoHist + 2 dot products per block
@@ -2370,9 +2633,10 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
                   h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
-                  h->d_lwfc, h->d_mu_wfc, h->d_qm32, h->d_Edd};
+                  h->d_lwfc, h->d_mu_wfc, h->d_qm32, h->d_Edd, h->d_fsr, h->d_hist_save};
   for (void* q : ptrs)
     if (q) cudaFree(q);
+  step_graph_free(h);
   if (h->cg_exec) cudaGraphExecDestroy(h->cg_exec);
   if (h->cg_graph) cudaGraphDestroy(h->cg_graph);
   if (h->h_scal) cudaFreeHost(h->h_scal);

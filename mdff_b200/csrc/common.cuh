@@ -197,6 +197,16 @@ __device__ __forceinline__ void tt_damp_k(R b, R c, R r, int order, R& f, R& fd)
 }
 
 // ---------------------------------------------------------------------------
+// Programmatic dependent launch.  A kernel launched with the PDL attribute
+// (pdl_launch on the host) may be scheduled while its predecessor on the
+// stream is still finishing: pdl_wait(), the first statement of such a
+// kernel, returns once the predecessor grid has completed and its writes are
+// visible; pdl_trigger() lets this kernel's own successor be scheduled.  Both
+// are no-ops in a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// ---------------------------------------------------------------------------
 // warp / block reductions (fixed order -> deterministic)
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {

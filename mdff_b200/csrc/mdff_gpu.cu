@@ -283,6 +283,34 @@ static int dalloc(mdff_ctx* h, T** p, size_t n) {
     if (s_) return s_;                          \
   } while (0)
 
+// launch with programmatic stream serialization (kernels that start with
+// pdl_wait): the kernel may be scheduled while its predecessor on the stream
+// finishes, which hides the launch latency between short dependent kernels
+template <typename... KP, typename... A>
+static cudaError_t pdl_launch(void (*k)(KP...), dim3 g, dim3 b, size_t smem, cudaStream_t st, A... args) {
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = g;
+  cfg.blockDim = b;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
+#define PDL_CHECK(call)                                                                  \
+  do {                                                                                   \
+    h->launches++;                                                                       \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      h->err = std::string("kernel launch: ") + cudaGetErrorString(e_);                  \
+      return MDFF_ERR_CUDA;                                                              \
+    }                                                                                    \
+  } while (0)
+
 __global__ void k_seti(int* p, int v) {
   if (threadIdx.x == 0) *p = v;
 }
@@ -548,8 +576,8 @@ static int list_update(mdff_ctx* h) {
 }
 
 static int reduce_into(mdff_ctx* h, int nblk, int nv, double* out) {
-  k_reduce_partials<<<nv, 256, 0, h->st>>>(h->d_part, nblk, nv, out);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_reduce_partials, dim3(nv), dim3(256), 0, h->st, (const double*)h->d_part, nblk,
+                       nv, out));
   return MDFF_OK;
 }
 
@@ -652,15 +680,21 @@ static void launch_rho_tc_n(mdff_ctx* h, const RecMesh& M, int n, int has_q, int
   size_t smem = rho_tc_smem_n(NB, M.kmax[0], M.kmax[1], M.kmax[2]);
   int* err = h->d_cata + 1;
   const int* wcfg = h->d_cata + 3;
+  const float2* tab = h->d_tab32;
+  const float4* w = h->d_w32;
+  // (a launch error surfaces at the caller's LAUNCH_CHECK)
   if (has_mu) {
     dim3 g((unsigned)cdiv(M.nrows, 32), (unsigned)h->n_tc_chunks);
     if (has_q)
-      k_rec_rho_tc<true, true, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err, wcfg);
+      (void)pdl_launch(k_rec_rho_tc<true, true, NB>, g, dim3(kRhoTcThreads), smem, h->st, tab, w, n,
+                       h->tc_chunk, M, h->d_rho_part, err, wcfg);
     else
-      k_rec_rho_tc<false, true, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err, wcfg);
+      (void)pdl_launch(k_rec_rho_tc<false, true, NB>, g, dim3(kRhoTcThreads), smem, h->st, tab, w, n,
+                       h->tc_chunk, M, h->d_rho_part, err, wcfg);
   } else {
     dim3 g((unsigned)cdiv(M.nrows, 64), (unsigned)h->n_tc_chunks);
-    k_rec_rho_tc<true, false, NB><<<g, kRhoTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, h->tc_chunk, M, h->d_rho_part, err, wcfg);
+    (void)pdl_launch(k_rec_rho_tc<true, false, NB>, g, dim3(kRhoTcThreads), smem, h->st, tab, w, n,
+                     h->tc_chunk, M, h->d_rho_part, err, wcfg);
   }
 }
 
@@ -680,12 +714,20 @@ static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int
   size_t bsmem = (size_t)kBtRows * (2 * M.kmax[2] + 1) * sizeof(double2);
   dim3 gb((unsigned)ntile, (unsigned)(rpt / kBtRows));
   int* err = h->d_cata + 1;
+  const double2* rhoA = h->d_rhoA;
+  const double2* rpart = h->d_rho_part;
+  const float2* tab = h->d_tab32;
+  const float4* w = h->d_w32;
+  const uint32_t* fb = h->d_fb;
+  h->launches++;  // two launches here; the caller's LAUNCH_CHECK counts one
   if (muf) {
-    k_rec_field_btiles<true, KF><<<gb, 128, bsmem, h->st>>>(M, h->d_rhoA, h->d_rho_part, npart, h->d_fb);
-    k_rec_field_tc<true, KF><<<g, kFieldTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, M, h->d_fb, tpg, h->d_G, h->d_H, err);
+    (void)pdl_launch(k_rec_field_btiles<true, KF>, gb, dim3(128), bsmem, h->st, M, rhoA, rpart, npart, h->d_fb);
+    (void)pdl_launch(k_rec_field_tc<true, KF>, g, dim3(kFieldTcThreads), smem, h->st, tab, w, n, M, fb, tpg,
+                     h->d_G, h->d_H, err);
   } else {
-    k_rec_field_btiles<false, KF><<<gb, 128, bsmem, h->st>>>(M, h->d_rhoA, h->d_rho_part, npart, h->d_fb);
-    k_rec_field_tc<false, KF><<<g, kFieldTcThreads, smem, h->st>>>(h->d_tab32, h->d_w32, n, M, h->d_fb, tpg, h->d_G, h->d_H, err);
+    (void)pdl_launch(k_rec_field_btiles<false, KF>, gb, dim3(128), bsmem, h->st, M, rhoA, rpart, npart, h->d_fb);
+    (void)pdl_launch(k_rec_field_tc<false, KF>, g, dim3(kFieldTcThreads), smem, h->st, tab, w, n, M, fb, tpg,
+                     h->d_G, h->d_H, err);
   }
   return ng;
 }
@@ -1385,6 +1427,8 @@ static int solve_ko_v4(mdff_ctx* h, int itime, bool fp32) {
 // the recurrence residual, and (inside the graph) the while-loop condition
 __global__ void k_cg_inner_check(double* __restrict__ sc, int npol, int in_graph,
                                  cudaGraphConditionalHandle hc) {
+  pdl_wait();
+  pdl_trigger();
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   sc[0] = sc[3];
   double it = sc[6] + 1.0;
@@ -1429,17 +1473,17 @@ static int cg_iteration(mdff_ctx* h, bool fp32, int in_graph, cudaGraphCondition
   PolDev P = poldev(h);
   double* sc = h->d_scal + S_CG;
   if ((s = field_of_mu(h, h->d_pv, 1, fp32, h->d_Tp, fp32))) return s;
-  k_cg_Ap<<<nb, 256, 0, h->st>>>(h->d_pv, h->d_Tp, P, n, h->d_qv, h->d_part);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_cg_Ap, dim3(nb), dim3(256), 0, h->st, (const double4*)h->d_pv,
+                       (const double4*)h->d_Tp, P, n, h->d_qv, h->d_part));
   if ((s = reduce_into(h, nb, 1, sc + 2))) return s;
-  k_cg_update<<<nb, 256, 0, h->st>>>(sc + 0, sc + 2, P, n, h->d_pv, h->d_qv, h->d_mu_ind, h->d_r, h->d_z, h->d_part);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_cg_update, dim3(nb), dim3(256), 0, h->st, (const double*)(sc + 0),
+                       (const double*)(sc + 2), P, n, h->d_pv, (const double4*)h->d_qv, h->d_mu_ind, h->d_r,
+                       h->d_z, h->d_part));
   if ((s = reduce_into(h, nb, 2, sc + 3))) return s;
-  k_cg_dir<<<nb, 256, 0, h->st>>>(sc + 0, sc + 3, n, h->d_z, h->d_pv, h->d_cell,
-                                  fp32 ? h->d_w32 : nullptr, h->d_mu32);
-  LAUNCH_CHECK();
-  k_cg_inner_check<<<1, 32, 0, h->st>>>(sc, h->npol, in_graph, hc);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_cg_dir, dim3(nb), dim3(256), 0, h->st, (const double*)(sc + 0),
+                       (const double*)(sc + 3), n, (const double4*)h->d_z, h->d_pv,
+                       (const CellC*)h->d_cell, fp32 ? h->d_w32 : (float4*)nullptr, h->d_mu32));
+  PDL_CHECK(pdl_launch(k_cg_inner_check, dim3(1), dim3(32), 0, h->st, sc, h->npol, in_graph, hc));
   return MDFF_OK;
 }
 

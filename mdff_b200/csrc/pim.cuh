@@ -207,6 +207,8 @@ __global__ void k_cg_init(const double4* __restrict__ b, const double4* __restri
 // q = alpha^-1 p - Tp (polarisable ions); partial p.q
 __global__ void k_cg_Ap(const double4* __restrict__ p, const double4* __restrict__ Tp, PolDev P,
                         int natm, double4* __restrict__ qv, double* __restrict__ part) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double red[32];
   double v[1] = {0.0};
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -230,6 +232,8 @@ __global__ void k_cg_update(const double* __restrict__ rz_p, const double* __res
                             const double4* __restrict__ qv, double4* __restrict__ x,
                             double4* __restrict__ r, double4* __restrict__ z,
                             double* __restrict__ part) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double red[2 * 32];
   double v[2] = {0.0, 0.0};
   double rz = *rz_p, pq = *pq_p;
@@ -265,6 +269,8 @@ __global__ void k_cg_dir(const double* __restrict__ rz_p, const double* __restri
                          int natm, const double4* __restrict__ z, double4* __restrict__ p,
                          const CellC* __restrict__ cell, float4* __restrict__ w32,
                          float4* __restrict__ mu32) {
+  pdl_wait();
+  pdl_trigger();
   double rz = *rz_p, rzn = *rzn_p;
   double be = (rz != 0.0) ? rzn / rz : 0.0;
   int i = blockIdx.x * blockDim.x + threadIdx.x;

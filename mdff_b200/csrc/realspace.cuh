@@ -895,6 +895,8 @@ static __global__ void __launch_bounds__(256) k_es_efg(
 // one block per value (grid = nv), the same order for every launch
 static __global__ void k_reduce_partials(const double* __restrict__ part, int nblk, int nv,
                                          double* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double sh[256];
   const int v = blockIdx.x;
   double acc = 0.0;

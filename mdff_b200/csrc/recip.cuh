@@ -494,6 +494,8 @@ static __global__ void __launch_bounds__(256) k_dd_cached_rec(
     const int* __restrict__ cj, const int* __restrict__ cn, int cap, int natm,
     const double4* __restrict__ Gpart, int nchunk, const CellC* __restrict__ cell, double scale,
     SelfField sf, double4* __restrict__ E, const double4* __restrict__ Edd) {
+  pdl_wait();
+  pdl_trigger();
   int lane = threadIdx.x & 31;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= natm) return;

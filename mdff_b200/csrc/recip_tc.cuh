@@ -174,6 +174,8 @@ template <bool HAS_Q, bool HAS_MU, int N>
 static __global__ void __launch_bounds__(kRhoTcThreads) k_rec_rho_tc(
     const float2* __restrict__ tab, const float4* __restrict__ w, int natm, int chunk, RecMesh M,
     double2* __restrict__ part, int* __restrict__ err, const int* __restrict__ wait_cfg) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NT = kRhoTcThreads;
   constexpr int RPT = HAS_MU ? 32 : 64;         // mesh rows per tile
   constexpr int KB = tc::KB;
@@ -473,6 +475,8 @@ template <bool HAS_H, int KF>
 static __global__ void __launch_bounds__(128) k_rec_field_btiles(RecMesh M, const double2* __restrict__ rhoA,
                                                                  const double2* __restrict__ part, int npart,
                                                                  uint32_t* __restrict__ fb) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int CPR = HAS_H ? 8 : 4, RPT = 128 / CPR;
   constexpr int TILE = 128 * KF * 4;
   const int kz = M.kmax[2], nzc = kz + 1, nzs = 2 * kz + 1;
@@ -534,6 +538,8 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
     const float2* __restrict__ tab, const float4* __restrict__ w, int natm, RecMesh M,
     const uint32_t* __restrict__ fb, int tiles_per_group, double4* __restrict__ Gpart,
     double4* __restrict__ Hpart, int* __restrict__ err) {
+  pdl_wait();
+  pdl_trigger();
   constexpr int NT = kFieldTcThreads;
   constexpr int CPR = HAS_H ? 8 : 4;     // columns per mesh row (6 used with H)
   constexpr int RPT = 128 / CPR;         // mesh rows per tile

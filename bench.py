@@ -302,7 +302,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     dist_barrier(world)
     clk = Clocks(local_rank) if rank == 0 else None
-    step_ms, launches, iters = [], 0, []
+    step_ms, launches, iters, rms0, nres = [], 0, [], [], []
     torch.cuda.synchronize()
     dist_barrier(world)
     for _ in range(args.steps):
@@ -314,6 +314,8 @@ def run_ours(args, rank, world, local_rank):
         step_ms.append(st["ms_last"])
         launches += st["n_launches"]
         iters.append(st["n_pol_iter"])
+        rms0.append(st["rmsd_initial"])
+        nres.append(st["n_fp64_residuals"])
     torch.cuda.synchronize()
     dist_barrier(world)
     clocks = clk.stop() if clk else None
@@ -334,6 +336,8 @@ def run_ours(args, rank, world, local_rank):
     value, total_s = replicas.throughput(world, args.steps, sum(step_ms) / 1e3)
     res = dict(value=value, ms_per_step=1e3 * total_s / args.steps, launches=launches,
                cg_iters_mean=float(np.mean(iters)), clocks=clocks, wl=wl,
+               cg_first_residual_rmsd_mean=float(np.mean(rms0)),
+               cg_fp64_residuals_mean=float(np.mean(nres)),
                kms=kms, kl=kl, kw=kw, prof_steps=min(args.steps, 30))
     if rank != 0:
         return res, None
@@ -873,6 +877,8 @@ def main():
             "ns_per_day": res["value"] / world * 86400 * DT_FS * 1e-6,
             "atom_steps_per_s": res["value"] * wl["natm"],
             "cg_iters_mean": res["cg_iters_mean"],
+            "cg_first_residual_rmsd_mean": res["cg_first_residual_rmsd_mean"],
+            "cg_fp64_residuals_mean": res["cg_fp64_residuals_mean"],
             "gpu_launches": int(res["launches"]),
             "clocks": res["clocks"],
         }

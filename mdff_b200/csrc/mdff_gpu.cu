@@ -333,6 +333,8 @@ __global__ void k_unpack3(const double* __restrict__ in, int natm, double4* __re
 __global__ void k_vv_kick_drift(double* __restrict__ pos, double* __restrict__ vel,
                                 const double* __restrict__ f, const double* __restrict__ invm,
                                 int natm, double dt) {
+  pdl_wait();
+  pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   for (int a = 0; a < 3; ++a) {
@@ -345,6 +347,8 @@ __global__ void k_vv_kick_drift(double* __restrict__ pos, double* __restrict__ v
 __global__ void k_vv_kick(double* __restrict__ vel, const double* __restrict__ f,
                           const double* __restrict__ invm, int natm, double dt,
                           double* __restrict__ part) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double red[32];
   double e[1] = {0.0};
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -545,31 +549,22 @@ static int list_update(mdff_ctx* h) {
     LAUNCH_CHECK();
   } else {
     int nb = cdiv(n, 256);
-    k_disp_partial<<<nb, 256, 0, h->st>>>(h->d_s, h->L.sref, n, h->d_cell, h->d_disp_part);
-    LAUNCH_CHECK();
-    k_disp_final<<<1, 32, 0, h->st>>>(h->d_disp_part, nb, h->L.skindiff, h->L.flags,
-                                      h->d_scal + S_DISP);
-    LAUNCH_CHECK();
+    PDL_CHECK(pdl_launch(k_disp_partial, dim3(nb), dim3(256), 0, h->st, h->d_s, h->L.sref, n, h->d_cell, h->d_disp_part));
+    PDL_CHECK(pdl_launch(k_disp_final, dim3(1), dim3(32), 0, h->st, h->d_disp_part, nb, h->L.skindiff, h->L.flags,
+                                      h->d_scal + S_DISP));
   }
-  k_cell_count<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_s, n, h->L);
-  LAUNCH_CHECK();
-  k_cell_scan<<<1, 1024, 0, h->st>>>(h->L, h->ncell);
-  LAUNCH_CHECK();
-  k_cell_scatter<<<cdiv(n, 256), 256, 0, h->st>>>(n, h->L);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_cell_count, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_s, n, h->L));
+  PDL_CHECK(pdl_launch(k_cell_scan, dim3(1), dim3(1024), 0, h->st, h->L, h->ncell));
+  PDL_CHECK(pdl_launch(k_cell_scatter, dim3(cdiv(n, 256)), dim3(256), 0, h->st, n, h->L));
   // grid-stride build and sort: a step without a rebuild launches a few
   // blocks per SM that read the flag and leave
   int nsm = h->nsm > 0 ? h->nsm : 148;
-  k_build_rows<<<std::min(cdiv((long)n * 32, 256), 8 * nsm), 256, 0, h->st>>>(h->d_s, n, h->d_cell, h->L);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_build_rows, dim3(std::min(cdiv((long)n * 32, 256), 8 * nsm)), dim3(256), 0, h->st, h->d_s, n, h->d_cell, h->L));
   int P = 1;
   while (P < h->L.cap) P <<= 1;
-  k_sort_rows<<<std::min(n, 8 * nsm), 256, P * sizeof(int), h->st>>>(h->L, n);
-  LAUNCH_CHECK();
-  k_build_done<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_s, n, h->L);
-  LAUNCH_CHECK();
-  k_build_clear<<<1, 256, 0, h->st>>>(h->L, h->ncell);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_sort_rows, dim3(std::min(n, 8 * nsm)), dim3(256), P * sizeof(int), h->st, h->L, n));
+  PDL_CHECK(pdl_launch(k_build_done, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_s, n, h->L));
+  PDL_CHECK(pdl_launch(k_build_clear, dim3(1), dim3(256), 0, h->st, h->L, h->ncell));
   prof_end(h, pr);
   h->have_list = true;
   return MDFF_OK;
@@ -627,8 +622,7 @@ static int rs_join(mdff_ctx* h) {
 // moments [qtot(3), mutot(3), qsq, musq] of (q?, mu) into out (device)
 static int moments(mdff_ctx* h, const double4* mu, int has_q, double* out) {
   int n = h->natm, nb = cdiv(n, 256);
-  k_moments_part<<<nb, 256, 0, h->st>>>(h->d_pos, h->d_q, mu, n, has_q, h->d_part);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_moments_part, dim3(nb), dim3(256), 0, h->st, h->d_pos, h->d_q, mu, n, has_q, h->d_part));
   return reduce_into(h, nb, 8, out);
 }
 
@@ -659,19 +653,19 @@ static void launch_rho(mdff_ctx* h, dim3 g, const typename cplx<R>::T* tab, int 
   if constexpr (std::is_same<R, float>::value) {
     // FP32: two ions per thread in packed FP32x2 lanes
     if (has_q && has_mu)
-      k_rec_rho_x2<true, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w32, n, chunk, M, ntiles, h->d_rho_part);
+      (void)pdl_launch(k_rec_rho_x2<true, true, NZT>, dim3(g), dim3(kRhoThreads), 0, h->st, tab, h->d_w32, n, chunk, M, ntiles, h->d_rho_part);
     else if (has_q)
-      k_rec_rho_x2<true, false, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w32, n, chunk, M, ntiles, h->d_rho_part);
+      (void)pdl_launch(k_rec_rho_x2<true, false, NZT>, dim3(g), dim3(kRhoThreads), 0, h->st, tab, h->d_w32, n, chunk, M, ntiles, h->d_rho_part);
     else
-      k_rec_rho_x2<false, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w32, n, chunk, M, ntiles, h->d_rho_part);
+      (void)pdl_launch(k_rec_rho_x2<false, true, NZT>, dim3(g), dim3(kRhoThreads), 0, h->st, tab, h->d_w32, n, chunk, M, ntiles, h->d_rho_part);
     return;
   }
   if (has_q && has_mu)
-    k_rec_rho<R, true, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
+    (void)pdl_launch(k_rec_rho<R, true, true, NZT>, dim3(g), dim3(kRhoThreads), 0, h->st, tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
   else if (has_q)
-    k_rec_rho<R, true, false, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
+    (void)pdl_launch(k_rec_rho<R, true, false, NZT>, dim3(g), dim3(kRhoThreads), 0, h->st, tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
   else
-    k_rec_rho<R, false, true, NZT><<<g, kRhoThreads, 0, h->st>>>(tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
+    (void)pdl_launch(k_rec_rho<R, false, true, NZT>, dim3(g), dim3(kRhoThreads), 0, h->st, tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
 }
 
 // FP32 structure factor on the tensor cores into d_rho_part (n_tc_chunks chunks)
@@ -773,9 +767,8 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   constexpr bool F32 = std::is_same<R, float>::value;
   // (the FP32 CG direction kernels write the FP32 weights themselves)
   if (!(F32 && weights_ready)) {
-    k_rec_weights<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_q, mu, n, h->d_cell, has_q, has_mu, h->d_w,
-                                                   F32 ? h->d_w32 : nullptr, mu32);
-    LAUNCH_CHECK();
+    PDL_CHECK(pdl_launch(k_rec_weights, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_q, mu, n, h->d_cell, has_q, has_mu, h->d_w,
+                                                   F32 ? h->d_w32 : nullptr, mu32));
   }
   int nzt = pick_nzt(2 * M.kmax[2] + 1);
   int ntiles = cdiv(2 * M.kmax[2] + 1, nzt);
@@ -814,14 +807,12 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   int npart = 0;
   const bool field_tc = F32 && h->field_tc;
   if (e_out || (nparts > 4 && !field_tc)) {
-    k_rec_sum<<<cdiv(h->nk, 256), 256, 0, h->st>>>(h->d_rho_part, nparts, M, h->d_rhoA, h->d_str);
-    LAUNCH_CHECK();
+    PDL_CHECK(pdl_launch(k_rec_sum, dim3(cdiv(h->nk, 256)), dim3(256), 0, h->st, h->d_rho_part, nparts, M, h->d_rhoA, h->d_str));
   } else {
     npart = nparts;
   }
   if (e_out) {
-    k_rec_energy<<<1, 1024, 0, h->st>>>(h->d_str, M, tpi_V, h->omega, 1, e_out);
-    LAUNCH_CHECK();
+    PDL_CHECK(pdl_launch(k_rec_energy, dim3(1), dim3(1024), 0, h->st, h->d_str, M, tpi_V, h->omega, 1, e_out));
   }
   int nch = (int)h->rchunk.size() - 1;
   dim3 gf((unsigned)cdiv(n, kFieldThreads), (unsigned)nch);
@@ -833,14 +824,13 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   } else if constexpr (std::is_same<R, float>::value) {
     dim3 gx((unsigned)cdiv(n, 2 * kFieldThreads), (unsigned)nch);
     if (muf)
-      k_rec_field_x2<true><<<gx, kFieldThreads, smem, h->st>>>(tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
+      (void)pdl_launch(k_rec_field_x2<true>, dim3(gx), dim3(kFieldThreads), smem, h->st, tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
     else
-      k_rec_field_x2<false><<<gx, kFieldThreads, smem, h->st>>>(tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
+      (void)pdl_launch(k_rec_field_x2<false>, dim3(gx), dim3(kFieldThreads), smem, h->st, tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
   } else if (muf)
-    k_rec_field<R, true><<<gf, kFieldThreads, smem, h->st>>>(tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
+    (void)pdl_launch(k_rec_field<R, true>, dim3(gf), dim3(kFieldThreads), smem, h->st, tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
   else
-    k_rec_field<R, false><<<gf, kFieldThreads, smem, h->st>>>(tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
-  LAUNCH_CHECK();
+    PDL_CHECK(pdl_launch(k_rec_field<R, false>, dim3(gf), dim3(kFieldThreads), smem, h->st, tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H));
   prof_end(h, pr);
   double fpi_V = 2.0 * tpi_V;
   // the real-space half of this pass (side stream) adds into the same E / forces
@@ -883,11 +873,9 @@ static int build_tables(mdff_ctx* h) {
   if (h->nk == 0) return MDFF_OK;
   int n = h->natm;
   int kzt = std::max(h->p.kES[2], 4);
-  k_rec_tables<double><<<cdiv(n, 128), 128, 0, h->st>>>(h->d_s, n, h->p.kES[0], h->p.kES[1], kzt, h->d_tab64);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_rec_tables<double>, dim3(cdiv(n, 128)), dim3(128), 0, h->st, h->d_s, n, h->p.kES[0], h->p.kES[1], kzt, h->d_tab64));
   if (h->p.precision == MDFF_PREC_MIXED) {
-    k_rec_tables<float><<<cdiv(n, 128), 128, 0, h->st>>>(h->d_s, n, h->p.kES[0], h->p.kES[1], kzt, h->d_tab32);
-    LAUNCH_CHECK();
+    PDL_CHECK(pdl_launch(k_rec_tables<float>, dim3(cdiv(n, 128)), dim3(128), 0, h->st, h->d_s, n, h->p.kES[0], h->p.kES[1], kzt, h->d_tab32));
   }
   return MDFF_OK;
 }
@@ -1050,8 +1038,7 @@ static int aspc_predict(mdff_ctx* h, int itime) {
   int ord;
   double B[5], w;
   aspc_coef(itime, h->p.extrapolate_order, &ord, B, &w);
-  k_aspc_predict<<<cdiv(h->natm, 256), 256, 0, h->st>>>(h->d_hist, h->natm, ord, B[0], B[1], B[2], B[3], B[4], h->d_mu_ind);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_aspc_predict, dim3(cdiv(h->natm, 256)), dim3(256), 0, h->st, h->d_hist, h->natm, ord, B[0], B[1], B[2], B[3], B[4], h->d_mu_ind));
   return MDFF_OK;
 }
 
@@ -1461,6 +1448,8 @@ __global__ void k_cg_plan(double* __restrict__ sc, double* __restrict__ plan, in
 }
 
 __global__ void k_setd2(double* __restrict__ a, double va, double* __restrict__ b, double vb) {
+  pdl_wait();
+  pdl_trigger();
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     *a = va;
     *b = vb;
@@ -1570,10 +1559,8 @@ static int cg_prologue(mdff_ctx* h, int itime) {
   }
   double* sc = h->d_scal + S_CG;
   double* plan = h->d_scal + S_CGP;
-  k_setd2<<<1, 32, 0, h->st>>>(sc + 6, 0.0, sc + 7, (double)cg_maxit_of(h));
-  LAUNCH_CHECK();
-  k_setd2<<<1, 32, 0, h->st>>>(plan + 1, 0.0, plan + 2, 0.0);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_setd2, dim3(1), dim3(32), 0, h->st, sc + 6, 0.0, sc + 7, (double)cg_maxit_of(h)));
+  PDL_CHECK(pdl_launch(k_setd2, dim3(1), dim3(32), 0, h->st, plan + 1, 0.0, plan + 2, 0.0));
   return MDFF_OK;
 }
 
@@ -1583,9 +1570,8 @@ static int cg_residual(mdff_ctx* h, bool fp32) {
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
   if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp))) return s;
-  k_cg_init<<<nb, 256, 0, h->st>>>(h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
-                                   h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_cg_init, dim3(nb), dim3(256), 0, h->st, h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
+                                   h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32));
   return reduce_into(h, nb, 2, h->d_scal + S_CG);
 }
 
@@ -1612,8 +1598,7 @@ static bool cg_graph_outcome(const mdff_ctx* h, double* rmsd, int* it) {
 static int cg_epilogue(mdff_ctx* h) {
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
-  k_upol_part<<<nb, 256, 0, h->st>>>(h->d_mu_ind, P, n, h->d_part);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_upol_part, dim3(nb), dim3(256), 0, h->st, h->d_mu_ind, P, n, h->d_part));
   if ((s = reduce_into(h, nb, 1, h->d_scal + S_UPOL))) return s;
   CK(cudaMemcpyAsync(h->d_hist, h->d_mu_ind, sizeof(double4) * n, cudaMemcpyDeviceToDevice, h->st));
   return MDFF_OK;
@@ -1718,8 +1703,7 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
 
 static int ef_front(mdff_ctx* h, bool fp32) {
   int n = h->natm, s;
-  k_kardir<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_pos, n, h->d_cell, h->d_s);
-  LAUNCH_CHECK();
+  PDL_CHECK(pdl_launch(k_kardir, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_pos, n, h->d_cell, h->d_s));
   if ((s = list_update(h))) return s;
   CK(cudaMemsetAsync(h->d_scal, 0, sizeof(double) * S_NSCAL, h->st));
   int nbw = cdiv((long)n * 32, 256);
@@ -1782,10 +1766,9 @@ static int ef_back(mdff_ctx* h, bool fp32) {
                                             h->d_cell, h->p.rcut_wfc, h->d_mu_wfc, h->d_cata + 2);
       LAUNCH_CHECK();
     }
-    k_mu_total<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_dipia, h->d_mu_ind,
+    PDL_CHECK(pdl_launch(k_mu_total, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_dipia, h->d_mu_ind,
                                                 (h->lwannier && h->p.ldip_wfc) ? h->d_mu_wfc : nullptr, n,
-                                                h->d_mu_tot, h->d_cata, h->d_q, fp32 ? h->d_qm32 : nullptr);
-    LAUNCH_CHECK();
+                                                h->d_mu_tot, h->d_cata, h->d_q, fp32 ? h->d_qm32 : nullptr));
     CK(cudaMemsetAsync(h->d_E, 0, sizeof(double4) * n, h->st));
   }
   // the forces start from the short-range pass's (zero without one)
@@ -2501,13 +2484,11 @@ int mdff_gpu_md_nve(mdff_handle h, double* d_pos, double* d_vel, const double* d
   }
   h->md_valid = false;
   for (int step = 0; step < nsteps; ++step) {
-    k_vv_kick_drift<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_pos, d_vel, h->d_force, d_invmass, n, dt);
-    LAUNCH_CHECK();
+    PDL_CHECK(pdl_launch(k_vv_kick_drift, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_pos, d_vel, h->d_force, d_invmass, n, dt));
     s = engforce_retry(h, itime0 + step + 1);
     if (s) return s;
     int nb = cdiv(n, 256);
-    k_vv_kick<<<nb, 256, 0, h->st>>>(d_vel, h->d_force, d_invmass, n, dt, h->d_ekin_part);
-    LAUNCH_CHECK();
+    PDL_CHECK(pdl_launch(k_vv_kick, dim3(nb), dim3(256), 0, h->st, d_vel, h->d_force, d_invmass, n, dt, h->d_ekin_part));
     k_reduce_partials<<<1, 256, 0, h->st>>>(h->d_ekin_part, nb, 1, h->d_scal + S_NSCAL - 1);
     LAUNCH_CHECK();
     h->launches_call += 3;

@@ -32,6 +32,8 @@ struct ListDev {
 // direct coordinates (kardir) of the Cartesian SoA positions
 __global__ void k_kardir(const double* __restrict__ pos, int natm, const CellC* __restrict__ cell,
                          double4* __restrict__ s) {
+  pdl_wait();
+  pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   double sx, sy, sz;
@@ -43,6 +45,8 @@ __global__ void k_kardir(const double* __restrict__ pos, int natm, const CellC* 
 // (minimum image); one partial (max1, max2) per block.
 __global__ void k_disp_partial(const double4* __restrict__ s, const double4* __restrict__ sref,
                                int natm, const CellC* __restrict__ cell, double2* __restrict__ part) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double m1s[32], m2s[32];
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   double m1 = 0.0, m2 = 0.0;
@@ -80,6 +84,8 @@ __global__ void k_disp_partial(const double4* __restrict__ s, const double4* __r
 
 __global__ void k_disp_final(const double2* __restrict__ part, int nb, double skindiff,
                              int* __restrict__ flags, double* __restrict__ disp_out) {
+  pdl_wait();
+  pdl_trigger();
   if (threadIdx.x != 0) return;
   double a = 0.0, b = 0.0;
   for (int k = 0; k < nb; ++k) {
@@ -101,6 +107,8 @@ __device__ __forceinline__ int cell_index(double s, int n) {
 }
 
 __global__ void k_cell_count(const double4* __restrict__ s, int natm, ListDev L) {
+  pdl_wait();
+  pdl_trigger();
   if (L.flags[0] == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
@@ -113,6 +121,8 @@ __global__ void k_cell_count(const double4* __restrict__ s, int natm, ListDev L)
 
 // single-block exclusive scan of the cell counts
 __global__ void k_cell_scan(ListDev L, int ncell) {
+  pdl_wait();
+  pdl_trigger();
   if (L.flags[0] == 0) return;
   __shared__ int warp_tot[32];
   __shared__ int carry;
@@ -151,6 +161,8 @@ __global__ void k_cell_scan(ListDev L, int ncell) {
 }
 
 __global__ void k_cell_scatter(int natm, ListDev L) {
+  pdl_wait();
+  pdl_trigger();
   if (L.flags[0] == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
@@ -221,6 +233,8 @@ __device__ __forceinline__ void build_row(const double4* __restrict__ s, int i, 
 // costs a few blocks): enumerate neighbour cells, exact distance test, append.
 __global__ void k_build_rows(const double4* __restrict__ s, int natm, const CellC* __restrict__ cell,
                              ListDev L) {
+  pdl_wait();
+  pdl_trigger();
   if (L.flags[0] == 0) return;
   int lane = threadIdx.x & 31;
   int nwarp = (gridDim.x * blockDim.x) >> 5;
@@ -231,6 +245,8 @@ __global__ void k_build_rows(const double4* __restrict__ s, int natm, const Cell
 // block per row (grid-stride over rows): bitonic sort of the row into
 // ascending j (the reference's row order); P = power of two >= cap, smem P ints.
 __global__ void k_sort_rows(ListDev L, int natm) {
+  pdl_wait();
+  pdl_trigger();
   if (L.flags[0] == 0) return;
   extern __shared__ int sh[];
   for (int i = blockIdx.x; i < natm; i += gridDim.x) {
@@ -262,12 +278,16 @@ __global__ void k_sort_rows(ListDev L, int natm) {
 
 // after a build: remember positions for the next check, clear the request
 __global__ void k_build_done(const double4* __restrict__ s, int natm, ListDev L) {
+  pdl_wait();
+  pdl_trigger();
   if (L.flags[0] == 0) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < natm) L.sref[i] = s[i];
 }
 
 __global__ void k_build_clear(ListDev L, int ncell) {
+  pdl_wait();
+  pdl_trigger();
   // runs as one block after k_build_done; resets the cell counters
   if (L.flags[0] == 0) return;
   for (int c = threadIdx.x; c < ncell; c += blockDim.x) L.cell_count[c] = 0;

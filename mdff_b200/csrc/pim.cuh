@@ -40,6 +40,8 @@ __global__ void k_induce(const double4* __restrict__ E, PolDev P, int natm, doub
 // ASPC predictor: mu = sum_k B_k hist[k]; hist[k] = hist[k-1] for k = ord..1
 __global__ void k_aspc_predict(double4* __restrict__ hist, int natm, int ord, double b0, double b1,
                                double b2, double b3, double b4, double4* __restrict__ mu) {
+  pdl_wait();
+  pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   double B[5] = {b0, b1, b2, b3, b4};
@@ -69,6 +71,8 @@ __global__ void k_aspc_correct(const double4* __restrict__ E, PolDev P, int natm
 // partials of u_pol = 1/2 sum mu alpha^-1 mu  (slot 0)
 __global__ void k_upol_part(const double4* __restrict__ mu, PolDev P, int natm,
                             double* __restrict__ part) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double red[32];
   double v[1] = {0.0};
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -116,6 +120,8 @@ __global__ void k_add4(const double4* __restrict__ a, const double4* __restrict_
 __global__ void k_moments_part(const double* __restrict__ pos, const double* __restrict__ q,
                                const double4* __restrict__ mu, int natm, int has_q,
                                double* __restrict__ part) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double red[8 * 32];
   double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -177,6 +183,8 @@ __global__ void k_cg_init(const double4* __restrict__ b, const double4* __restri
                           double4* __restrict__ z, double4* __restrict__ p, double* __restrict__ part,
                           const CellC* __restrict__ cell, float4* __restrict__ w32,
                           float4* __restrict__ mu32) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double red[2 * 32];
   double v[2] = {0.0, 0.0};
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -346,6 +354,8 @@ __global__ void k_mu_total(const double4* __restrict__ dip, const double4* __res
                            const double4* __restrict__ mu_wfc, int natm, double4* __restrict__ mu_tot,
                            int* __restrict__ flag, const double* __restrict__ q = nullptr,
                            float4* __restrict__ qm32 = nullptr) {
+  pdl_wait();
+  pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   double4 a = dip[i], b = mu_ind[i];

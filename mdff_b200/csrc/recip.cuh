@@ -56,6 +56,8 @@ struct RecMesh {
 template <typename R>
 static __global__ void k_rec_tables(const double4* __restrict__ s, int natm, int kx, int ky, int kz,
                              typename cplx<R>::T* __restrict__ tab) {
+  pdl_wait();
+  pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   double sv[3] = {s[i].x, s[i].y, s[i].z};
@@ -80,6 +82,8 @@ static __global__ void k_rec_weights(const double* __restrict__ q, const double4
                               int natm, const CellC* __restrict__ cell, int has_q, int has_mu,
                               double4* __restrict__ w, float4* __restrict__ w32,
                               float4* __restrict__ mu32) {
+  pdl_wait();
+  pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   const double* B = cell->B;
@@ -150,6 +154,8 @@ static __global__ void __launch_bounds__(128) k_rec_rho(const typename cplx<R>::
                                                  const double4* __restrict__ w, int natm,
                                                  int chunk, RecMesh M, int ntiles,
                                                  double2* __restrict__ part) {
+  pdl_wait();
+  pdl_trigger();
   typedef typename cplx<R>::T C;
   __shared__ double red[2 * NZT][4];
   int row = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
@@ -234,6 +240,8 @@ static __device__ __forceinline__ double2 rho_prime(const double2* __restrict__ 
 // rho = sum over chunks; rhoA = A_k rho; str = A_k |rho|^2
 static __global__ void k_rec_sum(const double2* __restrict__ part, int nchunk, RecMesh M,
                           double2* __restrict__ rhoA, double* __restrict__ str) {
+  pdl_wait();
+  pdl_trigger();
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= M.nk) return;
   double r = 0.0, im = 0.0;
@@ -251,6 +259,8 @@ static __global__ void k_rec_sum(const double2* __restrict__ part, int nchunk, R
 // u, tau xx yy zz xy xz yz.  One block.
 static __global__ void k_rec_energy(const double* __restrict__ str, RecMesh M, double tpi_V,
                              double omega, int do_stress, double* __restrict__ out) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double red[7 * 32];
   double v[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int k = threadIdx.x; k < M.nk; k += blockDim.x) {
@@ -284,6 +294,8 @@ static __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>
                                                    const double2* __restrict__ part, int npart,
                                                    double4* __restrict__ Gpart,
                                                    double4* __restrict__ Hpart) {
+  pdl_wait();
+  pdl_trigger();
   typedef typename cplx<R>::T C;
   extern __shared__ unsigned char shraw[];
   C* sh = reinterpret_cast<C*>(shraw);
@@ -585,6 +597,8 @@ static __global__ void __launch_bounds__(128) k_rec_rho_x2(const float2* __restr
                                                     const float4* __restrict__ w, int natm,
                                                     int chunk, RecMesh M, int ntiles,
                                                     double2* __restrict__ part) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double red[2 * NZT][4];
   int row = blockIdx.x / ntiles, tile = blockIdx.x % ntiles;
   int4 ri = M.rows[row];
@@ -674,6 +688,8 @@ static __global__ void __launch_bounds__(128) k_rec_field_x2(const float2* __res
                                                       const double2* __restrict__ part, int npart,
                                                       double4* __restrict__ Gpart,
                                                       double4* __restrict__ Hpart) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ unsigned char shraw[];
   float2* sh = reinterpret_cast<float2*>(shraw);
   int r0 = rchunk[blockIdx.y], r1 = rchunk[blockIdx.y + 1];

@@ -1439,7 +1439,7 @@ __global__ void k_cg_plan(double* __restrict__ sc, double* __restrict__ plan, in
   plan[1] = stop ? 1.0 : 0.0;
   if (!stop) {
     const bool trust = !fp32 || kCgGap * rmsd <= 0.5 * tol;
-    sc[5] = !fp32 ? tol : (trust ? 0.5 * tol : fmax(tol, 1e-4 * rmsd));
+    sc[5] = !fp32 ? tol : (trust ? tol - kCgGap * rmsd : fmax(tol, 1e-4 * rmsd));
     sc[7] = maxit;
     plan[2] = outer + 1.0;
     plan[3] = trust ? 1.0 : 0.0;
@@ -1662,14 +1662,14 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
     // Inner CG on the residual.  FP64: the recurrence residual is exact to
     // rounding, so its convergence is final.  FP32 operator: the recurrence
     // drifts from the true residual by about the FP32 matvec error (~1e-6
-    // relative) summed over the corrections, i.e. a few 1e-6 of the residual
-    // it started from; when that start is small enough the recurrence is
-    // trusted to half the tolerance and no second FP64 residual is formed
-    // (on the 12k-ion SiO2 MD the true residual then ends at <= 0.26 tol),
-    // else it reduces the residual by 1e-4 and a new FP64 residual restarts
-    // it (iterative refinement).
+    // relative) summed over the corrections, at most kCgGap = 3e-6 of the
+    // residual it started from (measured); when that bound is at most half
+    // the tolerance the recurrence is trusted down to the tolerance less the
+    // bound and no second FP64 residual is formed, else it reduces the
+    // residual by 1e-4 and a new FP64 residual restarts it (iterative
+    // refinement).
     bool trust = !fp32 || kCgGap * rmsd <= 0.5 * tol;
-    double tol_in = !fp32 ? tol : (trust ? 0.5 * tol : std::max(tol, 1e-4 * rmsd));
+    double tol_in = !fp32 ? tol : (trust ? tol - kCgGap * rmsd : std::max(tol, 1e-4 * rmsd));
     k_setd2<<<1, 32, 0, h->st>>>(sc + 5, tol_in, sc + 7, (double)maxit);
     LAUNCH_CHECK();
     while (true) {

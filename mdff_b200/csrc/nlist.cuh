@@ -82,18 +82,27 @@ __global__ void k_disp_partial(const double4* __restrict__ s, const double4* __r
   }
 }
 
+// one warp: lanes merge strided block partials, then the warp's top-2 merge
+// (the top two of a multiset do not depend on the order of the merges)
 __global__ void k_disp_final(const double2* __restrict__ part, int nb, double skindiff,
                              int* __restrict__ flags, double* __restrict__ disp_out) {
   pdl_wait();
   pdl_trigger();
-  if (threadIdx.x != 0) return;
   double a = 0.0, b = 0.0;
-  for (int k = 0; k < nb; ++k) {
+  for (int k = threadIdx.x; k < nb; k += 32) {
     double n1 = fmax(a, part[k].x);
     double n2 = fmax(fmin(a, part[k].x), fmax(b, part[k].y));
     a = n1;
     b = n2;
   }
+  for (int o = 16; o > 0; o >>= 1) {
+    double a1 = __shfl_xor_sync(FULL_MASK, a, o), b1 = __shfl_xor_sync(FULL_MASK, b, o);
+    double n1 = fmax(a, a1);
+    double n2 = fmax(fmin(a, a1), fmax(b, b1));
+    a = n1;
+    b = n2;
+  }
+  if (threadIdx.x != 0) return;
   if (disp_out) disp_out[0] = a + b;
   // tools.f90:513: if ( drneimax + drneimax2 .gt. skindiff ) rebuild
   if (a + b > skindiff) flags[0] = 1;

@@ -469,7 +469,7 @@ __host__ __device__ constexpr size_t field_tc_smem(int KF) { return (size_t)6 * 
 // memory, zero outside the row's nz range: from rhoA, or (npart > 0) summed
 // from the structure-factor chunk partials in chunk order (rho_prime, the same
 // sums as k_rec_sum), which saves that pass when no energy is needed.
-constexpr int kBtRows = 4;
+constexpr int kBtRows = 1;
 
 template <bool HAS_H, int KF>
 static __global__ void __launch_bounds__(128) k_rec_field_btiles(RecMesh M, const double2* __restrict__ rhoA,

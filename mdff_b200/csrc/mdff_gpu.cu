@@ -1575,6 +1575,66 @@ static int cg_residual(mdff_ctx* h, bool fp32) {
   return reduce_into(h, nb, 2, h->d_scal + S_CG);
 }
 
+// The static pass can merge with the first FP64 residual when the first
+// guess does not need the static field: the ASPC predictor (calc md / opt)
+// of the CG solver, without static dipoles (whose field the static pass adds)
+static bool cg_merged(const mdff_ctx* h) {
+  return h->p.lcoulomb && h->lpolar && h->p.solver == MDFF_SOLVER_CG && !h->ldip_static &&
+         (h->p.calc == MDFF_CALC_MD || h->p.calc == MDFF_CALC_OPT);
+}
+
+// the static field plus the field of the first guess x0 (FP64, real space on
+// the side stream with the FP32 pair cache of the mixed CG operator,
+// reciprocal space with the charges and x0 together), then the CG start
+// vectors from b + T x0 as one vector: one pass over pairs and k vectors
+// instead of the static pass and a residual pass
+static int merged_residual(mdff_ctx* h, bool fp32) {
+  int n = h->natm, nb = cdiv(n, 256), s;
+  PolDev P = poldev(h);
+  double4* E = h->d_Tp;
+  CK(cudaMemsetAsync(E, 0, sizeof(double4) * n, h->st));
+  double cutsq = h->p.cutlongrange * h->p.cutlongrange;
+  int nbw = cdiv((long)n * 32, 256);
+  if (h->p.lsurf && (s = moments(h, h->d_mu_ind, 1, h->d_scal + S_MOM2))) return s;
+  cudaStream_t rs;
+  if ((s = rs_fork(h, &rs))) return s;
+  int pr = prof_begin(h, KC_ESFIELD, 0);
+  if (fp32 && h->d_ddr) {
+#define SRC(K)                                                                                      \
+  k_static_res_cache<K><<<nbw, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu_ind,  \
+                                             h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, \
+                                             h->ntype, h->p.alphaES, cutsq, h->task_qq ? 1 : 0, E,   \
+                                             h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->p.thole_type)
+    if (h->tt_k == 4) SRC(4);
+    else SRC(0);
+#undef SRC
+    h->dd_cache_ok = true;
+  } else {
+#define ESF2(K)                                                                                    \
+  k_es_field<double, true, true, K><<<nbw, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar,  \
+                                                         h->d_mu_ind, h->L.nbr, h->L.nnb, h->L.cap, \
+                                                         n, h->d_cell, h->d_estab, h->ntype,       \
+                                                         h->p.alphaES, cutsq, 1, 1, E, h->p.thole_type)
+    if (h->tt_k == 4) ESF2(4);
+    else ESF2(0);
+#undef ESF2
+  }
+  LAUNCH_CHECK();
+  prof_end(h, pr);
+  if ((s = rec_pass(h, false, h->d_mu_ind, h->task_qq ? 1 : 0, 1, 0, E, nullptr,
+                    self_field(h, h->d_mu_ind, h->d_scal + S_MOM2))))
+    return s;
+  PDL_CHECK(pdl_launch(k_cg_init, dim3(nb), dim3(256), 0, h->st, (const double4*)nullptr, (const double4*)E,
+                       (const double4*)h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
+                       (const CellC*)h->d_cell, fp32 ? h->d_w32 : (float4*)nullptr, h->d_mu32));
+  return reduce_into(h, nb, 2, h->d_scal + S_CG);
+}
+
+// the solve's first FP64 residual: merged with the static pass when it can be
+static int cg_first_residual(mdff_ctx* h, bool fp32) {
+  return cg_merged(h) ? merged_residual(h, fp32) : cg_residual(h, fp32);
+}
+
 // outcome of one launch of the CG graph from the host copies of the scalars:
 // true when the solve is finished; *rmsd, *it as the loop leaves them
 static bool cg_graph_outcome(const mdff_ctx* h, double* rmsd, int* it) {
@@ -1614,10 +1674,17 @@ static void cg_stats(mdff_ctx* h, double rmsd0, double rmsd, int it, int nres) {
 
 // further outer iterations after a first graph launch that did not finish
 // the solve (the FP64 residual of the dipoles it left, then the CG graph)
-// (*first: the rmsd of the first FP64 residual of the solve, when it is this call's)
-static int cg_continue(mdff_ctx* h, bool fp32, double* rmsd, int* it, int* nres, double* first) {
+// (*first: the rmsd of the first FP64 residual of the solve, when it is this
+// call's; estat_missing: the static field was merged into the first
+// residual and is formed alone before the next one)
+static int cg_continue(mdff_ctx* h, bool fp32, double* rmsd, int* it, int* nres, double* first,
+                       bool estat_missing) {
   int s;
   while (true) {
+    if (estat_missing) {
+      if ((s = static_field(h, fp32))) return s;
+      estat_missing = false;
+    }
     if ((s = cg_residual(h, fp32))) return s;
     ++*nres;
     CK(cudaGraphLaunch(h->cg_exec, h->st));
@@ -1635,21 +1702,41 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
   int maxit = cg_maxit_of(h);
   double* sc = h->d_scal + S_CG;
   bool use_graph = !h->prof;
-  if (use_graph && (h->cg_exec == nullptr || h->cg_gen != h->gen || h->cg_fp32 != (fp32 ? 1 : 0)))
-    if ((s = build_cg_graph(h, fp32))) return s;
   if ((s = cg_prologue(h, itime))) return s;
   double rmsd = HUGE_VAL, rmsd0 = HUGE_VAL;
   int outer = 0, it = 0, nres = 0;
+  const bool merged = cg_merged(h);
   if (use_graph) {
-    if ((s = cg_continue(h, fp32, &rmsd, &it, &nres, &rmsd0))) return s;
+    if ((s = cg_first_residual(h, fp32))) return s;
+    nres = 1;
+    // (built after the first residual, which decides whether the FP32 pair
+    // cache serves the operator)
+    if (h->cg_exec == nullptr || h->cg_gen != h->gen || h->cg_fp32 != (fp32 ? 1 : 0))
+      if ((s = build_cg_graph(h, fp32))) return s;
+    CK(cudaGraphLaunch(h->cg_exec, h->st));
+    CK(cudaMemcpyAsync(h->h_scal + S_CG, h->d_scal + S_CG, sizeof(double) * (S_CGP + 4 - S_CG),
+                       cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    rmsd0 = h->h_scal[S_CGP];
+    if (!cg_graph_outcome(h, &rmsd, &it) &&
+        (s = cg_continue(h, fp32, &rmsd, &it, &nres, nullptr, merged)))
+      return s;
     h->launches += h->cg_body_launches * it + nres;  // + one k_cg_plan per graph launch
     cg_stats(h, rmsd0, rmsd, it, nres);
     return cg_epilogue(h);
   }
-  bool need_residual = true;
+  bool need_residual = true, estat_missing = merged;
   while (true) {
     if (need_residual) {
-      if ((s = cg_residual(h, fp32))) return s;
+      if (nres == 0) {
+        if ((s = cg_first_residual(h, fp32))) return s;
+      } else {
+        if (estat_missing) {
+          if ((s = static_field(h, fp32))) return s;
+          estat_missing = false;
+        }
+        if ((s = cg_residual(h, fp32))) return s;
+      }
       CK(cudaMemcpyAsync(h->h_scal + S_CG, sc, sizeof(double) * 9, cudaMemcpyDeviceToHost, h->st));
       CK(cudaStreamSynchronize(h->st));
       ++nres;
@@ -1741,7 +1828,8 @@ static int ef_front(mdff_ctx* h, bool fp32) {
       if (h->d_hist_save)
         CK(cudaMemcpyAsync(h->d_hist_save, h->d_hist, sizeof(double4) * MDFF_ASPC_DEPTH * n,
                            cudaMemcpyDeviceToDevice, h->st));
-      if ((s = static_field(h, fp32))) return s;
+      // (merged into the solve's first residual when it can be)
+      if (!cg_merged(h) && (s = static_field(h, fp32))) return s;
     }
   }
   return MDFF_OK;
@@ -1898,6 +1986,8 @@ static int build_step_graph(mdff_ctx* h, int itime, bool fp32) {
   step_graph_free(h);
   const bool cg = h->p.lcoulomb && h->lpolar;
   int s;
+  // the operator reads the FP32 pair cache when the front fills it
+  if (cg && fp32 && h->d_ddr) h->dd_cache_ok = true;
   if (cg && (h->cg_exec == nullptr || h->cg_gen != h->gen || h->cg_fp32 != (fp32 ? 1 : 0)))
     if ((s = build_cg_graph(h, fp32))) return s;
   bool prof = h->prof;
@@ -1910,7 +2000,7 @@ static int build_step_graph(mdff_ctx* h, int itime, bool fp32) {
   if ((s = capture_begin(h))) return s;
   s = ef_front(h, fp32);
   if (!s && cg) s = cg_prologue(h, itime);
-  if (!s && cg) s = cg_residual(h, fp32);
+  if (!s && cg) s = cg_first_residual(h, fp32);
   // a capture ends joined: the short-range pass (~100 us) joins at the end of
   // the front, which takes longer (static field + FP64 residual)
   if (!s) s = sr_join(h);
@@ -2008,7 +2098,7 @@ static int run_engforce_graph(mdff_ctx* h, int itime, bool* used) {
       // another outer iteration: from the dipoles the graph left, then the
       // back part again on the converged dipoles
       h->call_overlap = h->overlap;
-      if ((s = cg_continue(h, fp32, &rmsd, &it, &nres, nullptr))) return s;
+      if ((s = cg_continue(h, fp32, &rmsd, &it, &nres, nullptr, cg_merged(h)))) return s;
       if ((s = cg_epilogue(h)) || (s = ef_back(h, fp32))) return s;
       CK(cudaStreamSynchronize(h->st));
     }

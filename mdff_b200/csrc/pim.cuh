@@ -192,7 +192,9 @@ __global__ void k_cg_init(const double4* __restrict__ b, const double4* __restri
     double4 ri = make_double4(0, 0, 0, 0), zi = make_double4(0, 0, 0, 0);
     if (P.ipolar[i]) {
       double4 ax = matvec3(P.invpol + 9 * (size_t)i, x[i]);
-      ri = make_double4(b[i].x + Tx[i].x - ax.x, b[i].y + Tx[i].y - ax.y, b[i].z + Tx[i].z - ax.z, 0);
+      // b = nullptr: Tx already holds b + T x (the merged static pass)
+      const double4 bi = b ? b[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+      ri = make_double4(bi.x + Tx[i].x - ax.x, bi.y + Tx[i].y - ax.y, bi.z + Tx[i].z - ax.z, 0);
       zi = matvec3(P.pol + 9 * (size_t)i, ri);
       const double* a = P.pol + 9 * (size_t)i;
       double rr[3] = {ri.x, ri.y, ri.z};

@@ -446,10 +446,9 @@ static __global__ void __launch_bounds__(256) k_es_field(
   if (QQ || dip_i) {
     for (int k = lane; k < n; k += 32) {
       int j = row[k];
-      double4 sj = s[j];
-      R rx, ry, rz;
-      R r2 = pair_vec<R>(cA, si, sj, rx, ry, rz);
-      if (r2 > rc2) continue;  // ewald_dir.f90:202 ( d2 .gt. cutsq ) cycle
+      // the partner's charge and dipole first: a pair with neither term
+      // skips the minimum image (the non-polarisable partners of a dipole
+      // field of the solver)
       M4 muj{};
       bool dd = false;
       if (DD && dip_i) {
@@ -458,6 +457,10 @@ static __global__ void __launch_bounds__(256) k_es_field(
       }
       double qj = QQ ? q[j] : 0.0;
       if (!dd && (!QQ || qj == 0.0)) continue;
+      double4 sj = s[j];
+      R rx, ry, rz;
+      R r2 = pair_vec<R>(cA, si, sj, rx, ry, rz);
+      if (r2 > rc2) continue;  // ewald_dir.f90:202 ( d2 .gt. cutsq ) cycle
       int tj = ((QQ && damp) || (DD && thole)) ? itype[j] : 0;
       es_field_pair<R, QQ, DD, K>(stab, ntype, i, j, ti, tj, rx, ry, rz, r2, (R)alpha, damp, qj, dd,
                                DD ? (R)muj.x : R(0), DD ? (R)muj.y : R(0), DD ? (R)muj.z : R(0),
@@ -567,6 +570,112 @@ static __global__ void __launch_bounds__(256) k_static_cache(
   if (lane == 0) {
     double4 o = E[i];
     E[i] = make_double4(o.x + dx, o.y + dy, o.z + dz, 0.0);
+    cn[i] = m;
+  }
+}
+
+// The static pass merged with the dipole solve's first FP64 residual, for a
+// first guess x0 that does not depend on the static field (the ASPC
+// predictor): adds into E, in FP64, the damped charge field of every
+// partner (the static field, moment_from_pola.f90:327-330; ewald_dir.f90:
+// 533-541) and the undamped dipole field T2(r) x0_j of every polarisable
+// partner (the induced field of x0, :401-404; ewald_dir.f90:566-571), and
+// writes the FP32 pair cache of the CG operator as k_static_cache does (here
+// from the FP64 pair values).  Inclusion by the reference's FP64 test d2 > rc2.
+template <int K>
+static __global__ void __launch_bounds__(256) k_static_res_cache(
+    const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
+    const int* __restrict__ ipolar, const double4* __restrict__ x0, const int* __restrict__ nbr,
+    const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
+    const ESPair* __restrict__ tab, int ntype, double alpha, double cutsq, int has_q,
+    double4* __restrict__ E, float4* __restrict__ cr, float* __restrict__ cb1, int* __restrict__ cj,
+    int* __restrict__ cn, int thole = 0) {
+  __shared__ ESPair stab[MDFF_NT * MDFF_NT];
+  __shared__ double cA[9];
+  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
+  if (threadIdx.x < 9) cA[threadIdx.x] = cell->A[threadIdx.x];
+  __syncthreads();
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= natm) return;
+  const double4 si = s[i];
+  const int ti = itype[i];
+  const bool pol_i = ipolar[i] != 0;
+  const int n = nnb[i];
+  const int* row = nbr + (size_t)i * cap;
+  const size_t cbase = (size_t)i * cap;
+  double ex = 0.0, ey = 0.0, ez = 0.0;
+  int m = 0;
+  for (int k0 = 0; k0 < n; k0 += 32) {
+    int k = k0 + lane;
+    bool keep = false;
+    float4 rc = make_float4(0.f, 0.f, 0.f, 0.f);
+    float b1 = 0.f;
+    int j = 0;
+    if (k < n) {
+      j = row[k];
+      const double qj = has_q ? q[j] : 0.0;
+      const bool pp = pol_i && ipolar[j] != 0;
+      if (qj != 0.0 || pp) {
+        double rx, ry, rz;
+        const double r2 = pair_vec<double>(cA, si, s[j], rx, ry, rz);
+        if (r2 <= cutsq) {  // ewald_dir.f90:202
+          Radial<double> g;
+          radial<double, false>(r2, alpha, g);
+          if (qj != 0.0) {
+            double F1d = 0.0;
+            const int tj = itype[j];
+            const bool i_is_a = half_mask(i, j);
+            const ESPair& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
+            if (P.ldamp && (i_is_a ? P.ca : P.cb) != 0.0) {  // c = 0 damps nothing
+              double fdm, fdd;
+              if (i_is_a)
+                tt_damp_k<double, K>(P.ba, P.ca, g.d, P.ka, fdm, fdd);
+              else
+                tt_damp_k<double, K>(P.bb, P.cb, g.d, P.kb, fdm, fdd);
+              F1d = 1.0 - fdm;
+            }
+            const double c = qj * g.dm3 * (g.F1 - F1d);
+            ex += c * rx;
+            ey += c * ry;
+            ez += c * rz;
+          }
+          if (pp) {
+            double F1 = g.F1, F2 = g.F2;
+            if (thole) {
+              const int tj = itype[j];
+              const bool i_is_a = half_mask(i, j);
+              const ESPair& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
+              if (P.thole) thole_radial<double>(P, g.d, F1, F2);
+            }
+            const double B1 = F1 * g.dm3, B2 = 3.0 * F2 * g.dm5;
+            const double4 xj = x0[j];
+            const double rm = rx * xj.x + ry * xj.y + rz * xj.z;
+            ex += B2 * rx * rm - B1 * xj.x;
+            ey += B2 * ry * rm - B1 * xj.y;
+            ez += B2 * rz * rm - B1 * xj.z;
+            keep = true;
+            rc = make_float4((float)rx, (float)ry, (float)rz, (float)B2);
+            b1 = (float)B1;
+          }
+        }
+      }
+    }
+    unsigned bal = __ballot_sync(FULL_MASK, keep);
+    if (keep) {
+      int pos = m + __popc(bal & ((1u << lane) - 1u));
+      cr[cbase + pos] = rc;
+      cb1[cbase + pos] = b1;
+      cj[cbase + pos] = j;
+    }
+    m += __popc(bal);
+  }
+  ex = warp_sum(ex);
+  ey = warp_sum(ey);
+  ez = warp_sum(ez);
+  if (lane == 0) {
+    double4 o = E[i];
+    E[i] = make_double4(o.x + ex, o.y + ey, o.z + ez, 0.0);
     cn[i] = m;
   }
 }

@@ -66,3 +66,37 @@ def test_mixed_precision_nacl(oracle):
         g = eng.engforce(*s.soa())
     assert rms_rel(forces(g), forces(o)) <= 1e-5
     assert abs(g["u_coul"] - o["u_coul"]) / abs(o["u_coul"]) <= 1e-6
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_cg_md_sequence_matches_oracle(oracle, prec):
+    """An MD sequence with the CG solver and the ASPC predictor (calc md): the
+    static pass merged into the first FP64 residual, the order ramp on the
+    launch-by-launch path and the whole-step graph after it.  Every step
+    against the oracle's SCF on the same positions and history: FP64 to
+    1e-9, mixed within the 1e-5 force bar; the ASPC history at the end."""
+    s = systems.sio2(nsio2=150, seed=9, calc=_abi.CALC_MD, conv_tol_ind=1e-12,
+                     max_scf_pol_iter=500, extrapolate_order=2)
+    orc = oracle.Oracle(params_copy(s.params), s.cell)
+    p = params_copy(s.params)
+    p.solver = _abi.SOLVER_CG
+    p.cg_tol = 1e-12
+    p.cg_max_iter = 500
+    if prec == "mixed":
+        p.precision = _abi.PREC_MIXED
+    rng = np.random.default_rng(5)
+    pos = s.pos.copy()
+    with ForceEngine(p, s.cell) as eng:
+        for itime in range(8):
+            soa = tuple(np.ascontiguousarray(pos[:, a]) for a in range(3))
+            g = eng.engforce(*soa, itime=itime)
+            o = orc.engforce(*soa, itime=itime)
+            if prec == "fp64":
+                compare(g, o, 1e-9)
+            else:
+                assert rms_rel(forces(g), forces(o)) <= 1e-5, itime
+                assert rms_rel(g["mu"], o["mu"]) <= 1e-5, itime
+            pos = pos + rng.uniform(-0.01, 0.01, pos.shape)
+        h = eng.aspc_history()
+    ho = orc.get_aspc()
+    assert rel(h, ho) <= (1e-9 if prec == "fp64" else 1e-5)

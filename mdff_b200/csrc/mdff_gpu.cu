@@ -885,7 +885,7 @@ static int build_tables(mdff_ctx* h) {
 // weights_ready: d_w32 / d_mu32 already hold the FP32 operands of mu (written
 // by the CG direction kernels)
 static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, double4* E,
-                       bool weights_ready = false) {
+                       bool weights_ready = false, bool cached64 = false) {
   int n = h->natm;
   // FP32 CG operator with the pair cache: one kernel writes E (reciprocal +
   // self + cached real-space dipole field)
@@ -903,11 +903,15 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   int nch = 0;
   SelfField sf = self_field(h, mu, h->d_scal + S_MOM2);
   if (!fp32) {
-    // FP64: the real-space dipole field beside the reciprocal pass
+    // FP64: the real-space dipole field beside the reciprocal pass (cached64:
+    // the FP32 operator's cached pair tensor, FP64 products and sums)
     cudaStream_t rs;
     if ((s = rs_fork(h, &rs))) return s;
     int pr = prof_begin(h, KC_ESFIELD, 0);
-    k_es_field<double, false, true><<<nb, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E, h->p.thole_type);
+    if (cached64 && dd_mask == 1 && h->dd_cache_ok)
+      k_dd_cached64<<<nb, 256, 0, rs>>>(mu, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n, E);
+    else
+      k_es_field<double, false, true><<<nb, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, mu, h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, h->ntype, h->p.alphaES, cutsq, 0, dd_mask, E, h->p.thole_type);
     LAUNCH_CHECK();
     prof_end(h, pr);
     return rec_pass(h, false, mu, 0, 1, 0, E, nullptr, sf);
@@ -1565,11 +1569,13 @@ static int cg_prologue(mdff_ctx* h, int itime) {
 }
 
 // true residual of the current dipoles (FP64 matvec), the CG start vectors
-// and their norms (sc[0], sc[1])
+// and their norms (sc[0], sc[1]).  With the FP32 operator's pair cache the
+// real-space half applies the cached pair tensor (FP64 products and sums):
+// the refinement then converges on the system its operator approximates.
 static int cg_residual(mdff_ctx* h, bool fp32) {
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
-  if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp))) return s;
+  if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp, false, fp32))) return s;
   PDL_CHECK(pdl_launch(k_cg_init, dim3(nb), dim3(256), 0, h->st, h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
                                    h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32));
   return reduce_into(h, nb, 2, h->d_scal + S_CG);
@@ -1583,11 +1589,12 @@ static bool cg_merged(const mdff_ctx* h) {
          (h->p.calc == MDFF_CALC_MD || h->p.calc == MDFF_CALC_OPT);
 }
 
-// the static field plus the field of the first guess x0 (FP64, real space on
-// the side stream with the FP32 pair cache of the mixed CG operator,
-// reciprocal space with the charges and x0 together), then the CG start
-// vectors from b + T x0 as one vector: one pass over pairs and k vectors
-// instead of the static pass and a residual pass
+// the static field plus the field of the first guess x0 (real space on the
+// side stream: FP64, or in the mixed engine the FP32 static pass that writes
+// the pair cache of its CG operator and applies the cached pair tensor to x0
+// with FP64 products and sums; reciprocal space in FP64 with the charges and
+// x0 together), then the CG start vectors from b + T x0 as one vector: one
+// pass over pairs and k vectors instead of the static pass and a residual pass
 static int merged_residual(mdff_ctx* h, bool fp32) {
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
@@ -1600,11 +1607,12 @@ static int merged_residual(mdff_ctx* h, bool fp32) {
   if ((s = rs_fork(h, &rs))) return s;
   int pr = prof_begin(h, KC_ESFIELD, 0);
   if (fp32 && h->d_ddr) {
-#define SRC(K)                                                                                      \
-  k_static_res_cache<K><<<nbw, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->d_mu_ind,  \
-                                             h->L.nbr, h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab, \
-                                             h->ntype, h->p.alphaES, cutsq, h->task_qq ? 1 : 0, E,   \
-                                             h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->p.thole_type)
+#define SRC(K)                                                                                    \
+  k_static_cache<K, true><<<nbw, 256, 0, rs>>>(h->d_s, h->d_q, h->d_itype, h->d_ipolar, h->L.nbr,  \
+                                               h->L.nnb, h->L.cap, n, h->d_cell, h->d_estab,       \
+                                               h->ntype, h->p.alphaES, cutsq, h->task_qq ? 1 : 0,  \
+                                               E, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn,         \
+                                               h->p.thole_type, h->d_mu_ind)
     if (h->tt_k == 4) SRC(4);
     else SRC(0);
 #undef SRC

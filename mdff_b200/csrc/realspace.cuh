@@ -484,13 +484,23 @@ static __global__ void __launch_bounds__(256) k_es_field(
 // dipole solve then read these instead of recomputing erfc / exp per pair
 // (positions are fixed within a call).  K: compile-time Tang-Toennies order
 // (0 = per pair).
-template <int K>
+//
+// RES: the same pass merged with the dipole solve's first residual, for a
+// first guess x0 that does not depend on the static field (the ASPC
+// predictor): E also gets the undamped dipole field T2(r) x0_j of every
+// polarisable partner (the induced field of x0, moment_from_pola.f90:401-404;
+// ewald_dir.f90:566-571) from the cached FP32 terms, with FP64 products and
+// sums, so that the residual sees the same pair tensor as the FP32 operator
+// (k_dd_cached_rec) and the FP64 residuals after it (k_dd_cached64).  The
+// charge field is the same code and order as without RES.
+template <int K, bool RES = false>
 static __global__ void __launch_bounds__(256) k_static_cache(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
     const int* __restrict__ ipolar, const int* __restrict__ nbr, const int* __restrict__ nnb,
     int cap, int natm, const CellC* __restrict__ cell, const ESPair* __restrict__ tab, int ntype,
     double alpha, double cutsq, int has_q, double4* __restrict__ E, float4* __restrict__ cr,
-    float* __restrict__ cb1, int* __restrict__ cj, int* __restrict__ cn, int thole = 0) {
+    float* __restrict__ cb1, int* __restrict__ cj, int* __restrict__ cn, int thole = 0,
+    const double4* __restrict__ x0 = nullptr) {
   __shared__ ESPair stab[MDFF_NT * MDFF_NT];
   __shared__ double cA[9];
   for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
@@ -506,6 +516,7 @@ static __global__ void __launch_bounds__(256) k_static_cache(
   const int* row = nbr + (size_t)i * cap;
   size_t cbase = (size_t)i * cap;
   float ex = 0.f, ey = 0.f, ez = 0.f;
+  double tx = 0.0, ty = 0.0, tz = 0.0;  // RES: T2 x0
   const float rc2 = (float)cutsq;
   int m = 0;
   for (int k0 = 0; k0 < n; k0 += 32) {
@@ -553,6 +564,14 @@ static __global__ void __launch_bounds__(256) k_static_cache(
             }
             B1 = F1 * g.dm3;
             B2 = 3.f * F2 * g.dm5;
+            if (RES) {
+              const double4 xj = x0[j];
+              const double drx = rx, dry = ry, drz = rz, dB1 = B1, dB2 = B2;
+              const double rm = drx * xj.x + dry * xj.y + drz * xj.z;
+              tx += dB2 * drx * rm - dB1 * xj.x;
+              ty += dB2 * dry * rm - dB1 * xj.y;
+              tz += dB2 * drz * rm - dB1 * xj.z;
+            }
           }
         }
       }
@@ -567,115 +586,14 @@ static __global__ void __launch_bounds__(256) k_static_cache(
     m += __popc(bal);
   }
   double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
+  if (RES) {
+    dx += warp_sum(tx);
+    dy += warp_sum(ty);
+    dz += warp_sum(tz);
+  }
   if (lane == 0) {
     double4 o = E[i];
     E[i] = make_double4(o.x + dx, o.y + dy, o.z + dz, 0.0);
-    cn[i] = m;
-  }
-}
-
-// The static pass merged with the dipole solve's first FP64 residual, for a
-// first guess x0 that does not depend on the static field (the ASPC
-// predictor): adds into E, in FP64, the damped charge field of every
-// partner (the static field, moment_from_pola.f90:327-330; ewald_dir.f90:
-// 533-541) and the undamped dipole field T2(r) x0_j of every polarisable
-// partner (the induced field of x0, :401-404; ewald_dir.f90:566-571), and
-// writes the FP32 pair cache of the CG operator as k_static_cache does (here
-// from the FP64 pair values).  Inclusion by the reference's FP64 test d2 > rc2.
-template <int K>
-static __global__ void __launch_bounds__(256) k_static_res_cache(
-    const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
-    const int* __restrict__ ipolar, const double4* __restrict__ x0, const int* __restrict__ nbr,
-    const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
-    const ESPair* __restrict__ tab, int ntype, double alpha, double cutsq, int has_q,
-    double4* __restrict__ E, float4* __restrict__ cr, float* __restrict__ cb1, int* __restrict__ cj,
-    int* __restrict__ cn, int thole = 0) {
-  __shared__ ESPair stab[MDFF_NT * MDFF_NT];
-  __shared__ double cA[9];
-  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
-  if (threadIdx.x < 9) cA[threadIdx.x] = cell->A[threadIdx.x];
-  __syncthreads();
-  int lane = threadIdx.x & 31;
-  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (i >= natm) return;
-  const double4 si = s[i];
-  const int ti = itype[i];
-  const bool pol_i = ipolar[i] != 0;
-  const int n = nnb[i];
-  const int* row = nbr + (size_t)i * cap;
-  const size_t cbase = (size_t)i * cap;
-  double ex = 0.0, ey = 0.0, ez = 0.0;
-  int m = 0;
-  for (int k0 = 0; k0 < n; k0 += 32) {
-    int k = k0 + lane;
-    bool keep = false;
-    float4 rc = make_float4(0.f, 0.f, 0.f, 0.f);
-    float b1 = 0.f;
-    int j = 0;
-    if (k < n) {
-      j = row[k];
-      const double qj = has_q ? q[j] : 0.0;
-      const bool pp = pol_i && ipolar[j] != 0;
-      if (qj != 0.0 || pp) {
-        double rx, ry, rz;
-        const double r2 = pair_vec<double>(cA, si, s[j], rx, ry, rz);
-        if (r2 <= cutsq) {  // ewald_dir.f90:202
-          Radial<double> g;
-          radial<double, false>(r2, alpha, g);
-          if (qj != 0.0) {
-            double F1d = 0.0;
-            const int tj = itype[j];
-            const bool i_is_a = half_mask(i, j);
-            const ESPair& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
-            if (P.ldamp && (i_is_a ? P.ca : P.cb) != 0.0) {  // c = 0 damps nothing
-              double fdm, fdd;
-              if (i_is_a)
-                tt_damp_k<double, K>(P.ba, P.ca, g.d, P.ka, fdm, fdd);
-              else
-                tt_damp_k<double, K>(P.bb, P.cb, g.d, P.kb, fdm, fdd);
-              F1d = 1.0 - fdm;
-            }
-            const double c = qj * g.dm3 * (g.F1 - F1d);
-            ex += c * rx;
-            ey += c * ry;
-            ez += c * rz;
-          }
-          if (pp) {
-            double F1 = g.F1, F2 = g.F2;
-            if (thole) {
-              const int tj = itype[j];
-              const bool i_is_a = half_mask(i, j);
-              const ESPair& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
-              if (P.thole) thole_radial<double>(P, g.d, F1, F2);
-            }
-            const double B1 = F1 * g.dm3, B2 = 3.0 * F2 * g.dm5;
-            const double4 xj = x0[j];
-            const double rm = rx * xj.x + ry * xj.y + rz * xj.z;
-            ex += B2 * rx * rm - B1 * xj.x;
-            ey += B2 * ry * rm - B1 * xj.y;
-            ez += B2 * rz * rm - B1 * xj.z;
-            keep = true;
-            rc = make_float4((float)rx, (float)ry, (float)rz, (float)B2);
-            b1 = (float)B1;
-          }
-        }
-      }
-    }
-    unsigned bal = __ballot_sync(FULL_MASK, keep);
-    if (keep) {
-      int pos = m + __popc(bal & ((1u << lane) - 1u));
-      cr[cbase + pos] = rc;
-      cb1[cbase + pos] = b1;
-      cj[cbase + pos] = j;
-    }
-    m += __popc(bal);
-  }
-  ex = warp_sum(ex);
-  ey = warp_sum(ey);
-  ez = warp_sum(ez);
-  if (lane == 0) {
-    double4 o = E[i];
-    E[i] = make_double4(o.x + ex, o.y + ey, o.z + ez, 0.0);
     cn[i] = m;
   }
 }
@@ -684,11 +602,15 @@ static __global__ void __launch_bounds__(256) k_static_res_cache(
 // 32, ... in that order.  Four entries per lane are in flight at once (their
 // cache words first, then the four dipole gathers), so the row costs a
 // quarter of the dependent load round trips of a one-entry loop.
-__device__ __forceinline__ void dd_cached_row(const float4* __restrict__ mu,
+// (R = float: FP32 dipoles and sums; R = double: FP64 dipoles, the cached
+// terms widened, FP64 products and sums)
+template <typename R>
+__device__ __forceinline__ void dd_cached_row(const typename vec4t<R>::T* __restrict__ mu,
                                               const float4* __restrict__ cr,
                                               const float* __restrict__ cb1,
                                               const int* __restrict__ cj, size_t base, int n,
-                                              int lane, float& ex, float& ey, float& ez) {
+                                              int lane, R& ex, R& ey, R& ez) {
+  typedef typename vec4t<R>::T M4;
   constexpr int U = 4;
   for (int k0 = lane; k0 < n; k0 += 32 * U) {
     float4 r[U];
@@ -702,16 +624,17 @@ __device__ __forceinline__ void dd_cached_row(const float4* __restrict__ mu,
       r[u] = ok ? cr[base + k] : make_float4(0.f, 0.f, 0.f, 0.f);
       b1[u] = ok ? cb1[base + k] : 0.f;
     }
-    float4 m[U];
+    M4 m[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) m[u] = (k0 + 32 * u < n) ? mu[j[u]] : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int u = 0; u < U; ++u) m[u] = (k0 + 32 * u < n) ? mu[j[u]] : M4{};
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (k0 + 32 * u >= n) break;
-      float rm = r[u].x * m[u].x + r[u].y * m[u].y + r[u].z * m[u].z;
-      ex += r[u].w * r[u].x * rm - b1[u] * m[u].x;
-      ey += r[u].w * r[u].y * rm - b1[u] * m[u].y;
-      ez += r[u].w * r[u].z * rm - b1[u] * m[u].z;
+      const R x = r[u].x, y = r[u].y, z = r[u].z, w = r[u].w, b = b1[u];
+      R rm = x * m[u].x + y * m[u].y + z * m[u].z;
+      ex += w * x * rm - b * m[u].x;
+      ey += w * y * rm - b * m[u].y;
+      ez += w * z * rm - b * m[u].z;
     }
   }
 }
@@ -728,7 +651,7 @@ static __global__ void __launch_bounds__(256) k_dd_cached_part(
   if (i >= natm) return;
   int n = cn[i];
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  dd_cached_row(mu, cr, cb1, cj, (size_t)i * cap, n, lane, ex, ey, ez);
+  dd_cached_row<float>(mu, cr, cb1, cj, (size_t)i * cap, n, lane, ex, ey, ez);
   double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
   if (lane == 0) Edd[i] = make_double4(dx, dy, dz, 0.0);
 }
@@ -747,11 +670,34 @@ static __global__ void __launch_bounds__(256) k_dd_cached(
   if (n == 0) return;
   size_t base = (size_t)i * cap;
   float ex = 0.f, ey = 0.f, ez = 0.f;
-  dd_cached_row(mu, cr, cb1, cj, base, n, lane, ex, ey, ez);
+  dd_cached_row<float>(mu, cr, cb1, cj, base, n, lane, ex, ey, ez);
   double dx = warp_sum((double)ex), dy = warp_sum((double)ey), dz = warp_sum((double)ez);
   if (lane == 0) {
     double4 o = E[i];
     E[i] = make_double4(o.x + dx, o.y + dy, o.z + dz, 0.0);
+  }
+}
+
+// FP64 dipole field of mu (double4) from the same pair cache, FP64 products
+// and sums: the real-space half of the mixed solver's FP64 residuals, which
+// thus see the pair tensor of its FP32 operator
+static __global__ void __launch_bounds__(256) k_dd_cached64(
+    const double4* __restrict__ mu, const float4* __restrict__ cr, const float* __restrict__ cb1,
+    const int* __restrict__ cj, const int* __restrict__ cn, int cap, int natm,
+    double4* __restrict__ E) {
+  int lane = threadIdx.x & 31;
+  int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= natm) return;
+  int n = cn[i];
+  if (n == 0) return;
+  double ex = 0.0, ey = 0.0, ez = 0.0;
+  dd_cached_row<double>(mu, cr, cb1, cj, (size_t)i * cap, n, lane, ex, ey, ez);
+  ex = warp_sum(ex);
+  ey = warp_sum(ey);
+  ez = warp_sum(ez);
+  if (lane == 0) {
+    double4 o = E[i];
+    E[i] = make_double4(o.x + ex, o.y + ey, o.z + ez, 0.0);
   }
 }
 

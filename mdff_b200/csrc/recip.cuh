@@ -531,7 +531,7 @@ static __global__ void __launch_bounds__(256) k_dd_cached_rec(
     dz = v.z;
   } else {
     float ex = 0.f, ey = 0.f, ez = 0.f;
-    dd_cached_row(mu, cr, cb1, cj, (size_t)i * cap, cn[i], lane, ex, ey, ez);
+    dd_cached_row<float>(mu, cr, cb1, cj, (size_t)i * cap, cn[i], lane, ex, ey, ez);
     dx = warp_sum((double)ex);
     dy = warp_sum((double)ey);
     dz = warp_sum((double)ez);

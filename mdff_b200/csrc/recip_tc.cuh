@@ -469,7 +469,7 @@ __host__ __device__ constexpr size_t field_tc_smem(int KF) { return (size_t)6 * 
 // memory, zero outside the row's nz range: from rhoA, or (npart > 0) summed
 // from the structure-factor chunk partials in chunk order (rho_prime, the same
 // sums as k_rec_sum), which saves that pass when no energy is needed.
-constexpr int kBtRows = 1;
+constexpr int kBtRows = 4;
 
 template <bool HAS_H, int KF>
 static __global__ void __launch_bounds__(128) k_rec_field_btiles(RecMesh M, const double2* __restrict__ rhoA,
@@ -622,43 +622,26 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
   const int ionc = ion_ok ? ion : 0;
   float4 wi = ion_ok ? w[ion] : make_float4(0.f, 0.f, 0.f, 0.f);
   double G[3] = {0.0, 0.0, 0.0}, H[3] = {0.0, 0.0, 0.0};
-  // the epilogue's per-(ion, row) phases X_nx Y_ny of one 32-column chunk;
-  // those of the first chunk of a tile are loaded before the wait for the
-  // tile's matrix products, so that their latency overlaps it
-  struct Phases {
-    int nx[RPC], ny[RPC];
-    float ok[RPC];
-    float2 X[RPC], Y[RPC];
-  };
-  auto load_phases = [&](int t, int ch, Phases& ph) {
-#pragma unroll
-    for (int jj = 0; jj < RPC; ++jj) {
-      int row = t * RPT + ch * RPC + jj;
-      bool ok = row < M.nrows;
-      int4 ri = M.rows[ok ? row : 0];
-      ph.nx[jj] = ri.x;
-      ph.ny[jj] = ri.y;
-      ph.ok[jj] = (ok && ion_ok) ? 1.f : 0.f;
-      int ay = ri.y < 0 ? -ri.y : ri.y;
-      ph.X[jj] = tab[(size_t)ri.x * natm + ionc];
-      ph.Y[jj] = tab[(size_t)(kx + 1 + ay) * natm + ionc];
-    }
-  };
-  Phases pre;  // first chunk of the next epilogue's tile
   auto epilogue = [&](int t, int b) {
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc) {
       int ch = hh + 2 * cc;
-      Phases cur;
-      if (cc == 0)
-        cur = pre;
-      else
-        load_phases(t, ch, cur);
-      int* nxr = cur.nx;
-      int* nyr = cur.ny;
-      float* okr = cur.ok;
-      float2* X = cur.X;
-      float2* Y = cur.Y;
+      // the chunk's rows and this ion's phases X_nx Y_ny first (loads in flight together)
+      int nxr[RPC], nyr[RPC];
+      float okr[RPC];
+      float2 X[RPC], Y[RPC];
+#pragma unroll
+      for (int jj = 0; jj < RPC; ++jj) {
+        int row = t * RPT + ch * RPC + jj;
+        bool ok = row < M.nrows;
+        int4 ri = M.rows[ok ? row : 0];
+        nxr[jj] = ri.x;
+        nyr[jj] = ri.y;
+        okr[jj] = (ok && ion_ok) ? 1.f : 0.f;
+        int ay = ri.y < 0 ? -ri.y : ri.y;
+        X[jj] = tab[(size_t)ri.x * natm + ionc];
+        Y[jj] = tab[(size_t)(kx + 1 + ay) * natm + ionc];
+      }
       float v[32];
       tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 128 + ch * 32), v);
 #pragma unroll
@@ -690,7 +673,6 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
   for (int k = 0; k < T; ++k) {
     const int b = k & 1;
     if (k >= 1) {
-      load_phases(tbeg + k - 1, hh, pre);
       // tile k - 1 multiplied: B buffer (k + 1) & 1 is free, its D is ready
       if (tid == 0 && !tc::mbar_wait(tc::smem_u32(&mbar[(k - 1) & 1]), ((k - 1) >> 1) & 1, tc::kWaitLimit))
         abort_flag = 1;
@@ -731,7 +713,6 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (!abort_flag && issued > done) {
-    load_phases(tbeg + issued - 1, hh, pre);
     if (tid == 0 && !tc::mbar_wait(tc::smem_u32(&mbar[(issued - 1) & 1]), ((issued - 1) >> 1) & 1, tc::kWaitLimit))
       abort_flag = 1;
     __syncthreads();

@@ -120,7 +120,8 @@ struct mdff_ctx {
   int n_rho_chunks = 0;
   int nsm = 0;  // SMs of the device
   // FP32 structure factor of the CG operator on the tensor cores
-  // (k_rec_rho_tc): ion chunk size and count; off when kz > 31 or
+  // (k_rec_rho_tc): ion chunk size and count; off when the mesh does not
+  // fit (6 (kz + 1) > 256 B rows, or more shared memory than one CTA has) or
   // MDFF_REC_TC=0 in the environment
   bool rho_tc = false;
   int tc_chunk = 0, n_tc_chunks = 0;
@@ -426,27 +427,18 @@ static int build_mesh(mdff_ctx* h) {
   DALLOC(h->d_rchunk, h->rchunk.size());
   h->n_rho_chunks = cdiv(h->natm, kRhoChunk);
   {
-    // tensor-core structure factor: about two CTAs per SM over (row tiles x ion chunks)
+    // tensor-core structure factor: one CTA per SM over (row tiles x ion chunks)
     const char* env = std::getenv("MDFF_REC_TC");
-    h->rho_tc = rho_tc_nb(h->p.kES[2]) > 0 && nrows > 0 && !(env && env[0] == '0') &&
-                rho_tc_smem(h->p.kES[0], h->p.kES[1], h->p.kES[2]) <= 227 * 1024;
-    int tiles = cdiv(nrows, 32);
-    int nchunk = std::max(1, (2 * (h->nsm > 0 ? h->nsm : 148)) / std::max(tiles, 1));
-    h->tc_chunk = std::max(tc::KB, cdiv(cdiv(h->natm, nchunk), tc::KB) * tc::KB);
+    h->rho_tc = rho_tc_fits(h->p.kES[0], h->p.kES[1], h->p.kES[2]) && nrows > 0 && !(env && env[0] == '0');
+    int tiles = cdiv(nrows, kRhoTcRows);
+    int nchunk = std::max(1, (h->nsm > 0 ? h->nsm : 148) / std::max(tiles, 1));
+    h->tc_chunk = std::max(kRhoTcKB, cdiv(cdiv(h->natm, nchunk), kRhoTcKB) * kRhoTcKB);
     h->n_tc_chunks = cdiv(h->natm, h->tc_chunk);
   }
   DALLOC(h->d_rho_part, (size_t)std::max(h->n_rho_chunks, h->n_tc_chunks) * std::max(nk, 1));
-  if (h->rho_tc) {
-    int smem = (int)rho_tc_smem(h->p.kES[0], h->p.kES[1], h->p.kES[2]);
-#define TC_ATTR(Q, MU, NB) \
-  CK(cudaFuncSetAttribute(k_rec_rho_tc<Q, MU, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem))
-    if (rho_tc_nb(h->p.kES[2]) == 32) {
-      TC_ATTR(true, true, 32); TC_ATTR(false, true, 32); TC_ATTR(true, false, 32);
-    } else {
-      TC_ATTR(true, true, 64); TC_ATTR(false, true, 64); TC_ATTR(true, false, 64);
-    }
-#undef TC_ATTR
-  }
+  if (h->rho_tc)
+    CK(cudaFuncSetAttribute(k_rec_rho_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            (int)rho_tc_smem(h->p.kES[0], h->p.kES[1], h->p.kES[2])));
   {
     const char* env = std::getenv("MDFF_FIELD_TC");
     int kf = field_tc_kf(h->p.kES[2]);
@@ -668,28 +660,14 @@ static void launch_rho(mdff_ctx* h, dim3 g, const typename cplx<R>::T* tab, int 
     (void)pdl_launch(k_rec_rho<R, false, true, NZT>, dim3(g), dim3(kRhoThreads), 0, h->st, tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
 }
 
-// FP32 structure factor on the tensor cores into d_rho_part (n_tc_chunks chunks)
-template <int NB>
-static void launch_rho_tc_n(mdff_ctx* h, const RecMesh& M, int n, int has_q, int has_mu) {
-  size_t smem = rho_tc_smem_n(NB, M.kmax[0], M.kmax[1], M.kmax[2]);
-  int* err = h->d_cata + 1;
-  const int* wcfg = h->d_cata + 3;
-  const float2* tab = h->d_tab32;
-  const float4* w = h->d_w32;
-  // (a launch error surfaces at the caller's LAUNCH_CHECK)
-  if (has_mu) {
-    dim3 g((unsigned)cdiv(M.nrows, 32), (unsigned)h->n_tc_chunks);
-    if (has_q)
-      (void)pdl_launch(k_rec_rho_tc<true, true, NB>, g, dim3(kRhoTcThreads), smem, h->st, tab, w, n,
-                       h->tc_chunk, M, h->d_rho_part, err, wcfg);
-    else
-      (void)pdl_launch(k_rec_rho_tc<false, true, NB>, g, dim3(kRhoTcThreads), smem, h->st, tab, w, n,
-                       h->tc_chunk, M, h->d_rho_part, err, wcfg);
-  } else {
-    dim3 g((unsigned)cdiv(M.nrows, 64), (unsigned)h->n_tc_chunks);
-    (void)pdl_launch(k_rec_rho_tc<true, false, NB>, g, dim3(kRhoTcThreads), smem, h->st, tab, w, n,
-                     h->tc_chunk, M, h->d_rho_part, err, wcfg);
-  }
+// FP32 structure factor of the dipoles on the tensor cores into d_rho_part
+// (n_tc_chunks chunks); a launch error surfaces at the caller's LAUNCH_CHECK
+static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n) {
+  size_t smem = rho_tc_smem(M.kmax[0], M.kmax[1], M.kmax[2]);
+  dim3 g((unsigned)cdiv(M.nrows, kRhoTcRows), (unsigned)h->n_tc_chunks);
+  (void)pdl_launch(k_rec_rho_tc, g, dim3(kRhoTcThreads), smem, h->st, (const float2*)h->d_tab32,
+                   (const float4*)h->d_w32, n, h->tc_chunk, M, h->d_rho_part, h->d_cata + 1,
+                   (const int*)(h->d_cata + 3));
 }
 
 // FP32 field / force partials on the tensor cores into d_G / d_H (B tiles
@@ -729,13 +707,6 @@ static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int
 static int launch_field_tc(mdff_ctx* h, const RecMesh& M, int n, bool muf, int npart) {
   if (field_tc_kf(M.kmax[2]) == 32) return launch_field_tc_k<32>(h, M, n, muf, npart);
   return launch_field_tc_k<64>(h, M, n, muf, npart);
-}
-
-static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n, int has_q, int has_mu) {
-  if (rho_tc_nb(M.kmax[2]) == 32)
-    launch_rho_tc_n<32>(h, M, n, has_q, has_mu);
-  else
-    launch_rho_tc_n<64>(h, M, n, has_q, has_mu);
 }
 
 // reciprocal pass: E += rec field (+ the self / surface field sf, when on);
@@ -787,7 +758,7 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   // with round-to-nearest)
   if (F32 && h->rho_tc && !has_q && has_mu && !forces) {
     nparts = h->n_tc_chunks;
-    launch_rho_tc(h, M, n, has_q, has_mu);
+    launch_rho_tc(h, M, n);
   } else {
     switch (nzt) {
       case 8: launch_rho<R, 8>(h, g, tab, n, chunk, M, ntiles, has_q, has_mu); break;

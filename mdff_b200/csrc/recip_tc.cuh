@@ -2,26 +2,27 @@
 // tensor cores (tcgen05, kind::tf32, accumulator in tensor memory).
 //
 // rho(k) = sum_i (q_i + i k.mu_i) e^{i k.r_i}   (ewald_rec.f90:118-148)
-// With e^{i k.r} = X_nx Y_ny Z_nz (per-ion phase tables) and k.mu = nx m1 + ny m2
-// + nz m3 (m = 2 pi B^T mu), each mesh row (nx, ny) and each nz:
-//   rho(nx, ny, nz) = sum_i U_i Z_nz(i) + nz sum_i V_i Z_nz(i),
-//   U_i = (q_i + i (nx m1_i + ny m2_i)) X_nx Y_ny,   V_i = i m3_i X_nx Y_ny.
-// For a tile of mesh rows this is a real GEMM over the ions:
+// The tensor cores serve the FP32 CG operator, where only dipoles contribute.
+// With e^{i k.r} = X_nx Y_ny Z_nz (per-ion phase tables), P = X_nx Y_ny and
+// k.mu = nx m1 + ny m2 + nz m3 (m = 2 pi B^T mu), each mesh row (nx, ny) and nz:
+//   rho(nx, ny, nz) = i (nx S_1 + ny S_2 + nz S_3),   S_a = sum_i P_i m_a,i Z_nz(i).
+// For a tile of 64 mesh rows this is a real GEMM over the ions:
 //   D[m][c] = sum_i A[m][i] B[c][i],
-//   A rows m = (component, row), components Re U, Im U, Re V, Im V,
-//   B rows c = Re Z_0..Re Z_kz, Im Z_0..Im Z_kz (zero-padded to N),
+//   A rows m = Re P of the 64 rows, then Im P of the 64 rows (M = 128),
+//   B rows c = m_a Re Z_n, m_a Im Z_n for a = 1..3, n = 0..kz (N = 6 (kz + 1),
+//   zero-padded to a multiple of 16),
 // and Z_{-n} = conj Z_n gives both signs of nz from the same D.
 //
-// Each CTA (256 threads) owns 32 mesh rows (64 without dipoles: U only) and one
-// ion chunk.  Per block of 32 ions the threads generate A and B in shared memory
-// in the canonical no-swizzle K-major layout (8-row x 16-byte core matrices),
-// split into TF32 high and low parts (round-to-nearest), and one thread issues
-// A_hi [B_hi | B_lo] (N = 2 x 32) and A_lo B_hi per k-step of 8 (the three
-// products of split TF32); D stays in tensor memory across the whole chunk.  Two stages: the
-// threads fill one while the tensor core reads the other, released by
-// tcgen05.commit on an mbarrier.  The epilogue reads D (tcgen05.ld), combines
-// the components in FP64 and writes per-chunk partials rho(k) in the same layout
-// as the CUDA-core kernels (k_rec_sum adds the chunks in order).
+// Each CTA (one per SM) owns 64 mesh rows and one ion chunk.  Per block of 32
+// ions, 16 warps generate A and B in shared memory in the canonical no-swizzle
+// K-major layout (8-row x 16-byte core matrices), split into TF32 high and low
+// parts (round-to-nearest), and one thread of a 17th warp issues A_hi B_hi,
+// A_hi B_lo and A_lo B_hi per k-step of 8 (the three products of split TF32)
+// into one accumulator; D stays in tensor memory across the whole chunk.  Two
+// operand stages and three table stagings, handed over by mbarriers only (no
+// CTA-wide barrier in the K loop).  The epilogue reads D (tcgen05.ld), combines
+// the products in FP64 and writes per-chunk partials rho(k) in the same layout
+// as the CUDA-core kernels (the consumers add the chunks in order).
 //
 // Every wait is bounded: a wait that gives up sets err[0] = 1, the CTA stops
 // issuing, waits (bounded) for what it issued, frees its tensor memory and
@@ -125,43 +126,46 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int c = 0; c < 32; ++c) v[c] = __uint_as_float(r[c]);
 }
 
-constexpr int KB = 32;                 // ions per K block
 constexpr long kWaitLimit = 1L << 22;  // try_wait polls before a wait gives up
-
-// bytes of one pipeline stage: A hi + lo (128 x KB), B hi + lo (N x KB)
-__host__ __device__ constexpr int stage_bytes(int N) { return 2 * 128 * KB * 4 + 2 * N * KB * 4; }
 
 }  // namespace tc
 
-// B rows of the structure-factor GEMM for kz: 2 (kz + 1) rounded up to 16
-__host__ __device__ constexpr int rho_tc_n(int kz) { return ((2 * (kz + 1) + 15) / 16) * 16; }
+// B rows of the structure-factor GEMM for kz: 6 (kz + 1) rounded up to 16 (one
+// MMA takes N <= 256)
+__host__ __device__ constexpr int rho_tc_n(int kz) { return ((6 * (kz + 1) + 15) / 16) * 16; }
+// tensor-memory columns allocated for N accumulator columns (a power of two >= 32)
+__host__ __device__ constexpr int rho_tc_cols(int N) {
+  return N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+}
+
+constexpr int kRhoTcRows = 64;                          // mesh rows per tile (A rows: Re P, Im P)
+constexpr int kRhoTcGen = 512;                          // operand-generating threads (16 warps)
+constexpr int kRhoTcThreads = kRhoTcGen + 32;           // + one warp issuing the MMAs; one CTA per SM
+constexpr int kRhoTcKB = 32;                            // ions per K block
+constexpr int kRhoTcStg = 3;                            // table staging buffers
+
+// bytes of one operand stage: A hi + lo (128 x KB), B hi + lo (N x KB)
+__host__ __device__ constexpr int rho_tc_stage(int N) {
+  return 2 * 128 * kRhoTcKB * 4 + 2 * N * kRhoTcKB * 4;
+}
 
 // table staging of one K block: rows X_0..X_kx, Y_0..Y_ky, Z_0..Z_kz of the
-// phase tables (32 ions each, row stride 272 bytes so that lanes on different
-// rows hit different banks) and the 32 weights
-constexpr int kStageRow = 32 * 8 + 16;
+// phase tables (KB ions each, row stride KB x 8 + 16 bytes so that lanes on
+// different rows hit different banks) and the KB weights
+constexpr int kStageRow = kRhoTcKB * 8 + 16;
 __host__ __device__ constexpr int rho_tc_staging(int kx, int ky, int kz) {
-  return (kx + ky + kz + 3) * kStageRow + 32 * 16;
+  return (kx + ky + kz + 3) * kStageRow + kRhoTcKB * 16;
 }
 
-// B rows of the kernel instantiation that serves kz (32 or 64; 0: none)
-__host__ __device__ constexpr int rho_tc_nb(int kz) {
-  return rho_tc_n(kz) <= 32 ? 32 : (rho_tc_n(kz) <= 64 ? 64 : 0);
+// dynamic shared memory of k_rec_rho_tc: two operand stages, the table
+// stagings, alignment slack
+__host__ __device__ constexpr size_t rho_tc_smem(int kx, int ky, int kz) {
+  return 2 * (size_t)rho_tc_stage(rho_tc_n(kz)) + kRhoTcStg * (size_t)rho_tc_staging(kx, ky, kz) + 1024;
 }
-
-// dynamic shared memory of k_rec_rho_tc<., ., N>: two operand stages, two
-// table stagings, alignment slack
-__host__ __device__ constexpr size_t rho_tc_smem_n(int N, int kx, int ky, int kz) {
-  return 2 * (size_t)tc::stage_bytes(N) + 2 * (size_t)rho_tc_staging(kx, ky, kz) + 1024;
+// the mesh fits one MMA's N and one CTA's shared memory
+inline bool rho_tc_fits(int kx, int ky, int kz) {
+  return rho_tc_n(kz) <= 256 && rho_tc_smem(kx, ky, kz) <= 227 * 1024;
 }
-inline size_t rho_tc_smem(int kx, int ky, int kz) { return rho_tc_smem_n(rho_tc_nb(kz), kx, ky, kz); }
-
-// structure factor on the tensor cores.  grid = (row tiles, ion chunks),
-// kRhoTcThreads threads; part[chunk][k] = this chunk's rho(k).  Requires
-// N = rho_tc_n(kz) <= 64.  The table rows and weights of K block kb + 1 are
-// copied to shared memory (cp.async, coalesced) while the threads generate
-// block kb from the staged copy and the tensor core multiplies block kb - 1.
-constexpr int kRhoTcThreads = 256;
 
 __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
@@ -170,39 +174,79 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int by
   asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 }
 
-template <bool HAS_Q, bool HAS_MU, int N>
-static __global__ void __launch_bounds__(kRhoTcThreads) k_rec_rho_tc(
+namespace tc {
+// bounded wait on an mbarrier phase that also gives up once another thread of
+// the CTA has set the abort flag
+__device__ __forceinline__ bool mbar_wait_ab(uint32_t bar, uint32_t parity, long limit,
+                                             const volatile int* abort) {
+  for (long it = 0; it < limit; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3; "
+        "selp.b32 %0, 1, 0, p; }"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity), "r"(kSuspendNs)
+        : "memory");
+    if (ok) return true;
+    if (*abort) return false;
+  }
+  return false;
+}
+__device__ __forceinline__ void mbar_init_n(uint32_t bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("{ .reg .b64 st; mbarrier.arrive.shared::cta.b64 st, [%0]; }" ::"r"(bar) : "memory");
+}
+// the mbarrier receives one arrival once this thread's earlier cp.async
+// copies have landed
+__device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
+}  // namespace tc
+
+// structure factor of the dipoles on the tensor cores.  grid = (row tiles of
+// 64 mesh rows, ion chunks), one CTA per SM; part[chunk][k] = this chunk's
+// rho(k).  Warps 0-15 stage the phase tables (cp.async) and generate the
+// operands; warp 16 issues the MMAs.  No CTA-wide barrier inside the K loop:
+// mbarriers carry each dependency,
+//   tfull[b]  the tables of a K block landed in staging buffer b (every
+//             generating thread's copies, cp.async.mbarrier.arrive),
+//   full[s]   operand stage s written (every generating thread, after
+//             fence.proxy.async),
+//   empty[s]  the MMAs that read stage s are complete (tcgen05.commit),
+// so the tables of K block kb + 1 load while block kb is generated and block
+// kb - 1 multiplied, and warps drift apart by up to two K blocks.
+static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
     const float2* __restrict__ tab, const float4* __restrict__ w, int natm, int chunk, RecMesh M,
     double2* __restrict__ part, int* __restrict__ err, const int* __restrict__ wait_cfg) {
   pdl_wait();
   pdl_trigger();
-  constexpr int NT = kRhoTcThreads;
-  constexpr int RPT = HAS_MU ? 32 : 64;         // mesh rows per tile
-  constexpr int KB = tc::KB;
-  constexpr int AJ = RPT * (KB / 4) / NT;       // A items (row, 4 ions) per thread
+  constexpr int NG = kRhoTcGen, RPT = kRhoTcRows, KB = kRhoTcKB, KC = KB / 4, NS = kRhoTcStg;
+  static_assert(RPT * KC == NG, "A items: one (row, 4 ions) per generating thread");
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ __align__(8) uint64_t full[2], empty[2], tfull[NS];
   __shared__ uint32_t tslot;
-  __shared__ int abort_flag;
+  __shared__ int abort_flag, issued_sh;
+  const volatile int* abort_v = &abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int kx = M.kmax[0], ky = M.kmax[1], kz = M.kmax[2];
   const int nzc = kz + 1;
-  static_assert(N == 32 || N == 64, "B rows: 32 or 64");
-  // tensor memory: columns [0, N) A_hi B_hi + A_lo B_hi, [N, 2N) A_hi B_lo
-  constexpr int ncols = 2 * N;
-  const int stage = tc::stage_bytes(N);
+  const int N = rho_tc_n(kz);
+  const int ncols = rho_tc_cols(N);
+  const int stage = rho_tc_stage(N);
   {
-    // the launch must provide this instantiation's shared memory
+    // the launch must provide the mesh's shared memory
     uint32_t dyn;
     asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-    if (dyn < rho_tc_smem_n(N, kx, ky, kz) || rho_tc_nb(kz) != N) {
-      if (threadIdx.x == 0) atomicExch(err, 2);
+    if (dyn < rho_tc_smem(kx, ky, kz) || N > 256) {
+      if (tid == 0) atomicExch(err, 2);
       return;
     }
   }
-  // B is one tile of 2N rows: B_hi rows [0, N), B_lo rows [N, 2N)
-  const int offAL = 128 * KB * 4, offB = 2 * 128 * KB * 4;
+  // stage layout: A_hi (128 x KB), A_lo, B_hi (N x KB), B_lo
+  const int offAL = 128 * KB * 4, offB = 2 * 128 * KB * 4, offBL = offB + N * KB * 4;
   const int TR = kx + ky + kz + 3;  // staged table rows
   const int sbytes = rho_tc_staging(kx, ky, kz);
   unsigned char* stg0 = sm + 2 * stage;
@@ -215,9 +259,23 @@ static __global__ void __launch_bounds__(kRhoTcThreads) k_rec_rho_tc(
   }
   if (tid == 0) {
     abort_flag = 0;
-    tc::mbar_init(tc::smem_u32(&mbar[0]));
-    tc::mbar_init(tc::smem_u32(&mbar[1]));
+    issued_sh = 0;
+    for (int s = 0; s < 2; ++s) {
+      tc::mbar_init_n(tc::smem_u32(&full[s]), NG);
+      tc::mbar_init_n(tc::smem_u32(&empty[s]), 1);
+    }
+    for (int b = 0; b < NS; ++b) tc::mbar_init_n(tc::smem_u32(&tfull[b]), NG);
     asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  {
+    // B padding rows [6 nzc, N) are zero in both stages, hi and lo
+    const int padr = N - 6 * nzc;
+    for (int e = tid; e < 4 * padr * KC; e += blockDim.x) {
+      const int kc = e % KC, rest = e / KC;
+      const int c = 6 * nzc + rest % padr, sp = rest / padr;
+      unsigned char* S = sm + (sp >> 1) * stage + ((sp & 1) ? offBL : offB);
+      *reinterpret_cast<uint4*>(S + tc::canon(c, kc * 4, N)) = make_uint4(0u, 0u, 0u, 0u);
+    }
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -227,163 +285,176 @@ static __global__ void __launch_bounds__(kRhoTcThreads) k_rec_rho_tc(
   const int r0 = blockIdx.x * RPT;
   const int a0 = blockIdx.y * chunk;
   const int a1 = min(a0 + chunk, natm);
-  // this thread's mesh row (fixed: NT is a multiple of RPT)
-  const int rl = tid % RPT;
-  const bool row_ok = r0 + rl < M.nrows;
-  int nx = 0, ny = 0;
-  if (row_ok) {
-    int4 ri = M.rows[r0 + rl];
-    nx = ri.x;
-    ny = ri.y;
-  }
-  const int ay = ny < 0 ? -ny : ny;
-  const float sy = ny < 0 ? -1.f : 1.f;
-  const float fnx = (float)nx, fny = (float)ny;
-  const float rowf = row_ok ? 1.f : 0.f;  // rows past the mesh generate zeros
-  const uint32_t idesc1 = tc::idesc_tf32(128, 2 * N), idesc2 = tc::idesc_tf32(128, N);
-  const uint32_t lboA = (128 / 8) * 128, lboB = (uint32_t)(2 * N / 8) * 128;
-
-  // copy table rows t (global row t of the [X | Y | Z] tables) and weights of
-  // K block kb into staging buffer kb & 1; ions past a1 are zero-filled
-  // element e = tid + NT q of a block is table row t = tid / 32 + 8 q, ion
-  // j = lane: the same ion for all of this thread's copies
-  const size_t row_step = (size_t)(NT / 32) * natm;
-  auto stage_tables = [&](int kb) {
-    const int i = a0 + kb * KB + lane;
-    const bool ok = i < a1;
-    const int nb = ok ? 8 : 0;
-    uint32_t dst = tc::smem_u32(stg0 + (kb & 1) * sbytes) + (uint32_t)(warp * kStageRow + lane * 8);
-    const float2* src = tab + (size_t)warp * natm + (ok ? i : a0);
-    for (int t = warp; t < TR; t += NT / 32) {
-      cp_async8(dst, src, nb);
-      dst += (NT / 32) * kStageRow;
-      src += row_step;
-    }
-    if (tid < 32)
-      cp_async16(tc::smem_u32(stg0 + (kb & 1) * sbytes + TR * kStageRow + lane * 16), w + (ok ? i : a0),
-                 ok ? 16 : 0);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  };
-
   const int nkb = (a1 - a0 + KB - 1) / KB;
-  // polls of the wait for a free operand stage: tc::kWaitLimit unless the
-  // host set a limit (a test hook; the drain wait below keeps kWaitLimit)
-  const long opwait = *wait_cfg >= 0 ? (long)*wait_cfg : tc::kWaitLimit;
-  if (nkb > 0) stage_tables(0);
-  int issued = 0;  // K blocks committed by thread 0
-  for (int kb = 0; kb < nkb; ++kb) {
-    const int st = kb & 1;
-    unsigned char* S = sm + st * stage;
-    const unsigned char* T = stg0 + st * sbytes;
-    if (kb + 1 < nkb) {
-      stage_tables(kb + 1);
-      asm volatile("cp.async.wait_group 1;" ::: "memory");
-    } else {
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
+  const uint32_t lboA = (128 / 8) * 128, lboB = (uint32_t)(N / 8) * 128;
+
+  if (warp < NG / 32) {
+    // ---- operand generation ------------------------------------------------
+    // A item of this thread: mesh row rl (fixed), ions 4 kcA .. 4 kcA + 3;
+    // rows past the mesh take row (0, 0) and their products are never read
+    const int rl = tid % RPT, kcA = tid / RPT;
+    int nx = 0, ny = 0;
+    if (r0 + rl < M.nrows) {
+      int4 ri = M.rows[r0 + rl];
+      nx = ri.x;
+      ny = ri.y;
     }
-    // one thread waits for the tensor core to release stage st; the barrier
-    // holds the others
-    if (kb >= 2 && tid == 0 &&
-        !tc::mbar_wait(tc::smem_u32(&mbar[st]), ((kb - 2) >> 1) & 1, opwait))
-      abort_flag = 1;
-    __syncthreads();
-    if (abort_flag) break;
-    const float4* Tw = reinterpret_cast<const float4*>(T + TR * kStageRow);
+    const int ay = ny < 0 ? -ny : ny;
+    const float sy = ny < 0 ? -1.f : 1.f;  // Y_{-n} = conj Y_n
+    const int xoff = nx * kStageRow + kcA * 32, yoff = (kx + 1 + ay) * kStageRow + kcA * 32;
+    const uint32_t oA = tc::canon(rl, kcA * 4, 128), oAi = tc::canon(RPT + rl, kcA * 4, 128);
+    // B items (at most two per thread: 3 nzc KC <= 2 NG for N <= 256): rows
+    // (2a) nzc + n = m_a Re Z_n and (2a + 1) nzc + n = m_a Im Z_n, ions 4 kc ..;
+    // consecutive threads take consecutive n (rows 16 bytes apart)
+    const int nB = 3 * nzc * KC;
+    int zoff[2], woff[2];
+    uint32_t oB[2], oBi[2];
 #pragma unroll
-    for (int j = 0; j < AJ; ++j) {
-      int kc = tid / RPT + j * (NT / RPT);
-      const float4* Xr = reinterpret_cast<const float4*>(T + nx * kStageRow + kc * 32);
-      const float4* Yr = reinterpret_cast<const float4*>(T + (kx + 1 + ay) * kStageRow + kc * 32);
-      float4 x01 = Xr[0], x23 = Xr[1], y01 = Yr[0], y23 = Yr[1];
-      float2 X[4] = {make_float2(x01.x, x01.y), make_float2(x01.z, x01.w), make_float2(x23.x, x23.y),
-                     make_float2(x23.z, x23.w)};
-      float2 Y[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w), make_float2(y23.x, y23.y),
-                     make_float2(y23.z, y23.w)};
-      float v[4][4];  // [component][ion]
+    for (int q = 0; q < 2; ++q) {
+      const int it = tid + q * NG;
+      const int n = it % nzc, rest = it / nzc;
+      const int kc = rest % KC, a = rest / KC;
+      zoff[q] = (kx + 1 + ky + 1 + n) * kStageRow + kc * 32;
+      woff[q] = TR * kStageRow + kc * 64 + (a + 1) * 4;  // weight component m_a of ion 4 kc
+      oB[q] = tc::canon(2 * a * nzc + n, kc * 4, N);
+      oBi[q] = tc::canon((2 * a + 1) * nzc + n, kc * 4, N);
+    }
+    // copy table rows t (global row t of the [X | Y | Z] tables) and weights
+    // of K block kb into staging buffer kb % NS; ions past a1 are zero-filled.
+    // Element e = t KB + j: consecutive threads copy consecutive ions.
+    auto stage_tables = [&](int kb) {
+      const int ib = a0 + kb * KB;
+      const int b = kb % NS;
+      const uint32_t dst0 = tc::smem_u32(stg0 + b * sbytes);
+      for (int e = tid; e < TR * KB; e += NG) {
+        const int t = e / KB, j = e % KB;
+        const int i = ib + j;
+        const bool ok = i < a1;
+        cp_async8(dst0 + (uint32_t)(t * kStageRow + j * 8), tab + (size_t)t * natm + (ok ? i : a0), ok ? 8 : 0);
+      }
+      if (tid < KB) {
+        const int i = ib + tid;
+        const bool ok = i < a1;
+        cp_async16(dst0 + (uint32_t)(TR * kStageRow + tid * 16), w + (ok ? i : a0), ok ? 16 : 0);
+      }
+      tc::cp_async_arrive(tc::smem_u32(&tfull[b]));
+    };
+    // polls of the wait for a free operand stage: tc::kWaitLimit unless the
+    // host set a limit (a test hook)
+    const long opwait = *wait_cfg >= 0 ? (long)*wait_cfg : tc::kWaitLimit;
+    if (nkb > 0) stage_tables(0);
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int st = kb & 1, b = kb % NS;
+      if (kb + 1 < nkb) {
+        // staging buffer (kb + 1) % NS last held block kb - 2: every thread
+        // has generated that block once its full[] phase completed
+        if (kb >= 2 && !tc::mbar_wait_ab(tc::smem_u32(&full[st]), ((kb - 2) >> 1) & 1, tc::kWaitLimit, abort_v)) {
+          abort_flag = 1;
+          break;
+        }
+        stage_tables(kb + 1);
+      }
+      if (!tc::mbar_wait_ab(tc::smem_u32(&tfull[b]), (kb / NS) & 1, tc::kWaitLimit, abort_v)) {
+        abort_flag = 1;
+        break;
+      }
+      // operand stage st is free once the MMAs of block kb - 2 completed
+      if (kb >= 2 && !tc::mbar_wait_ab(tc::smem_u32(&empty[st]), ((kb - 2) >> 1) & 1, opwait, abort_v)) {
+        abort_flag = 1;
+        break;
+      }
+      unsigned char* S = sm + st * stage;
+      const unsigned char* T = stg0 + b * sbytes;
+      {
+        const float4* Xr = reinterpret_cast<const float4*>(T + xoff);
+        const float4* Yr = reinterpret_cast<const float4*>(T + yoff);
+        const float4 x01 = Xr[0], x23 = Xr[1], y01 = Yr[0], y23 = Yr[1];
+        const float xr[4] = {x01.x, x01.z, x23.x, x23.z}, xi[4] = {x01.y, x01.w, x23.y, x23.w};
+        const float yr[4] = {y01.x, y01.z, y23.x, y23.z};
+        const float yi[4] = {sy * y01.y, sy * y01.w, sy * y23.y, sy * y23.w};
+        uint32_t ph[4], pl[4], qh[4], ql[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        float4 wi = Tw[kc * 4 + u];
-        float Pr = X[u].x * Y[u].x - X[u].y * (sy * Y[u].y);
-        float Pi = X[u].x * (sy * Y[u].y) + X[u].y * Y[u].x;
-        float q = HAS_Q ? rowf * wi.x : 0.f;
-        float km = HAS_MU ? rowf * (fnx * wi.y + fny * wi.z) : 0.f;
-        float m3 = HAS_MU ? rowf * wi.w : 0.f;
-        v[0][u] = q * Pr - km * Pi;
-        v[1][u] = q * Pi + km * Pr;
-        v[2][u] = -m3 * Pi;
-        v[3][u] = m3 * Pr;
+        for (int u = 0; u < 4; ++u) {
+          tc::tf32_split(xr[u] * yr[u] - xi[u] * yi[u], ph[u], pl[u]);
+          tc::tf32_split(xr[u] * yi[u] + xi[u] * yr[u], qh[u], ql[u]);
+        }
+        *reinterpret_cast<uint4*>(S + oA) = make_uint4(ph[0], ph[1], ph[2], ph[3]);
+        *reinterpret_cast<uint4*>(S + offAL + oA) = make_uint4(pl[0], pl[1], pl[2], pl[3]);
+        *reinterpret_cast<uint4*>(S + oAi) = make_uint4(qh[0], qh[1], qh[2], qh[3]);
+        *reinterpret_cast<uint4*>(S + offAL + oAi) = make_uint4(ql[0], ql[1], ql[2], ql[3]);
       }
 #pragma unroll
-      for (int c = 0; c < (HAS_MU ? 4 : 2); ++c) {
-        uint32_t hi[4], lo[4];
+      for (int q = 0; q < 2; ++q) {
+        if (tid + q * NG >= nB) break;
+        const float4* Zr = reinterpret_cast<const float4*>(T + zoff[q]);
+        const float4 z01 = Zr[0], z23 = Zr[1];
+        const float zr[4] = {z01.x, z01.z, z23.x, z23.z}, zi[4] = {z01.y, z01.w, z23.y, z23.w};
+        const float* wm = reinterpret_cast<const float*>(T + woff[q]);
+        uint32_t rh[4], rlo[4], ih[4], ilo[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) tc::tf32_split(v[c][u], hi[u], lo[u]);
-        uint32_t o = tc::canon(c * RPT + rl, kc * 4, 128);
-        *reinterpret_cast<uint4*>(S + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-        *reinterpret_cast<uint4*>(S + offAL + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        for (int u = 0; u < 4; ++u) {
+          const float m = wm[4 * u];
+          tc::tf32_split(m * zr[u], rh[u], rlo[u]);
+          tc::tf32_split(m * zi[u], ih[u], ilo[u]);
+        }
+        *reinterpret_cast<uint4*>(S + offB + oB[q]) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
+        *reinterpret_cast<uint4*>(S + offBL + oB[q]) = make_uint4(rlo[0], rlo[1], rlo[2], rlo[3]);
+        *reinterpret_cast<uint4*>(S + offB + oBi[q]) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
+        *reinterpret_cast<uint4*>(S + offBL + oBi[q]) = make_uint4(ilo[0], ilo[1], ilo[2], ilo[3]);
       }
+      tc::fence_async_smem();
+      tc::mbar_arrive(tc::smem_u32(&full[st]));
     }
-    // B: rows c = Re Z_c | Im Z_(c - nzc) | 0, high parts then low parts
-    for (int it = tid; it < N * (KB / 4); it += NT) {
-      int c = it % N, kc = it / N;
-      bool im = c >= nzc;
-      int n = im ? c - nzc : c;
-      float z[4] = {0.f, 0.f, 0.f, 0.f};
-      if (c < 2 * nzc) {
-        const float4* Zr = reinterpret_cast<const float4*>(T + (kx + 1 + ky + 1 + n) * kStageRow + kc * 32);
-        float4 z01 = Zr[0], z23 = Zr[1];
-        z[0] = im ? z01.y : z01.x;
-        z[1] = im ? z01.w : z01.z;
-        z[2] = im ? z23.y : z23.x;
-        z[3] = im ? z23.w : z23.z;
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (lane == 0) {
+    // ---- MMA issue: the three products of split TF32 into one accumulator --
+    const uint32_t idesc = tc::idesc_tf32(128, N);
+    int issued = 0;
+    for (int kb = 0; kb < nkb; ++kb) {
+      const int st = kb & 1;
+      if (!tc::mbar_wait_ab(tc::smem_u32(&full[st]), (kb >> 1) & 1, tc::kWaitLimit, abort_v)) {
+        abort_flag = 1;
+        break;
       }
-      uint32_t hi[4], lo[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) tc::tf32_split(z[u], hi[u], lo[u]);
-      *reinterpret_cast<uint4*>(S + offB + tc::canon(c, kc * 4, 2 * N)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-      *reinterpret_cast<uint4*>(S + offB + tc::canon(N + c, kc * 4, 2 * N)) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-    }
-    tc::fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
       tc::fence_after_sync();
-      const uint32_t base = tc::smem_u32(S);
+      const uint32_t base = tc::smem_u32(sm + st * stage);
 #pragma unroll
       for (int s = 0; s < KB / 8; ++s) {
-        uint32_t oa = (uint32_t)s * 2 * lboA, ob = (uint32_t)s * 2 * lboB;
-        uint64_t aH = tc::smem_desc(base + oa, lboA, 128), aL = tc::smem_desc(base + offAL + oa, lboA, 128);
-        // the first N rows of the B tile are B_hi: the same descriptor with N rows
-        uint64_t bB = tc::smem_desc(base + offB + ob, lboB, 128);
-        tc::mma_tf32(tmem, aH, bB, idesc1, (kb > 0 || s > 0) ? 1u : 0u);
-        tc::mma_tf32(tmem, aL, bB, idesc2, 1u);
+        const uint32_t oa = (uint32_t)s * 2 * lboA, ob = (uint32_t)s * 2 * lboB;
+        const uint64_t aH = tc::smem_desc(base + oa, lboA, 128), aL = tc::smem_desc(base + offAL + oa, lboA, 128);
+        const uint64_t bH = tc::smem_desc(base + offB + ob, lboB, 128), bL = tc::smem_desc(base + offBL + ob, lboB, 128);
+        tc::mma_tf32(tmem, aH, bH, idesc, (kb > 0 || s > 0) ? 1u : 0u);
+        tc::mma_tf32(tmem, aH, bL, idesc, 1u);
+        tc::mma_tf32(tmem, aL, bH, idesc, 1u);
       }
-      tc::mma_commit(tc::smem_u32(&mbar[st]));
+      tc::mma_commit(tc::smem_u32(&empty[st]));
+      issued = kb + 1;
     }
-    issued = kb + 1;
-  }
-  asm volatile("cp.async.wait_group 0;" ::: "memory");
-  if (issued > 0 && tid == 0) {
-    // the last commit covers every MMA issued before it
-    int last = issued - 1;
-    if (!tc::mbar_wait(tc::smem_u32(&mbar[last & 1]), (last >> 1) & 1, tc::kWaitLimit))
-      abort_flag = 1;
+    // the last commit covers every MMA issued before it (waited for even
+    // after an abort: tensor memory is freed only once they are done)
+    if (issued > 0) {
+      const int last = issued - 1;
+      if (!tc::mbar_wait(tc::smem_u32(&empty[last & 1]), (last >> 1) & 1, tc::kWaitLimit)) abort_flag = 1;
+    }
+    issued_sh = issued;
   }
   __syncthreads();
-  const bool all_ok = abort_flag == 0 && issued == nkb;
+  const bool all_ok = abort_flag == 0 && issued_sh == nkb;
   if (!all_ok && tid == 0) atomicExch(err, 1);
-  // epilogue: D (128 lanes x N columns) -> shared (row stride N + 1) -> rho.
-  // Warps 0-3 read the four 32-lane quarters of tensor memory.
+  // epilogue: D (128 lanes x N columns) -> shared (row stride N + 1).  Warp w
+  // < 16 reads lane quarter w % 4, column blocks w / 4, w / 4 + 4, ...
   float* Dsm = reinterpret_cast<float*>(sm);
-  if (all_ok && nkb > 0 && warp < 4) {
+  const int ldd = N + 1;
+  if (all_ok && nkb > 0 && warp < NG / 32) {
     tc::fence_after_sync();
-    for (int c0 = 0; c0 < N; c0 += 32) {
-      float v[32], vl[32];
-      tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-      tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(N + c0), vl);
-      int m = warp * 32 + lane;
+    const int q = warp & 3;
+    for (int cb = warp >> 2; cb * 32 < N; cb += NG / 128) {
+      float v[32];
+      tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cb * 32), v);
+      const int m = q * 32 + lane;
 #pragma unroll
       for (int c = 0; c < 32; ++c)
-        if (c0 + c < N) Dsm[m * (N + 1) + c0 + c] = v[c] + vl[c];
+        if (cb * 32 + c < N) Dsm[m * ldd + cb * 32 + c] = v[c];
     }
   }
   tc::fence_before_sync();
@@ -393,28 +464,34 @@ static __global__ void __launch_bounds__(kRhoTcThreads) k_rec_rho_tc(
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols));
   }
   if (!all_ok) return;
+  // rho(nz) = i (nx S1 + ny S2 + nz S3), S_a(+-n) from the four real products
+  // of (Re P, Im P) with (m_a Re Z_n, m_a Im Z_n), combined in FP64
   const int nzs = 2 * kz + 1;
-  for (int idx = tid; idx < RPT * nzs; idx += NT) {
-    int lr = idx / nzs, t = idx % nzs;
-    int r = r0 + lr;
+  for (int idx = tid; idx < RPT * nzs; idx += blockDim.x) {
+    const int lr = idx / nzs, t = idx % nzs;
+    const int r = r0 + lr;
     if (r >= M.nrows) continue;
-    int4 ri = M.rows[r];
-    int nz = ri.z + t;
+    const int4 ri = M.rows[r];
+    const int nz = ri.z + t;
     if (nz > kz) continue;
-    int n = nz < 0 ? -nz : nz;
-    double s = nz < 0 ? -1.0 : 1.0;
+    const int n = nz < 0 ? -nz : nz;
+    const double s = nz < 0 ? -1.0 : 1.0;
     double re = 0.0, imv = 0.0;
     if (nkb > 0) {
-      const float* Ur = Dsm + (size_t)(0 * RPT + lr) * (N + 1);
-      const float* Ui = Dsm + (size_t)(1 * RPT + lr) * (N + 1);
-      re = (double)Ur[n] - s * (double)Ui[nzc + n];
-      imv = s * (double)Ur[nzc + n] + (double)Ui[n];
-      if (HAS_MU) {
-        const float* Vr = Dsm + (size_t)(2 * RPT + lr) * (N + 1);
-        const float* Vi = Dsm + (size_t)(3 * RPT + lr) * (N + 1);
-        re += (double)nz * ((double)Vr[n] - s * (double)Vi[nzc + n]);
-        imv += (double)nz * (s * (double)Vr[nzc + n] + (double)Vi[n]);
+      const float* Dr = Dsm + (size_t)lr * ldd;
+      const float* Di = Dsm + (size_t)(RPT + lr) * ldd;
+      const double coef[3] = {(double)ri.x, (double)ri.y, (double)nz};
+      double Tr = 0.0, Ti = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const int cr = 2 * a * nzc + n, ci = (2 * a + 1) * nzc + n;
+        const double Sr = (double)Dr[cr] - s * (double)Di[ci];
+        const double Si = (double)Di[cr] + s * (double)Dr[ci];
+        Tr += coef[a] * Sr;
+        Ti += coef[a] * Si;
       }
+      re = -Ti;
+      imv = Tr;
     }
     part[(size_t)blockIdx.y * M.nk + ri.w + t] = make_double2(re, imv);
   }

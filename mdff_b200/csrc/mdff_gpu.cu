@@ -125,6 +125,10 @@ struct mdff_ctx {
   // MDFF_REC_TC=0 in the environment
   bool rho_tc = false;
   int tc_chunk = 0, n_tc_chunks = 0;
+  // its phase tables blocked by K block of kRhoTcKB ions (tc_nkb blocks),
+  // built per call with the FP32 tables
+  float2* d_rho_timg = nullptr;
+  int tc_nkb = 0;
   // FP32 reciprocal field / force partials on the tensor cores
   // (k_rec_field_tc, B tiles in d_fb); off when kz > 31 or MDFF_FIELD_TC=0
   // in the environment
@@ -434,6 +438,11 @@ static int build_mesh(mdff_ctx* h) {
     int nchunk = std::max(1, (h->nsm > 0 ? h->nsm : 148) / std::max(tiles, 1));
     h->tc_chunk = std::max(kRhoTcKB, cdiv(cdiv(h->natm, nchunk), kRhoTcKB) * kRhoTcKB);
     h->n_tc_chunks = cdiv(h->natm, h->tc_chunk);
+    h->tc_nkb = cdiv(h->natm, kRhoTcKB);
+    cudaFree(h->d_rho_timg);
+    h->d_rho_timg = nullptr;
+    if (h->rho_tc)
+      DALLOC(h->d_rho_timg, (size_t)h->tc_nkb * rho_tc_staging(h->p.kES[0], h->p.kES[1], h->p.kES[2]) / sizeof(float2));
   }
   DALLOC(h->d_rho_part, (size_t)std::max(h->n_rho_chunks, h->n_tc_chunks) * std::max(nk, 1));
   if (h->rho_tc)
@@ -665,7 +674,7 @@ static void launch_rho(mdff_ctx* h, dim3 g, const typename cplx<R>::T* tab, int 
 static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n) {
   size_t smem = rho_tc_smem(M.kmax[0], M.kmax[1], M.kmax[2]);
   dim3 g((unsigned)cdiv(M.nrows, kRhoTcRows), (unsigned)h->n_tc_chunks);
-  (void)pdl_launch(k_rec_rho_tc, g, dim3(kRhoTcThreads), smem, h->st, (const float2*)h->d_tab32,
+  (void)pdl_launch(k_rec_rho_tc, g, dim3(kRhoTcThreads), smem, h->st, (const float2*)h->d_rho_timg,
                    (const float4*)h->d_w32, n, h->tc_chunk, M, h->d_rho_part, h->d_cata + 1,
                    (const int*)(h->d_cata + 3));
 }
@@ -847,6 +856,11 @@ static int build_tables(mdff_ctx* h) {
   PDL_CHECK(pdl_launch(k_rec_tables<double>, dim3(cdiv(n, 128)), dim3(128), 0, h->st, h->d_s, n, h->p.kES[0], h->p.kES[1], kzt, h->d_tab64));
   if (h->p.precision == MDFF_PREC_MIXED) {
     PDL_CHECK(pdl_launch(k_rec_tables<float>, dim3(cdiv(n, 128)), dim3(128), 0, h->st, h->d_s, n, h->p.kES[0], h->p.kES[1], kzt, h->d_tab32));
+    // the same tables blocked by K block for the tensor-core structure
+    // factor of the dipole solve
+    if (h->rho_tc && h->lpolar)
+      PDL_CHECK(pdl_launch(k_rec_rho_timg, dim3((unsigned)h->tc_nkb), dim3(256), 0, h->st, (const float2*)h->d_tab32, n,
+                           h->p.kES[0], h->p.kES[1], h->p.kES[2], h->d_rho_timg));
   }
   return MDFF_OK;
 }
@@ -2301,7 +2315,7 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
     DALLOC(h->d_tab64, (size_t)ntab * n);
     if (p.precision == MDFF_PREC_MIXED) DALLOC(h->d_tab32, (size_t)ntab * n);
     DALLOC(h->d_w, n);
-    DALLOC(h->d_w32, n);
+    DALLOC(h->d_w32, (size_t)cdiv(n, kRhoTcKB) * kRhoTcKB);  // whole K blocks, zero past the ions
   }
   // pim and outputs
   DALLOC(h->d_Estat, n);
@@ -2727,7 +2741,8 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_part, h->d_scal, h->d_cata, h->d_pack, h->d_ekin_part, h->d_ddr,
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
                   h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
-                  h->d_lwfc, h->d_mu_wfc, h->d_qm32, h->d_Edd, h->d_fsr, h->d_hist_save};
+                  h->d_lwfc, h->d_mu_wfc, h->d_qm32, h->d_Edd, h->d_fsr, h->d_hist_save,
+                  h->d_rho_timg};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   step_graph_free(h);

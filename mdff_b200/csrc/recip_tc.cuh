@@ -9,18 +9,18 @@
 // For a tile of 64 mesh rows this is a real GEMM over the ions:
 //   D[m][c] = sum_i A[m][i] B[c][i],
 //   A rows m = Re P of the 64 rows, then Im P of the 64 rows (M = 128),
-//   B rows c = m_a Re Z_n, m_a Im Z_n for a = 1..3, n = 0..kz (N = 6 (kz + 1),
-//   zero-padded to a multiple of 16),
+//   B rows c = m_a Re Z_n, m_a Im Z_n for a = 1..3, n = 0..kz (6 (kz + 1)
+//   rows, zero-padded),
 // and Z_{-n} = conj Z_n gives both signs of nz from the same D.
 //
 // Each CTA (one per SM) owns 64 mesh rows and one ion chunk.  Per block of 32
 // ions, 16 warps generate A and B in shared memory in the canonical no-swizzle
 // K-major layout (8-row x 16-byte core matrices), split into TF32 high and low
-// parts (round-to-nearest), and one thread of a 17th warp issues A_hi B_hi,
-// A_hi B_lo and A_lo B_hi per k-step of 8 (the three products of split TF32)
-// into one accumulator; D stays in tensor memory across the whole chunk.  Two
-// operand stages and three table stagings, handed over by mbarriers only (no
-// CTA-wide barrier in the K loop).  The epilogue reads D (tcgen05.ld), combines
+// parts (round-to-nearest), and one thread of a 17th warp issues the three
+// products of split TF32 per k-step of 8, A_hi [B_hi | B_lo] as one product
+// where N allows and A_lo B_hi; D stays in tensor memory across the whole
+// chunk.  Two operand stages and three table stagings, handed over by
+// mbarriers only (no CTA-wide barrier in the K loop).  The epilogue reads D (tcgen05.ld), combines
 // the products in FP64 and writes per-chunk partials rho(k) in the same layout
 // as the CUDA-core kernels (the consumers add the chunks in order).
 //
@@ -130,23 +130,32 @@ constexpr long kWaitLimit = 1L << 22;  // try_wait polls before a wait gives up
 
 }  // namespace tc
 
-// B rows of the structure-factor GEMM for kz: 6 (kz + 1) rounded up to 16 (one
-// MMA takes N <= 256)
-__host__ __device__ constexpr int rho_tc_n(int kz) { return ((6 * (kz + 1) + 15) / 16) * 16; }
-// tensor-memory columns allocated for N accumulator columns (a power of two >= 32)
-__host__ __device__ constexpr int rho_tc_cols(int N) {
-  return N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+// B rows of one split part of the structure-factor GEMM for kz: 6 (kz + 1)
+// rounded up to 32 when the high and low parts fit one MMA (2 Nr <= 256: B_hi
+// and B_lo in one N = 2 Nr product, the low part's accumulator columns start
+// 32-aligned), else rounded up to 16 (three products of N = Nr)
+__host__ __device__ constexpr int rho_tc_nr(int kz) {
+  return 2 * (((6 * (kz + 1) + 31) / 32) * 32) <= 256 ? ((6 * (kz + 1) + 31) / 32) * 32
+                                                      : ((6 * (kz + 1) + 15) / 16) * 16;
+}
+__host__ __device__ constexpr bool rho_tc_fused(int kz) { return 2 * rho_tc_nr(kz) <= 256; }
+// tensor-memory columns allocated for the accumulator (a power of two >= 32)
+__host__ __device__ constexpr int rho_tc_cols(int kz) {
+  return (rho_tc_fused(kz) ? 2 : 1) * rho_tc_nr(kz) <= 32    ? 32
+         : (rho_tc_fused(kz) ? 2 : 1) * rho_tc_nr(kz) <= 64  ? 64
+         : (rho_tc_fused(kz) ? 2 : 1) * rho_tc_nr(kz) <= 128 ? 128
+                                                              : 256;
 }
 
-constexpr int kRhoTcRows = 64;                          // mesh rows per tile (A rows: Re P, Im P)
-constexpr int kRhoTcGen = 512;                          // operand-generating threads (16 warps)
-constexpr int kRhoTcThreads = kRhoTcGen + 32;           // + one warp issuing the MMAs; one CTA per SM
-constexpr int kRhoTcKB = 32;                            // ions per K block
-constexpr int kRhoTcStg = 3;                            // table staging buffers
+constexpr int kRhoTcRows = 64;                        // mesh rows per tile (A rows: Re P, Im P)
+constexpr int kRhoTcKB = 32;                          // ions per K block
+constexpr int kRhoTcGen = kRhoTcRows * kRhoTcKB / 4;  // operand-generating threads: one A item each
+constexpr int kRhoTcThreads = kRhoTcGen + 64;         // + the MMA warp and the copy warp; one CTA per SM
+constexpr int kRhoTcStg = 3;                          // table staging buffers
 
-// bytes of one operand stage: A hi + lo (128 x KB), B hi + lo (N x KB)
-__host__ __device__ constexpr int rho_tc_stage(int N) {
-  return 2 * 128 * kRhoTcKB * 4 + 2 * N * kRhoTcKB * 4;
+// bytes of one operand stage: A hi + lo (128 x KB), B hi then lo (2 Nr x KB)
+__host__ __device__ constexpr int rho_tc_stage(int Nr) {
+  return 2 * 128 * kRhoTcKB * 4 + 2 * Nr * kRhoTcKB * 4;
 }
 
 // table staging of one K block: rows X_0..X_kx, Y_0..Y_ky, Z_0..Z_kz of the
@@ -157,19 +166,23 @@ __host__ __device__ constexpr int rho_tc_staging(int kx, int ky, int kz) {
   return (kx + ky + kz + 3) * kStageRow + kRhoTcKB * 16;
 }
 
-// dynamic shared memory of k_rec_rho_tc: two operand stages, the table
-// stagings, alignment slack
+// dynamic shared memory of k_rec_rho_tc: two operand stages and the table
+// stagings (the epilogue's accumulator copy, 128 x (Nr + 1) floats, reuses
+// them), alignment slack
+__host__ __device__ constexpr size_t rho_tc_pipe_bytes(int kx, int ky, int kz) {
+  return 2 * (size_t)rho_tc_stage(rho_tc_nr(kz)) + kRhoTcStg * (size_t)rho_tc_staging(kx, ky, kz);
+}
 __host__ __device__ constexpr size_t rho_tc_smem(int kx, int ky, int kz) {
-  return 2 * (size_t)rho_tc_stage(rho_tc_n(kz)) + kRhoTcStg * (size_t)rho_tc_staging(kx, ky, kz) + 1024;
+  return (rho_tc_pipe_bytes(kx, ky, kz) > (size_t)128 * (rho_tc_nr(kz) + 1) * 4
+              ? rho_tc_pipe_bytes(kx, ky, kz)
+              : (size_t)128 * (rho_tc_nr(kz) + 1) * 4) +
+         1024;
 }
 // the mesh fits one MMA's N and one CTA's shared memory
 inline bool rho_tc_fits(int kx, int ky, int kz) {
-  return rho_tc_n(kz) <= 256 && rho_tc_smem(kx, ky, kz) <= 227 * 1024;
+  return rho_tc_nr(kz) <= 256 && rho_tc_smem(kx, ky, kz) <= 227 * 1024;
 }
 
-__device__ __forceinline__ void cp_async8(uint32_t dst, const void* src, int bytes) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
-}
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int bytes) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes) : "memory");
 }
@@ -198,27 +211,56 @@ __device__ __forceinline__ void mbar_init_n(uint32_t bar, int count) {
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
   asm volatile("{ .reg .b64 st; mbarrier.arrive.shared::cta.b64 st, [%0]; }" ::"r"(bar) : "memory");
 }
-// the mbarrier receives one arrival once this thread's earlier cp.async
-// copies have landed
-__device__ __forceinline__ void cp_async_arrive(uint32_t bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+// the phase also waits for tx_bytes of asynchronous copies
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t tx_bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(tx_bytes) : "memory");
+}
+// bulk copy global -> this CTA's shared memory (no multicast), completion
+// counted in bytes on the mbarrier; 16-byte aligned, size a multiple of 16
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
 }
 }  // namespace tc
 
+// The phase tables of the structure factor blocked by K block, once per call
+// (positions fixed): block kb holds the rows X_0..X_kx, Y_0..Y_ky, Z_0..Z_kz
+// of ions 32 kb .. 32 kb + 31 (zero past the ions), each row 32 complex values
+// and 16 bytes of padding (kStageRow bytes: the bank-spread row stride of the
+// staging buffers), so that one bulk copy stages a K block.
+// grid = K blocks, 256 threads.
+static __global__ void __launch_bounds__(256) k_rec_rho_timg(const float2* __restrict__ tab, int natm, int kx,
+                                                             int ky, int kz, float2* __restrict__ img) {
+  pdl_wait();
+  pdl_trigger();
+  constexpr int RW = kStageRow / (int)sizeof(float2);  // row width in float2 (32 ions + padding)
+  const int TR = kx + ky + kz + 3;
+  float2* blk = img + (size_t)blockIdx.x * TR * RW;
+  for (int e = threadIdx.x; e < TR * RW; e += blockDim.x) {
+    const int t = e / RW, j = e % RW;
+    const int i = blockIdx.x * kRhoTcKB + j;
+    blk[e] = (j < kRhoTcKB && i < natm) ? tab[(size_t)t * natm + i] : make_float2(0.f, 0.f);
+  }
+}
+
 // structure factor of the dipoles on the tensor cores.  grid = (row tiles of
-// 64 mesh rows, ion chunks), one CTA per SM; part[chunk][k] = this chunk's
-// rho(k).  Warps 0-15 stage the phase tables (cp.async) and generate the
-// operands; warp 16 issues the MMAs.  No CTA-wide barrier inside the K loop:
-// mbarriers carry each dependency,
-//   tfull[b]  the tables of a K block landed in staging buffer b (every
-//             generating thread's copies, cp.async.mbarrier.arrive),
-//   full[s]   operand stage s written (every generating thread, after
-//             fence.proxy.async),
+// 64 mesh rows, ion chunks of a multiple of 32 ions), one CTA per SM;
+// part[chunk][k] = this chunk's rho(k).  Warps 0-15 generate the operands
+// from staged tables; one thread of warp 16 issues the MMAs; one thread of
+// warp 17 stages each K block's table block (from the blocked image) and
+// weights with two bulk copies.  No CTA-wide barrier inside the K loop:
+// mbarriers carry each dependency, with one arrival per generating warp,
+//   tfull[b]  the tables and weights of a K block landed in staging buffer b
+//             (bytes of the bulk copies),
+//   sfree[b]  every warp has generated the block staged in buffer b,
+//   full[s]   operand stage s written (after each lane's fence.proxy.async),
 //   empty[s]  the MMAs that read stage s are complete (tcgen05.commit),
-// so the tables of K block kb + 1 load while block kb is generated and block
-// kb - 1 multiplied, and warps drift apart by up to two K blocks.
+// so the copies run up to three K blocks ahead of the generation, which runs
+// up to two ahead of the products.
 static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
-    const float2* __restrict__ tab, const float4* __restrict__ w, int natm, int chunk, RecMesh M,
+    const float2* __restrict__ timg, const float4* __restrict__ w, int natm, int chunk, RecMesh M,
     double2* __restrict__ part, int* __restrict__ err, const int* __restrict__ wait_cfg) {
   pdl_wait();
   pdl_trigger();
@@ -226,27 +268,31 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
   static_assert(RPT * KC == NG, "A items: one (row, 4 ions) per generating thread");
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-  __shared__ __align__(8) uint64_t full[2], empty[2], tfull[NS];
+  __shared__ __align__(8) uint64_t full[2], empty[2], tfull[NS], sfree[NS];
   __shared__ uint32_t tslot;
   __shared__ int abort_flag, issued_sh;
   const volatile int* abort_v = &abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int kx = M.kmax[0], ky = M.kmax[1], kz = M.kmax[2];
   const int nzc = kz + 1;
-  const int N = rho_tc_n(kz);
-  const int ncols = rho_tc_cols(N);
-  const int stage = rho_tc_stage(N);
+  const int Nr = rho_tc_nr(kz);
+  const bool fused = rho_tc_fused(kz);
+  const int ncols = rho_tc_cols(kz);
+  const int stage = rho_tc_stage(Nr);
   {
     // the launch must provide the mesh's shared memory
     uint32_t dyn;
     asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-    if (dyn < rho_tc_smem(kx, ky, kz) || N > 256) {
+    if (dyn < rho_tc_smem(kx, ky, kz) || Nr > 256) {
       if (tid == 0) atomicExch(err, 2);
       return;
     }
   }
-  // stage layout: A_hi (128 x KB), A_lo, B_hi (N x KB), B_lo
-  const int offAL = 128 * KB * 4, offB = 2 * 128 * KB * 4, offBL = offB + N * KB * 4;
+  // stage layout: A_hi (128 x KB), A_lo, then one B tile of 2 Nr rows: B_hi
+  // rows [0, Nr), B_lo rows [Nr, 2 Nr) ((Nr / 8) 8-row groups of 128 bytes on)
+  const int offAL = 128 * KB * 4, offB = 2 * 128 * KB * 4;
+  const int NB2 = 2 * Nr;
+  const uint32_t offLo = (uint32_t)(Nr / 8) * 128;
   const int TR = kx + ky + kz + 3;  // staged table rows
   const int sbytes = rho_tc_staging(kx, ky, kz);
   unsigned char* stg0 = sm + 2 * stage;
@@ -261,20 +307,23 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
     abort_flag = 0;
     issued_sh = 0;
     for (int s = 0; s < 2; ++s) {
-      tc::mbar_init_n(tc::smem_u32(&full[s]), NG);
+      tc::mbar_init_n(tc::smem_u32(&full[s]), NG / 32);
       tc::mbar_init_n(tc::smem_u32(&empty[s]), 1);
     }
-    for (int b = 0; b < NS; ++b) tc::mbar_init_n(tc::smem_u32(&tfull[b]), NG);
+    for (int b = 0; b < NS; ++b) {
+      tc::mbar_init_n(tc::smem_u32(&tfull[b]), 1);
+      tc::mbar_init_n(tc::smem_u32(&sfree[b]), NG / 32);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;");
   }
   {
-    // B padding rows [6 nzc, N) are zero in both stages, hi and lo
-    const int padr = N - 6 * nzc;
+    // B padding rows [6 nzc, Nr) of both parts are zero in both stages
+    const int padr = Nr - 6 * nzc;
     for (int e = tid; e < 4 * padr * KC; e += blockDim.x) {
       const int kc = e % KC, rest = e / KC;
       const int c = 6 * nzc + rest % padr, sp = rest / padr;
-      unsigned char* S = sm + (sp >> 1) * stage + ((sp & 1) ? offBL : offB);
-      *reinterpret_cast<uint4*>(S + tc::canon(c, kc * 4, N)) = make_uint4(0u, 0u, 0u, 0u);
+      unsigned char* S = sm + (sp >> 1) * stage + offB;
+      *reinterpret_cast<uint4*>(S + tc::canon((sp & 1) * Nr + c, kc * 4, NB2)) = make_uint4(0u, 0u, 0u, 0u);
     }
   }
   tc::fence_before_sync();
@@ -285,8 +334,9 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
   const int r0 = blockIdx.x * RPT;
   const int a0 = blockIdx.y * chunk;
   const int a1 = min(a0 + chunk, natm);
+  const int kb0 = a0 / KB;
   const int nkb = (a1 - a0 + KB - 1) / KB;
-  const uint32_t lboA = (128 / 8) * 128, lboB = (uint32_t)(N / 8) * 128;
+  const uint32_t lboA = (128 / 8) * 128, lboB = (uint32_t)(NB2 / 8) * 128;
 
   if (warp < NG / 32) {
     // ---- operand generation ------------------------------------------------
@@ -303,7 +353,7 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
     const float sy = ny < 0 ? -1.f : 1.f;  // Y_{-n} = conj Y_n
     const int xoff = nx * kStageRow + kcA * 32, yoff = (kx + 1 + ay) * kStageRow + kcA * 32;
     const uint32_t oA = tc::canon(rl, kcA * 4, 128), oAi = tc::canon(RPT + rl, kcA * 4, 128);
-    // B items (at most two per thread: 3 nzc KC <= 2 NG for N <= 256): rows
+    // B items (at most two per thread: 3 nzc KC <= 2 NG for Nr <= 256): rows
     // (2a) nzc + n = m_a Re Z_n and (2a + 1) nzc + n = m_a Im Z_n, ions 4 kc ..;
     // consecutive threads take consecutive n (rows 16 bytes apart)
     const int nB = 3 * nzc * KC;
@@ -316,50 +366,22 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
       const int kc = rest % KC, a = rest / KC;
       zoff[q] = (kx + 1 + ky + 1 + n) * kStageRow + kc * 32;
       woff[q] = TR * kStageRow + kc * 64 + (a + 1) * 4;  // weight component m_a of ion 4 kc
-      oB[q] = tc::canon(2 * a * nzc + n, kc * 4, N);
-      oBi[q] = tc::canon((2 * a + 1) * nzc + n, kc * 4, N);
+      oB[q] = tc::canon(2 * a * nzc + n, kc * 4, NB2);
+      oBi[q] = tc::canon((2 * a + 1) * nzc + n, kc * 4, NB2);
     }
-    // copy table rows t (global row t of the [X | Y | Z] tables) and weights
-    // of K block kb into staging buffer kb % NS; ions past a1 are zero-filled.
-    // Element e = t KB + j: consecutive threads copy consecutive ions.
-    auto stage_tables = [&](int kb) {
-      const int ib = a0 + kb * KB;
-      const int b = kb % NS;
-      const uint32_t dst0 = tc::smem_u32(stg0 + b * sbytes);
-      for (int e = tid; e < TR * KB; e += NG) {
-        const int t = e / KB, j = e % KB;
-        const int i = ib + j;
-        const bool ok = i < a1;
-        cp_async8(dst0 + (uint32_t)(t * kStageRow + j * 8), tab + (size_t)t * natm + (ok ? i : a0), ok ? 8 : 0);
-      }
-      if (tid < KB) {
-        const int i = ib + tid;
-        const bool ok = i < a1;
-        cp_async16(dst0 + (uint32_t)(TR * kStageRow + tid * 16), w + (ok ? i : a0), ok ? 16 : 0);
-      }
-      tc::cp_async_arrive(tc::smem_u32(&tfull[b]));
-    };
     // polls of the wait for a free operand stage: tc::kWaitLimit unless the
     // host set a limit (a test hook)
     const long opwait = *wait_cfg >= 0 ? (long)*wait_cfg : tc::kWaitLimit;
-    if (nkb > 0) stage_tables(0);
+    // the warp leaves the loop together: a wait counts when every lane's did
+    auto warp_ok = [](bool ok) { return __all_sync(0xffffffffu, ok) != 0; };
     for (int kb = 0; kb < nkb; ++kb) {
       const int st = kb & 1, b = kb % NS;
-      if (kb + 1 < nkb) {
-        // staging buffer (kb + 1) % NS last held block kb - 2: every thread
-        // has generated that block once its full[] phase completed
-        if (kb >= 2 && !tc::mbar_wait_ab(tc::smem_u32(&full[st]), ((kb - 2) >> 1) & 1, tc::kWaitLimit, abort_v)) {
-          abort_flag = 1;
-          break;
-        }
-        stage_tables(kb + 1);
-      }
-      if (!tc::mbar_wait_ab(tc::smem_u32(&tfull[b]), (kb / NS) & 1, tc::kWaitLimit, abort_v)) {
+      if (!warp_ok(tc::mbar_wait_ab(tc::smem_u32(&tfull[b]), (kb / NS) & 1, tc::kWaitLimit, abort_v))) {
         abort_flag = 1;
         break;
       }
       // operand stage st is free once the MMAs of block kb - 2 completed
-      if (kb >= 2 && !tc::mbar_wait_ab(tc::smem_u32(&empty[st]), ((kb - 2) >> 1) & 1, opwait, abort_v)) {
+      if (kb >= 2 && !warp_ok(tc::mbar_wait_ab(tc::smem_u32(&empty[st]), ((kb - 2) >> 1) & 1, opwait, abort_v))) {
         abort_flag = 1;
         break;
       }
@@ -398,17 +420,50 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
           tc::tf32_split(m * zi[u], ih[u], ilo[u]);
         }
         *reinterpret_cast<uint4*>(S + offB + oB[q]) = make_uint4(rh[0], rh[1], rh[2], rh[3]);
-        *reinterpret_cast<uint4*>(S + offBL + oB[q]) = make_uint4(rlo[0], rlo[1], rlo[2], rlo[3]);
+        *reinterpret_cast<uint4*>(S + offB + offLo + oB[q]) = make_uint4(rlo[0], rlo[1], rlo[2], rlo[3]);
         *reinterpret_cast<uint4*>(S + offB + oBi[q]) = make_uint4(ih[0], ih[1], ih[2], ih[3]);
-        *reinterpret_cast<uint4*>(S + offBL + oBi[q]) = make_uint4(ilo[0], ilo[1], ilo[2], ilo[3]);
+        *reinterpret_cast<uint4*>(S + offB + offLo + oBi[q]) = make_uint4(ilo[0], ilo[1], ilo[2], ilo[3]);
       }
+      // every lane's writes visible to the tensor core, then one arrival per
+      // warp: operand stage st written, staging buffer b read
       tc::fence_async_smem();
-      tc::mbar_arrive(tc::smem_u32(&full[st]));
+      __syncwarp();
+      if (lane == 0) {
+        tc::mbar_arrive(tc::smem_u32(&full[st]));
+        tc::mbar_arrive(tc::smem_u32(&sfree[b]));
+      }
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp == NG / 32 + 1) {
+    // ---- copies: the table block and the weights of K block kb into staging
+    // buffer kb % NS once every warp has generated block kb - NS from it
+    if (lane == 0) {
+      const size_t tblk = (size_t)TR * kStageRow / sizeof(float2);  // table image block, float2
+      const uint32_t tbytes = (uint32_t)(TR * kStageRow), wbytes = 16u * KB;
+      int copied = 0;
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int b = kb % NS;
+        if (kb >= NS && !tc::mbar_wait_ab(tc::smem_u32(&sfree[b]), (kb / NS - 1) & 1, tc::kWaitLimit, abort_v)) {
+          abort_flag = 1;
+          break;
+        }
+        const uint32_t dst = tc::smem_u32(stg0 + b * sbytes), fb = tc::smem_u32(&tfull[b]);
+        tc::mbar_expect_tx(fb, tbytes + wbytes);
+        tc::bulk_g2s(dst, timg + (size_t)(kb0 + kb) * tblk, tbytes, fb);
+        tc::bulk_g2s(dst + tbytes, w + (size_t)(kb0 + kb) * KB, wbytes, fb);
+        copied = kb + 1;
+      }
+      // no copy may still be landing when the CTA leaves (after an abort):
+      // wait (bounded) for the last block copied into each buffer
+      for (int b = 0; b < NS && b < copied; ++b) {
+        const int last = b + NS * ((copied - 1 - b) / NS);
+        if (!tc::mbar_wait(tc::smem_u32(&tfull[b]), (last / NS) & 1, tc::kWaitLimit)) abort_flag = 1;
+      }
+    }
   } else if (lane == 0) {
-    // ---- MMA issue: the three products of split TF32 into one accumulator --
-    const uint32_t idesc = tc::idesc_tf32(128, N);
+    // ---- MMA issue: the three products of split TF32.  Fused: A_hi [B_hi |
+    // B_lo] (N = 2 Nr: columns [0, Nr) and [Nr, 2 Nr)) and A_lo B_hi into
+    // columns [0, Nr); else all three into columns [0, Nr).
+    const uint32_t idesc = tc::idesc_tf32(128, Nr), idesc2 = tc::idesc_tf32(128, NB2);
     int issued = 0;
     for (int kb = 0; kb < nkb; ++kb) {
       const int st = kb & 1;
@@ -422,9 +477,14 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
       for (int s = 0; s < KB / 8; ++s) {
         const uint32_t oa = (uint32_t)s * 2 * lboA, ob = (uint32_t)s * 2 * lboB;
         const uint64_t aH = tc::smem_desc(base + oa, lboA, 128), aL = tc::smem_desc(base + offAL + oa, lboA, 128);
-        const uint64_t bH = tc::smem_desc(base + offB + ob, lboB, 128), bL = tc::smem_desc(base + offBL + ob, lboB, 128);
-        tc::mma_tf32(tmem, aH, bH, idesc, (kb > 0 || s > 0) ? 1u : 0u);
-        tc::mma_tf32(tmem, aH, bL, idesc, 1u);
+        const uint64_t bH = tc::smem_desc(base + offB + ob, lboB, 128);
+        const uint32_t acc = (kb > 0 || s > 0) ? 1u : 0u;
+        if (fused) {
+          tc::mma_tf32(tmem, aH, bH, idesc2, acc);
+        } else {
+          tc::mma_tf32(tmem, aH, bH, idesc, acc);
+          tc::mma_tf32(tmem, aH, tc::smem_desc(base + offB + offLo + ob, lboB, 128), idesc, 1u);
+        }
         tc::mma_tf32(tmem, aL, bH, idesc, 1u);
       }
       tc::mma_commit(tc::smem_u32(&empty[st]));
@@ -441,20 +501,28 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
   __syncthreads();
   const bool all_ok = abort_flag == 0 && issued_sh == nkb;
   if (!all_ok && tid == 0) atomicExch(err, 1);
-  // epilogue: D (128 lanes x N columns) -> shared (row stride N + 1).  Warp w
-  // < 16 reads lane quarter w % 4, column blocks w / 4, w / 4 + 4, ...
+  // epilogue: D (128 lanes x Nr columns, plus the low part's Nr when fused)
+  // -> shared (row stride Nr + 1).  A generating warp w reads lane quarter
+  // w % 4, column blocks w / 4, w / 4 + NG / 128, ...
   float* Dsm = reinterpret_cast<float*>(sm);
-  const int ldd = N + 1;
+  const int ldd = Nr + 1;
   if (all_ok && nkb > 0 && warp < NG / 32) {
     tc::fence_after_sync();
     const int q = warp & 3;
-    for (int cb = warp >> 2; cb * 32 < N; cb += NG / 128) {
+    for (int cb = warp >> 2; cb * 32 < Nr; cb += NG / 128) {
       float v[32];
-      tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cb * 32), v);
+      const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cb * 32);
+      tc::tmem_ld32(ta, v);
+      if (fused) {
+        float v2[32];
+        tc::tmem_ld32(ta + (uint32_t)Nr, v2);
+#pragma unroll
+        for (int c = 0; c < 32; ++c) v[c] += v2[c];
+      }
       const int m = q * 32 + lane;
 #pragma unroll
       for (int c = 0; c < 32; ++c)
-        if (cb * 32 + c < N) Dsm[m * ldd + cb * 32 + c] = v[c];
+        if (cb * 32 + c < Nr) Dsm[m * ldd + cb * 32 + c] = v[c];
     }
   }
   tc::fence_before_sync();

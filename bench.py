@@ -564,7 +564,7 @@ KCLS = ("list_build", "short_range", "real_space_field", "real_space_force",
 # SiO2 workload, from one ncu capture (profiles/k_rec_rho_tc_k_rec_field_tc_sio2_12000.md,
 # profiles/realspace_kernels_sio2_12000.md); the working set is L2-resident
 TRAFFIC = {
-    "structure_factor": {"kernel": "k_rec_rho_tc", "bytes": 3.968e6},
+    "structure_factor": {"kernel": "k_rec_rho_tc", "bytes": 4.211e6},
     "reciprocal_field": {"kernel": "k_rec_field_tc<0, 32>", "bytes": 4.118e6},
     "real_space_force": {"kernel": "k_es_force<float>", "bytes": 20.09e6},
     "short_range": {"kernel": "k_shortrange<double, 1>", "bytes": 18.96e6},

@@ -451,13 +451,14 @@ static int build_mesh(mdff_ctx* h) {
   {
     const char* env = std::getenv("MDFF_FIELD_TC");
     int kf = field_tc_kf(h->p.kES[2]);
-    h->field_tc = kf > 0 && nrows > 0 && !(env && env[0] == '0');
+    h->field_tc = kf > 0 && nrows > 0 && !(env && env[0] == '0') &&
+                  field_tc_smem(kf, h->p.kES[1]) <= 227 * 1024;
     cudaFree(h->d_fb);
     h->d_fb = nullptr;
     if (h->field_tc) {
       // B tiles for the smaller row tile (with dipole forces): hi + lo per tile
       DALLOC(h->d_fb, (size_t)cdiv(nrows, field_tc_rpt(true)) * 2 * 128 * kf);
-      int smem = (int)field_tc_smem(kf);
+      int smem = (int)field_tc_smem(kf, h->p.kES[1]);
       if (kf == 32) {
         CK(cudaFuncSetAttribute(k_rec_field_tc<true, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         CK(cudaFuncSetAttribute(k_rec_field_tc<false, 32>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -691,7 +692,7 @@ static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int
   int tpg = cdiv(ntile, ng);
   ng = cdiv(ntile, tpg);
   dim3 g((unsigned)ion_tiles, (unsigned)ng);
-  size_t smem = field_tc_smem(KF);
+  size_t smem = field_tc_smem(KF, M.kmax[1]);
   size_t bsmem = (size_t)kBtRows * (2 * M.kmax[2] + 1) * sizeof(double2);
   dim3 gb((unsigned)ntile, (unsigned)(rpt / kBtRows));
   int* err = h->d_cata + 1;

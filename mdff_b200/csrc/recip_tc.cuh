@@ -604,8 +604,11 @@ __host__ __device__ constexpr int field_tc_kf(int kz) {
 }
 // rows per 128-column tile
 __host__ __device__ constexpr int field_tc_rpt(bool has_h) { return has_h ? 16 : 32; }
-// A hi + lo and two B buffers (hi + lo), each 128 x KF TF32, + alignment slack
-__host__ __device__ constexpr size_t field_tc_smem(int KF) { return (size_t)6 * 128 * KF * 4 + 1024; }
+// A hi + lo and two B buffers (hi + lo), each 128 x KF TF32, the Y_0..Y_ky
+// phases of the CTA's 128 ions (the epilogue's), + alignment slack
+__host__ __device__ constexpr size_t field_tc_smem(int KF, int ky) {
+  return (size_t)6 * 128 * KF * 4 + (size_t)(ky + 1) * 128 * 8 + 1024;
+}
 
 // B tiles of the field GEMM, once per pass: tile t = [hi | lo], each 128
 // columns x KF features in the canonical K-major layout (the shared-memory
@@ -703,7 +706,7 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
   {
     uint32_t dyn;
     asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dyn));
-    if (dyn < field_tc_smem(KF) || field_tc_kf(kz) != KF) {
+    if (dyn < field_tc_smem(KF, ky) || field_tc_kf(kz) != KF) {
       if (tid == 0) atomicExch(err, 2);
       return;
     }
@@ -731,6 +734,7 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
   unsigned char* Ahi = sm;
   unsigned char* Alo = sm + TILE;
   auto Bbuf = [&](int b) { return sm + 2 * TILE + b * 2 * TILE; };
+  float2* Ys = reinterpret_cast<float2*>(sm + 6 * TILE);  // [ky + 1][128]
   const int T = tend - tbeg;
   // B tile t (hi | lo, 2 TILE bytes) -> buffer b, 16-byte copies
   auto load_b = [&](int t, int b) {
@@ -760,21 +764,59 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
     *reinterpret_cast<uint4*>(Ahi + o) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
     *reinterpret_cast<uint4*>(Alo + o) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
   }
+  // the epilogue's Y_ny phases of the CTA's ions (zero past the ions); made
+  // visible by the barrier before the first products
+  for (int e = tid; e < (ky + 1) * 128; e += NT) {
+    const int a = e >> 7, i = i0 + (e & 127);
+    Ys[e] = i < natm ? tab[(size_t)(kx + 1 + a) * natm + i] : make_float2(0.f, 0.f);
+  }
   // per-thread sums: ion m = 32 (warp & 3) + lane, column chunks (warp >> 2) and +2
   const int q = warp & 3, hh = warp >> 2;
   const int m = q * 32 + lane, ion = i0 + m;
   const bool ion_ok = ion < natm;
   const int ionc = ion_ok ? ion : 0;
-  float4 wi = ion_ok ? w[ion] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float4 wi = ion_ok ? w[ion] : make_float4(0.f, 0.f, 0.f, 0.f);
   double G[3] = {0.0, 0.0, 0.0}, H[3] = {0.0, 0.0, 0.0};
+  // The rows a thread visits come in non-decreasing nx.  With conj(P) =
+  // conj(X_nx) conj(Y'_ny) (Y' = Y, conjugated for ny < 0) and Q = conj(Y') T,
+  // the rows of one nx are accumulated in FP32,
+  //   W0 = sum Q, W1 = sum ny Q, V0 = sum conj(Y') T1
+  //   (+ W2 = sum ny^2 Q, V1 = sum ny conj(Y') T1, U0 = sum conj(Y') T2 with H),
+  // and conj(X_nx) and the FP64 sums are applied once per nx (flush):
+  //   G += (nx Im(cX W0), Im(cX W1), Im(cX V0)),
+  //   H += (nx (m1 nx Re(cX W0) + m2 Re(cX W1) + m3 Re(cX V0)),
+  //         m1 nx Re(cX W1) + m2 Re(cX W2) + m3 Re(cX V1),
+  //         m1 nx Re(cX V0) + m2 Re(cX V1) + m3 Re(cX U0)).
+  int gnx = -1;
+  float2 xval = make_float2(0.f, 0.f);
+  float2 W0{}, W1{}, V0{}, W2{}, V1{}, U0{};
+  auto flush = [&]() {
+    if (gnx >= 0) {
+      const float xr = xval.x, xi = xval.y;
+      auto cre = [&](float2 a) { return xr * a.x + xi * a.y; };
+      auto cim = [&](float2 a) { return xr * a.y - xi * a.x; };
+      const double dnx = (double)gnx;
+      G[0] += dnx * (double)cim(W0);
+      G[1] += (double)cim(W1);
+      G[2] += (double)cim(V0);
+      if (HAS_H) {
+        const float fx = (float)gnx, rW0 = cre(W0), rW1 = cre(W1), rV0 = cre(V0), rV1 = cre(V1);
+        H[0] += dnx * (double)(wi.y * fx * rW0 + wi.z * rW1 + wi.w * rV0);
+        H[1] += (double)(wi.y * fx * rW1 + wi.z * cre(W2) + wi.w * rV1);
+        H[2] += (double)(wi.y * fx * rV0 + wi.z * rV1 + wi.w * cre(U0));
+      }
+    }
+    W0 = W1 = V0 = W2 = V1 = U0 = make_float2(0.f, 0.f);
+  };
   auto epilogue = [&](int t, int b) {
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc) {
       int ch = hh + 2 * cc;
-      // the chunk's rows and this ion's phases X_nx Y_ny first (loads in flight together)
+      // the chunk's rows and this ion's Y_ny (shared) first
       int nxr[RPC], nyr[RPC];
       float okr[RPC];
-      float2 X[RPC], Y[RPC];
+      bool rok[RPC];
+      float2 Y[RPC];
 #pragma unroll
       for (int jj = 0; jj < RPC; ++jj) {
         int row = t * RPT + ch * RPC + jj;
@@ -782,32 +824,39 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
         int4 ri = M.rows[ok ? row : 0];
         nxr[jj] = ri.x;
         nyr[jj] = ri.y;
+        rok[jj] = ok;
         okr[jj] = (ok && ion_ok) ? 1.f : 0.f;
         int ay = ri.y < 0 ? -ri.y : ri.y;
-        X[jj] = tab[(size_t)ri.x * natm + ionc];
-        Y[jj] = tab[(size_t)(kx + 1 + ay) * natm + ionc];
+        Y[jj] = Ys[ay * 128 + m];
       }
       float v[32];
       tc::tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * 128 + ch * 32), v);
 #pragma unroll
       for (int jj = 0; jj < RPC; ++jj) {
-        int nx = nxr[jj], ny = nyr[jj];
-        float Yi = ny < 0 ? -Y[jj].y : Y[jj].y;
-        float Pr = okr[jj] * (X[jj].x * Y[jj].x - X[jj].y * Yi);
-        float Pi = okr[jj] * (X[jj].x * Yi + X[jj].y * Y[jj].x);
+        if (rok[jj] && nxr[jj] != gnx) {
+          flush();
+          gnx = nxr[jj];
+          xval = tab[(size_t)gnx * natm + ionc];
+        }
+        const int ny = nyr[jj];
+        const float fy = (float)ny;
+        const float yr = okr[jj] * Y[jj].x, yi = okr[jj] * (ny < 0 ? -Y[jj].y : Y[jj].y);
         const float* d = v + jj * CPR;
-        float s0 = Pr * d[1] - Pi * d[0];
-        float sz = Pr * d[3] - Pi * d[2];
-        G[0] += (double)nx * (double)s0;
-        G[1] += (double)ny * (double)s0;
-        G[2] += (double)sz;
+        const float qr = yr * d[0] + yi * d[1], qi = yr * d[1] - yi * d[0];
+        const float vr = yr * d[2] + yi * d[3], vi = yr * d[3] - yi * d[2];
+        W0.x += qr;
+        W0.y += qi;
+        W1.x += fy * qr;
+        W1.y += fy * qi;
+        V0.x += vr;
+        V0.y += vi;
         if (HAS_H) {
-          float reA = Pr * d[0] + Pi * d[1], reB = Pr * d[2] + Pi * d[3], reC = Pr * d[4] + Pi * d[5];
-          float km = (float)nx * wi.y + (float)ny * wi.z;
-          float t0 = km * reA + wi.w * reB, tz = km * reB + wi.w * reC;
-          H[0] += (double)nx * (double)t0;
-          H[1] += (double)ny * (double)t0;
-          H[2] += (double)tz;
+          W2.x += fy * fy * qr;
+          W2.y += fy * fy * qi;
+          V1.x += fy * vr;
+          V1.y += fy * vi;
+          U0.x += yr * d[4] + yi * d[5];
+          U0.y += yr * d[5] - yi * d[4];
         }
       }
     }
@@ -880,6 +929,7 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
     if (tid == 0) atomicExch(err, 1);
     return;
   }
+  flush();
   // combine the two column halves of each ion (A is free: every MMA is done)
   double* red = reinterpret_cast<double*>(sm);
   if (hh == 1) {

@@ -91,6 +91,10 @@ struct mdff_ctx {
   double4* d_s = nullptr;
   int* d_itype = nullptr;
   int* d_ipolar = nullptr;
+  // the polarisable ions (ascending index): the ions where the dipole
+  // solve's fields are needed
+  std::vector<int> polidx;
+  int* d_polidx = nullptr;
   double* d_q = nullptr;
   double* d_qzero = nullptr;
   double4* d_dipia = nullptr;
@@ -681,12 +685,14 @@ static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n) {
 }
 
 // FP32 field / force partials on the tensor cores into d_G / d_H (B tiles
-// built first into d_fb); returns the number of partial chunks written
+// built first into d_fb); returns the number of partial chunks written.
+// imap (nion entries): the ions whose partials are wanted (nullptr: all n)
 template <int KF>
-static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int npart) {
+static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int npart, const int* imap,
+                             int nion) {
   int rpt = field_tc_rpt(muf);
   int ntile = cdiv(M.nrows, rpt);
-  int ion_tiles = cdiv(n, 128);
+  int ion_tiles = cdiv(nion, 128);
   int nalloc = (int)h->rchunk.size() - 1;
   int ng = std::max(1, std::min({(2 * (h->nsm > 0 ? h->nsm : 148)) / std::max(ion_tiles, 1), ntile, nalloc}));
   int tpg = cdiv(ntile, ng);
@@ -704,19 +710,20 @@ static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int
   h->launches++;  // two launches here; the caller's LAUNCH_CHECK counts one
   if (muf) {
     (void)pdl_launch(k_rec_field_btiles<true, KF>, gb, dim3(128), bsmem, h->st, M, rhoA, rpart, npart, h->d_fb);
-    (void)pdl_launch(k_rec_field_tc<true, KF>, g, dim3(kFieldTcThreads), smem, h->st, tab, w, n, M, fb, tpg,
-                     h->d_G, h->d_H, err);
+    (void)pdl_launch(k_rec_field_tc<true, KF>, g, dim3(kFieldTcThreads), smem, h->st, tab, w, n, imap, nion,
+                     M, fb, tpg, h->d_G, h->d_H, err);
   } else {
     (void)pdl_launch(k_rec_field_btiles<false, KF>, gb, dim3(128), bsmem, h->st, M, rhoA, rpart, npart, h->d_fb);
-    (void)pdl_launch(k_rec_field_tc<false, KF>, g, dim3(kFieldTcThreads), smem, h->st, tab, w, n, M, fb, tpg,
-                     h->d_G, h->d_H, err);
+    (void)pdl_launch(k_rec_field_tc<false, KF>, g, dim3(kFieldTcThreads), smem, h->st, tab, w, n, imap, nion,
+                     M, fb, tpg, h->d_G, h->d_H, err);
   }
   return ng;
 }
 
-static int launch_field_tc(mdff_ctx* h, const RecMesh& M, int n, bool muf, int npart) {
-  if (field_tc_kf(M.kmax[2]) == 32) return launch_field_tc_k<32>(h, M, n, muf, npart);
-  return launch_field_tc_k<64>(h, M, n, muf, npart);
+static int launch_field_tc(mdff_ctx* h, const RecMesh& M, int n, bool muf, int npart, const int* imap,
+                           int nion) {
+  if (field_tc_kf(M.kmax[2]) == 32) return launch_field_tc_k<32>(h, M, n, muf, npart, imap, nion);
+  return launch_field_tc_k<64>(h, M, n, muf, npart, imap, nion);
 }
 
 // reciprocal pass: E += rec field (+ the self / surface field sf, when on);
@@ -801,7 +808,11 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   bool muf = forces && has_mu;
   pr = prof_begin(h, KC_RECF, (double)h->nk * n * ops_fld);
   if (field_tc) {
-    nch = launch_field_tc(h, M, n, muf, npart);
+    // the dipole solve's operator (its partials summed by the caller's
+    // kernel) needs the field at the polarisable ions only
+    const bool pol_only = defer_nch && !has_q && has_mu && !forces && h->d_polidx;
+    nch = launch_field_tc(h, M, n, muf, npart, pol_only ? h->d_polidx : nullptr,
+                          pol_only ? (int)h->polidx.size() : n);
   } else if constexpr (std::is_same<R, float>::value) {
     dim3 gx((unsigned)cdiv(n, 2 * kFieldThreads), (unsigned)nch);
     if (muf)
@@ -919,7 +930,7 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
   if (fused)
     k_dd_cached_rec<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n,
                                            h->d_G, nch, h->d_cell, 2.0 * (2.0 * (kTwoPi / h->omega)), sf, E,
-                                           dd_side ? h->d_Edd : nullptr);
+                                           dd_side ? h->d_Edd : nullptr, h->d_ipolar);
   else if (fp32 && dd_mask == 1 && h->dd_cache_ok)
     k_dd_cached<<<nb, 256, 0, h->st>>>(h->d_mu32, h->d_ddr, h->d_ddb1, h->d_ddj, h->d_ddn, h->L.cap, n, E);
   else
@@ -2260,6 +2271,13 @@ static int create_impl(mdff_ctx* h, const mdff_params* pin, const double* cellA)
   DALLOC(h->d_invpol, 9 * (size_t)n);
   CK(cudaMemcpyAsync(h->d_itype, S.itype.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->st));
   CK(cudaMemcpyAsync(h->d_ipolar, S.ipol.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->st));
+  for (int i = 0; i < n; ++i)
+    if (S.ipol[i]) h->polidx.push_back(i);
+  if (!h->polidx.empty()) {
+    DALLOC(h->d_polidx, h->polidx.size());
+    CK(cudaMemcpyAsync(h->d_polidx, h->polidx.data(), sizeof(int) * h->polidx.size(), cudaMemcpyHostToDevice,
+                       h->st));
+  }
   CK(cudaMemcpyAsync(h->d_q, S.q.data(), sizeof(double) * n, cudaMemcpyHostToDevice, h->st));
   CK(cudaMemcpyAsync(h->d_dipia, S.dip.data(), sizeof(double4) * n, cudaMemcpyHostToDevice, h->st));
   CK(cudaMemcpyAsync(h->d_pol, S.pol.data(), sizeof(double) * 9 * n, cudaMemcpyHostToDevice, h->st));
@@ -2743,7 +2761,7 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
                   h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
                   h->d_lwfc, h->d_mu_wfc, h->d_qm32, h->d_Edd, h->d_fsr, h->d_hist_save,
-                  h->d_rho_timg};
+                  h->d_rho_timg, h->d_polidx};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   step_graph_free(h);

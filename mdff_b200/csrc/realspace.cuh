@@ -476,7 +476,9 @@ static __global__ void __launch_bounds__(256) k_es_field(
 
 // --------------------------------------------------------------------------
 // FP32 static pass with a pair cache.  Same damped charge field as
-// k_es_field<float, true, false>, and in the same sweep the rows of the
+// k_es_field<float, true, false>, at the polarisable ions only (the dipole
+// solvers read the static field there; other rows are left at zero), and in
+// the same sweep the rows of the
 // polarisable ions keep, for every polarisable partner within rc, the FP32
 // terms of the undamped dipole field T2(r) mu = B2 r (r.mu) - B1 mu:
 //   cr[i][m] = (rx, ry, rz, B2), cb1[i][m] = B1, cj[i][m] = j,  cn[i] = count
@@ -509,9 +511,15 @@ static __global__ void __launch_bounds__(256) k_static_cache(
   int lane = threadIdx.x & 31;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= natm) return;
+  bool pol_i = ipolar[i] != 0;
+  // the static field is wanted at the polarisable ions only (the dipole
+  // solvers read it there); other rows keep E = 0 and an empty cache row
+  if (!pol_i) {
+    if (lane == 0) cn[i] = 0;
+    return;
+  }
   double4 si = s[i];
   int ti = itype[i];
-  bool pol_i = ipolar[i] != 0;
   int n = nnb[i];
   const int* row = nbr + (size_t)i * cap;
   size_t cbase = (size_t)i * cap;

@@ -505,12 +505,19 @@ static __global__ void __launch_bounds__(256) k_dd_cached_rec(
     const float4* __restrict__ mu, const float4* __restrict__ cr, const float* __restrict__ cb1,
     const int* __restrict__ cj, const int* __restrict__ cn, int cap, int natm,
     const double4* __restrict__ Gpart, int nchunk, const CellC* __restrict__ cell, double scale,
-    SelfField sf, double4* __restrict__ E, const double4* __restrict__ Edd) {
+    SelfField sf, double4* __restrict__ E, const double4* __restrict__ Edd,
+    const int* __restrict__ ipolar) {
   pdl_wait();
   pdl_trigger();
   int lane = threadIdx.x & 31;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= natm) return;
+  // (ipolar: the operator is wanted at the polarisable ions only; its
+  // reciprocal partials may cover only those)
+  if (ipolar && !ipolar[i]) {
+    if (lane == 0) E[i] = make_double4(0.0, 0.0, 0.0, 0.0);
+    return;
+  }
   // lanes 0-3: strided chunk sums of the reciprocal partials, as the four
   // threads of an ion in k_rec_field_sum (loads issued before the pair loop)
   double g[3] = {0.0, 0.0, 0.0};

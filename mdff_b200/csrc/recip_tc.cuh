@@ -591,7 +591,9 @@ namespace mdff {
 // is short; operands are split TF32 (A_hi B_hi + A_hi B_lo + A_lo B_hi).
 //
 // B tiles are built once per pass (k_rec_field_btiles, which also sums the
-// structure-factor chunks when no energy is needed).  CTA = 128 ions x a
+// structure-factor chunks when no energy is needed).  The ions are all of them
+// or the subset imap (the polarisable ions, where the dipole solve's operator
+// needs its field).  CTA = 128 ions x a
 // group of row tiles (128 columns each), 256 threads: the next B tile is copied
 // in (cp.async) while the tensor core multiplies the current one into one half
 // of a double-buffered tensor-memory accumulator and the threads reduce the
@@ -683,7 +685,8 @@ static __global__ void __launch_bounds__(128) k_rec_field_btiles(RecMesh M, cons
 
 template <bool HAS_H, int KF>
 static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
-    const float2* __restrict__ tab, const float4* __restrict__ w, int natm, RecMesh M,
+    const float2* __restrict__ tab, const float4* __restrict__ w, int natm, const int* __restrict__ imap,
+    int nion, RecMesh M,
     const uint32_t* __restrict__ fb, int tiles_per_group, double4* __restrict__ Gpart,
     double4* __restrict__ Hpart, int* __restrict__ err) {
   pdl_wait();
@@ -744,17 +747,19 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
   if (T > 0) load_b(tbeg, 0);
+  // the ion of tile slot s (imap: a subset of the ions), -1 past the ions
+  auto ion_of = [&](int s) { return s < nion ? (imap ? imap[s] : s) : -1; };
 
   // A: ion features, items (ion m, 4 features) with m = it % 128
   for (int it = tid; it < 128 * (KF / 4); it += NT) {
     int m = it & 127, fc = it >> 7;
-    int i = i0 + m;
+    int i = ion_of(i0 + m);
     uint32_t hi[4], lo[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       int f = fc * 4 + u;
       float x = 0.f;
-      if (i < natm && f < 2 * nzc) {
+      if (i >= 0 && f < 2 * nzc) {
         float2 Z = tab[(zoff + (f < nzc ? f : f - nzc)) * natm + i];
         x = f < nzc ? Z.x : Z.y;
       }
@@ -767,13 +772,13 @@ static __global__ void __launch_bounds__(kFieldTcThreads) k_rec_field_tc(
   // the epilogue's Y_ny phases of the CTA's ions (zero past the ions); made
   // visible by the barrier before the first products
   for (int e = tid; e < (ky + 1) * 128; e += NT) {
-    const int a = e >> 7, i = i0 + (e & 127);
-    Ys[e] = i < natm ? tab[(size_t)(kx + 1 + a) * natm + i] : make_float2(0.f, 0.f);
+    const int a = e >> 7, i = ion_of(i0 + (e & 127));
+    Ys[e] = i >= 0 ? tab[(size_t)(kx + 1 + a) * natm + i] : make_float2(0.f, 0.f);
   }
   // per-thread sums: ion m = 32 (warp & 3) + lane, column chunks (warp >> 2) and +2
   const int q = warp & 3, hh = warp >> 2;
-  const int m = q * 32 + lane, ion = i0 + m;
-  const bool ion_ok = ion < natm;
+  const int m = q * 32 + lane, ion = ion_of(i0 + m);
+  const bool ion_ok = ion >= 0;
   const int ionc = ion_ok ? ion : 0;
   const float4 wi = ion_ok ? w[ion] : make_float4(0.f, 0.f, 0.f, 0.f);
   double G[3] = {0.0, 0.0, 0.0}, H[3] = {0.0, 0.0, 0.0};

@@ -438,11 +438,13 @@ static int build_mesh(mdff_ctx* h) {
     // tensor-core structure factor: one CTA per SM over (row tiles x ion chunks)
     const char* env = std::getenv("MDFF_REC_TC");
     h->rho_tc = rho_tc_fits(h->p.kES[0], h->p.kES[1], h->p.kES[2]) && nrows > 0 && !(env && env[0] == '0');
+    // its K dimension: the polarisable ions (where induced dipoles live)
+    int nion = h->polidx.empty() ? h->natm : (int)h->polidx.size();
     int tiles = cdiv(nrows, kRhoTcRows);
     int nchunk = std::max(1, (h->nsm > 0 ? h->nsm : 148) / std::max(tiles, 1));
-    h->tc_chunk = std::max(kRhoTcKB, cdiv(cdiv(h->natm, nchunk), kRhoTcKB) * kRhoTcKB);
-    h->n_tc_chunks = cdiv(h->natm, h->tc_chunk);
-    h->tc_nkb = cdiv(h->natm, kRhoTcKB);
+    h->tc_chunk = std::max(kRhoTcKB, cdiv(cdiv(nion, nchunk), kRhoTcKB) * kRhoTcKB);
+    h->n_tc_chunks = cdiv(nion, h->tc_chunk);
+    h->tc_nkb = cdiv(nion, kRhoTcKB);
     cudaFree(h->d_rho_timg);
     h->d_rho_timg = nullptr;
     if (h->rho_tc)
@@ -674,14 +676,18 @@ static void launch_rho(mdff_ctx* h, dim3 g, const typename cplx<R>::T* tab, int 
     (void)pdl_launch(k_rec_rho<R, false, true, NZT>, dim3(g), dim3(kRhoThreads), 0, h->st, tab, h->d_w, n, chunk, M, ntiles, h->d_rho_part);
 }
 
+// ion slots of the tensor-core structure factor: the polarisable ions
+static int rho_tc_nion(const mdff_ctx* h) { return h->polidx.empty() ? h->natm : (int)h->polidx.size(); }
+
 // FP32 structure factor of the dipoles on the tensor cores into d_rho_part
 // (n_tc_chunks chunks); a launch error surfaces at the caller's LAUNCH_CHECK
 static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n) {
   size_t smem = rho_tc_smem(M.kmax[0], M.kmax[1], M.kmax[2]);
   dim3 g((unsigned)cdiv(M.nrows, kRhoTcRows), (unsigned)h->n_tc_chunks);
+  (void)n;
   (void)pdl_launch(k_rec_rho_tc, g, dim3(kRhoTcThreads), smem, h->st, (const float2*)h->d_rho_timg,
-                   (const float4*)h->d_w32, n, h->tc_chunk, M, h->d_rho_part, h->d_cata + 1,
-                   (const int*)(h->d_cata + 3));
+                   (const float4*)h->d_w32, (const int*)h->d_polidx, rho_tc_nion(h), h->tc_chunk, M,
+                   h->d_rho_part, h->d_cata + 1, (const int*)(h->d_cata + 3));
 }
 
 // FP32 field / force partials on the tensor cores into d_G / d_H (B tiles
@@ -732,7 +738,7 @@ static int launch_field_tc(mdff_ctx* h, const RecMesh& M, int n, bool muf, int n
 template <typename R>
 static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4* mu, int has_q,
                       int has_mu, int forces, double4* E, double* e_out, float4* mu32,
-                      SelfField sf, int* defer_nch, bool weights_ready) {
+                      SelfField sf, int* defer_nch, bool weights_ready, bool pol_dipoles) {
   int n = h->natm;
   if (h->nk == 0) {
     int e = rs_join(h);
@@ -773,7 +779,7 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   // alone, no forces), whose error the FP64 residual refinement removes; the
   // static field and the force pass keep the CUDA-core kernels (FP32 sums
   // with round-to-nearest)
-  if (F32 && h->rho_tc && !has_q && has_mu && !forces) {
+  if (F32 && h->rho_tc && pol_dipoles && !has_q && has_mu && !forces) {
     nparts = h->n_tc_chunks;
     launch_rho_tc(h, M, n);
   } else {
@@ -840,11 +846,15 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   return MDFF_OK;
 }
 
+// pol_dipoles: the dipoles mu are nonzero at the polarisable ions only (the
+// induced dipoles and the solver's directions)
 static int rec_pass(mdff_ctx* h, bool fp32, const double4* mu, int has_q, int has_mu, int forces,
                     double4* E, double* e_out, SelfField sf, float4* mu32 = nullptr,
-                    int* defer_nch = nullptr, bool weights_ready = false) {
-  if (fp32) return rec_pass_t<float>(h, h->d_tab32, mu, has_q, has_mu, forces, E, e_out, mu32, sf, defer_nch, weights_ready);
-  return rec_pass_t<double>(h, h->d_tab64, mu, has_q, has_mu, forces, E, e_out, mu32, sf, defer_nch, false);
+                    int* defer_nch = nullptr, bool weights_ready = false, bool pol_dipoles = false) {
+  if (fp32)
+    return rec_pass_t<float>(h, h->d_tab32, mu, has_q, has_mu, forces, E, e_out, mu32, sf, defer_nch, weights_ready,
+                             pol_dipoles);
+  return rec_pass_t<double>(h, h->d_tab64, mu, has_q, has_mu, forces, E, e_out, mu32, sf, defer_nch, false, false);
 }
 
 // the self field 2 selfa2 mu (+ surface field of the reduced moments in mom
@@ -872,7 +882,8 @@ static int build_tables(mdff_ctx* h) {
     // factor of the dipole solve
     if (h->rho_tc && h->lpolar)
       PDL_CHECK(pdl_launch(k_rec_rho_timg, dim3((unsigned)h->tc_nkb), dim3(256), 0, h->st, (const float2*)h->d_tab32, n,
-                           h->p.kES[0], h->p.kES[1], h->p.kES[2], h->d_rho_timg));
+                           (const int*)h->d_polidx, rho_tc_nion(h), h->p.kES[0], h->p.kES[1], h->p.kES[2],
+                           h->d_rho_timg));
   }
   return MDFF_OK;
 }
@@ -924,7 +935,7 @@ static int field_of_mu(mdff_ctx* h, const double4* mu, int dd_mask, bool fp32, d
                                                 h->L.cap, n, h->d_Edd);
     LAUNCH_CHECK();
   }
-  s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, sf, h->d_mu32, fused ? &nch : nullptr, weights_ready);
+  s = rec_pass(h, fp32, mu, 0, 1, 0, E, nullptr, sf, h->d_mu32, fused ? &nch : nullptr, weights_ready, true);
   if (s) return s;
   int pr = prof_begin(h, KC_ESFIELD, 0);
   if (fused)

@@ -809,16 +809,18 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
     PDL_CHECK(pdl_launch(k_rec_energy, dim3(1), dim3(1024), 0, h->st, h->d_str, M, tpi_V, h->omega, 1, e_out));
   }
   int nch = (int)h->rchunk.size() - 1;
-  dim3 gf((unsigned)cdiv(n, kFieldThreads), (unsigned)nch);
+  // a pass without forces feeds the dipole solvers, which read its field at
+  // the polarisable ions only: the field kernels run over those (ion map)
+  // and the final sum leaves the other ions' reciprocal part out
+  const bool field_pol = !forces && h->d_polidx;
+  const int* imap = field_pol ? h->d_polidx : nullptr;
+  const int nion = field_pol ? (int)h->polidx.size() : n;
+  dim3 gf((unsigned)cdiv(nion, kFieldThreads), (unsigned)nch);
   size_t smem = (size_t)h->max_chunk_k * sizeof(typename cplx<R>::T);
   bool muf = forces && has_mu;
   pr = prof_begin(h, KC_RECF, (double)h->nk * n * ops_fld);
   if (field_tc) {
-    // the dipole solve's operator (its partials summed by the caller's
-    // kernel) needs the field at the polarisable ions only
-    const bool pol_only = defer_nch && !has_q && has_mu && !forces && h->d_polidx;
-    nch = launch_field_tc(h, M, n, muf, npart, pol_only ? h->d_polidx : nullptr,
-                          pol_only ? (int)h->polidx.size() : n);
+    nch = launch_field_tc(h, M, n, muf, npart, imap, nion);
   } else if constexpr (std::is_same<R, float>::value) {
     dim3 gx((unsigned)cdiv(n, 2 * kFieldThreads), (unsigned)nch);
     if (muf)
@@ -826,9 +828,9 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
     else
       (void)pdl_launch(k_rec_field_x2<false>, dim3(gx), dim3(kFieldThreads), smem, h->st, tab, h->d_w32, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
   } else if (muf)
-    (void)pdl_launch(k_rec_field<R, true>, dim3(gf), dim3(kFieldThreads), smem, h->st, tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
+    (void)pdl_launch(k_rec_field<R, true>, dim3(gf), dim3(kFieldThreads), smem, h->st, tab, h->d_w, n, imap, nion, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H);
   else
-    PDL_CHECK(pdl_launch(k_rec_field<R, false>, dim3(gf), dim3(kFieldThreads), smem, h->st, tab, h->d_w, n, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H));
+    PDL_CHECK(pdl_launch(k_rec_field<R, false>, dim3(gf), dim3(kFieldThreads), smem, h->st, tab, h->d_w, n, imap, nion, M, h->d_rchunk, h->d_rhoA, h->d_rho_part, npart, h->d_G, h->d_H));
   prof_end(h, pr);
   double fpi_V = 2.0 * tpi_V;
   // the real-space half of this pass (side stream) adds into the same E / forces
@@ -841,7 +843,7 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   }
   k_rec_field_sum<<<cdiv((long)n * 4, 256), 256, 0, h->st>>>(h->d_G, h->d_H, nch, n, h->d_cell, h->d_q,
                                                    2.0 * fpi_V, muf ? 1 : 0, forces, h->coul_unit, E,
-                                                   h->d_force, sf);
+                                                   h->d_force, sf, field_pol ? h->d_ipolar : nullptr);
   LAUNCH_CHECK();
   return MDFF_OK;
 }

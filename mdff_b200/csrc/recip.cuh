@@ -289,6 +289,7 @@ static __global__ void k_rec_energy(const double* __restrict__ str, RecMesh M, d
 template <typename R, bool HAS_MU_FORCE>
 static __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>::T* __restrict__ tab,
                                                    const double4* __restrict__ w, int natm,
+                                                   const int* __restrict__ imap, int nion,
                                                    RecMesh M, const int* __restrict__ rchunk,
                                                    const double2* __restrict__ rhoA,
                                                    const double2* __restrict__ part, int npart,
@@ -310,8 +311,10 @@ static __global__ void __launch_bounds__(128) k_rec_field(const typename cplx<R>
     sh[k - k0] = c;
   }
   __syncthreads();
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= natm) return;
+  // thread slot -> ion (imap: the ions whose field is wanted, else all)
+  const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sl >= nion) return;
+  const int i = imap ? imap[sl] : sl;
   const int kx = M.kmax[0], ky = M.kmax[1], kz = M.kmax[2];
   double4 wi = w[i];
   R m3 = (R)wi.w;
@@ -441,7 +444,7 @@ static __global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const 
                                 const double* __restrict__ q, double scale /* 2 fpi_V */,
                                 int has_mu_force, int do_forces, double coul_unit,
                                 double4* __restrict__ E, double* __restrict__ force,
-                                SelfField sf) {
+                                SelfField sf, const int* __restrict__ ipolar) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int i = t >> 2, sub = t & 3;
   double g[3] = {0, 0, 0}, h[3] = {0, 0, 0};
@@ -467,6 +470,9 @@ static __global__ void k_rec_field_sum(const double4* __restrict__ Gpart, const 
     h[a] += __shfl_xor_sync(FULL_MASK, h[a], 2);
   }
   if (i >= natm || sub != 0) return;
+  // (ipolar: the partials cover the polarisable ions only, the field is
+  // wanted there; other ions keep their real-space part)
+  if (ipolar && !ipolar[i]) return;
   const double* B = cell->B;
   double e[3], fm[3];
   for (int a = 0; a < 3; ++a) {

@@ -57,6 +57,8 @@ enum {
 // FP32 CG: the recurrence residual drifts from the true one by about the FP32
 // matvec error, a few 1e-6 of the residual it started from (see solve_cg)
 constexpr double kCgGap = 3e-6;
+// what a reciprocal pass does with the CG solve's accumulated rho' (rec_mode)
+enum { REC_PLAIN = 0, REC_SAVE_ACC = 1, REC_NEED_RHOA = 2, REC_FROM_ACC = 3 };
 
 thread_local std::string g_err;
 
@@ -120,6 +122,13 @@ struct mdff_ctx {
   float4* d_w32 = nullptr;
   double2* d_rho_part = nullptr;
   double2* d_rhoA = nullptr;
+  // rho' of the charges and the dipoles of the CG solve, accumulated over
+  // its steps (the structure factor is linear in the dipoles) for the force
+  // pass; rho_acc_ok once this call's merged first residual seeded it.
+  // rec_mode selects what the next reciprocal pass does with it.
+  double2* d_rho_acc = nullptr;
+  bool rho_acc_ok = false;
+  int rec_mode = 0;
   double* d_str = nullptr;
   int n_rho_chunks = 0;
   int nsm = 0;  // SMs of the device
@@ -475,6 +484,9 @@ static int build_mesh(mdff_ctx* h) {
     }
   }
   DALLOC(h->d_rhoA, std::max(nk, 1));
+  cudaFree(h->d_rho_acc);
+  h->d_rho_acc = nullptr;
+  DALLOC(h->d_rho_acc, std::max(nk, 1));
   DALLOC(h->d_str, std::max(nk, 1));
   DALLOC(h->d_G, (size_t)(h->rchunk.size() - 1) * h->natm);
   DALLOC(h->d_H, (size_t)(h->rchunk.size() - 1) * h->natm);
@@ -775,11 +787,17 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   double ops_fld = (forces && has_mu) ? 32.0 : (forces ? 17.0 : 20.0);
   int pr = prof_begin(h, KC_RHO, (double)h->nk * n * ops_rho);
   int nparts = h->n_rho_chunks;
+  const int mode = h->rec_mode;
   // the tensor-core structure factor serves the FP32 CG operator (dipoles
   // alone, no forces), whose error the FP64 residual refinement removes; the
   // static field and the force pass keep the CUDA-core kernels (FP32 sums
-  // with round-to-nearest)
-  if (F32 && h->rho_tc && pol_dipoles && !has_q && has_mu && !forces) {
+  // with round-to-nearest).  The force pass after a CG solve takes the
+  // solve's accumulated rho' instead (REC_FROM_ACC).
+  if (mode == REC_FROM_ACC) {
+    nparts = 0;
+    PDL_CHECK(pdl_launch(k_rec_acc_finish, dim3(cdiv(h->nk, 256)), dim3(256), 0, h->st,
+                         (const double2*)h->d_rho_acc, M, h->d_rhoA, h->d_str));
+  } else if (F32 && h->rho_tc && pol_dipoles && !has_q && has_mu && !forces) {
     nparts = h->n_tc_chunks;
     launch_rho_tc(h, M, n);
   } else {
@@ -800,8 +818,13 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   // B-tile builder always)
   int npart = 0;
   const bool field_tc = F32 && h->field_tc;
-  if (e_out || (nparts > 4 && !field_tc)) {
-    PDL_CHECK(pdl_launch(k_rec_sum, dim3(cdiv(h->nk, 256)), dim3(256), 0, h->st, h->d_rho_part, nparts, M, h->d_rhoA, h->d_str));
+  if (mode == REC_FROM_ACC) {
+    // rhoA and str are in place
+  } else if (e_out || (nparts > 4 && !field_tc) || mode == REC_SAVE_ACC || mode == REC_NEED_RHOA) {
+    // (REC_SAVE_ACC: this rho' starts the solve's accumulation; REC_NEED_RHOA:
+    // the CG step after this operator adds it)
+    PDL_CHECK(pdl_launch(k_rec_sum, dim3(cdiv(h->nk, 256)), dim3(256), 0, h->st, (const double2*)h->d_rho_part, nparts,
+                         M, h->d_rhoA, h->d_str, mode == REC_SAVE_ACC ? h->d_rho_acc : (double2*)nullptr));
   } else {
     npart = nparts;
   }
@@ -1471,17 +1494,26 @@ __global__ void k_setd2(double* __restrict__ a, double va, double* __restrict__ 
 }
 
 // one inner CG iteration: p -> T p -> q = A p; x, r, z updated; p <- z + beta p
+static bool rho_acc_enabled(const mdff_ctx* h);
+
 static int cg_iteration(mdff_ctx* h, bool fp32, int in_graph, cudaGraphConditionalHandle hc) {
   int n = h->natm, nb = cdiv(n, 256), s;
   PolDev P = poldev(h);
   double* sc = h->d_scal + S_CG;
-  if ((s = field_of_mu(h, h->d_pv, 1, fp32, h->d_Tp, fp32))) return s;
+  // with the accumulated structure factor the operator's rho'(p) stays in
+  // rhoA for the update, which adds al rho'(p)
+  const bool acc = rho_acc_enabled(h);
+  h->rec_mode = acc ? REC_NEED_RHOA : REC_PLAIN;
+  s = field_of_mu(h, h->d_pv, 1, fp32, h->d_Tp, fp32);
+  h->rec_mode = REC_PLAIN;
+  if (s) return s;
   PDL_CHECK(pdl_launch(k_cg_Ap, dim3(nb), dim3(256), 0, h->st, (const double4*)h->d_pv,
                        (const double4*)h->d_Tp, P, n, h->d_qv, h->d_part));
   if ((s = reduce_into(h, nb, 1, sc + 2))) return s;
   PDL_CHECK(pdl_launch(k_cg_update, dim3(nb), dim3(256), 0, h->st, (const double*)(sc + 0),
                        (const double*)(sc + 2), P, n, h->d_pv, (const double4*)h->d_qv, h->d_mu_ind, h->d_r,
-                       h->d_z, h->d_part));
+                       h->d_z, h->d_part, acc ? h->d_rho_acc : (double2*)nullptr, (const double2*)h->d_rhoA,
+                       h->nk));
   if ((s = reduce_into(h, nb, 2, sc + 3))) return s;
   PDL_CHECK(pdl_launch(k_cg_dir, dim3(nb), dim3(256), 0, h->st, (const double*)(sc + 0),
                        (const double*)(sc + 3), n, (const double4*)h->d_z, h->d_pv,
@@ -1599,6 +1631,13 @@ static bool cg_merged(const mdff_ctx* h) {
          (h->p.calc == MDFF_CALC_MD || h->p.calc == MDFF_CALC_OPT);
 }
 
+// The force pass takes its structure factor from the solve's accumulation:
+// after the merged first residual (rho' of the charges and x0) every CG step
+// adds al rho'(p), so the accumulation is rho' of the charges and the final
+// dipoles, which are the total dipoles here (no static dipoles, no Wannier
+// centres)
+static bool rho_acc_enabled(const mdff_ctx* h) { return cg_merged(h) && !h->lwannier && h->nk > 0; }
+
 // the static field plus the field of the first guess x0 (real space on the
 // side stream: FP64, or in the mixed engine the FP32 static pass that writes
 // the pair cache of its CG operator and applies the cached pair tensor to x0
@@ -1639,9 +1678,14 @@ static int merged_residual(mdff_ctx* h, bool fp32) {
   }
   LAUNCH_CHECK();
   prof_end(h, pr);
-  if ((s = rec_pass(h, false, h->d_mu_ind, h->task_qq ? 1 : 0, 1, 0, E, nullptr,
-                    self_field(h, h->d_mu_ind, h->d_scal + S_MOM2))))
-    return s;
+  // (its rho' of the charges and x0 also starts the solve's accumulation)
+  const bool acc = rho_acc_enabled(h);
+  h->rec_mode = acc ? REC_SAVE_ACC : REC_PLAIN;
+  s = rec_pass(h, false, h->d_mu_ind, h->task_qq ? 1 : 0, 1, 0, E, nullptr,
+               self_field(h, h->d_mu_ind, h->d_scal + S_MOM2));
+  h->rec_mode = REC_PLAIN;
+  if (s) return s;
+  h->rho_acc_ok = acc;
   PDL_CHECK(pdl_launch(k_cg_init, dim3(nb), dim3(256), 0, h->st, (const double4*)nullptr, (const double4*)E,
                        (const double4*)h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
                        (const CellC*)h->d_cell, fp32 ? h->d_w32 : (float4*)nullptr, h->d_mu32));
@@ -1808,6 +1852,7 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
 
 static int ef_front(mdff_ctx* h, bool fp32) {
   int n = h->natm, s;
+  h->rho_acc_ok = false;
   PDL_CHECK(pdl_launch(k_kardir, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_pos, n, h->d_cell, h->d_s));
   if ((s = list_update(h))) return s;
   CK(cudaMemsetAsync(h->d_scal, 0, sizeof(double) * S_NSCAL, h->st));
@@ -1910,9 +1955,11 @@ static int ef_back(mdff_ctx* h, bool fp32) {
     LAUNCH_CHECK();
     int has_mu = (h->task_qd || h->task_dd) ? 1 : 0;
     if ((s = moments(h, h->d_mu_tot, 1, h->d_scal + S_MOM))) return s;
-    if ((s = rec_pass(h, fp32, h->d_mu_tot, h->task_qq ? 1 : 0, has_mu, 1, h->d_E, h->d_scal + S_REC,
-                      self_field(h, h->d_mu_tot, h->d_scal + S_MOM))))
-      return s;
+    h->rec_mode = (h->rho_acc_ok && rho_acc_enabled(h)) ? REC_FROM_ACC : REC_PLAIN;
+    s = rec_pass(h, fp32, h->d_mu_tot, h->task_qq ? 1 : 0, has_mu, 1, h->d_E, h->d_scal + S_REC,
+                 self_field(h, h->d_mu_tot, h->d_scal + S_MOM));
+    h->rec_mode = REC_PLAIN;
+    if (s) return s;
   }
   if ((s = rs_join(h))) return s;
   CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * S_NSCAL, cudaMemcpyDeviceToHost, h->st));
@@ -2774,7 +2821,7 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
                   h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
                   h->d_lwfc, h->d_mu_wfc, h->d_qm32, h->d_Edd, h->d_fsr, h->d_hist_save,
-                  h->d_rho_timg, h->d_polidx};
+                  h->d_rho_timg, h->d_polidx, h->d_rho_acc};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   step_graph_free(h);

@@ -237,17 +237,26 @@ __global__ void k_cg_Ap(const double4* __restrict__ p, const double4* __restrict
 
 // al = rz / pq ; x += al p ; r -= al q ; z = alpha_pol r ;
 // partial r.z (new) and rmsd^2
+// (acc: the structure factor is linear in the dipoles, so acc += al rho'(p)
+// with rho'(p) = rhoA of this step's operator keeps acc = rho' of the charges
+// and the current x; nk k vectors, grid-stride)
 __global__ void k_cg_update(const double* __restrict__ rz_p, const double* __restrict__ pq_p,
                             PolDev P, int natm, const double4* __restrict__ p,
                             const double4* __restrict__ qv, double4* __restrict__ x,
                             double4* __restrict__ r, double4* __restrict__ z,
-                            double* __restrict__ part) {
+                            double* __restrict__ part, double2* __restrict__ acc = nullptr,
+                            const double2* __restrict__ rhoA = nullptr, int nk = 0) {
   pdl_wait();
   pdl_trigger();
   __shared__ double red[2 * 32];
   double v[2] = {0.0, 0.0};
   double rz = *rz_p, pq = *pq_p;
   double al = (pq != 0.0) ? rz / pq : 0.0;
+  if (acc)
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nk; k += gridDim.x * blockDim.x) {
+      const double2 a = acc[k], d = rhoA[k];
+      acc[k] = make_double2(a.x + al * d.x, a.y + al * d.y);
+    }
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < natm && P.ipolar[i]) {
     double4 xi = x[i], ri = r[i], pi = p[i], qi = qv[i];

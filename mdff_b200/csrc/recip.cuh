@@ -237,9 +237,11 @@ static __device__ __forceinline__ double2 rho_prime(const double2* __restrict__ 
   return make_double2(A * r, A * im);
 }
 
-// rho = sum over chunks; rhoA = A_k rho; str = A_k |rho|^2
+// rho = sum over chunks; rhoA = A_k rho; str = A_k |rho|^2 (acc: also a
+// copy of rhoA, the start of the dipole solve's accumulated rho')
 static __global__ void k_rec_sum(const double2* __restrict__ part, int nchunk, RecMesh M,
-                          double2* __restrict__ rhoA, double* __restrict__ str) {
+                          double2* __restrict__ rhoA, double* __restrict__ str,
+                          double2* __restrict__ acc = nullptr) {
   pdl_wait();
   pdl_trigger();
   int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -253,6 +255,21 @@ static __global__ void k_rec_sum(const double2* __restrict__ part, int nchunk, R
   double A = M.Ak[k];
   rhoA[k] = make_double2(A * r, A * im);
   str[k] = (r * r + im * im) * A;
+  if (acc) acc[k] = make_double2(A * r, A * im);
+}
+
+// rhoA and str of the force pass from the dipole solve's accumulated rho'
+// (rho' of the charges and the first guess, plus alpha_k rho'(p_k) of every
+// CG step: the structure factor is linear in the dipoles); str = |rho'|^2 / A_k
+static __global__ void k_rec_acc_finish(const double2* __restrict__ acc, RecMesh M,
+                                        double2* __restrict__ rhoA, double* __restrict__ str) {
+  pdl_wait();
+  pdl_trigger();
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= M.nk) return;
+  const double2 a = acc[k];
+  rhoA[k] = a;
+  str[k] = (a.x * a.x + a.y * a.y) / M.Ak[k];
 }
 
 // u_rec (x2 x tpi_V) and tau_rec (x2, symmetric, x tpi_V/omega): out[0..6] =

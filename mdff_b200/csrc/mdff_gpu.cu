@@ -707,7 +707,7 @@ static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n) {
 // imap (nion entries): the ions whose partials are wanted (nullptr: all n)
 template <int KF>
 static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int npart, const int* imap,
-                             int nion) {
+                             int nion, double2* rho_out) {
   int rpt = field_tc_rpt(muf);
   int ntile = cdiv(M.nrows, rpt);
   int ion_tiles = cdiv(nion, 128);
@@ -727,11 +727,11 @@ static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int
   const uint32_t* fb = h->d_fb;
   h->launches++;  // two launches here; the caller's LAUNCH_CHECK counts one
   if (muf) {
-    (void)pdl_launch(k_rec_field_btiles<true, KF>, gb, dim3(128), bsmem, h->st, M, rhoA, rpart, npart, h->d_fb);
+    (void)pdl_launch(k_rec_field_btiles<true, KF>, gb, dim3(128), bsmem, h->st, M, rhoA, rpart, npart, h->d_fb, rho_out);
     (void)pdl_launch(k_rec_field_tc<true, KF>, g, dim3(kFieldTcThreads), smem, h->st, tab, w, n, imap, nion,
                      M, fb, tpg, h->d_G, h->d_H, err);
   } else {
-    (void)pdl_launch(k_rec_field_btiles<false, KF>, gb, dim3(128), bsmem, h->st, M, rhoA, rpart, npart, h->d_fb);
+    (void)pdl_launch(k_rec_field_btiles<false, KF>, gb, dim3(128), bsmem, h->st, M, rhoA, rpart, npart, h->d_fb, rho_out);
     (void)pdl_launch(k_rec_field_tc<false, KF>, g, dim3(kFieldTcThreads), smem, h->st, tab, w, n, imap, nion,
                      M, fb, tpg, h->d_G, h->d_H, err);
   }
@@ -739,9 +739,9 @@ static int launch_field_tc_k(mdff_ctx* h, const RecMesh& M, int n, bool muf, int
 }
 
 static int launch_field_tc(mdff_ctx* h, const RecMesh& M, int n, bool muf, int npart, const int* imap,
-                           int nion) {
-  if (field_tc_kf(M.kmax[2]) == 32) return launch_field_tc_k<32>(h, M, n, muf, npart, imap, nion);
-  return launch_field_tc_k<64>(h, M, n, muf, npart, imap, nion);
+                           int nion, double2* rho_out) {
+  if (field_tc_kf(M.kmax[2]) == 32) return launch_field_tc_k<32>(h, M, n, muf, npart, imap, nion, rho_out);
+  return launch_field_tc_k<64>(h, M, n, muf, npart, imap, nion, rho_out);
 }
 
 // reciprocal pass: E += rec field (+ the self / surface field sf, when on);
@@ -820,9 +820,10 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   const bool field_tc = F32 && h->field_tc;
   if (mode == REC_FROM_ACC) {
     // rhoA and str are in place
-  } else if (e_out || (nparts > 4 && !field_tc) || mode == REC_SAVE_ACC || mode == REC_NEED_RHOA) {
+  } else if (e_out || (nparts > 4 && !field_tc) || mode == REC_SAVE_ACC || (mode == REC_NEED_RHOA && !field_tc)) {
     // (REC_SAVE_ACC: this rho' starts the solve's accumulation; REC_NEED_RHOA:
-    // the CG step after this operator adds it)
+    // the CG step after this operator adds it, which the tensor-core B-tile
+    // builder writes while it sums the partials)
     PDL_CHECK(pdl_launch(k_rec_sum, dim3(cdiv(h->nk, 256)), dim3(256), 0, h->st, (const double2*)h->d_rho_part, nparts,
                          M, h->d_rhoA, h->d_str, mode == REC_SAVE_ACC ? h->d_rho_acc : (double2*)nullptr));
   } else {
@@ -843,7 +844,8 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   bool muf = forces && has_mu;
   pr = prof_begin(h, KC_RECF, (double)h->nk * n * ops_fld);
   if (field_tc) {
-    nch = launch_field_tc(h, M, n, muf, npart, imap, nion);
+    nch = launch_field_tc(h, M, n, muf, npart, imap, nion,
+                          (mode == REC_NEED_RHOA && npart) ? h->d_rhoA : (double2*)nullptr);
   } else if constexpr (std::is_same<R, float>::value) {
     dim3 gx((unsigned)cdiv(n, 2 * kFieldThreads), (unsigned)nch);
     if (muf)

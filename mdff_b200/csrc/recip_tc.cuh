@@ -637,13 +637,15 @@ __host__ __device__ constexpr size_t field_tc_smem(int KF, int ky) {
 // builds the columns of kBtRows mesh rows.  rho'(row, nz) is staged in shared
 // memory, zero outside the row's nz range: from rhoA, or (npart > 0) summed
 // from the structure-factor chunk partials in chunk order (rho_prime, the same
-// sums as k_rec_sum), which saves that pass when no energy is needed.
+// sums as k_rec_sum), which saves that pass when no energy is needed; rho_out
+// (optional) receives those rho' values.
 constexpr int kBtRows = 4;
 
 template <bool HAS_H, int KF>
 static __global__ void __launch_bounds__(128) k_rec_field_btiles(RecMesh M, const double2* __restrict__ rhoA,
                                                                  const double2* __restrict__ part, int npart,
-                                                                 uint32_t* __restrict__ fb) {
+                                                                 uint32_t* __restrict__ fb,
+                                                                 double2* __restrict__ rho_out) {
   pdl_wait();
   pdl_trigger();
   constexpr int CPR = HAS_H ? 8 : 4, RPT = 128 / CPR;
@@ -660,6 +662,7 @@ static __global__ void __launch_bounds__(128) k_rec_field_btiles(RecMesh M, cons
       if (nz >= ri.z) {
         int k = ri.w + nz - ri.z;
         v = npart ? rho_prime(part, npart, M.Ak, M.nk, k) : rhoA[k];
+        if (rho_out) rho_out[k] = v;  // each k is staged by one CTA
       }
     }
     rs[e] = v;

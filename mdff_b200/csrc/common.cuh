@@ -237,4 +237,17 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* smem) {
   __syncthreads();
 }
 
+// FP32 weights at the ion slots of the tensor-core structure factor: w32s[slot[i]]
+// for the ions with a slot (slot[i] >= 0); inactive without w32s
+struct SlotW {
+  float4* w32s = nullptr;
+  const int* slot = nullptr;
+  __device__ __forceinline__ void put(int i, float4 v) const {
+    if (w32s) {
+      const int sl = slot[i];
+      if (sl >= 0) w32s[sl] = v;
+    }
+  }
+};
+
 }  // namespace mdff

@@ -142,6 +142,10 @@ struct mdff_ctx {
   // built per call with the FP32 tables
   float2* d_rho_timg = nullptr;
   int tc_nkb = 0;
+  // its FP32 weights in slot order (written beside d_w32 by the weight and CG
+  // direction kernels), and the slot of each ion (-1: none)
+  float4* d_w32s = nullptr;
+  int* d_polslot = nullptr;
   // FP32 reciprocal field / force partials on the tensor cores
   // (k_rec_field_tc, B tiles in d_fb); off when kz > 31 or MDFF_FIELD_TC=0
   // in the environment
@@ -455,9 +459,22 @@ static int build_mesh(mdff_ctx* h) {
     h->n_tc_chunks = cdiv(nion, h->tc_chunk);
     h->tc_nkb = cdiv(nion, kRhoTcKB);
     cudaFree(h->d_rho_timg);
+    cudaFree(h->d_w32s);
+    cudaFree(h->d_polslot);
     h->d_rho_timg = nullptr;
-    if (h->rho_tc)
+    h->d_w32s = nullptr;
+    h->d_polslot = nullptr;
+    if (h->rho_tc) {
       DALLOC(h->d_rho_timg, (size_t)h->tc_nkb * rho_tc_staging(h->p.kES[0], h->p.kES[1], h->p.kES[2]) / sizeof(float2));
+      DALLOC(h->d_w32s, (size_t)h->tc_nkb * kRhoTcKB);  // zero past the slots
+      std::vector<int> slot(h->natm, -1);
+      if (h->polidx.empty())
+        for (int i = 0; i < h->natm; ++i) slot[i] = i;
+      else
+        for (size_t k = 0; k < h->polidx.size(); ++k) slot[h->polidx[k]] = (int)k;
+      DALLOC(h->d_polslot, h->natm);
+      CK(cudaMemcpy(h->d_polslot, slot.data(), sizeof(int) * h->natm, cudaMemcpyHostToDevice));
+    }
   }
   DALLOC(h->d_rho_part, (size_t)std::max(h->n_rho_chunks, h->n_tc_chunks) * std::max(nk, 1));
   if (h->rho_tc)
@@ -647,6 +664,15 @@ static int moments(mdff_ctx* h, const double4* mu, int has_q, double* out) {
 }
 
 static PolDev poldev(mdff_ctx* h) { return PolDev{h->d_pol, h->d_invpol, h->d_ipolar}; }
+// the slot-ordered FP32 weights of the tensor-core structure factor (inactive without it)
+static SlotW slotw(const mdff_ctx* h) {
+  SlotW sw;
+  if (h->d_w32s) {
+    sw.w32s = h->d_w32s;
+    sw.slot = h->d_polslot;
+  }
+  return sw;
+}
 
 // nz tile of the structure factor: the width (8, 11, 13 or 16) that wastes
 // the fewest accumulator slots on rows of nzmax consecutive nz
@@ -698,7 +724,7 @@ static void launch_rho_tc(mdff_ctx* h, const RecMesh& M, int n) {
   dim3 g((unsigned)cdiv(M.nrows, kRhoTcRows), (unsigned)h->n_tc_chunks);
   (void)n;
   (void)pdl_launch(k_rec_rho_tc, g, dim3(kRhoTcThreads), smem, h->st, (const float2*)h->d_rho_timg,
-                   (const float4*)h->d_w32, (const int*)h->d_polidx, rho_tc_nion(h), h->tc_chunk, M,
+                   (const float4*)h->d_w32s, rho_tc_nion(h), h->tc_chunk, M,
                    h->d_rho_part, h->d_cata + 1, (const int*)(h->d_cata + 3));
 }
 
@@ -774,7 +800,7 @@ static int rec_pass_t(mdff_ctx* h, const typename cplx<R>::T* tab, const double4
   // (the FP32 CG direction kernels write the FP32 weights themselves)
   if (!(F32 && weights_ready)) {
     PDL_CHECK(pdl_launch(k_rec_weights, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_q, mu, n, h->d_cell, has_q, has_mu, h->d_w,
-                                                   F32 ? h->d_w32 : nullptr, mu32));
+                         F32 ? h->d_w32 : nullptr, mu32, slotw(h)));
   }
   int nzt = pick_nzt(2 * M.kmax[2] + 1);
   int ntiles = cdiv(2 * M.kmax[2] + 1, nzt);
@@ -1519,7 +1545,7 @@ static int cg_iteration(mdff_ctx* h, bool fp32, int in_graph, cudaGraphCondition
   if ((s = reduce_into(h, nb, 2, sc + 3))) return s;
   PDL_CHECK(pdl_launch(k_cg_dir, dim3(nb), dim3(256), 0, h->st, (const double*)(sc + 0),
                        (const double*)(sc + 3), n, (const double4*)h->d_z, h->d_pv,
-                       (const CellC*)h->d_cell, fp32 ? h->d_w32 : (float4*)nullptr, h->d_mu32));
+                       (const CellC*)h->d_cell, fp32 ? h->d_w32 : (float4*)nullptr, h->d_mu32, slotw(h)));
   PDL_CHECK(pdl_launch(k_cg_inner_check, dim3(1), dim3(32), 0, h->st, sc, h->npol, in_graph, hc));
   return MDFF_OK;
 }
@@ -1621,7 +1647,7 @@ static int cg_residual(mdff_ctx* h, bool fp32) {
   PolDev P = poldev(h);
   if ((s = field_of_mu(h, h->d_mu_ind, 1, false, h->d_Tp, false, fp32))) return s;
   PDL_CHECK(pdl_launch(k_cg_init, dim3(nb), dim3(256), 0, h->st, h->d_Estat, h->d_Tp, h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
-                                   h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32));
+                                   h->d_cell, fp32 ? h->d_w32 : nullptr, h->d_mu32, slotw(h)));
   return reduce_into(h, nb, 2, h->d_scal + S_CG);
 }
 
@@ -1690,7 +1716,7 @@ static int merged_residual(mdff_ctx* h, bool fp32) {
   h->rho_acc_ok = acc;
   PDL_CHECK(pdl_launch(k_cg_init, dim3(nb), dim3(256), 0, h->st, (const double4*)nullptr, (const double4*)E,
                        (const double4*)h->d_mu_ind, P, n, h->d_r, h->d_z, h->d_pv, h->d_part,
-                       (const CellC*)h->d_cell, fp32 ? h->d_w32 : (float4*)nullptr, h->d_mu32));
+                       (const CellC*)h->d_cell, fp32 ? h->d_w32 : (float4*)nullptr, h->d_mu32, slotw(h)));
   return reduce_into(h, nb, 2, h->d_scal + S_CG);
 }
 
@@ -2823,7 +2849,7 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
                   h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
                   h->d_lwfc, h->d_mu_wfc, h->d_qm32, h->d_Edd, h->d_fsr, h->d_hist_save,
-                  h->d_rho_timg, h->d_polidx, h->d_rho_acc};
+                  h->d_rho_timg, h->d_polidx, h->d_rho_acc, h->d_w32s, h->d_polslot};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   step_graph_free(h);

@@ -168,21 +168,25 @@ __global__ void k_self_surf_field(const double4* __restrict__ mu, int natm, doub
 // r = b + Tx - alpha^-1 x ; z = alpha r ; p = z ; partial r.z and rmsd
 // FP32 operands of the next operator application of the direction p (when w32
 // is given): w32 = (0, m), m = 2 pi B^T p, mu32 = p, as k_rec_weights writes them
+// (and w32 again at the ion's slot in w32s, when the ion has one)
 __device__ __forceinline__ void cg_dir_weights(const CellC* __restrict__ cell, double4 u, int i,
-                                               float4* __restrict__ w32, float4* __restrict__ mu32) {
+                                               float4* __restrict__ w32, float4* __restrict__ mu32,
+                                               const SlotW& sw) {
   const double* B = cell->B;
   double m1 = kTwoPi * (B[0] * u.x + B[3] * u.y + B[6] * u.z);
   double m2 = kTwoPi * (B[1] * u.x + B[4] * u.y + B[7] * u.z);
   double m3 = kTwoPi * (B[2] * u.x + B[5] * u.y + B[8] * u.z);
-  w32[i] = make_float4(0.f, (float)m1, (float)m2, (float)m3);
+  const float4 wv = make_float4(0.f, (float)m1, (float)m2, (float)m3);
+  w32[i] = wv;
   mu32[i] = make_float4((float)u.x, (float)u.y, (float)u.z, 0.f);
+  sw.put(i, wv);
 }
 
 __global__ void k_cg_init(const double4* __restrict__ b, const double4* __restrict__ Tx,
                           const double4* __restrict__ x, PolDev P, int natm, double4* __restrict__ r,
                           double4* __restrict__ z, double4* __restrict__ p, double* __restrict__ part,
                           const CellC* __restrict__ cell, float4* __restrict__ w32,
-                          float4* __restrict__ mu32) {
+                          float4* __restrict__ mu32, SlotW sw) {
   pdl_wait();
   pdl_trigger();
   __shared__ double red[2 * 32];
@@ -204,7 +208,7 @@ __global__ void k_cg_init(const double4* __restrict__ b, const double4* __restri
     r[i] = ri;
     z[i] = zi;
     p[i] = zi;
-    if (w32) cg_dir_weights(cell, zi, i, w32, mu32);
+    if (w32) cg_dir_weights(cell, zi, i, w32, mu32, sw);
     v[0] = ri.x * zi.x + ri.y * zi.y + ri.z * zi.z;
   }
   block_sum<2>(v, red);
@@ -287,7 +291,7 @@ __global__ void k_cg_update(const double* __restrict__ rz_p, const double* __res
 __global__ void k_cg_dir(const double* __restrict__ rz_p, const double* __restrict__ rzn_p,
                          int natm, const double4* __restrict__ z, double4* __restrict__ p,
                          const CellC* __restrict__ cell, float4* __restrict__ w32,
-                         float4* __restrict__ mu32) {
+                         float4* __restrict__ mu32, SlotW sw) {
   pdl_wait();
   pdl_trigger();
   double rz = *rz_p, rzn = *rzn_p;
@@ -297,7 +301,7 @@ __global__ void k_cg_dir(const double* __restrict__ rz_p, const double* __restri
     double4 pi = p[i], zi = z[i];
     double4 pn = make_double4(zi.x + be * pi.x, zi.y + be * pi.y, zi.z + be * pi.z, 0.0);
     p[i] = pn;
-    if (w32) cg_dir_weights(cell, pn, i, w32, mu32);
+    if (w32) cg_dir_weights(cell, pn, i, w32, mu32, sw);
   }
 }
 

@@ -81,7 +81,7 @@ static __global__ void k_rec_tables(const double4* __restrict__ s, int natm, int
 static __global__ void k_rec_weights(const double* __restrict__ q, const double4* __restrict__ mu,
                               int natm, const CellC* __restrict__ cell, int has_q, int has_mu,
                               double4* __restrict__ w, float4* __restrict__ w32,
-                              float4* __restrict__ mu32) {
+                              float4* __restrict__ mu32, SlotW sw = SlotW()) {
   pdl_wait();
   pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -96,7 +96,11 @@ static __global__ void k_rec_weights(const double* __restrict__ q, const double4
     m3 = kTwoPi * (B[2] * u.x + B[5] * u.y + B[8] * u.z);
   }
   w[i] = make_double4(qi, m1, m2, m3);
-  if (w32) w32[i] = make_float4((float)qi, (float)m1, (float)m2, (float)m3);
+  if (w32) {
+    const float4 wv = make_float4((float)qi, (float)m1, (float)m2, (float)m3);
+    w32[i] = wv;
+    sw.put(i, wv);
+  }
   if (mu32) {
     double4 u = mu[i];
     mu32[i] = make_float4((float)u.x, (float)u.y, (float)u.z, 0.f);

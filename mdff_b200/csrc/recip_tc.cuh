@@ -251,23 +251,21 @@ static __global__ void __launch_bounds__(256) k_rec_rho_timg(const float2* __res
 // structure factor of the dipoles on the tensor cores.  grid = (row tiles of
 // 64 mesh rows, ion chunks of a multiple of 32 ions), one CTA per SM;
 // part[chunk][k] = this chunk's rho(k).  The K dimension runs over ion slots
-// (slot s = ion imap[s]: the polarisable ions, where the induced dipoles
-// live).  Warps 0-15 generate the operands from staged tables; one thread of
-// warp 16 issues the MMAs; warp 17 stages each K block's table block (from
-// the blocked image, one bulk copy) and gathers its weights through the map.  No CTA-wide barrier inside the K loop:
+// (the polarisable ions, where the induced dipoles live; the weights ws and
+// the blocked tables are in slot order).  Warps 0-15 generate the operands
+// from staged tables; one thread of warp 16 issues the MMAs; one thread of
+// warp 17 stages each K block's table block and weights with two bulk copies.  No CTA-wide barrier inside the K loop:
 // mbarriers carry each dependency, with one arrival per generating warp,
 //   tfull[b]  the tables and weights of a K block landed in staging buffer b
-//             (bytes of the bulk copy, and the copy warp after its weight
-//             stores),
+//             (bytes of the bulk copies),
 //   sfree[b]  every warp has generated the block staged in buffer b,
 //   full[s]   operand stage s written (after each lane's fence.proxy.async),
 //   empty[s]  the MMAs that read stage s are complete (tcgen05.commit),
 // so the copies run up to three K blocks ahead of the generation, which runs
 // up to two ahead of the products.
 static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
-    const float2* __restrict__ timg, const float4* __restrict__ w, const int* __restrict__ imap, int nion,
-    int chunk, RecMesh M, double2* __restrict__ part, int* __restrict__ err,
-    const int* __restrict__ wait_cfg) {
+    const float2* __restrict__ timg, const float4* __restrict__ ws, int nion, int chunk, RecMesh M,
+    double2* __restrict__ part, int* __restrict__ err, const int* __restrict__ wait_cfg) {
   pdl_wait();
   pdl_trigger();
   constexpr int NG = kRhoTcGen, RPT = kRhoTcRows, KB = kRhoTcKB, KC = KB / 4, NS = kRhoTcStg;
@@ -317,7 +315,7 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
       tc::mbar_init_n(tc::smem_u32(&empty[s]), 1);
     }
     for (int b = 0; b < NS; ++b) {
-      tc::mbar_init_n(tc::smem_u32(&tfull[b]), 2);
+      tc::mbar_init_n(tc::smem_u32(&tfull[b]), 1);
       tc::mbar_init_n(tc::smem_u32(&sfree[b]), NG / 32);
     }
     asm volatile("fence.mbarrier_init.release.cluster;");
@@ -440,44 +438,32 @@ static __global__ void __launch_bounds__(kRhoTcThreads, 1) k_rec_rho_tc(
       }
     }
   } else if (warp == NG / 32 + 1) {
-    // ---- copies: the table block (one bulk copy, lane 0) and the weights of
-    // K block kb (lane j gathers slot j's through the ion map) into staging
-    // buffer kb % NS once every warp has generated block kb - NS from it;
-    // two arrivals on tfull: the bulk copy's and the warp's after its stores
-    const size_t tblk = (size_t)TR * kStageRow / sizeof(float2);  // table image block, float2
-    const uint32_t tbytes = (uint32_t)(TR * kStageRow);
-    int copied = 0;
-    for (int kb = 0; kb < nkb; ++kb) {
-      const int b = kb % NS;
-      int ok = 1;
-      if (kb >= NS && lane == 0)
-        ok = tc::mbar_wait_ab(tc::smem_u32(&sfree[b]), (kb / NS - 1) & 1, tc::kWaitLimit, abort_v) ? 1 : 0;
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      __syncwarp();
-      if (!ok) {
-        if (lane == 0) abort_flag = 1;
-        break;
+    // ---- copies: the table block and the weights of K block kb (both in slot
+    // order) into staging buffer kb % NS once every warp has generated block
+    // kb - NS from it, two bulk copies
+    if (lane == 0) {
+      const size_t tblk = (size_t)TR * kStageRow / sizeof(float2);  // table image block, float2
+      const uint32_t tbytes = (uint32_t)(TR * kStageRow), wbytes = 16u * KB;
+      int copied = 0;
+      for (int kb = 0; kb < nkb; ++kb) {
+        const int b = kb % NS;
+        if (kb >= NS && !tc::mbar_wait_ab(tc::smem_u32(&sfree[b]), (kb / NS - 1) & 1, tc::kWaitLimit, abort_v)) {
+          abort_flag = 1;
+          break;
+        }
+        const uint32_t dst = tc::smem_u32(stg0 + b * sbytes), fb = tc::smem_u32(&tfull[b]);
+        tc::mbar_expect_tx(fb, tbytes + wbytes);
+        tc::bulk_g2s(dst, timg + (size_t)(kb0 + kb) * tblk, tbytes, fb);
+        tc::bulk_g2s(dst + tbytes, ws + (size_t)(kb0 + kb) * KB, wbytes, fb);
+        copied = kb + 1;
       }
-      const uint32_t fb = tc::smem_u32(&tfull[b]);
-      if (lane == 0) {
-        tc::mbar_expect_tx(fb, tbytes);
-        tc::bulk_g2s(tc::smem_u32(stg0 + b * sbytes), timg + (size_t)(kb0 + kb) * tblk, tbytes, fb);
-      }
-      const int sl = (kb0 + kb) * KB + lane;
-      const int ion = sl < nion ? (imap ? imap[sl] : sl) : -1;
-      reinterpret_cast<float4*>(stg0 + b * sbytes + tbytes)[lane] =
-          ion >= 0 ? w[ion] : make_float4(0.f, 0.f, 0.f, 0.f);
-      __syncwarp();
-      if (lane == 0) tc::mbar_arrive(fb);
-      copied = kb + 1;
-    }
-    // no copy may still be landing when the CTA leaves (after an abort):
-    // wait (bounded) for the last block copied into each buffer
-    if (lane == 0)
+      // no copy may still be landing when the CTA leaves (after an abort):
+      // wait (bounded) for the last block copied into each buffer
       for (int b = 0; b < NS && b < copied; ++b) {
         const int last = b + NS * ((copied - 1 - b) / NS);
         if (!tc::mbar_wait(tc::smem_u32(&tfull[b]), (last / NS) & 1, tc::kWaitLimit)) abort_flag = 1;
       }
+    }
   } else if (lane == 0) {
     // ---- MMA issue: the three products of split TF32.  Fused: A_hi [B_hi |
     // B_lo] (N = 2 Nr: columns [0, Nr) and [Nr, 2 Nr)) and A_lo B_hi into

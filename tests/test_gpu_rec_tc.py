@@ -6,7 +6,10 @@ The mixed engine on the tensor cores (default) must agree with the same
 engine on the CUDA-core kernels (MDFF_REC_TC=0, MDFF_FIELD_TC=0) to the CG
 tolerance, on boxes that reach both B-tile widths (kz 7 -> 32 rows, kz 16
 -> 64 rows), a triclinic cell, a box with fewer ions than one K block and an
-odd ion count; both must meet the 1e-5 force bar against the CPU oracle."""
+odd ion count, a box whose polarisable ions sit in two type blocks with a
+non-polarisable block between them (the structure factor's ion slots and the
+fields' ion map are not one index range); both must meet the 1e-5 force bar
+against the CPU oracle."""
 import numpy as np
 import pytest
 
@@ -28,6 +31,8 @@ def _cases():
         systems.random_ionic((19, 18), L=12.0, seed=8, q=(1.2, -1.2), calc=_abi.CALC_OTHER),
         systems.mgo(ncell=2, kmax=16, calc=_abi.CALC_OTHER),
         systems.sio2(nsio2=150, seed=9, calc=_abi.CALC_OTHER),
+        systems.random_ionic((20, 30, 20), L=13.0, seed=17, q=(-1.5, 2.0, -1.5), pol=(1.1, 0.0, 1.1),
+                             calc=_abi.CALC_OTHER),
     ]
 
 
@@ -45,7 +50,7 @@ def _run(s, tc, monkeypatch):
     return r
 
 
-@pytest.mark.parametrize("case", range(6))
+@pytest.mark.parametrize("case", range(7))
 def test_tensor_core_operator_matches_cuda_core(oracle, case, monkeypatch):
     s = _cases()[case]
     a = _run(s, True, monkeypatch)

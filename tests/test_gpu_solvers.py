@@ -100,3 +100,38 @@ def test_cg_md_sequence_matches_oracle(oracle, prec):
         h = eng.aspc_history()
     ho = orc.get_aspc()
     assert rel(h, ho) <= (1e-9 if prec == "fp64" else 1e-5)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_split_polarisable_blocks_md_sequence(oracle, prec):
+    """Polarisable ions in two type blocks with a non-polarisable block between
+    them (types: polarisable anion, cation, polarisable anion), so the ion map
+    of the dipole solve's fields and the ion slots of the tensor-core structure
+    factor are not one index range; an MD sequence with the CG solver and the
+    ASPC predictor (merged first residual, force-pass structure factor from
+    the solve's accumulation) against the oracle at every step: FP64 to 1e-9,
+    mixed within the 1e-5 force bar."""
+    s = systems.random_ionic((20, 30, 20), L=13.0, seed=17, q=(-1.5, 2.0, -1.5), pol=(1.1, 0.0, 1.1),
+                             calc=_abi.CALC_MD, conv_tol_ind=1e-12, max_scf_pol_iter=500,
+                             extrapolate_order=2)
+    orc = oracle.Oracle(params_copy(s.params), s.cell)
+    p = params_copy(s.params)
+    p.solver = _abi.SOLVER_CG
+    p.cg_tol = 1e-12
+    p.cg_max_iter = 500
+    if prec == "mixed":
+        p.precision = _abi.PREC_MIXED
+    rng = np.random.default_rng(23)
+    pos = s.pos.copy()
+    with ForceEngine(p, s.cell) as eng:
+        for itime in range(6):
+            soa = tuple(np.ascontiguousarray(pos[:, a]) for a in range(3))
+            g = eng.engforce(*soa, itime=itime)
+            o = orc.engforce(*soa, itime=itime)
+            if prec == "fp64":
+                compare(g, o, 1e-9)
+            else:
+                assert rms_rel(forces(g), forces(o)) <= 1e-5, itime
+                assert rms_rel(g["mu"], o["mu"]) <= 1e-5, itime
+                assert abs(g["u_coul"] - o["u_coul"]) <= 1e-6 * abs(o["u_coul"]), itime
+            pos = pos + rng.uniform(-0.01, 0.01, pos.shape)

@@ -48,6 +48,18 @@ MODULE engforce_gpu
     real(c_double) :: u_lj, vir_lj, u_bmhft, vir_bmhft, u_coul, u_pol, pvirial_coul
     real(c_double) :: tau_nonb(3,3), tau_coul(3,3), tau(3,3)   ! C [a][b] = transpose
   END TYPE
+  TYPE, bind(c) :: mdff_stats
+    integer(c_int) :: n_pol_iter, converged
+    real(c_double) :: rmsd
+    integer(c_int) :: list_rebuilds, list_capacity, list_needed, nk
+    real(c_double) :: alphaES
+    integer(c_int) :: kES(3)
+    real(c_double) :: cutlongrange
+    integer(c_int) :: n_launches
+    real(c_double) :: ms_last, rmsd_initial
+    integer(c_int) :: n_fp64_residuals
+    integer(c_int) :: n_kardir                 ! in-place kardir/dirkar round trips of the call
+  END TYPE
   INTERFACE
     integer(c_int) FUNCTION mdff_gpu_create(p, cellA, h) bind(c)
       import; type(mdff_params) :: p; real(c_double) :: cellA(9); type(c_ptr) :: h
@@ -59,11 +71,22 @@ MODULE engforce_gpu
     integer(c_int) FUNCTION mdff_gpu_set_cell(h, cellA) bind(c)
       import; type(c_ptr), value :: h; real(c_double) :: cellA(9)
     END FUNCTION
+    integer(c_int) FUNCTION mdff_gpu_get_stats(h, st) bind(c)
+      import; type(c_ptr), value :: h; type(mdff_stats) :: st
+    END FUNCTION
+    integer(c_int) FUNCTION mdff_gpu_kardir_roundtrips(h, rx, ry, rz, count) bind(c)
+      import; type(c_ptr), value :: h; real(c_double) :: rx(*), ry(*), rz(*)
+      integer(c_int), value :: count
+    END FUNCTION
     type(c_ptr) FUNCTION mdff_gpu_strerror(s) bind(c)
       import; integer(c_int), value :: s
     END FUNCTION
   END INTERFACE
   type(c_ptr), save :: handle = c_null_ptr
+  ! .true.: after each call rx, ry, rz hold what the reference's engforce
+  ! leaves in them, its in-place kardir/dirkar round trips included
+  ! (ewald_dir.f90:138,739, non_bonded.f90:1113,1221, moment_from_pola.f90:685,803)
+  logical, save :: mimic_kardir = .false.
   real(c_double), allocatable, target, save :: mu_buf(:,:), ef_buf(:,:)
 CONTAINS
   SUBROUTINE engforce   ! replaces engforce_driver.f90:102-190
@@ -73,6 +96,7 @@ CONTAINS
     USE md, ONLY : itime
     type(mdff_params) :: p
     type(mdff_result) :: res
+    type(mdff_stats) :: stats
     real(c_double), target :: cA(9)
     integer(c_int) :: st
     if ( .not. c_associated(handle) ) then
@@ -96,6 +120,10 @@ CONTAINS
     tau_nonb = transpose(res%tau_nonb); tau_coul = transpose(res%tau_coul)
     tau = transpose(res%tau)                  ! = tau_nonb + 2 tau_coul, as the reference
     mu_t = mu_buf; ef_t = ef_buf
+    if ( mimic_kardir ) then
+      st = mdff_gpu_get_stats(handle, stats)
+      if ( stats%n_kardir .gt. 0 ) st = mdff_gpu_kardir_roundtrips(handle, rx, ry, rz, stats%n_kardir)
+    endif
   END SUBROUTINE engforce
 
   ! the namelist modules after their *_init routines (tables already

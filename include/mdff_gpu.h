@@ -196,7 +196,15 @@ typedef struct mdff_stats {
   double ms_last;                         /* device time of last call (ms)       */
   double rmsd_initial;                    /* CG: rmsd of the first guess (e/A^2) */
   int n_fp64_residuals;                   /* CG: FP64 residual evaluations       */
-  int pad;
+  int n_kardir;                           /* in-place kardir/dirkar round trips
+                                             the reference's engforce makes for
+                                             this call (one per short-range
+                                             routine, per multipole_ES_dir and
+                                             for the Wannier centres); -1 when
+                                             the solve is not the reference's
+                                             SCF.  The MD loop's vnlistcheck
+                                             (runmd.f90:304) adds one more, three
+                                             when it rebuilds (tools.f90:474-526) */
 } mdff_stats;
 
 typedef struct mdff_ctx* mdff_handle;
@@ -233,6 +241,16 @@ int mdff_gpu_engforce(mdff_handle h, const double* rx, const double* ry,
 int mdff_gpu_engforce_device(mdff_handle h, const double* d_pos, int itime,
                              double* d_force, double* d_mu, double* d_ef,
                              mdff_result* out);
+
+/* The reference converts the global positions to direct coordinates and
+   back in place around each pass over the pairs (kardir / dirkar,
+   lattice.f90:183-270; ewald_dir.f90:138,739, non_bonded.f90:1113,1221,
+   moment_from_pola.f90:685,803, tools.f90:474,502), which moves them by an
+   ulp or so each time; the engine leaves the caller's positions alone.  A
+   caller that wants the reference's positions after an engforce applies
+   count = stats.n_kardir round trips here (same cell as the handle; host
+   arrays rx, ry, rz [natm], in place, in the reference's arithmetic). */
+int mdff_gpu_kardir_roundtrips(mdff_handle h, double* rx, double* ry, double* rz, int count);
 
 /* ASPC history dipia_ind_t(5,3,natm) (coulomb.f90:435) for RESTART:
    buf = [MDFF_ASPC_DEPTH][natm][3]. */
@@ -327,7 +345,10 @@ void mdff_gpu_destroy(mdff_handle h);
    history): forces, energies, stress, dipoles and fields, the dipoles from PCG
    (cg_tol, else conv_tol_ind; cg_max_iter).  precision of parameter set 0
    selects FP64 or mixed for the whole batch.  The real-space pairs are all
-   minimum-image pairs within the cutoffs (the Verlet list's pair set). */
+   minimum-image pairs within the cutoffs (the Verlet list's pair set).
+   Thole functions and Wannier centres act as in mdff_gpu_create (a missing
+   centre: MDFF_ERR_BAD_ARGS); the kO dipole algorithms are not built here
+   (MDFF_ERR_UNSUPPORTED: the batch solves with PCG). */
 #define MDFF_BATCH_MAXTYPES 4
 #define MDFF_BATCH_MAXATM 2048
 

@@ -85,7 +85,7 @@ class MdffStats(ctypes.Structure):
         ("list_rebuilds", _i), ("list_capacity", _i), ("list_needed", _i),
         ("nk", _i), ("alphaES", _d), ("kES", _i * 3), ("cutlongrange", _d),
         ("n_launches", _i), ("ms_last", _d), ("rmsd_initial", _d), ("n_fp64_residuals", _i),
-        ("pad", _i),
+        ("n_kardir", _i),
     ]
 
 
@@ -123,6 +123,7 @@ SIGNATURES = {
     "mdff_gpu_engforce_device": (_i, [_P, _P, _i, _P, _P, _P, ctypes.POINTER(MdffResult)]),
     "mdff_gpu_get_aspc_history": (_i, [_P, _DP]),
     "mdff_gpu_set_aspc_history": (_i, [_P, _DP]),
+    "mdff_gpu_kardir_roundtrips": (_i, [_P, _DP, _DP, _DP, _i]),
     "mdff_gpu_get_stats": (_i, [_P, ctypes.POINTER(MdffStats)]),
     "mdff_gpu_verlet_half_list": (_i, [_P, _i, _DP, _DP, _DP, _IP, _IP, _i, _IP]),
     "mdff_gpu_verlet_half_list_noalloc": (_i, [ctypes.POINTER(MdffParams), _DP, _i, _DP, _DP, _DP,

@@ -37,6 +37,35 @@ __device__ __forceinline__ void kardir_exact(const double* B, double x, double y
   sz = xadd(xadd(xmul(x, B[2]), xmul(y, B[5])), xmul(z, B[8]));
 }
 
+// The fourth word of an ion's direct coordinates (s[i].w) carries its FP32
+// charge (bits 0-31), type (bits 32-47) and polarisable flag (bit 48), so that
+// a pair kernel's gather of a neighbour's coordinates brings them along in the
+// same 32-byte sector instead of three more gathers.  Bit patterns only: no
+// arithmetic is ever done on the word.
+__device__ __forceinline__ double ion_tag(float q, int type, int pol) {
+  unsigned long long b = (unsigned long long)(unsigned)__float_as_int(q) |
+                         ((unsigned long long)(type & 0xffff) << 32) |
+                         ((unsigned long long)(pol != 0) << 48);
+  return __longlong_as_double((long long)b);
+}
+__device__ __forceinline__ int tag_type(double w) {
+  return (int)((__double_as_longlong(w) >> 32) & 0xffff);
+}
+__device__ __forceinline__ bool tag_pol(double w) {
+  return ((__double_as_longlong(w) >> 48) & 1) != 0;
+}
+__device__ __forceinline__ float tag_q(double w) {
+  return __int_as_float((int)(__double_as_longlong(w) & 0xffffffffll));
+}
+
+// dirkar (lattice.f90:232-270): x = (s1*A11 + s2*A12) + s3*A13, ...
+__device__ __forceinline__ void dirkar_exact(const double* A, double sx, double sy, double sz,
+                                             double& x, double& y, double& z) {
+  x = xadd(xadd(xmul(sx, A[0]), xmul(sy, A[1])), xmul(sz, A[2]));
+  y = xadd(xadd(xmul(sx, A[3]), xmul(sy, A[4])), xmul(sz, A[5]));
+  z = xadd(xadd(xmul(sx, A[6]), xmul(sy, A[7])), xmul(sz, A[8]));
+}
+
 // Fortran NINT: round half away from zero (C round()).
 __device__ __forceinline__ double fnint(double x) { return round(x); }
 

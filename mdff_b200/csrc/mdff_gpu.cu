@@ -159,6 +159,7 @@ struct mdff_ctx {
   double4 *d_r = nullptr, *d_z = nullptr, *d_pv = nullptr, *d_qv = nullptr, *d_Tp = nullptr;
   float4* d_mu32 = nullptr;      // FP32 copy of the dipoles of an FP32 pass
   float4* d_qm32 = nullptr;      // (mu_tot, q) in FP32 for the mixed final pass
+  double* d_rtpos = nullptr;     // [3][natm] positions of mdff_gpu_kardir_roundtrips
   double4* d_Edd = nullptr;      // cached real-space dipole field of a CG operator (side stream)
   double* d_fsr = nullptr;       // short-range forces SoA [3][natm] (copied into d_force by ef_back)
   double4* d_hist_save = nullptr;  // ASPC history at the start of a call ([5][natm])
@@ -352,6 +353,23 @@ __global__ void k_unpack3(const double* __restrict__ in, int natm, double4* __re
 }
 
 // velocity Verlet halves (prop_velocity_verlet, integration.f90:132-194)
+// count in-place kardir/dirkar round trips (lattice.f90:183-270) of SoA
+// positions [3][natm], in the reference's two-rounding arithmetic
+__global__ void k_kardir_roundtrips(double* __restrict__ pos, int natm,
+                                    const CellC* __restrict__ cell, int count) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= natm) return;
+  double x = pos[i], y = pos[natm + i], z = pos[2 * natm + i];
+  for (int k = 0; k < count; ++k) {
+    double sx, sy, sz;
+    kardir_exact(cell->B, x, y, z, sx, sy, sz);
+    dirkar_exact(cell->A, sx, sy, sz, x, y, z);
+  }
+  pos[i] = x;
+  pos[natm + i] = y;
+  pos[2 * natm + i] = z;
+}
+
 __global__ void k_vv_kick_drift(double* __restrict__ pos, double* __restrict__ vel,
                                 const double* __restrict__ f, const double* __restrict__ invm,
                                 int natm, double dt) {
@@ -1881,7 +1899,8 @@ static int solve_cg(mdff_ctx* h, int itime, bool fp32) {
 static int ef_front(mdff_ctx* h, bool fp32) {
   int n = h->natm, s;
   h->rho_acc_ok = false;
-  PDL_CHECK(pdl_launch(k_kardir, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_pos, n, h->d_cell, h->d_s));
+  PDL_CHECK(pdl_launch(k_kardir, dim3(cdiv(n, 256)), dim3(256), 0, h->st, h->d_pos, n, h->d_cell, h->d_itype,
+                       h->d_ipolar, h->d_q, h->d_s));
   if ((s = list_update(h))) return s;
   CK(cudaMemsetAsync(h->d_scal, 0, sizeof(double) * S_NSCAL, h->st));
   int nbw = cdiv((long)n * 32, 256);
@@ -1996,8 +2015,24 @@ static int ef_back(mdff_ctx* h, bool fp32) {
   return MDFF_OK;
 }
 
+// in-place kardir/dirkar round trips of the global positions that the
+// reference's engforce makes for this call: one per short-range routine
+// (non_bonded.f90:716,823 and :1113,1221), one per multipole_ES_dir
+// (ewald_dir.f90:138,739: the static field, one per SCF iteration, the final
+// pass) and one for the Wannier centres (moment_from_pola.f90:685,803).
+// Defined for the reference's own solver (SCF, algorithm 'scf'); -1 otherwise.
+static int kardir_count(const mdff_ctx* h) {
+  if (h->p.lcoulomb && h->lpolar &&
+      (h->p.solver != MDFF_SOLVER_SCF || h->p.algo_moment_from_pola != MDFF_ALGO_SCF))
+    return -1;
+  int n = (h->p.lnmlj ? 1 : 0) + ((h->p.lbmhft || h->p.lbmhftd) ? 1 : 0);
+  if (h->p.lcoulomb) n += 1 + (h->lpolar ? 1 + h->stats.n_pol_iter : 0) + (h->lwannier ? 1 : 0);
+  return n;
+}
+
 // status of a call from the host copies of its flags (after the sync)
 static int ef_status(mdff_ctx* h) {
+  h->stats.n_kardir = kardir_count(h);
   h->stats.list_rebuilds = h->h_flags[3];
   h->stats.list_needed = h->h_flags[2] * h->natm;
   if (h->h_flags[1]) return MDFF_ERR_LIST_OVERFLOW;
@@ -2602,6 +2637,25 @@ int mdff_gpu_set_aspc_history(mdff_handle h, const double* buf) {
   return MDFF_OK;
 }
 
+int mdff_gpu_kardir_roundtrips(mdff_handle h, double* rx, double* ry, double* rz, int count) {
+  if (!h || !rx || !ry || !rz || count < 0) return MDFF_ERR_BAD_ARGS;
+  CK(cudaSetDevice(h->device));
+  const int n = h->natm;
+  if (n == 0 || count == 0) return MDFF_OK;
+  if (!h->d_rtpos) DALLOC(h->d_rtpos, 3 * (size_t)n);
+  double* host[3] = {rx, ry, rz};
+  for (int a = 0; a < 3; ++a)
+    CK(cudaMemcpyAsync(h->d_rtpos + (size_t)a * n, host[a], sizeof(double) * n,
+                       cudaMemcpyHostToDevice, h->st));
+  k_kardir_roundtrips<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_rtpos, n, h->d_cell, count);
+  LAUNCH_CHECK();
+  for (int a = 0; a < 3; ++a)
+    CK(cudaMemcpyAsync(host[a], h->d_rtpos + (size_t)a * n, sizeof(double) * n,
+                       cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return MDFF_OK;
+}
+
 int mdff_gpu_get_stats(mdff_handle h, mdff_stats* s) {
   if (!h || !s) return MDFF_ERR_BAD_ARGS;
   *s = h->stats;
@@ -2621,7 +2675,8 @@ int mdff_gpu_verlet_half_list(mdff_handle h, int which, const double* rx, const 
   CK(cudaMemcpyAsync(h->d_pos + 2 * (size_t)n, rz, sizeof(double) * n, cudaMemcpyHostToDevice, h->st));
   for (int tries = 0; tries < 4; ++tries) {
     h->launches = 0;
-    k_kardir<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_pos, n, h->d_cell, h->d_s);
+    k_kardir<<<cdiv(n, 256), 256, 0, h->st>>>(h->d_pos, n, h->d_cell, h->d_itype, h->d_ipolar, h->d_q,
+                                                h->d_s);
     LAUNCH_CHECK();
     h->have_list = false;
     if ((s = list_update(h))) return s;
@@ -2849,7 +2904,8 @@ void mdff_gpu_destroy(mdff_handle h) {
                   h->d_ddb1, h->d_ddj, h->d_ddn, h->d_efg, h->d_fb, h->d_ko_f, h->d_ko_dmu,
                   h->d_ko_g, h->d_ko_muprev, h->d_ko_fdir, h->d_Fh, h->d_muh, h->d_ko_x, h->d_part2,
                   h->d_lwfc, h->d_mu_wfc, h->d_qm32, h->d_Edd, h->d_fsr, h->d_hist_save,
-                  h->d_rho_timg, h->d_polidx, h->d_rho_acc, h->d_w32s, h->d_polslot};
+                  h->d_rho_timg, h->d_polidx, h->d_rho_acc, h->d_w32s, h->d_polslot,
+                  h->d_rtpos};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   step_graph_free(h);

@@ -30,15 +30,17 @@ struct ListDev {
 };
 
 // direct coordinates (kardir) of the Cartesian SoA positions
+// with the ion's tag (charge, type, polarisable flag) in the fourth word
 __global__ void k_kardir(const double* __restrict__ pos, int natm, const CellC* __restrict__ cell,
-                         double4* __restrict__ s) {
+                         const int* __restrict__ itype, const int* __restrict__ ipolar,
+                         const double* __restrict__ q, double4* __restrict__ s) {
   pdl_wait();
   pdl_trigger();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= natm) return;
   double sx, sy, sz;
   kardir_exact(cell->B, pos[i], pos[natm + i], pos[2 * natm + i], sx, sy, sz);
-  s[i] = make_double4(sx, sy, sz, 0.0);
+  s[i] = make_double4(sx, sy, sz, ion_tag((float)q[i], itype[i], ipolar[i]));
 }
 
 // vnlistcheck: largest and second largest displacement since the last build

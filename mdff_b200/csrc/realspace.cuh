@@ -34,11 +34,38 @@ struct ESPair {        // per ordered role pair (ta = type of "ia", tb = type of
   double th_a, th_A;   // thole_param(ta,tb), (alpha_xx(ta) alpha_xx(tb))^(1/6)
 };
 
+// FP32 copy of an ESPair for the FP32 passes: the damping and Thole
+// parameters converted once per block instead of once per pair visit
+struct ESPairF {
+  int ldamp, ka, kb, thole;
+  float ba, ca, bb, cb;
+  float th_a, th_A;
+};
+__device__ __forceinline__ ESPairF espair_f(const ESPair& P) {
+  return ESPairF{P.ldamp, P.ka, P.kb, P.thole, (float)P.ba, (float)P.ca, (float)P.bb,
+                 (float)P.cb, (float)P.th_a, (float)P.th_A};
+}
+// the table a pass of precision R keeps in shared memory
+template <typename R>
+struct espair_t {
+  typedef ESPair T;
+};
+template <>
+struct espair_t<float> {
+  typedef ESPairF T;
+};
+template <typename PT>
+__device__ __forceinline__ PT espair_as(const ESPair& P);
+template <>
+__device__ __forceinline__ ESPair espair_as<ESPair>(const ESPair& P) { return P; }
+template <>
+__device__ __forceinline__ ESPairF espair_as<ESPairF>(const ESPair& P) { return espair_f(P); }
+
 // Thole functions on the dipole-dipole tensor (ewald_dir.f90:305-430): the
 // radial functions F1, F2 of T2 = 3 r r F2 / d^5 - F1 / d^3 for the field and
 // energy of a pair of polarisable ions (the force keeps the plain tensor)
-template <typename R>
-__device__ __forceinline__ void thole_radial(const ESPair& P, R d, R& F1, R& F2) {
+template <typename R, typename PT = ESPair>
+__device__ __forceinline__ void thole_radial(const PT& P, R d, R& F1, R& F2) {
   switch (P.thole) {
     case 1: {  // linear: no Ewald screening inside s = a A (:316-347)
       R sth = (R)(P.th_a * P.th_A);
@@ -141,7 +168,7 @@ __device__ __forceinline__ void sr_pair_lj(const NBPair& P, int trunc, R rijsq, 
 // MODE bit 0: BMH / BMHFTD (+ wall), bit 1: n-m LJ.  One instantiation per
 // mode keeps the accumulators of the absent potential out of the registers.
 template <typename R, int MODE>
-static __global__ void __launch_bounds__(256, MODE == 3 ? 2 : 3) k_shortrange(
+static __global__ void __launch_bounds__(256, MODE == 3 ? 2 : 4) k_shortrange(
     const double4* __restrict__ s, const int* __restrict__ itype, const int* __restrict__ nbr,
     const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
     const NBPair* __restrict__ tab, int ntype, int lbmhftd, int trunc,
@@ -165,7 +192,7 @@ static __global__ void __launch_bounds__(256, MODE == 3 ? 2 : 3) k_shortrange(
     for (int k = lane; k < n; k += 32) {
       int j = row[k];
       double4 sj = s[j];
-      int tj = itype[j];
+      int tj = tag_type(sj.w);
       double rxd, ryd, rzd;
       double r2d = min_image_exact(cell->A, xsub(si.x, sj.x), xsub(si.y, sj.y), xsub(si.z, sj.z),
                                    rxd, ryd, rzd);
@@ -358,6 +385,17 @@ __device__ __forceinline__ float pair_vec<float>(const double* A, double4 si, do
   return rx * rx + ry * ry + rz * rz;
 }
 
+// the same FP32 pair vector with the cell matrix already in FP32 registers
+__device__ __forceinline__ float pair_vec_f(const float (&A)[9], double4 si, double4 sj, float& rx,
+                                            float& ry, float& rz) {
+  double ddx = si.x - sj.x, ddy = si.y - sj.y, ddz = si.z - sj.z;
+  float dx = (float)(ddx - rint(ddx)), dy = (float)(ddy - rint(ddy)), dz = (float)(ddz - rint(ddz));
+  rx = dx * A[0] + dy * A[1] + dz * A[2];
+  ry = dx * A[3] + dy * A[4] + dz * A[5];
+  rz = dx * A[6] + dy * A[7] + dz * A[8];
+  return rx * rx + ry * ry + rz * rz;
+}
+
 // field at i from j of the field-only passes (k_es_field): the charge field
 // q_j r dm3 (F1 - F1d) with the pair's damping roles, and the dipole field
 // T2 . mu_j (ewald_dir.f90:533-541, 566-571); added into (ex, ey, ez).
@@ -503,11 +541,14 @@ static __global__ void __launch_bounds__(256) k_static_cache(
     double alpha, double cutsq, int has_q, double4* __restrict__ E, float4* __restrict__ cr,
     float* __restrict__ cb1, int* __restrict__ cj, int* __restrict__ cn, int thole = 0,
     const double4* __restrict__ x0 = nullptr) {
-  __shared__ ESPair stab[MDFF_NT * MDFF_NT];
+  __shared__ ESPairF stab[MDFF_NT * MDFF_NT];
   __shared__ double cA[9];
-  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
+  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = espair_f(tab[k]);
   if (threadIdx.x < 9) cA[threadIdx.x] = cell->A[threadIdx.x];
   __syncthreads();
+  float A32[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) A32[k] = (float)cA[k];
   int lane = threadIdx.x & 31;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= natm) return;
@@ -535,28 +576,28 @@ static __global__ void __launch_bounds__(256) k_static_cache(
     if (k < n) {
       j = row[k];
       double4 sj = s[j];
-      float r2 = pair_vec<float>(cA, si, sj, rx, ry, rz);
+      float r2 = pair_vec_f(A32, si, sj, rx, ry, rz);
       if (r2 <= rc2) {  // ewald_dir.f90:202
-        double qj = has_q ? q[j] : 0.0;
-        bool pp = pol_i && ipolar[j] != 0;
-        if (pp || qj != 0.0) {
+        const float qj = has_q ? tag_q(sj.w) : 0.f;
+        const bool pp = pol_i && tag_pol(sj.w);
+        if (pp || qj != 0.f) {
           Radial<float> g;
           radial<float, false>(r2, (float)alpha, g);
-          if (qj != 0.0) {
+          if (qj != 0.f) {
             float F1d = 0.f;
-            int tj = itype[j];
+            const int tj = tag_type(sj.w);
             bool i_is_a = half_mask(i, j);
             int ta = i_is_a ? ti : tj, tb = i_is_a ? tj : ti;
-            const ESPair& P = stab[ta * ntype + tb];
-            if (P.ldamp && (i_is_a ? P.ca : P.cb) != 0.0) {  // c = 0 damps nothing
+            const ESPairF& P = stab[ta * ntype + tb];
+            if (P.ldamp && (i_is_a ? P.ca : P.cb) != 0.f) {  // c = 0 damps nothing
               float fdm, fdd;
               if (i_is_a)
-                tt_damp_k<float, K>((float)P.ba, (float)P.ca, g.d, P.ka, fdm, fdd);
+                tt_damp_k<float, K>(P.ba, P.ca, g.d, P.ka, fdm, fdd);
               else
-                tt_damp_k<float, K>((float)P.bb, (float)P.cb, g.d, P.kb, fdm, fdd);
+                tt_damp_k<float, K>(P.bb, P.cb, g.d, P.kb, fdm, fdd);
               F1d = 1.f - fdm;
             }
-            float c = (float)qj * g.dm3 * (g.F1 - F1d);
+            float c = qj * g.dm3 * (g.F1 - F1d);
             ex += c * rx;
             ey += c * ry;
             ez += c * rz;
@@ -565,10 +606,10 @@ static __global__ void __launch_bounds__(256) k_static_cache(
             keep = true;
             float F1 = g.F1, F2 = g.F2;
             if (thole) {
-              int tj = itype[j];
+              const int tj = tag_type(sj.w);
               bool i_is_a = half_mask(i, j);
-              const ESPair& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
-              if (P.thole) thole_radial<float>(P, g.d, F1, F2);
+              const ESPairF& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
+              if (P.thole) thole_radial<float, ESPairF>(P, g.d, F1, F2);
             }
             B1 = F1 * g.dm3;
             B2 = 3.f * F2 * g.dm5;
@@ -727,8 +768,8 @@ constexpr int kESPart = 7;
 //   u   = q_i q_j B0 + dd: -(m_i.T2.m_j) + qd: q_i (B1 - B1d_j)(r.m_j) - q_j (B1 - B1d_i)(r.m_i)
 // (f_i = the reference's -f_ij when i is "ia", +f_ij when i is "ja").  Only
 // i's field is formed.  K: compile-time Tang-Toennies order (0 = per pair).
-template <typename R, int K, bool THOLE>
-__device__ __forceinline__ void es_force_ipair(const ESPair& P, bool i_is_a, bool ldamp, R d2,
+template <typename R, int K, bool THOLE, typename PT = ESPair>
+__device__ __forceinline__ void es_force_ipair(const PT& P, bool i_is_a, bool ldamp, R d2,
                                                R alpha, const R (&r)[3], R qi, R qj,
                                                const R (&mi)[3], const R (&mj)[3], bool dip_i,
                                                bool dip_j, int task_qq, int task_qd, int task_dd,
@@ -770,7 +811,7 @@ __device__ __forceinline__ void es_force_ipair(const ESPair& P, bool i_is_a, boo
     R B1t = B1, B2t = B2;
     if (THOLE && P.thole) {
       R F1t = g.F1, F2t = g.F2;
-      thole_radial<R>(P, g.d, F1t, F2t);
+      thole_radial<R, PT>(P, g.d, F1t, F2t);
       B1t = F1t * g.dm3;
       B2t = R(3) * F2t * g.dm5;
     }
@@ -822,20 +863,41 @@ __device__ __forceinline__ void load_qm<float>(const double*, const double4*, co
 
 // final real-space pass, warp per ion over the full list; each visit of a
 // pair adds i's force and field and half the pair's energy and stress.
+// A lane sums its visits in R (FP32 in the mixed engine: about nine visits
+// per lane on the 12k glass, so no FP64 conversion and add per visit) and the
+// lanes' sums are widened to FP64 for the warp and block reductions.
+template <typename R>
+__device__ __forceinline__ R pvec(const double* A, const float (&A32)[9], double4 si, double4 sj,
+                                  R (&r)[3]);
+template <>
+__device__ __forceinline__ double pvec<double>(const double* A, const float (&)[9], double4 si,
+                                               double4 sj, double (&r)[3]) {
+  return pair_vec<double>(A, si, sj, r[0], r[1], r[2]);
+}
+template <>
+__device__ __forceinline__ float pvec<float>(const double*, const float (&A32)[9], double4 si,
+                                             double4 sj, float (&r)[3]) {
+  return pair_vec_f(A32, si, sj, r[0], r[1], r[2]);
+}
+
 template <typename R, int K, bool THOLE>
-static __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_es_force(
+static __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2) k_es_force(
     const double4* __restrict__ s, const double* __restrict__ q, const int* __restrict__ itype,
     const double4* __restrict__ mu, const float4* __restrict__ qm32, const int* __restrict__ nbr,
     const int* __restrict__ nnb, int cap, int natm, const CellC* __restrict__ cell,
     const ESPair* __restrict__ tab, int ntype, double alpha, double cutsq, int task_qq,
     int task_qd, int task_dd, int damp_ind, double fscale, double4* __restrict__ E,
     double* __restrict__ force /* SoA [3][natm], += */, double* __restrict__ part) {
-  __shared__ ESPair stab[MDFF_NT * MDFF_NT];
+  typedef typename espair_t<R>::T PT;
+  __shared__ PT stab[MDFF_NT * MDFF_NT];
   __shared__ double cA[9];
   __shared__ double red[kESPart * 8];
-  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = tab[k];
+  for (int k = threadIdx.x; k < ntype * ntype; k += blockDim.x) stab[k] = espair_as<PT>(tab[k]);
   if (threadIdx.x < 9) cA[threadIdx.x] = cell->A[threadIdx.x];
   __syncthreads();
+  float A32[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) A32[k] = (float)cA[k];
   int lane = threadIdx.x & 31;
   int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   double acc[kESPart];
@@ -850,45 +912,56 @@ static __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_es_force
     const int n = nnb[i];
     const int* row = nbr + (size_t)i * cap;
     const R rc2 = (R)cutsq, ra = (R)alpha;
-    double e[3] = {0, 0, 0}, f[3] = {0, 0, 0};
+    R e[3] = {0, 0, 0}, f[3] = {0, 0, 0};
+    R la[kESPart];
+#pragma unroll
+    for (int k = 0; k < kESPart; ++k) la[k] = R(0);
     for (int k = lane; k < n; k += 32) {
       const int j = row[k];
+      const double4 sj = s[j];
       R r[3];
-      const R r2 = pair_vec<R>(cA, si, s[j], r[0], r[1], r[2]);
+      const R r2 = pvec<R>(cA, A32, si, sj, r);
       if (r2 > rc2) continue;  // ewald_dir.f90:202 ( d2 .gt. cutsq ) cycle
       R qj, mj[3];
       load_qm<R>(q, mu, qm32, j, qj, mj);
       const bool dip_j = mj[0] != R(0) || mj[1] != R(0) || mj[2] != R(0);
-      const int tj = itype[j];
+      const int tj = tag_type(sj.w);
       const bool i_is_a = half_mask(i, j);
-      const ESPair& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
+      const PT& P = stab[(i_is_a ? ti : tj) * ntype + (i_is_a ? tj : ti)];
       R u, fi[3], Ei[3];
-      es_force_ipair<R, K, THOLE>(P, i_is_a, damp_ind && P.ldamp, r2, ra, r, qi, qj, mi, mj, dip_i,
-                                  dip_j, task_qq, task_qd, task_dd, u, fi, Ei);
+      es_force_ipair<R, K, THOLE, PT>(P, i_is_a, damp_ind && P.ldamp, r2, ra, r, qi, qj, mi, mj,
+                                      dip_i, dip_j, task_qq, task_qd, task_dd, u, fi, Ei);
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        f[c] += (double)fi[c];
-        e[c] += (double)Ei[c];
+        f[c] += fi[c];
+        e[c] += Ei[c];
       }
-      acc[0] += 0.5 * (double)u;
-      acc[1] += (double)(r[0] * fi[0]);
-      acc[2] += (double)(r[1] * fi[1]);
-      acc[3] += (double)(r[2] * fi[2]);
-      acc[4] += 0.5 * (double)(r[0] * fi[1] + r[1] * fi[0]);
-      acc[5] += 0.5 * (double)(r[0] * fi[2] + r[2] * fi[0]);
-      acc[6] += 0.5 * (double)(r[1] * fi[2] + r[2] * fi[1]);
+      la[0] += u;
+      la[1] += r[0] * fi[0];
+      la[2] += r[1] * fi[1];
+      la[3] += r[2] * fi[2];
+      la[4] += r[0] * fi[1] + r[1] * fi[0];
+      la[5] += r[0] * fi[2] + r[2] * fi[0];
+      la[6] += r[1] * fi[2] + r[2] * fi[1];
     }
+    // halves of the pair energy and of the off-diagonal stress sums
+    acc[0] = 0.5 * (double)la[0];
+#pragma unroll
+    for (int k = 1; k < 4; ++k) acc[k] = (double)la[k];
+#pragma unroll
+    for (int k = 4; k < kESPart; ++k) acc[k] = 0.5 * (double)la[k];
+    double ed[3], fd[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      e[c] = warp_sum(e[c]);
-      f[c] = warp_sum(f[c]);
+      ed[c] = warp_sum((double)e[c]);
+      fd[c] = warp_sum((double)f[c]);
     }
     if (lane == 0) {
       double4 o = E[i];
-      E[i] = make_double4(o.x + e[0], o.y + e[1], o.z + e[2], 0.0);
-      force[i] += f[0] * fscale;
-      force[natm + i] += f[1] * fscale;
-      force[2 * natm + i] += f[2] * fscale;
+      E[i] = make_double4(o.x + ed[0], o.y + ed[1], o.z + ed[2], 0.0);
+      force[i] += fd[0] * fscale;
+      force[natm + i] += fd[1] * fscale;
+      force[2 * natm + i] += fd[2] * fscale;
     }
   }
   block_sum<kESPart>(acc, red);

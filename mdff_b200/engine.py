@@ -131,6 +131,20 @@ class ForceEngine:
         b = np.ascontiguousarray(b, dtype=np.float64)
         self._check(self._lib.mdff_gpu_set_aspc_history(self._h, dptr(b)), "set_aspc_history")
 
+    def kardir_roundtrips(self, rx, ry, rz, count=None):
+        """The positions after the reference's in-place kardir/dirkar round
+        trips (lattice.f90:183-270), as new arrays: ``count`` of them, by
+        default the number the reference's engforce made for the last call
+        (``stats()["n_kardir"]``)."""
+        if count is None:
+            count = self.stats()["n_kardir"]
+            if count < 0:
+                raise ValueError("the last call's solve is not the reference's SCF")
+        rx, ry, rz = (np.array(a, dtype=np.float64) for a in (rx, ry, rz))
+        self._check(self._lib.mdff_gpu_kardir_roundtrips(self._h, dptr(rx), dptr(ry), dptr(rz),
+                                                         int(count)), "kardir_roundtrips")
+        return rx, ry, rz
+
     def verlet_half_list(self, rx, ry, rz, which, capacity=None):
         n = self.natm
         cap = capacity if capacity is not None else n * 2000

@@ -41,6 +41,7 @@ static const double PI = 3.14159265358979323846264338327950;
 struct or_ctx {
   mdff_params p;      /* after symmetrisation / clamp / lautoES */
   int natm;
+  int n_kardir;       /* in-place kardir/dirkar round trips of this engforce */
   int* itype;         /* [natm] 0-based */
   int* ipolar;        /* [natm] */
   double* qia;        /* [natm] */
@@ -158,6 +159,29 @@ static void or_kardir(const or_ctx* c, const double* rx, const double* ry, const
     sx[n] = vx * B[0][0] + vy * B[1][0] + vz * B[2][0];
     sy[n] = vx * B[0][1] + vy * B[1][1] + vz * B[2][1];
     sz[n] = vx * B[0][2] + vy * B[1][2] + vz * B[2][2];
+  }
+}
+
+/* The reference converts the global positions to direct coordinates and
+   back IN PLACE around each pass over the pairs (kardir lattice.f90:183-225,
+   dirkar :232-270; e.g. ewald_dir.f90:138,739).  One round trip: V = r B
+   then r = A V, each component summed left to right. */
+void or_kardir_roundtrips(or_ctx* c, double* rx, double* ry, double* rz, int count) {
+  const double(*A)[3] = c->A;
+  const double(*B)[3] = c->B;
+  for (int n = 0; n < c->natm; ++n) {
+    double vx = rx[n], vy = ry[n], vz = rz[n];
+    for (int k = 0; k < count; ++k) {
+      double v1 = vx * B[0][0] + vy * B[1][0] + vz * B[2][0];
+      double v2 = vx * B[0][1] + vy * B[1][1] + vz * B[2][1];
+      double v3 = vx * B[0][2] + vy * B[1][2] + vz * B[2][2];
+      vx = v1 * A[0][0] + v2 * A[0][1] + v3 * A[0][2];
+      vy = v1 * A[1][0] + v2 * A[1][1] + v3 * A[1][2];
+      vz = v1 * A[2][0] + v2 * A[2][1] + v3 * A[2][2];
+    }
+    rx[n] = vx;
+    ry[n] = vy;
+    rz[n] = vz;
   }
 }
 
@@ -1241,6 +1265,7 @@ static void multipole_ES(or_ctx* c, const double* rx, const double* ry, const do
   rec.f = calloc((size_t)natm * 3, sizeof(double));
   rec.efg = calloc((size_t)natm * 9, sizeof(double));
   es_dir(c, sx, sy, sz, L, q, mu, task, damp_ind, do_efield, do_efg, do_forces, do_stress, &dir);
+  c->n_kardir++; /* ewald_dir.f90:138,739 */
   if (do_rec) es_rec(c, rx, ry, rz, q, mu, task, do_efield, do_efg, do_forces, do_stress, &rec);
 
   double u_surf = (qtot[0] * qtot[0] + qtot[1] * qtot[1] + qtot[2] * qtot[2]) +
@@ -1854,6 +1879,7 @@ int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
   memset(out->tau_coul, 0, sizeof(out->tau_coul));
   out->u_lj = out->vir_lj = out->u_bmhft = out->vir_bmhft = 0.0;
   out->u_coul = out->u_pol = out->pvirial_coul = 0.0;
+  c->n_kardir = 0;
   if (ex) {
     ex->n_scf = 0;
     ex->rmsd = 0.0;
@@ -1864,10 +1890,12 @@ int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
     build_half(c, sx, sy, sz, c->p.cutshortrange, &Lv);
     if (c->p.lnmlj) {
       or_nmlj(c, sx, sy, sz, &Lv, fx, fy, fz, &out->u_lj, &out->vir_lj, out->tau_nonb);
+      c->n_kardir++; /* non_bonded.f90:716,823 */
       for (int a = 0; a < 9; ++a) (&out->tau[0][0])[a] += (&out->tau_nonb[0][0])[a];
     }
     if (c->p.lbmhft || c->p.lbmhftd) {
       or_bmhftd(c, sx, sy, sz, &Lv, fx, fy, fz, &out->u_bmhft, &out->vir_bmhft, out->tau_nonb);
+      c->n_kardir++; /* non_bonded.f90:1113,1221 */
       for (int a = 0; a < 9; ++a) (&out->tau[0][0])[a] += (&out->tau_nonb[0][0])[a];
     }
     free_csr(&Lv);
@@ -1928,6 +1956,7 @@ int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
       if (lwannier) {
         double* mw = calloc(n3, sizeof(double));
         status = moment_from_wfc(c, sx, sy, sz, mw);
+        c->n_kardir++; /* moment_from_pola.f90:685,803 */
         if (status == MDFF_OK && c->p.ldip_wfc)
           for (size_t i = 0; i < n3; ++i) mu[i] = mu[i] + mw[i];
         free(mw);
@@ -1975,5 +2004,6 @@ int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
   free(fx);
   free(fy);
   free(fz);
+  if (ex) ex->n_kardir = c->n_kardir;
   return status;
 }

@@ -28,6 +28,7 @@ typedef struct or_extra {
   int n_scf;          /* out: SCF iterations                                 */
   double rmsd;        /* out: final SCF rmsd                                 */
   double u_dir, u_rec, u_self, u_surf; /* out: parts of the final u_coul (internal units) */
+  int n_kardir;       /* out: in-place kardir/dirkar round trips of the call  */
 } or_extra;
 
 or_ctx* or_create(const mdff_params* p, const double cell_A[9], int* status);
@@ -38,6 +39,10 @@ int or_get_threads(void);
 /* engforce (engforce_driver.f90:102-190).  ex may be NULL. */
 int or_engforce(or_ctx* c, const double* rx, const double* ry, const double* rz,
                 int itime, mdff_result* out, or_extra* ex);
+
+/* count in-place kardir/dirkar round trips (lattice.f90:183-270) of the
+   positions with the context's cell */
+void or_kardir_roundtrips(or_ctx* c, double* rx, double* ry, double* rz, int count);
 
 /* vnlist_pbc (tools.f90:273-368): which = 0 vdw, 1 coul; 1-based CSR. */
 int or_vnlist(or_ctx* c, const double* rx, const double* ry, const double* rz,

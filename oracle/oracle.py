@@ -28,7 +28,8 @@ class Extra(ctypes.Structure):
     _fields_ = [("efg", ctypes.POINTER(ctypes.c_double)), ("do_efg", ctypes.c_int),
                 ("n_scf", ctypes.c_int), ("rmsd", ctypes.c_double),
                 ("u_dir", ctypes.c_double), ("u_rec", ctypes.c_double),
-                ("u_self", ctypes.c_double), ("u_surf", ctypes.c_double)]
+                ("u_self", ctypes.c_double), ("u_surf", ctypes.c_double),
+                ("n_kardir", ctypes.c_int)]
 
 
 def build():
@@ -56,6 +57,8 @@ def lib():
         L.or_vnlist.argtypes = [P, DP, DP, DP, ctypes.c_int, IP, IP, ctypes.c_int, IP]
         L.or_vnlistcheck.restype = ctypes.c_int
         L.or_vnlistcheck.argtypes = [P, DP, DP, DP, DP, IP]
+        L.or_kardir_roundtrips.argtypes = [P, DP, DP, DP, ctypes.c_int]
+        L.or_kardir_roundtrips.restype = None
         L.or_get_aspc.argtypes = [P, DP]
         L.or_set_aspc.argtypes = [P, DP]
         L.or_get_setup.argtypes = [P, ctypes.POINTER(SetupInfo)]
@@ -153,9 +156,17 @@ class Oracle:
         for k in ("tau_nonb", "tau_coul", "tau"):
             out[k] = np.array([[getattr(r, k)[a][b] for b in range(3)] for a in range(3)])
         out["n_scf"] = ex.n_scf
+        out["n_kardir"] = ex.n_kardir
         out["rmsd"] = ex.rmsd
         out["u_parts"] = dict(dir=ex.u_dir, rec=ex.u_rec, self=ex.u_self, surf=ex.u_surf)
         return out
+
+    def kardir_roundtrips(self, rx, ry, rz, count):
+        """The positions after ``count`` in-place kardir/dirkar round trips
+        (lattice.f90:183-270), as new arrays."""
+        rx, ry, rz = (np.array(a, dtype=np.float64) for a in (rx, ry, rz))
+        lib().or_kardir_roundtrips(self._h, _abi.dptr(rx), _abi.dptr(ry), _abi.dptr(rz), int(count))
+        return rx, ry, rz
 
     def vnlist(self, rx, ry, rz, which, capacity=None):
         n = self.natm

@@ -107,7 +107,8 @@ def _fortran_layout(block):
     return out, (off + 7) // 8 * 8
 
 
-@pytest.mark.parametrize("tname,ctype", [("mdff_params", _abi.MdffParams), ("mdff_result", _abi.MdffResult)])
+@pytest.mark.parametrize("tname,ctype", [("mdff_params", _abi.MdffParams), ("mdff_result", _abi.MdffResult),
+                                         ("mdff_stats", _abi.MdffStats)])
 def test_fortran_shim_type_matches_header(tname, ctype):
     """The bind(c) derived types of the Fortran shim include/engforce_gpu.f90
     have the header's fields, in order, at the header's offsets, and the

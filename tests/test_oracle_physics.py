@@ -71,3 +71,37 @@ def test_tang_toennies_closed_form(oracle):
     # the reference's order-0 quirk (tt_damp.f90:85-93): f = 1 - c(1+br)e^{-br}
     f, fd = oracle.tt_damp(2.0, 1.0, 1.0, 0)
     assert abs(f - (1 - 3.0 * math.exp(-2.0))) < 1e-14
+
+
+def test_oracle_kardir_roundtrips_match_numpy(oracle):
+    """The oracle's in-place round trip (kardir then dirkar, lattice.f90:183-270)
+    restated in numpy with the same left-to-right sums: bit for bit."""
+    from mdff_b200 import _abi, systems
+    s = systems.random_ionic((20, 28), L=13.5, seed=22, triclinic=True, calc=_abi.CALC_OTHER)
+    orc = oracle.Oracle(s.params, s.cell)
+    A = np.asarray(s.cell, dtype=np.float64).reshape(3, 3)
+    B = np.array(orc.setup().B[:], dtype=np.float64).reshape(3, 3)
+    x, y, z = (np.array(a, dtype=np.float64) for a in s.soa())
+    for _ in range(7):
+        v1 = x * B[0, 0] + y * B[1, 0] + z * B[2, 0]
+        v2 = x * B[0, 1] + y * B[1, 1] + z * B[2, 1]
+        v3 = x * B[0, 2] + y * B[1, 2] + z * B[2, 2]
+        x = v1 * A[0, 0] + v2 * A[0, 1] + v3 * A[0, 2]
+        y = v1 * A[1, 0] + v2 * A[1, 1] + v3 * A[1, 2]
+        z = v1 * A[2, 0] + v2 * A[2, 1] + v3 * A[2, 2]
+    r = orc.kardir_roundtrips(*s.soa(), 7)
+    for a, b in zip(r, (x, y, z)):
+        assert np.array_equal(a, b)
+
+
+def test_oracle_counts_the_reference_roundtrips(oracle):
+    """One round trip per short-range routine, per multipole_ES_dir (static
+    field, each SCF iteration, final pass) and for the Wannier centres."""
+    from mdff_b200 import _abi, systems
+    s = systems.mgo(ncell=2, calc=_abi.CALC_OTHER)
+    o = oracle.Oracle(s.params, s.cell).engforce(*s.soa())
+    assert o["n_scf"] > 0
+    assert o["n_kardir"] == 1 + (1 + o["n_scf"] + 1)
+    s = systems.nacl(ncell=2, rcut=12.0, kmax=6)
+    o = oracle.Oracle(s.params, s.cell).engforce(*s.soa())
+    assert o["n_kardir"] == 1 + 1

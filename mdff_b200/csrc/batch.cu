@@ -277,7 +277,14 @@ int finish(mdff_batch* h, mdff_batch_conf* conf) {
     const double* sc = h->h_out + (size_t)c * kBSlots;
     int cata = sc[BS_CATA] != 0.0;
     int conv = (h->conf[c].flags & BF_POLAR) ? (sc[BS_CONV] != 0.0) : 1;
-    if (cata) status = MDFF_ERR_CATASTROPHE;
+    if ((h->conf[c].flags & BF_WFC) && sc[BS_STAT] != 0.0) {
+      status = (int)sc[BS_STAT];
+      h->err = "configuration " + std::to_string(c) +
+               ": a Wannier centre is missing for an ion of a type with lwfc > 0 "
+               "(moment_from_pola.f90:731-737)";
+    } else if (cata && status != MDFF_ERR_BAD_ARGS) {
+      status = MDFF_ERR_CATASTROPHE;
+    }
     else if (!conv && h->pconf[c].fail_on_nonconvergence && status == MDFF_OK)
       status = MDFF_ERR_NOT_CONVERGED;
     if (!conf) continue;
@@ -307,6 +314,7 @@ int finish(mdff_batch* h, mdff_batch_conf* conf) {
     o.pad = 0;
   }
   if (status == MDFF_ERR_CATASTROPHE) h->err = "polarisation catastrophe (moment_from_pola.f90:176-216)";
+  if (status == MDFF_ERR_BAD_ARGS) return status;
   if (status == MDFF_ERR_NOT_CONVERGED) h->err = "dipole solve did not converge";
   return status;
 }
@@ -351,11 +359,6 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
       h->err = "the kO dipole algorithms are not built into the batched engine (use mdff_gpu_create)";
       return MDFF_ERR_UNSUPPORTED;
     }
-    for (int t = 0; t < MDFF_NTYPEMAX; ++t)
-      if (p.lwfc[t] != 0) {
-        h->err = "Wannier centres are not built into the batched engine (use mdff_gpu_create)";
-        return MDFF_ERR_UNSUPPORTED;
-      }
     h->pset_of.push_back(ps);
     long n = 0;
     for (int t = 0; t < MDFF_NTYPEMAX; ++t) {
@@ -402,6 +405,13 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
     if (P.lsurf) fl |= BF_SURF;
     if (P.thole_type != MDFF_THOLE_NONE) fl |= BF_THOLE;
     if (S.ldip_static) fl |= BF_DIPST;
+    // Wannier centres (moment_from_pola.f90:130-147): a type with lwfc > 0
+    for (int t = 0; t < P.ntype; ++t) {
+      B.lwfc[t] = P.lwfc[t];
+      if (P.lcoulomb && P.lwfc[t] > 0) fl |= BF_WFC;
+    }
+    B.ldip_wfc = P.ldip_wfc;
+    B.rcut_wfc = P.rcut_wfc;
     B.flags = fl;
     B.trunc = P.trunc;
     B.maxit = P.cg_max_iter > 0 ? P.cg_max_iter : 200;
@@ -737,6 +747,10 @@ int mdff_gpu_batch_fit_define(mdff_batch_handle h, int nparam, const int* kind, 
     }
     if (h->pconf[c].thole_type != MDFF_THOLE_NONE) {
       h->err = "the fit gradient does not cover Thole functions";
+      return MDFF_ERR_UNSUPPORTED;
+    }
+    if (h->conf[c].flags & BF_WFC) {
+      h->err = "the fit gradient does not cover Wannier centres";
       return MDFF_ERR_UNSUPPORTED;
     }
   }

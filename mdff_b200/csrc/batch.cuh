@@ -56,7 +56,8 @@ enum {
 
 enum {
   BF_COUL = 1, BF_SR = 2, BF_BMH = 4, BF_BMHFTD = 8, BF_LJ = 16, BF_POLAR = 32,
-  BF_QQ = 64, BF_QD = 128, BF_DD = 256, BF_SURF = 512, BF_DIPST = 1024, BF_THOLE = 2048
+  BF_QQ = 64, BF_QD = 128, BF_DD = 256, BF_SURF = 512, BF_DIPST = 1024, BF_THOLE = 2048,
+  BF_WFC = 4096
 };
 
 struct BConf {
@@ -69,6 +70,9 @@ struct BConf {
   int nb_off, es_off, pad0, pad1;
   double A[9], B[9], omega;
   double alpha, rc2, coul_unit, tol;
+  int lwfc[kBMaxT];      // Wannier centres per type (BF_WFC): < 0 centre type
+  int ldip_wfc, pad2;
+  double rcut_wfc;
 };
 
 struct BatchArgs {
@@ -907,9 +911,10 @@ __device__ void bconfig(cgx::cluster_group& cl, const BatchArgs& a, BCtx& X, con
     bsolve<MIXED>(cl, a, X, S, a.Estat, a.x, tol, c.maxit, iters, rmsd);
     conv = rmsd <= tol ? 1 : 0;
   }
-  // ---- u_pol, total dipoles, catastrophe ---------------------------------
+  // ---- u_pol, total dipoles (+ Wannier centres), catastrophe -------------
   {
-    double v[2] = {0.0, 0.0};
+    const bool wfc = (c.flags & BF_WFC) != 0;
+    double v[3] = {0.0, 0.0, 0.0};
     for (int i = X.i0 + threadIdx.x; i < X.i1; i += blockDim.x) {
       int gi = X.off + i;
       double4 m = a.x[gi];
@@ -921,16 +926,43 @@ __device__ void bconfig(cgx::cluster_group& cl, const BatchArgs& a, BCtx& X, con
       }
       double4 d = a.dip[gi];
       double4 t = make_double4(d.x + m.x, d.y + m.y, d.z + m.z, 0.0);
+      if (wfc && c.lwfc[S.t[i]] >= 0) {
+        // moment_from_WFc (moment_from_pola.f90:686-738): -2 sum (r_c - r_i)
+        // over the centres c with |r|^2 < rcut_wfc, in ascending centre order
+        const double4 si = S.s[i];
+        double w[3] = {0.0, 0.0, 0.0};
+        int cnt = 0;
+        for (int j = 0; j < X.n; ++j) {
+          if (c.lwfc[S.t[j]] >= 0) continue;
+          const double4 sj = S.s[j];
+          double rx, ry, rz;
+          const double r2 = min_image_exact(c.A, xsub(sj.x, si.x), xsub(sj.y, si.y), xsub(sj.z, si.z),
+                                            rx, ry, rz);
+          if (r2 < c.rcut_wfc) {
+            ++cnt;
+            w[0] += rx;
+            w[1] += ry;
+            w[2] += rz;
+          }
+        }
+        if (c.lwfc[S.t[i]] > 0 && cnt != c.lwfc[S.t[i]]) v[2] = 1.0;  // :731-737
+        if (c.ldip_wfc) {
+          t.x = t.x + -2.0 * w[0];
+          t.y = t.y + -2.0 * w[1];
+          t.z = t.z + -2.0 * w[2];
+        }
+      }
       a.mu[gi] = t;
       if (t.x > 10.0 || t.y > 10.0 || t.z > 10.0) v[1] = 1.0;  // moment_from_pola.f90:176-178
     }
-    cluster_sum<2>(cl, X, S, v);
+    cluster_sum<3>(cl, X, S, v);
     if (X.rank == 0 && threadIdx.x == 0) {
       out[BS_UPOL] = v[0];
       out[BS_ITER] = iters;
       out[BS_CONV] = conv;
       out[BS_RMSD] = rmsd;
       out[BS_CATA] = v[1] > 0.0 ? 1.0 : 0.0;
+      out[BS_STAT] = v[2] > 0.0 ? (double)MDFF_ERR_BAD_ARGS : 0.0;
     }
   }
   // ---- final pass: forces, energy, field, stress --------------------------

@@ -62,7 +62,7 @@ def test_c_consumer_sees_the_library_layouts(lib, tmp_path):
 def test_c_host_program_reaches_the_engine(lib, tmp_path):
     """The C host driver (tests/c_abi/engforce_host.c) reads its inputs and
     calls mdff_gpu_create; without a device that returns MDFF_ERR_NO_DEVICE
-    (the GPU run is in tests/test_zzz_gpu_c_host.py)."""
+    (the GPU run is in tests/test_gpu_c_host.py)."""
     import subprocess
     import numpy as np
     from mdff_b200 import systems

@@ -55,7 +55,52 @@ def parse():
     ap.add_argument("--no-fit", action="store_true", help="skip the fitting-gradient measurement")
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the MgO 8,000 and NaCl 1,728 records")
+    ap.add_argument("--write-decks", metavar="DIR", default=None,
+                    help="write each workload's starting state as POSFF + control.F under DIR "
+                         "(the reference's input formats) and exit")
     return ap.parse_args()
+
+
+TYPE_NAMES = {"sio2": ["Si", "O"], "mgo": ["Mg", "O"], "nacl": ["Na", "Cl"]}
+
+
+def write_decks(outdir):
+    """The three workloads as the reference reads them: POSFF (positions and
+    velocities of the starting state, types grouped) and control.F (every
+    parameter as a namelist entry, calc = 'md').  The SiO2-like workload's
+    r^-24 wall has no keyword in the reference: its control file says so in a
+    comment, with the wall constants."""
+    from mdff_b200 import mdffio
+    out = {}
+    for name in ("sio2", "mgo", "nacl"):
+        s, wl = make_system(name)
+        pos, vel = s.pos, s.vel
+        st = load_state(name, s)
+        if st is not None:
+            pos, vel = st[0], st[1]
+        p = s.params
+        names = TYPE_NAMES[name]
+        natmi = [int(p.natmi[t]) for t in range(p.ntype)]
+        first = np.concatenate([[0], np.cumsum(natmi)[:-1]]).astype(int)
+        masses = [float(s.mass[i]) for i in first]
+        d = os.path.join(outdir, wl["workload"])
+        os.makedirs(d, exist_ok=True)
+        mdffio.write_posff(os.path.join(d, "POSFF"), wl["workload"], s.cell, names, natmi, pos, vel=vel)
+        ctl = os.path.join(d, "control.F")
+        mdffio.write_control(ctl, p, names, masses=masses, calc="md",
+                             extra_md={"dt": DT_FS * 1e-3, "npas": 5000})
+        walls = [(i, j, p.wall24[i][j]) for i in range(p.ntype) for j in range(p.ntype)
+                 if p.wall24[i][j] != 0.0]
+        if walls:
+            with open(ctl) as f:
+                body = f.read()
+            note = ["! extension used by this workload, not a keyword of the reference: a W/r^24",
+                    "! wall added to the Buckingham pairs (eV A^24):"]
+            note += [f"!   wall24({i + 1},{j + 1}) = {w!r}" for i, j, w in walls]
+            with open(ctl, "w") as f:
+                f.write("\n".join(note) + "\n" + body)
+        out[name] = d
+    return out
 
 
 def make_system(name):
@@ -851,6 +896,10 @@ def run_fit_bench(local_rank):
 
 def main():
     args = parse()
+    if args.write_decks:
+        for name, d in write_decks(args.write_decks).items():
+            print(f"{name}: {d}")
+        return
     rank, world, local_rank = replicas.world()
     if args.impl == "reference":
         run_reference(args, rank, world)

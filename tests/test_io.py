@@ -327,3 +327,31 @@ def test_control_file_round_trip_random(tmp_path):
                 if name in ("ldip_wfc", "rcut_wfc") and not any(p.lwfc[t] for t in range(nt)):
                     continue
                 assert a == b, (trial, name, a, b)
+
+
+def test_bench_workload_decks_read_back(tmp_path):
+    """bench.py --write-decks: each workload's POSFF + control.F read back by
+    the deck reader give the workload's parameters, types and positions."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "bench_mod", os.path.join(os.path.dirname(os.path.dirname(__file__)), "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    dirs = bench.write_decks(str(tmp_path))
+    for name, d in dirs.items():
+        s, _ = bench.make_system(name)
+        r = mdffio.read_posff(os.path.join(d, "POSFF"))
+        assert r["natm"] == s.natm and r["names"] == bench.TYPE_NAMES[name]
+        assert np.allclose(r["cell"], s.cell)
+        p = mdffio.load_deck(os.path.join(d, "POSFF"), os.path.join(d, "control.F"))
+        q = p["params"] if isinstance(p, dict) else p[0]
+        for k in ("natm", "ntype", "lcoulomb", "lbmhft", "lbmhftd", "calc"):
+            assert getattr(q, k) == getattr(s.params, k), (name, k)
+        for k in ("alphaES", "cutlongrange", "conv_tol_ind"):
+            assert getattr(q, k) == pytest.approx(getattr(s.params, k)), (name, k)
+        assert list(q.kES) == list(s.params.kES)
+        for i in range(s.params.ntype):
+            assert q.qch[i] == pytest.approx(s.params.qch[i])
+            assert q.Abmhftd[i][i] == pytest.approx(s.params.Abmhftd[i][i])
+    text = open(os.path.join(dirs["sio2"], "control.F")).read()
+    assert "wall24(1,2)" in text

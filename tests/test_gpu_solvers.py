@@ -40,7 +40,7 @@ def test_cg_fp64_matches_converged_scf(oracle, case):
 
 @pytest.mark.parametrize("case", range(3))
 def test_mixed_precision_force_error(oracle, case):
-    """north_star bar: force error <= 1e-5 relative RMS vs the FP64 oracle."""
+    """The mixed engine's bar: force error <= 1e-5 relative RMS vs the FP64 oracle."""
     s = _pim_cases()[case]
     o = oracle.Oracle(s.params, s.cell).engforce(*s.soa())
     p = params_copy(s.params)

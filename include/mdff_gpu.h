@@ -347,8 +347,10 @@ void mdff_gpu_destroy(mdff_handle h);
    selects FP64 or mixed for the whole batch.  The real-space pairs are all
    minimum-image pairs within the cutoffs (the Verlet list's pair set).
    Thole functions and Wannier centres act as in mdff_gpu_create (a missing
-   centre: MDFF_ERR_BAD_ARGS); the kO dipole algorithms are not built here
-   (MDFF_ERR_UNSUPPORTED: the batch solves with PCG). */
+   centre: MDFF_ERR_BAD_ARGS).  The dipoles always come from PCG: a parameter
+   set that selects kO_v1, kO_v2 or kO_v4_1 gets that algorithm's converged
+   dipoles (its fixed point, to the tolerance), not its iteration path or
+   iteration count, which mdff_gpu_create reproduces. */
 #define MDFF_BATCH_MAXTYPES 4
 #define MDFF_BATCH_MAXATM 2048
 

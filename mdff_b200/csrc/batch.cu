@@ -355,10 +355,13 @@ int create_impl(mdff_batch* h, const mdff_params* psets, int npsets, const mdff_
       return MDFF_ERR_BAD_ARGS;
     }
     mdff_params p = psets[ps];
-    if (p.algo_moment_from_pola != MDFF_ALGO_SCF) {
-      h->err = "the kO dipole algorithms are not built into the batched engine (use mdff_gpu_create)";
-      return MDFF_ERR_UNSUPPORTED;
-    }
+    // every parameter set's dipoles come from PCG: with kO_v1, kO_v2 or
+    // kO_v4_1 selected the batch returns that algorithm's converged dipoles
+    // (the same fixed point to the tolerance), not its iteration path, which
+    // mdff_gpu_create reproduces (kO_v3 / kO_v4_2 stay rejected there)
+    if (p.algo_moment_from_pola == MDFF_ALGO_KO_V1 || p.algo_moment_from_pola == MDFF_ALGO_KO_V2 ||
+        p.algo_moment_from_pola == MDFF_ALGO_KO_V4_1)
+      p.algo_moment_from_pola = MDFF_ALGO_SCF;
     h->pset_of.push_back(ps);
     long n = 0;
     for (int t = 0; t < MDFF_NTYPEMAX; ++t) {

@@ -13,8 +13,8 @@ the GPU against the CPU oracle.
   polint weights are the reference's own recurrence).
 * Boxes with non-polarisable ions, the surface term and a triclinic cell; the
   mixed engine (FP32 field passes) to the 1e-5 force bar.
-* kO_v3, kO_v4_2, kO with the CG solver, kO_v4_1 beyond 100 iterates and the
-  batched engine are rejected."""
+* kO_v3, kO_v4_2, kO with the CG solver and kO_v4_1 beyond 100 iterates are
+  rejected; the batched engine returns the kO fixed point (PCG)."""
 import numpy as np
 import pytest
 
@@ -123,6 +123,31 @@ def test_ko_rejections():
     with pytest.raises(MdffError) as e:
         ForceEngine(p, s.cell)
     assert e.value.status == _abi.MDFF_ERR_BAD_ARGS
-    p = _params(s, V2)
-    with pytest.raises(MdffError):
-        BatchEngine([p], [(0, [p.natmi[0], p.natmi[1]], s.cell)])
+
+
+@pytest.mark.parametrize("algo", [V1, V2, V41])
+def test_batch_gives_the_ko_fixed_point(oracle, algo):
+    """The batched engine solves a kO parameter set's dipoles with PCG: the
+    three boxes of the single-engine cases in one batch against the oracle's
+    kO iterations (kO_v1 / kO_v2 to 1e-11; kO_v4_1 stalls near 1e-8, so it
+    runs at 1e-6 and the comparison at 1e-5)."""
+    tol_o = 1e-6 if algo == V41 else 1e-11
+    bar = 1e-5 if algo == V41 else 1e-8
+    boxes = [_box(k) for k in range(3)]
+    psets, desc = [], []
+    for k, b in enumerate(boxes):
+        p = _params(b, algo, tol=tol_o)
+        p.cg_tol = 1e-11
+        psets.append(p)
+        desc.append((k, [b.params.natmi[0], b.params.natmi[1]], b.cell))
+    pos = [np.concatenate([b.soa()[a] for b in boxes]) for a in range(3)]
+    with BatchEngine(psets, desc) as be:
+        g = be.engforce(*pos)
+    off = 0
+    for b, p in zip(boxes, psets):
+        n = b.params.natm
+        o = oracle.Oracle(p, b.cell).engforce(*b.soa())
+        fg = np.stack([g["fx"][off:off + n], g["fy"][off:off + n], g["fz"][off:off + n]], 1)
+        assert rms_rel(fg, forces(o)) < bar
+        assert rms_rel(g["mu"][off:off + n], o["mu"]) < bar
+        off += n

@@ -249,7 +249,8 @@ int mdff_gpu_engforce_device(mdff_handle h, const double* d_pos, int itime,
    ulp or so each time; the engine leaves the caller's positions alone.  A
    caller that wants the reference's positions after an engforce applies
    count = stats.n_kardir round trips here (same cell as the handle; host
-   arrays rx, ry, rz [natm], in place, in the reference's arithmetic). */
+   arrays rx, ry, rz [natm], in place, in the reference's arithmetic);
+   0 <= count <= 1048576, else MDFF_ERR_BAD_ARGS. */
 int mdff_gpu_kardir_roundtrips(mdff_handle h, double* rx, double* ry, double* rz, int count);
 
 /* ASPC history dipia_ind_t(5,3,natm) (coulomb.f90:435) for RESTART:

@@ -353,6 +353,10 @@ __global__ void k_unpack3(const double* __restrict__ in, int natm, double4* __re
 }
 
 // velocity Verlet halves (prop_velocity_verlet, integration.f90:132-194)
+// an engforce makes a few more round trips than SCF iterations; a count far
+// above that is a caller's mistake, refused before a long launch
+constexpr int kMaxRoundTrips = 1 << 20;
+
 // count in-place kardir/dirkar round trips (lattice.f90:183-270) of SoA
 // positions [3][natm], in the reference's two-rounding arithmetic
 __global__ void k_kardir_roundtrips(double* __restrict__ pos, int natm,
@@ -2639,6 +2643,10 @@ int mdff_gpu_set_aspc_history(mdff_handle h, const double* buf) {
 
 int mdff_gpu_kardir_roundtrips(mdff_handle h, double* rx, double* ry, double* rz, int count) {
   if (!h || !rx || !ry || !rz || count < 0) return MDFF_ERR_BAD_ARGS;
+  if (count > kMaxRoundTrips) {
+    h->err = "mdff_gpu_kardir_roundtrips: count above " + std::to_string(kMaxRoundTrips);
+    return MDFF_ERR_BAD_ARGS;
+  }
   CK(cudaSetDevice(h->device));
   const int n = h->natm;
   if (n == 0 || count == 0) return MDFF_OK;

@@ -50,6 +50,16 @@ def test_roundtrips_move_positions_of_a_triclinic_cell(oracle):
         assert np.array_equal(a, b)
 
 
+def test_count_limit_is_refused():
+    s = systems.nacl(ncell=2, rcut=12.0, kmax=6)
+    with ForceEngine(params_copy(s.params), s.cell) as eng:
+        with pytest.raises(_abi.MdffError) as e:
+            eng.kardir_roundtrips(*s.soa(), (1 << 20) + 1)
+        assert e.value.status == _abi.MDFF_ERR_BAD_ARGS
+        x = s.soa()
+        assert all(np.array_equal(a, b) for a, b in zip(eng.kardir_roundtrips(*x, 0), x))
+
+
 def test_count_is_undefined_for_other_solvers():
     s = systems.mgo(ncell=2, calc=_abi.CALC_OTHER)
     p = params_copy(s.params)
